@@ -1,0 +1,118 @@
+/*
+ * volrus_b200.h — C ABI of the B200 narrow-band level-set advection library.
+ *
+ * This is the drop-in boundary for the Sharc.Volrus advection path.  The
+ * reference exposes that path as plain Rust free functions over Grid<f32>
+ * (re-exported at src/lib.rs:29-43); each entry point below names the
+ * function it replaces.  Grids cross the boundary as flat leaf arrays, the
+ * record the reference already uses for its flat layout NanoLeaf
+ * (src/nano/layout.rs:41-52) and its .vol format (src/io/vol_format.rs:1-21):
+ *   origins  int32[n][3]    leaf origins (multiples of 8), sorted (x, y, z)
+ *   masks    uint64[n][8]   activity bits, bit off = x*64 + y*8 + z (ZYX order)
+ *   values   float[n][512]  voxel values in ZYX order
+ * Device grids are opaque handles owned by a context; every buffer passed in
+ * is caller-owned host memory.  All functions return VLR_OK (0) or an error
+ * code; vlr_last_error() gives the message.  A context is thread-compatible:
+ * one thread at a time, one CUDA stream per context.
+ */
+#ifndef VOLRUS_B200_H
+#define VOLRUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    VLR_OK = 0,
+    VLR_ERR_INVALID = 1,   /* bad argument (null pointer, duplicate leaf, unaligned origin, ...) */
+    VLR_ERR_CUDA = 2,      /* CUDA runtime error */
+    VLR_ERR_CAPACITY = 3,  /* leaf pool or hash capacity exceeded */
+    VLR_ERR_EXTENT = 4,    /* grid spans more than 2^24 voxels along an axis */
+    VLR_ERR_REACH = 5,     /* a backtrace left the staged neighbourhood (time step too large) */
+    VLR_ERR_NOMEM = 6,     /* device allocation failed */
+    VLR_ERR_FORMAT = 7,    /* malformed flat-grid buffer */
+    VLR_ERR_TIMEOUT = 8,   /* a bounded device-side wait gave up */
+    VLR_ERR_UNSUPPORTED = 9
+};
+
+typedef struct vlr_ctx vlr_ctx;
+typedef struct vlr_grid vlr_grid;
+
+/* Transform of a grid: the legacy VoxelTransform (voxel_size, origin) that
+ * sample_trilinear uses (src/grid.rs:62-121) and the forward rows of the
+ * AffineMap that advect_level_set uses for index->world (src/grid.rs:131-257). */
+typedef struct vlr_transform {
+    double voxel_size;
+    double origin[3];
+    double affine[12];       /* rows 0..2 of the 4x4 forward matrix, row-major */
+    double affine_voxel_size;/* AffineMap::voxel_size() */
+} vlr_transform;
+
+/* ---- context ---------------------------------------------------------- */
+int vlr_ctx_create(int device, vlr_ctx** out);
+void vlr_ctx_destroy(vlr_ctx* ctx);
+const char* vlr_last_error(const vlr_ctx* ctx);
+int vlr_ctx_synchronize(vlr_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own
+ * work or events with the library's.  No counterpart in the reference. */
+int vlr_ctx_stream(vlr_ctx* ctx, void** stream);
+/* Per-kernel timing with CUDA events on the context stream: enable/disable,
+ * and read the accumulated milliseconds and launch count of one kernel
+ * (reading resets nothing; vlr_ctx_profile(ctx, 1) clears the totals).
+ * No counterpart in the reference. */
+int vlr_ctx_profile(vlr_ctx* ctx, int enable);
+int vlr_ctx_profile_read(vlr_ctx* ctx, const char* kernel, double* total_ms, long long* launches);
+
+/* ---- grids (reference semantics: f32 values in world units) ------------ */
+
+/* Upload a Grid<f32>: replaces NanoGrid::from_grid + upload (src/nano/layout.rs:89-170).
+ * Leaves must have distinct, 8-aligned origins; any order is accepted. */
+int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* origins,
+                    const uint64_t* masks, const float* values, size_t n_leaves, vlr_grid** out);
+/* Leaf count, active voxel count, background and transform of a grid. */
+int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
+                  vlr_transform* xf);
+/* Copy a grid back into caller buffers sized for at least vlr_grid_info's leaf
+ * count, sorted (x, y, z) like NanoGrid (src/nano/layout.rs:81-106). */
+int vlr_grid_download(vlr_ctx* ctx, const vlr_grid* g, int32_t* origins, uint64_t* masks, float* values,
+                      size_t cap_leaves);
+void vlr_grid_destroy(vlr_grid* g);
+
+/* make_level_set_sphere (src/tools/sphere.rs:17-59), generated on the device. */
+int vlr_make_level_set_sphere(vlr_ctx* ctx, double radius, const double center[3], double voxel_size,
+                              double half_width, vlr_grid** out);
+
+/* sample_trilinear (src/tools/interpolation.rs:11-48) at n world positions (host arrays). */
+int vlr_sample_trilinear(vlr_ctx* ctx, const vlr_grid* g, const double* world_xyz, size_t n, float* out);
+
+/* advect_level_set (src/tools/advection.rs:32-56): VelocityField{vx, vy, vz}
+ * (src/tools/advection.rs:10-24) as three grids.  Writes a new grid. */
+int vlr_advect_level_set(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, const vlr_grid* vy,
+                         const vlr_grid* vz, double dt, vlr_grid** out);
+
+/* find_zero_crossings (src/tools/level_set_track.rs:14-47): writes up to cap
+ * coordinates (int32[3] each, sorted (x, y, z)) and the total count. */
+int vlr_find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* coords, size_t cap, size_t* count);
+
+/* trim_narrow_band (src/tools/level_set_track.rs:53-68), in place. */
+int vlr_trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
+
+/* rebuild_narrow_band (src/tools/level_set_track.rs:80-114), in place. */
+int vlr_rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
+
+/* Host-buffer convenience: one step of the reference pipeline, advect_level_set
+ * then rebuild_narrow_band, from and to flat host arrays.  Upload, kernels and
+ * download run on the context stream.  out_* buffers hold cap_leaves leaves;
+ * *out_n receives the leaf count (VLR_ERR_CAPACITY if it exceeds cap_leaves). */
+int vlr_advect_rebuild_host(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* origins,
+                            const uint64_t* masks, const float* values, size_t n_leaves, const float velocity[3],
+                            double dt, float half_width, int32_t* out_origins, uint64_t* out_masks,
+                            float* out_values, size_t cap_leaves, size_t* out_n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VOLRUS_B200_H */

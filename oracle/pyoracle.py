@@ -1,0 +1,194 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrapper over ``oracle/lib/libvolrus_oracle.so``, the C++ restatement of
+the Sharc.Volrus advection path (``ref_tree.hpp``) and of the narrow-band
+method (``method_oracle.hpp``).  Imported only by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``, always as
+the checker or the timed CPU baseline, never as the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "lib" / "libvolrus_oracle.so"
+
+P = C.c_void_p
+dbl_p = C.POINTER(C.c_double)
+flt_p = C.POINTER(C.c_float)
+i32_p = C.POINTER(C.c_int32)
+u64_p = C.POINTER(C.c_uint64)
+size_p = C.POINTER(C.c_size_t)
+
+SIGS = {
+    "vo_grid_new": (P, [C.c_float, C.c_double, dbl_p, dbl_p, C.c_double]),
+    "vo_grid_free": (None, [P]),
+    "vo_grid_put_leaves": (None, [P, i32_p, u64_p, flt_p, C.c_size_t]),
+    "vo_grid_leaf_count": (C.c_size_t, [P]),
+    "vo_grid_active_count": (C.c_uint64, [P]),
+    "vo_grid_export": (None, [P, i32_p, u64_p, flt_p]),
+    "vo_grid_meta": (None, [P, flt_p, dbl_p, dbl_p, dbl_p, dbl_p]),
+    "vo_get": (C.c_float, [P, C.c_int32, C.c_int32, C.c_int32]),
+    "vo_is_active": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32]),
+    "vo_set": (None, [P, C.c_int32, C.c_int32, C.c_int32, C.c_float]),
+    "vo_deactivate": (None, [P, C.c_int32, C.c_int32, C.c_int32]),
+    "vo_make_level_set_sphere": (P, [C.c_double, dbl_p, C.c_double, C.c_double]),
+    "vo_sample_trilinear": (None, [P, dbl_p, C.c_size_t, flt_p]),
+    "vo_advect_level_set": (P, [P, P, P, P, C.c_double]),
+    "vo_find_zero_crossings": (C.c_size_t, [P, i32_p, C.c_size_t]),
+    "vo_trim_narrow_band": (None, [P, C.c_float]),
+    "vo_rebuild_narrow_band": (None, [P, C.c_float, C.c_int]),
+    "vo_dilate": (None, [P, C.c_uint]),
+    "vo_remove_empty_leaves": (None, [P]),
+    "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
+}
+
+_lib = None
+
+
+def build():
+    """Compile the oracle library (make, in this directory)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        lib = C.CDLL(str(LIB))
+        for name, (res, args) in SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class OGrid:
+    """Handle to an oracle grid (reference data structure, f32 values)."""
+
+    def __init__(self, handle):
+        self.lib = load()
+        self.h = handle
+
+    @classmethod
+    def new(cls, background, voxel_size=1.0, t_origin=(0.0, 0.0, 0.0), affine=None, affine_vs=None):
+        lib = load()
+        to = np.asarray(t_origin, np.float64)
+        if affine is None:
+            affine = np.zeros((3, 4))
+            affine[0, 0] = affine[1, 1] = affine[2, 2] = voxel_size
+        af = np.ascontiguousarray(affine, np.float64).reshape(12)
+        h = lib.vo_grid_new(C.c_float(background), voxel_size, _p(to, C.c_double), _p(af, C.c_double),
+                            voxel_size if affine_vs is None else affine_vs)
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, origins, masks, values, background, voxel_size=1.0, t_origin=(0.0, 0.0, 0.0), affine=None,
+                    affine_vs=None):
+        g = cls.new(background, voxel_size, t_origin, affine, affine_vs)
+        o = np.ascontiguousarray(origins, np.int32)
+        m = np.ascontiguousarray(masks, np.uint64)
+        v = np.ascontiguousarray(values, np.float32)
+        g.lib.vo_grid_put_leaves(g.h, _p(o, C.c_int32), _p(m, C.c_uint64), _p(v, C.c_float), len(o))
+        return g
+
+    @classmethod
+    def sphere(cls, radius, center, voxel_size, half_width):
+        lib = load()
+        c = np.asarray(center, np.float64)
+        return cls(lib.vo_make_level_set_sphere(radius, _p(c, C.c_double), voxel_size, half_width))
+
+    def arrays(self):
+        n = self.lib.vo_grid_leaf_count(self.h)
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((n, 8), np.uint64)
+        v = np.zeros((n, 512), np.float32)
+        if n:
+            self.lib.vo_grid_export(self.h, _p(o, C.c_int32), _p(m, C.c_uint64), _p(v, C.c_float))
+        return o, m, v
+
+    def meta(self):
+        bg = C.c_float()
+        vs = C.c_double()
+        to = np.zeros(3)
+        mat = np.zeros(12)
+        avs = C.c_double()
+        self.lib.vo_grid_meta(self.h, C.byref(bg), C.byref(vs), _p(to, C.c_double), _p(mat, C.c_double),
+                              C.byref(avs))
+        return bg.value, vs.value, to, mat.reshape(3, 4), avs.value
+
+    def leaf_count(self):
+        return self.lib.vo_grid_leaf_count(self.h)
+
+    def active_voxel_count(self):
+        return self.lib.vo_grid_active_count(self.h)
+
+    def get(self, c):
+        return self.lib.vo_get(self.h, *map(int, c))
+
+    def is_active(self, c):
+        return bool(self.lib.vo_is_active(self.h, *map(int, c)))
+
+    def set(self, c, v):
+        self.lib.vo_set(self.h, *map(int, c), C.c_float(v))
+
+    def deactivate(self, c):
+        self.lib.vo_deactivate(self.h, *map(int, c))
+
+    def sample_trilinear(self, world):
+        w = np.ascontiguousarray(world, np.float64).reshape(-1, 3)
+        out = np.zeros(len(w), np.float32)
+        self.lib.vo_sample_trilinear(self.h, _p(w, C.c_double), len(w), _p(out, C.c_float))
+        return out
+
+    def advect(self, vx, vy, vz, dt):
+        return OGrid(self.lib.vo_advect_level_set(self.h, vx.h, vy.h, vz.h, dt))
+
+    def zero_crossings(self):
+        n = self.lib.vo_find_zero_crossings(self.h, None, 0)
+        out = np.zeros((n, 3), np.int32)
+        if n:
+            self.lib.vo_find_zero_crossings(self.h, _p(out, C.c_int32), n)
+        return out
+
+    def trim(self, hw):
+        self.lib.vo_trim_narrow_band(self.h, C.c_float(hw))
+
+    def rebuild(self, hw, brute=False):
+        self.lib.vo_rebuild_narrow_band(self.h, C.c_float(hw), 1 if brute else 0)
+
+    def dilate(self, iterations=1):
+        self.lib.vo_dilate(self.h, iterations)
+
+    def remove_empty_leaves(self):
+        self.lib.vo_remove_empty_leaves(self.h)
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.vo_grid_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def uniform_velocity(voxel_size, vel, bbox_min=None, bbox_max=None):
+    """Oracle twin of the crate's ``make_uniform_velocity`` test helper (src/tools/advection.rs:116-134)."""
+    out = []
+    for a in range(3):
+        g = OGrid.new(float(np.float32(vel[a])), voxel_size)
+        for c in (bbox_min, bbox_max):
+            if c is not None:
+                g.set(c, vel[a])
+        out.append(g)
+    return out

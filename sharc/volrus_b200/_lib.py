@@ -1,0 +1,146 @@
+"""ctypes binding of ``lib/libvolrus_b200.so`` (the C ABI in include/volrus_b200.h).
+
+The library is loaded lazily on first use.  There is no fallback: if the
+shared library is missing or a CUDA device is unavailable, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvolrus_b200.so"
+
+VLR_OK = 0
+ERROR_NAMES = {
+    1: "VLR_ERR_INVALID", 2: "VLR_ERR_CUDA", 3: "VLR_ERR_CAPACITY", 4: "VLR_ERR_EXTENT",
+    5: "VLR_ERR_REACH", 6: "VLR_ERR_NOMEM", 7: "VLR_ERR_FORMAT", 8: "VLR_ERR_TIMEOUT",
+    9: "VLR_ERR_UNSUPPORTED",
+}
+
+
+class VolrusError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class vlr_transform(C.Structure):
+    _fields_ = [
+        ("voxel_size", C.c_double),
+        ("origin", C.c_double * 3),
+        ("affine", C.c_double * 12),
+        ("affine_voxel_size", C.c_double),
+    ]
+
+
+P = C.c_void_p
+PP = C.POINTER(C.c_void_p)
+dbl_p = C.POINTER(C.c_double)
+flt_p = C.POINTER(C.c_float)
+i32_p = C.POINTER(C.c_int32)
+u64_p = C.POINTER(C.c_uint64)
+size_p = C.POINTER(C.c_size_t)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "vlr_ctx_create": (C.c_int, [C.c_int, PP]),
+    "vlr_ctx_destroy": (None, [P]),
+    "vlr_last_error": (C.c_char_p, [P]),
+    "vlr_ctx_synchronize": (C.c_int, [P]),
+    "vlr_ctx_stream": (C.c_int, [P, PP]),
+    "vlr_ctx_profile": (C.c_int, [P, C.c_int]),
+    "vlr_ctx_profile_read": (C.c_int, [P, C.c_char_p, dbl_p, C.POINTER(C.c_longlong)]),
+    "vlr_grid_create": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t, PP]),
+    "vlr_grid_info": (C.c_int, [P, P, size_p, C.POINTER(C.c_uint64), flt_p, C.POINTER(vlr_transform)]),
+    "vlr_grid_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
+    "vlr_grid_destroy": (None, [P]),
+    "vlr_make_level_set_sphere": (C.c_int, [P, C.c_double, dbl_p, C.c_double, C.c_double, PP]),
+    "vlr_sample_trilinear": (C.c_int, [P, P, dbl_p, C.c_size_t, flt_p]),
+    "vlr_advect_level_set": (C.c_int, [P, P, P, P, P, C.c_double, PP]),
+    "vlr_find_zero_crossings": (C.c_int, [P, P, i32_p, C.c_size_t, size_p]),
+    "vlr_trim_narrow_band": (C.c_int, [P, P, C.c_float]),
+    "vlr_rebuild_narrow_band": (C.c_int, [P, P, C.c_float]),
+    "vlr_advect_rebuild_host": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t,
+                                          flt_p, C.c_double, C.c_float, i32_p, u64_p, flt_p, C.c_size_t, size_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load the shared library and bind every declared entry point."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m sharc.volrus_b200.build` "
+                    "(the CUDA path has no CPU fallback)")
+            lib = C.CDLL(str(LIB_PATH))
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Context:
+    """One CUDA device + stream; owns device grids created through it."""
+
+    _default: dict[int, "Context"] = {}
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.vlr_ctx_create(device, C.byref(h))
+        if rc != VLR_OK:
+            raise VolrusError(rc, f"vlr_ctx_create(device={device}) failed (is a CUDA device present?)")
+        self.handle = h
+        self.device = device
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = cls(device)
+        return cls._default[device]
+
+    def check(self, rc: int, what: str = ""):
+        if rc != VLR_OK:
+            msg = self.lib.vlr_last_error(self.handle)
+            raise VolrusError(rc, (what + ": " if what else "") + (msg.decode() if msg else ""))
+
+    def synchronize(self):
+        self.check(self.lib.vlr_ctx_synchronize(self.handle), "synchronize")
+
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        self.check(self.lib.vlr_ctx_stream(self.handle, C.byref(s)), "vlr_ctx_stream")
+        return s.value or 0
+
+    def profile(self, enable: bool):
+        self.check(self.lib.vlr_ctx_profile(self.handle, 1 if enable else 0), "vlr_ctx_profile")
+
+    def kernel_time(self, name: str):
+        """(total milliseconds, launches) of kernel ``name`` since profiling was enabled."""
+        ms = C.c_double()
+        n = C.c_longlong()
+        self.check(self.lib.vlr_ctx_profile_read(self.handle, name.encode(), C.byref(ms), C.byref(n)),
+                   "vlr_ctx_profile_read")
+        return ms.value, n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.vlr_ctx_destroy(self.handle)
+            self.handle = None

@@ -1,0 +1,16 @@
+// Host entry points of the reference-semantics kernels (ref_ops.cu).
+#pragma once
+#include "vlr_host.hpp"
+
+namespace vlr {
+
+GridView make_view(const vlr_grid* g);
+int advect_ref(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, const vlr_grid* vy, const vlr_grid* vz, double dt,
+               vlr_grid* out);
+int sample_points(vlr_ctx* ctx, const vlr_grid* g, const double* h_pts, size_t n, float* h_out);
+int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size_t cap, size_t* count);
+int trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
+int rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
+int make_sphere(vlr_ctx* ctx, double radius, const double c[3], double vs, double hw, vlr_grid* out);
+
+}  // namespace vlr

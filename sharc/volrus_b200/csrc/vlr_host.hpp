@@ -1,0 +1,103 @@
+// Host-side context and grid handles behind the C ABI (include/volrus_b200.h).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "vlr_common.cuh"
+#include "../../../include/volrus_b200.h"
+
+// Optional per-kernel timing with CUDA events on the context stream (enabled
+// by vlr_ctx_profile); durations are accumulated per kernel name.
+struct vlr_kernel_timer {
+    bool enabled = false;
+    struct Pending {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> free_events;
+    std::vector<std::pair<std::string, std::pair<double, long long>>> totals;  // name -> (ms, launches)
+};
+
+struct vlr_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    unsigned* d_errword = nullptr;      // device error bits (vlr::kErr*)
+    std::string last_error;
+    // Scratch reused across calls on this context (grown on demand).
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    void* pinned = nullptr;             // small pinned host buffer for scalar read-backs
+    vlr_kernel_timer timer;
+};
+
+// Value storage kinds.
+enum vlr_value_kind : int {
+    VLR_KIND_F32_WORLD = 0,   // f32 values in world units: reference semantics
+    VLR_KIND_F32_VOXEL = 1,   // f32 values in voxel units: narrow-band method, plain FP32
+    VLR_KIND_F16_VOXEL = 2,   // f16 values in voxel units: narrow-band method, FP16 leaves
+};
+
+struct vlr_grid {
+    vlr_ctx* ctx = nullptr;
+    int n = 0;          // live leaves (slots 0..n-1 in list order)
+    int cap = 0;        // allocated slots
+    int kind = VLR_KIND_F32_WORLD;
+    float background = 0.0f;
+    vlr_transform xf{};
+    long long base[3] = {0, 0, 0};
+    int4* origin = nullptr;
+    uint64_t* mask = nullptr;
+    void* values = nullptr;
+    int* nbr = nullptr;
+    uint64_t* hkey = nullptr;
+    int* hval = nullptr;
+    int hcap = 0;
+};
+
+namespace vlr {
+
+// Error helpers: record a message on the context and return a status.
+int set_error(vlr_ctx* ctx, int code, const std::string& msg);
+int check_cuda(vlr_ctx* ctx, cudaError_t e, const char* what);
+#define VLR_CUDA(ctx, call)                                   \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return vlr::check_cuda(ctx, _e, #call); \
+    } while (0)
+
+size_t value_bytes(int kind);
+
+// Allocation of a grid's device arrays for `cap` slots (values of `kind`).
+int grid_alloc(vlr_ctx* ctx, vlr_grid* g, int cap);
+void grid_free_arrays(vlr_grid* g);
+// (Re)build hash table and neighbour table for slots 0..n-1.
+int grid_index(vlr_ctx* ctx, vlr_grid* g);
+// Choose the hash-key base from the leaf-coordinate bounding box (host origins).
+int choose_base(vlr_ctx* ctx, const int32_t* origins, size_t n, long long base[3]);
+// Keep slots whose flag is non-zero (order preserved); rebuilds the index.
+int grid_compact(vlr_ctx* ctx, vlr_grid* g, const int* d_flags);
+// Scratch memory owned by the context (valid until the next call that grows it).
+int ctx_scratch(vlr_ctx* ctx, size_t bytes, void** out);
+// Exclusive scan of n ints on the context stream; writes total to *d_total (device).
+int scan_exclusive(vlr_ctx* ctx, const int* d_in, int* d_out, int n, int* d_total);
+// Read the device error word, clear it, and map it to a status.
+int consume_device_errors(vlr_ctx* ctx, const char* what);
+int read_int(vlr_ctx* ctx, const int* d_ptr, int* out);
+
+// Kernel timing: bracket a launch with timer_begin/timer_end (no-ops unless
+// profiling is enabled); timer_collect folds finished event pairs into totals.
+void timer_begin(vlr_ctx* ctx, const char* name);
+void timer_end(vlr_ctx* ctx);
+int timer_collect(vlr_ctx* ctx);
+#define VLR_TIMED(ctx, name, ...)    \
+    do {                             \
+        vlr::timer_begin(ctx, name); \
+        __VA_ARGS__;                 \
+        vlr::timer_end(ctx);         \
+    } while (0)
+
+}  // namespace vlr

@@ -1,0 +1,192 @@
+"""GPU implementations of the Sharc.Volrus advection-path tools.
+
+Each function keeps the name, arguments and semantics of the reference tool
+it replaces and runs on the B200 through the C ABI:
+
+    advect_level_set(grid, velocity, dt) -> Grid     src/tools/advection.rs:32-56
+    VelocityField(vx, vy, vz)                        src/tools/advection.rs:10-24
+    sample_trilinear(grid, world_pos) -> float       src/tools/interpolation.rs:11-48
+    find_zero_crossings(grid) -> list[Coord]         src/tools/level_set_track.rs:14-47
+    trim_narrow_band(grid, half_width)               src/tools/level_set_track.rs:53-68
+    rebuild_narrow_band(grid, half_width)            src/tools/level_set_track.rs:80-114
+    make_level_set_sphere(r, c, vs, hw) -> Grid      src/tools/sphere.rs:17-59
+
+Host ``Grid`` arguments are uploaded, processed and downloaded per call (the
+drop-in form); ``DeviceGrid`` arguments stay resident in HBM between calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import Context, ptr
+from .grid import AffineMap, Grid, GridClass, VoxelTransform
+
+
+class DeviceGrid:
+    """A world-unit f32 grid resident on the GPU (opaque ``vlr_grid*``)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, name: str = "", grid_class=GridClass.UNKNOWN):
+        self.ctx = ctx
+        self.handle = handle
+        self.name = name
+        self.grid_class = grid_class
+
+    @classmethod
+    def upload(cls, grid: Grid, ctx: Context | None = None) -> "DeviceGrid":
+        ctx = ctx or Context.default()
+        o, m, v = grid.to_arrays()
+        h = C.c_void_p()
+        t = grid.c_transform()
+        ctx.check(ctx.lib.vlr_grid_create(ctx.handle, C.byref(t), C.c_float(grid.background), ptr(o, C.c_int32),
+                                          ptr(m, C.c_uint64), ptr(v, C.c_float), len(o), C.byref(h)),
+                  "vlr_grid_create")
+        return cls(ctx, h, grid.name, grid.grid_class)
+
+    def info(self):
+        n = C.c_size_t()
+        a = C.c_uint64()
+        bg = C.c_float()
+        t = _lib.vlr_transform()
+        self.ctx.check(self.ctx.lib.vlr_grid_info(self.ctx.handle, self.handle, C.byref(n), C.byref(a), C.byref(bg),
+                                                  C.byref(t)), "vlr_grid_info")
+        return n.value, a.value, bg.value, t
+
+    def leaf_count(self) -> int:
+        return self.info()[0]
+
+    def active_voxel_count(self) -> int:
+        return self.info()[1]
+
+    def download(self) -> Grid:
+        n, _, bg, t = self.info()
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((n, 8), np.uint64)
+        v = np.zeros((n, 512), np.float32)
+        self.ctx.check(self.ctx.lib.vlr_grid_download(self.ctx.handle, self.handle, ptr(o, C.c_int32),
+                                                      ptr(m, C.c_uint64), ptr(v, C.c_float), n),
+                       "vlr_grid_download")
+        vt = VoxelTransform(t.voxel_size, tuple(t.origin))
+        am = AffineMap(np.array(list(t.affine), np.float64).reshape(3, 4), t.affine_voxel_size)
+        g = Grid.from_arrays(o, m, v, bg, vt, am)
+        g.name = self.name
+        g.grid_class = self.grid_class
+        return g
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.vlr_grid_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class VelocityField:
+    """``VelocityField{vx, vy, vz}`` (src/tools/advection.rs:10-14)."""
+    vx: Grid
+    vy: Grid
+    vz: Grid
+
+
+def _as_device(g, ctx):
+    if isinstance(g, DeviceGrid):
+        return g, False
+    return DeviceGrid.upload(g, ctx), True
+
+
+def _replace(host: Grid, new: Grid):
+    host._o, host._m, host._v, host._n, host._index = new._o, new._m, new._v, new._n, new._index
+
+
+def advect_level_set(grid, velocity: VelocityField, dt: float, ctx: Context | None = None):
+    """Semi-Lagrangian advection (src/tools/advection.rs:32-56) on the GPU."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    g, _ = _as_device(grid, ctx)
+    vs = [_as_device(c, ctx)[0] for c in (velocity.vx, velocity.vy, velocity.vz)]
+    h = C.c_void_p()
+    ctx.check(ctx.lib.vlr_advect_level_set(ctx.handle, g.handle, vs[0].handle, vs[1].handle, vs[2].handle,
+                                           C.c_double(dt), C.byref(h)), "vlr_advect_level_set")
+    out = DeviceGrid(ctx, h, g.name, g.grid_class)
+    if isinstance(grid, DeviceGrid):
+        return out
+    return out.download()
+
+
+def sample_trilinear(grid, world_pos, ctx: Context | None = None):
+    """``sample_trilinear`` (src/tools/interpolation.rs:11-48).  ``world_pos`` is
+    one [x, y, z] or an (n, 3) array; returns a float or an f32 array."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    g, _ = _as_device(grid, ctx)
+    p = np.ascontiguousarray(world_pos, np.float64)
+    single = p.ndim == 1
+    p = p.reshape(-1, 3)
+    out = np.zeros(len(p), np.float32)
+    ctx.check(ctx.lib.vlr_sample_trilinear(ctx.handle, g.handle, ptr(p, C.c_double), len(p), ptr(out, C.c_float)),
+              "vlr_sample_trilinear")
+    return float(out[0]) if single else out
+
+
+def find_zero_crossings(grid, ctx: Context | None = None) -> np.ndarray:
+    """``find_zero_crossings`` (src/tools/level_set_track.rs:14-47); (n, 3) int32 sorted (x, y, z)."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    g, _ = _as_device(grid, ctx)
+    cnt = C.c_size_t()
+    ctx.check(ctx.lib.vlr_find_zero_crossings(ctx.handle, g.handle, None, 0, C.byref(cnt)), "vlr_find_zero_crossings")
+    out = np.zeros((cnt.value, 3), np.int32)
+    if cnt.value:
+        ctx.check(ctx.lib.vlr_find_zero_crossings(ctx.handle, g.handle, ptr(out, C.c_int32), cnt.value,
+                                                  C.byref(cnt)), "vlr_find_zero_crossings")
+    return out
+
+
+def trim_narrow_band(grid, half_width: float, ctx: Context | None = None):
+    """``trim_narrow_band`` (src/tools/level_set_track.rs:53-68), in place."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    g, uploaded = _as_device(grid, ctx)
+    ctx.check(ctx.lib.vlr_trim_narrow_band(ctx.handle, g.handle, C.c_float(half_width)), "vlr_trim_narrow_band")
+    if uploaded:
+        _replace(grid, g.download())
+
+
+def rebuild_narrow_band(grid, half_width: float, ctx: Context | None = None):
+    """``rebuild_narrow_band`` (src/tools/level_set_track.rs:80-114), in place."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    g, uploaded = _as_device(grid, ctx)
+    ctx.check(ctx.lib.vlr_rebuild_narrow_band(ctx.handle, g.handle, C.c_float(half_width)),
+              "vlr_rebuild_narrow_band")
+    if uploaded:
+        _replace(grid, g.download())
+
+
+def make_level_set_sphere(radius: float, center, voxel_size: float, half_width: float, ctx: Context | None = None,
+                          device: bool = False):
+    """``make_level_set_sphere`` (src/tools/sphere.rs:17-59), generated on the GPU."""
+    ctx = ctx or Context.default()
+    c = np.ascontiguousarray(center, np.float64)
+    h = C.c_void_p()
+    ctx.check(ctx.lib.vlr_make_level_set_sphere(ctx.handle, C.c_double(radius), ptr(c, C.c_double),
+                                                C.c_double(voxel_size), C.c_double(half_width), C.byref(h)),
+              "vlr_make_level_set_sphere")
+    d = DeviceGrid(ctx, h, "sdf", GridClass.LEVEL_SET)
+    return d if device else d.download()
+
+
+def make_uniform_velocity(voxel_size: float, vel, bbox_min=None, bbox_max=None) -> VelocityField:
+    """Constant field as three grids, like the crate's test helper
+    ``make_uniform_velocity`` (src/tools/advection.rs:116-134)."""
+    comps = []
+    for a in range(3):
+        g = Grid(float(np.float32(vel[a])), voxel_size)
+        for c in (bbox_min, bbox_max):
+            if c is not None:
+                g.set(c, vel[a])
+        comps.append(g)
+    return VelocityField(*comps)
