@@ -103,6 +103,21 @@ int vlr_trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 /* rebuild_narrow_band (src/tools/level_set_track.rs:80-114), in place. */
 int vlr_rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 
+/* find_zero_crossings for callers that cannot allocate device memory (code
+ * inside a stream capture, real-time loops, hosts whose device memory belongs
+ * to another allocator).  No counterpart in the reference: it is an
+ * allocation-free variant of vlr_find_zero_crossings.  It enqueues its kernels
+ * on the context stream and returns without waiting; results are valid once
+ * that stream has been synchronised.  d_coords (int32[cap][3]) and d_count are
+ * caller-owned DEVICE buffers; crossings come in the grid's leaf order, ZYX
+ * within a leaf (not sorted), *d_count receives the total even when it
+ * exceeds cap.  Scratch is a fixed 4.5 MiB device array shared by all calls
+ * on a device: grids over 65,536 leaves are rejected (VLR_ERR_CAPACITY); the
+ * first call on a device resolves the array's address and should come before
+ * any stream capture; calls that overlap on the GPU race on the array. */
+int vlr_find_zero_crossings_noalloc(vlr_ctx* ctx, const vlr_grid* g, int32_t* d_coords, size_t cap,
+                                    unsigned long long* d_count);
+
 /* Host-buffer convenience: one step of the reference pipeline, advect_level_set
  * then rebuild_narrow_band, from and to flat host arrays.  Upload, kernels and
  * download run on the context stream.  out_* buffers hold cap_leaves leaves;

@@ -63,6 +63,7 @@ SIGNATURES = {
     "vlr_sample_trilinear": (C.c_int, [P, P, dbl_p, C.c_size_t, flt_p]),
     "vlr_advect_level_set": (C.c_int, [P, P, P, P, P, C.c_double, PP]),
     "vlr_find_zero_crossings": (C.c_int, [P, P, i32_p, C.c_size_t, size_p]),
+    "vlr_find_zero_crossings_noalloc": (C.c_int, [P, P, C.c_void_p, C.c_size_t, C.c_void_p]),
     "vlr_trim_narrow_band": (C.c_int, [P, P, C.c_float]),
     "vlr_rebuild_narrow_band": (C.c_int, [P, P, C.c_float]),
     "vlr_advect_rebuild_host": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t,
