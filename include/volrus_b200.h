@@ -127,6 +127,77 @@ int vlr_advect_rebuild_host(vlr_ctx* ctx, const vlr_transform* xf, float backgro
                             double dt, float half_width, int32_t* out_origins, uint64_t* out_masks,
                             float* out_values, size_t cap_leaves, size_t* out_n);
 
+/* ---- narrow-band method (no counterpart in the reference) --------------
+ *
+ * The reference's step (advect_level_set + rebuild_narrow_band) never moves
+ * the active set, so its band is lost within a few steps of motion.  The
+ * method grid below is a full narrow-band level-set step:
+ * semi-Lagrangian backtrace (Euler, RK2 midpoint or SSP-RK3) through an
+ * analytic velocity, two Godunov-upwind reinitialisation iterations, and
+ * dilation-based re-tracking of the band, with values stored in voxel units
+ * as f32 or f16 and arithmetic in f32.  A method grid holds one or more
+ * independent grids (a batch) in one leaf pool; each step is one CUDA-graph
+ * replay. */
+typedef struct vlr_level_set vlr_level_set;
+
+enum { VLR_PREC_F32 = 0, VLR_PREC_F16 = 1 };
+enum { VLR_VEL_CONSTANT = 0, VLR_VEL_VORTEX = 1, VLR_VEL_CURL = 2 };
+
+/* Analytic velocity of one grid.  Index space is voxels; world = w0 + voxel_size * index. */
+typedef struct vlr_velocity_desc {
+    int kind;
+    double constant[3];            /* CONSTANT: voxels per unit time */
+    double voxel_size;             /* VORTEX: deformation field on the unit cube (world units) */
+    double w0[3];
+    double period;                 /* VORTEX: T in cos(pi t / T) */
+    int octaves;                   /* CURL: v = sum_o grad f_o x e_o, voxels per unit time, */
+    double amp[4];                 /*   f_o = amp_o prod_a sin(wavenumber_o * p_a + phase_o[a]) */
+    double wavenumber[4];
+    double phase[4][3];
+    double dir[4][3];
+    int32_t domain_lo[3];          /* index box in which the field may be sampled; lo > hi: the */
+    int32_t domain_hi[3];          /*   unit cube + 16 voxels (VORTEX), initial box +- 256 (others) */
+} vlr_velocity_desc;
+
+typedef struct vlr_method_desc {
+    int precision;                 /* VLR_PREC_F32 or VLR_PREC_F16 */
+    float half_width;              /* band half width, voxels */
+    int integrator;                /* 1 Euler, 2 RK2 midpoint, 3 SSP-RK3 */
+    int reinit_iters;              /* 0, 1 or 2 Godunov iterations per step */
+    double dt;                     /* time step */
+    double t0;                     /* time of the initial state */
+    size_t capacity;               /* leaf slots; 0 = 2 x initial + 4096 */
+} vlr_method_desc;
+
+/* Sphere of `radius` (world units) at `center` (world), voxel size vs, world = w0 + vs * index. */
+int vlr_ls_create_sphere(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* vel, double radius,
+                         const double center[3], double voxel_size, const double w0[3], vlr_level_set** out);
+/* From leaves in voxel units (inactive values must hold +-half_width and every
+ * voxel within one voxel of an active one must lie in a given leaf). */
+int vlr_ls_create_from_leaves(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* vel,
+                              const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
+                              vlr_level_set** out);
+/* Advance n_steps steps (each one graph replay on the context stream) and
+ * wait for them; device-side errors are reported here. */
+int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
+/* Enqueue n_steps steps on the context stream and return without waiting;
+ * vlr_ctx_check() later waits and reports device-side errors. */
+int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
+int vlr_ctx_check(vlr_ctx* ctx);
+int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_t* n_active, double* time);
+/* Replace the state of a single-grid level set with host leaves (same layout
+ * and invariants as vlr_ls_create_from_leaves), keeping its time, velocity
+ * and allocations: the host-resident form of a step is upload, step, download. */
+int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                  size_t n_leaves);
+/* Allocated leaves (sorted (x, y, z)), masks, values in voxel units as f32. */
+int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uint64_t* masks, float* phi,
+                    size_t cap_leaves);
+/* Enclosed volume in voxel units^3 (FP64 smeared-delta surface integral
+ * V = 1/3 sum delta(phi) (p - ref) . grad phi, eps = 1.5 voxels). */
+int vlr_ls_volume(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* volume);
+void vlr_ls_destroy(vlr_level_set* ls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,14 @@ SIGS = {
     "vo_dilate": (None, [P, C.c_uint]),
     "vo_remove_empty_leaves": (None, [P]),
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
+    "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
+    "vm_free": (None, [P]),
+    "vm_leaf_count": (C.c_size_t, [P]),
+    "vm_export": (None, [P, i32_p, u64_p, dbl_p]),
+    "vm_import": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double]),
+    "vm_step": (C.c_int, [P, C.c_int, dbl_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
+    "vm_velocity": (None, [C.c_int, dbl_p, dbl_p, C.c_double, dbl_p]),
+    "vm_volume": (C.c_double, [P, dbl_p]),
 }
 
 _lib = None
@@ -192,3 +200,90 @@ def uniform_velocity(voxel_size, vel, bbox_min=None, bbox_max=None):
                 g.set(c, vel[a])
         out.append(g)
     return out
+
+
+# --------------------------------------------------------------------------
+# narrow-band method oracle (FP64), method_oracle.hpp
+
+VEL_CONSTANT, VEL_VORTEX, VEL_CURL = 0, 1, 2
+
+
+def pack_velocity(vel: dict) -> tuple[int, np.ndarray]:
+    """Velocity description -> (kind, packed f64 params) shared with the GPU side.
+
+    {"kind": "constant", "c": (ux, uy, uz)}            index units per unit time
+    {"kind": "vortex", "vs": vs, "w0": (x, y, z), "period": T}
+    {"kind": "curl", "octaves": [(A, k, (ph0, ph1, ph2), (e0, e1, e2)), ...]}
+    """
+    k = vel["kind"]
+    if k == "constant":
+        return VEL_CONSTANT, np.array(vel["c"], np.float64)
+    if k == "vortex":
+        return VEL_VORTEX, np.array([vel["vs"], *vel.get("w0", (0.0, 0.0, 0.0)), vel["period"]], np.float64)
+    if k == "curl":
+        p = [float(len(vel["octaves"]))]
+        for A, kk, ph, e in vel["octaves"]:
+            p += [A, kk, *ph, *e]
+        return VEL_CURL, np.array(p, np.float64)
+    raise ValueError(k)
+
+
+class MOGrid:
+    """FP64 method-oracle grid (values in voxel units)."""
+
+    def __init__(self, handle, hw):
+        self.lib = load()
+        self.h = handle
+        self.hw = hw
+
+    @classmethod
+    def sphere(cls, radius, center, voxel_size, half_width, w0=(0.0, 0.0, 0.0)):
+        lib = load()
+        c = np.asarray(center, np.float64)
+        w = np.asarray(w0, np.float64)
+        return cls(lib.vm_sphere(radius, _p(c, C.c_double), voxel_size, _p(w, C.c_double), half_width), half_width)
+
+    @classmethod
+    def from_arrays(cls, origins, masks, phi, half_width):
+        lib = load()
+        o = np.ascontiguousarray(origins, np.int32)
+        m = np.ascontiguousarray(masks, np.uint64)
+        v = np.ascontiguousarray(phi, np.float64)
+        return cls(lib.vm_import(_p(o, C.c_int32), _p(m, C.c_uint64), _p(v, C.c_double), len(o), half_width),
+                   half_width)
+
+    def arrays(self):
+        n = self.lib.vm_leaf_count(self.h)
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((n, 8), np.uint64)
+        v = np.zeros((n, 512), np.float64)
+        if n:
+            self.lib.vm_export(self.h, _p(o, C.c_int32), _p(m, C.c_uint64), _p(v, C.c_double))
+        return o, m, v
+
+    def leaf_count(self):
+        return self.lib.vm_leaf_count(self.h)
+
+    def step(self, vel: dict, integrator: int, reinit_iters: int, t: float, dt: float, nthreads: int = 8) -> bool:
+        kind, p = pack_velocity(vel)
+        return bool(self.lib.vm_step(self.h, kind, _p(p, C.c_double), integrator, reinit_iters, t, dt, nthreads))
+
+    def volume(self, ref=(0.0, 0.0, 0.0)):
+        r = np.asarray(ref, np.float64)
+        return self.lib.vm_volume(self.h, _p(r, C.c_double))
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.vm_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def velocity_at(vel: dict, p, t):
+    kind, prm = pack_velocity(vel)
+    pp = np.ascontiguousarray(p, np.float64)
+    u = np.zeros(3)
+    load().vm_velocity(kind, _p(prm, C.c_double), _p(pp, C.c_double), t, _p(u, C.c_double))
+    return u

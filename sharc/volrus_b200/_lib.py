@@ -38,6 +38,35 @@ class vlr_transform(C.Structure):
     ]
 
 
+class vlr_velocity_desc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("constant", C.c_double * 3),
+        ("voxel_size", C.c_double),
+        ("w0", C.c_double * 3),
+        ("period", C.c_double),
+        ("octaves", C.c_int),
+        ("amp", C.c_double * 4),
+        ("wavenumber", C.c_double * 4),
+        ("phase", (C.c_double * 3) * 4),
+        ("dir", (C.c_double * 3) * 4),
+        ("domain_lo", C.c_int32 * 3),
+        ("domain_hi", C.c_int32 * 3),
+    ]
+
+
+class vlr_method_desc(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int),
+        ("half_width", C.c_float),
+        ("integrator", C.c_int),
+        ("reinit_iters", C.c_int),
+        ("dt", C.c_double),
+        ("t0", C.c_double),
+        ("capacity", C.c_size_t),
+    ]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 dbl_p = C.POINTER(C.c_double)
@@ -68,6 +97,18 @@ SIGNATURES = {
     "vlr_rebuild_narrow_band": (C.c_int, [P, P, C.c_float]),
     "vlr_advect_rebuild_host": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t,
                                           flt_p, C.c_double, C.c_float, i32_p, u64_p, flt_p, C.c_size_t, size_p]),
+    "vlr_ls_create_sphere": (C.c_int, [P, C.POINTER(vlr_method_desc), C.POINTER(vlr_velocity_desc), C.c_double,
+                                       dbl_p, C.c_double, dbl_p, PP]),
+    "vlr_ls_create_from_leaves": (C.c_int, [P, C.POINTER(vlr_method_desc), C.POINTER(vlr_velocity_desc), i32_p, u64_p,
+                                            flt_p, C.c_size_t, PP]),
+    "vlr_ls_step": (C.c_int, [P, P, C.c_int]),
+    "vlr_ls_enqueue": (C.c_int, [P, P, C.c_int]),
+    "vlr_ctx_check": (C.c_int, [P]),
+    "vlr_ls_info": (C.c_int, [P, P, size_p, C.POINTER(C.c_uint64), dbl_p]),
+    "vlr_ls_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
+    "vlr_ls_upload": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
+    "vlr_ls_volume": (C.c_int, [P, P, dbl_p, dbl_p]),
+    "vlr_ls_destroy": (None, [P]),
 }
 
 _lib = None
@@ -123,6 +164,10 @@ class Context:
 
     def synchronize(self):
         self.check(self.lib.vlr_ctx_synchronize(self.handle), "synchronize")
+
+    def check_device(self):
+        """Wait for the context stream and raise on device-side errors."""
+        self.check(self.lib.vlr_ctx_check(self.handle), "vlr_ctx_check")
 
     def stream_ptr(self) -> int:
         """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

@@ -1,0 +1,592 @@
+// Host side of the narrow-band method: creation (device sphere generator or
+// uploaded leaves), per-grid velocity tables, graph-captured steps,
+// download and the FP64 volume.  C entry points vlr_ls_* (include/volrus_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "method_state.hpp"
+
+namespace vlr {
+
+size_t scan_scratch_ints(int n);
+
+static int next_pow2i(long long v) {
+    int p = 64;
+    while ((long long)p < v && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+void ls_free(vlr_level_set* ls) {
+    if (ls->graph_exec) cudaGraphExecDestroy(ls->graph_exec);
+    if (ls->graph) cudaGraphDestroy(ls->graph);
+    ls->graph_exec = nullptr;
+    ls->graph = nullptr;
+    void* ptrs[] = {ls->origin, ls->mask, ls->dmask, ls->vals[0], ls->vals[1], ls->nbr, ls->spill, ls->nonempty,
+                    ls->keep, ls->list, ls->list_new, ls->owned, ls->pos, ls->free_stack, ls->scalars, ls->hkey,
+                    ls->hval, ls->pkey, ls->pval, ls->d_params, ls->d_tab, ls->d_partial, ls->d_sum};
+    for (void* p : ptrs) cudaFree(p);
+    cudaFree(ls->staging);
+    ls->staging = nullptr;
+    ls->staging_bytes = 0;
+    ls->origin = nullptr;
+    ls->mask = ls->dmask = nullptr;
+    ls->vals[0] = ls->vals[1] = nullptr;
+    ls->nbr = ls->nonempty = ls->keep = ls->list = ls->list_new = ls->owned = ls->pos = ls->free_stack = nullptr;
+    ls->spill = nullptr;
+    ls->scalars = nullptr;
+    ls->hkey = ls->pkey = nullptr;
+    ls->hval = ls->pval = nullptr;
+    ls->d_params = nullptr;
+    ls->d_tab = nullptr;
+    ls->d_partial = ls->d_sum = nullptr;
+}
+
+int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
+    ls->cap = cap;
+    size_t vb = (ls->precision == VLR_PREC_F16) ? 2 : 4;
+    ls->hcap = next_pow2i(2ll * cap);
+    VLR_CUDA(ctx, cudaMalloc(&ls->origin, sizeof(int4) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->mask, 64ull * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->dmask, 64ull * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->vals[0], vb * kLeafVoxels * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->vals[1], vb * kLeafVoxels * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->nbr, sizeof(int) * kNbr * (size_t)cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->spill, sizeof(unsigned) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->nonempty, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->keep, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->list, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->list_new, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->owned, sizeof(int) * (cap + 1)));
+    VLR_CUDA(ctx, cudaMalloc(&ls->pos, sizeof(int) * (cap + 1 + scan_scratch_ints(cap))));
+    VLR_CUDA(ctx, cudaMalloc(&ls->free_stack, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->scalars, sizeof(int) * 8));
+    VLR_CUDA(ctx, cudaMalloc(&ls->hkey, sizeof(uint64_t) * ls->hcap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->hval, sizeof(int) * ls->hcap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->pkey, sizeof(uint64_t) * ls->hcap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->pval, sizeof(int) * ls->hcap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->d_partial, sizeof(double) * cap));
+    VLR_CUDA(ctx, cudaMalloc(&ls->d_sum, sizeof(double) * 2));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->scalars, 0, sizeof(int) * 8, ctx->stream));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->spill, 0, sizeof(unsigned) * cap, ctx->stream));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->nonempty, 0, sizeof(int) * cap, ctx->stream));
+    // list entries past a failed allocation must still name valid slots
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->list_new, 0, sizeof(int) * cap, ctx->stream));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->list, 0, sizeof(int) * cap, ctx->stream));
+    ls->grid_blocks = ctx->sm_count * 8;
+    return VLR_OK;
+}
+
+// Largest displacement per step along one axis (voxels) for the field.
+static double speed_bound(const vlr_velocity_desc* v) {
+    if (v->kind == VLR_VEL_CONSTANT)
+        return std::max({std::fabs(v->constant[0]), std::fabs(v->constant[1]), std::fabs(v->constant[2])});
+    if (v->kind == VLR_VEL_VORTEX) return 2.0 / v->voxel_size;
+    double b = 0.0;
+    for (int o = 0; o < v->octaves; ++o) b += 2.0 * std::fabs(v->amp[o] * v->wavenumber[o]);
+    return b;
+}
+
+// Per-grid parameters and sin/cos tables (computed in f64, stored as f32 pairs).
+static int grid_params(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* v, const int32_t bb_lo[3],
+                       const int32_t bb_hi[3], int key_bits, MGridParams& P, std::vector<float2>& tab) {
+    std::memset(&P, 0, sizeof(P));
+    P.hw = m->half_width;
+    P.vel_kind = v->kind;
+    int32_t lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        if (v->domain_lo[a] <= v->domain_hi[a]) {
+            lo[a] = v->domain_lo[a];
+            hi[a] = v->domain_hi[a];
+        } else if (v->kind == VLR_VEL_VORTEX && v->voxel_size > 0.0) {
+            // the deformation field lives on the unit cube: index box of [0, 1] + 16 voxels
+            lo[a] = (int32_t)std::floor(-v->w0[a] / v->voxel_size) - 16;
+            hi[a] = (int32_t)std::ceil((1.0 - v->w0[a]) / v->voxel_size) + 16;
+        } else {
+            lo[a] = bb_lo[a] - 256;
+            hi[a] = bb_hi[a] + 256;
+        }
+        long long centre = ((long long)(bb_lo[a] >> 3) + (long long)(bb_hi[a] >> 3)) / 2;
+        P.base[a] = centre - (1ll << (key_bits - 1));
+    }
+    const double pi = 3.14159265358979323846;
+    auto add_family = [&](int f, double dphi, const double ph[3], const double scale[3], const double offs[3]) {
+        P.dphi[f] = (float)dphi;
+        for (int a = 0; a < 3; ++a) {
+            P.tab_off[f][a] = (int)tab.size();
+            for (int32_t i = lo[a]; i <= hi[a]; ++i) {
+                double ang = scale[a] * (offs[a] + dphi / scale[a] * i) + ph[a];
+                tab.push_back(make_float2((float)std::sin(ang), (float)std::cos(ang)));
+            }
+        }
+    };
+    for (int a = 0; a < 3; ++a) {
+        P.tab_lo[a] = lo[a];
+        P.tab_len[a] = hi[a] - lo[a] + 1;
+        if (P.tab_len[a] <= 0 || P.tab_len[a] > (1 << 25))
+            return set_error(ctx, VLR_ERR_INVALID, "velocity domain box empty or too large");
+    }
+    if (v->kind == VLR_VEL_CONSTANT) {
+        for (int a = 0; a < 3; ++a) P.c[a] = (float)v->constant[a];
+        for (int a = 0; a < 3; ++a) P.tab_len[a] = 0;
+    } else if (v->kind == VLR_VEL_VORTEX) {
+        if (!(v->voxel_size > 0.0) || !(v->period != 0.0))
+            return set_error(ctx, VLR_ERR_INVALID, "vortex needs voxel_size > 0 and period != 0");
+        P.vel_scale = (float)(1.0 / v->voxel_size);
+        P.pi_over_T = (float)(pi / v->period);
+        // angle(i) = pi * (w0 + vs * i)
+        double ph[3] = {0, 0, 0}, sc[3] = {pi, pi, pi}, of[3] = {v->w0[0], v->w0[1], v->w0[2]};
+        add_family(0, pi * v->voxel_size, ph, sc, of);
+    } else if (v->kind == VLR_VEL_CURL) {
+        if (v->octaves < 1 || v->octaves > kMaxOctaves) return set_error(ctx, VLR_ERR_INVALID, "curl octaves 1..4");
+        P.octaves = v->octaves;
+        for (int o = 0; o < v->octaves; ++o) {
+            P.ak[o] = (float)(v->amp[o] * v->wavenumber[o]);
+            for (int a = 0; a < 3; ++a) P.e[o][a] = (float)v->dir[o][a];
+            // angle(i) = k * i + phase
+            double sc[3] = {1, 1, 1}, of[3] = {0, 0, 0};
+            add_family(o, v->wavenumber[o], v->phase[o], sc, of);
+        }
+    } else {
+        return set_error(ctx, VLR_ERR_INVALID, "unknown velocity kind");
+    }
+    return VLR_OK;
+}
+
+static int setup_common(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* v,
+                        const int32_t bb_lo[3], const int32_t bb_hi[3]) {
+    if (m->integrator < 1 || m->integrator > 3) return set_error(ctx, VLR_ERR_INVALID, "integrator must be 1, 2 or 3");
+    if (m->reinit_iters < 0 || m->reinit_iters > 2)
+        return set_error(ctx, VLR_ERR_UNSUPPORTED, "reinit_iters must be 0, 1 or 2");
+    if (!(m->half_width > 0.0f) || m->half_width > 7.0f)
+        return set_error(ctx, VLR_ERR_INVALID, "half_width must be in (0, 7] voxels");
+    if (!(m->dt > 0.0)) return set_error(ctx, VLR_ERR_INVALID, "dt must be positive");
+    double disp = speed_bound(v) * m->dt;
+    if (disp <= 1.0) ls->halo = 2;
+    else if (disp <= 2.0) ls->halo = 3;
+    else return set_error(ctx, VLR_ERR_REACH, "velocity * dt exceeds 2 voxels per step (CFL); reduce dt");
+    ls->reinit_iters = m->reinit_iters;
+    ls->sp.dt = (float)m->dt;
+    ls->sp.t0 = (float)m->t0;
+    ls->sp.integrator = m->integrator;
+    ls->sp.n_grids = 1;
+    ls->sp.key_bits = ls->key_bits;
+    MGridParams P;
+    std::vector<float2> tab;
+    int rc = grid_params(ctx, m, v, bb_lo, bb_hi, ls->key_bits, P, tab);
+    if (rc) return rc;
+    ls->h_params.assign(1, P);
+    VLR_CUDA(ctx, cudaMalloc(&ls->d_params, sizeof(MGridParams)));
+    VLR_CUDA(ctx, cudaMemcpy(ls->d_params, &P, sizeof(MGridParams), cudaMemcpyHostToDevice));
+    size_t nt = std::max<size_t>(tab.size(), 1);
+    VLR_CUDA(ctx, cudaMalloc(&ls->d_tab, sizeof(float2) * nt));
+    if (!tab.empty())
+        VLR_CUDA(ctx, cudaMemcpy(ls->d_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
+    return VLR_OK;
+}
+
+__global__ void k_iota(int* a, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+// free stack = slots [n, cap) (pops take the lowest slots first), list = 0..n-1,
+// count = n; `step` keeps its value unless reset.
+__global__ void k_init_lists(int* list, int* free_stack, int* scalars, int n, int cap, int reset_step) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+        if (i < n) list[i] = i;
+        if (i < cap - n) free_stack[i] = cap - 1 - i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scalars[0] = n;
+        if (reset_step) scalars[1] = 0;
+        scalars[2] = cap - n;
+        scalars[3] = 0;
+    }
+}
+
+static int init_lists(vlr_ctx* ctx, vlr_level_set* ls, int n, bool reset_step = true) {
+    k_init_lists<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, ls->free_stack, ls->scalars, n, ls->cap,
+                                                           reset_step ? 1 : 0);
+    VLR_CUDA(ctx, cudaGetLastError());
+    int rc = ls_enqueue_index(ctx, ls);
+    if (rc) return rc;
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return consume_device_errors(ctx, "method grid index");
+}
+
+// Staging buffer of at least `bytes` owned by the level set.
+static int ls_staging(vlr_ctx* ctx, vlr_level_set* ls, size_t bytes, void** out) {
+    if (bytes > ls->staging_bytes) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ls->staging);
+        ls->staging = nullptr;
+        ls->staging_bytes = 0;
+        VLR_CUDA(ctx, cudaMalloc(&ls->staging, bytes));
+        ls->staging_bytes = bytes;
+    }
+    *out = ls->staging;
+    return VLR_OK;
+}
+
+template <typename T>
+__global__ void k_pick(const int* flags, const int* pos, int n, const int4* o_in, const uint64_t* m_in,
+                       const T* v_in, int4* o_out, uint64_t* m_out, T* v_out) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        if (!flags[i]) continue;
+        int j = pos[i];
+        if (threadIdx.x == 0) o_out[j] = o_in[i];
+        if (threadIdx.x < 8) m_out[(size_t)j * 8 + threadIdx.x] = m_in[(size_t)i * 8 + threadIdx.x];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            v_out[(size_t)j * kLeafVoxels + t] = v_in[(size_t)i * kLeafVoxels + t];
+    }
+}
+
+template <typename T>
+__global__ void k_from_f32(const float* in, T* out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = from_f<T>(in[i]);
+}
+
+template <typename T>
+__global__ void k_gather_out(const int* list, int n, const int4* origin, const uint64_t* mask, const T* vals,
+                             int4* o_out, uint64_t* m_out, float* v_out) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        int s = list[i];
+        if (threadIdx.x == 0) o_out[i] = origin[s];
+        if (threadIdx.x < 8) m_out[(size_t)i * 8 + threadIdx.x] = mask[(size_t)s * 8 + threadIdx.x];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            v_out[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
+    }
+}
+
+__global__ void k_count_active(const int* list, const int* count_ptr, const uint64_t* mask,
+                               unsigned long long* out) {
+    int n = *count_ptr;
+    unsigned long long c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * 8; i += gridDim.x * blockDim.x)
+        c += __popcll(mask[(size_t)list[i >> 3] * 8 + (i & 7)]);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+}  // namespace vlr
+
+using namespace vlr;
+
+namespace {
+
+int create_sphere_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* vel,
+                       double radius, const double c[3], double vs, const double w0[3]) {
+    double hw = (double)m->half_width;
+    int32_t lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        double ci = (c[a] - w0[a]) / vs, ri = radius / vs;
+        lo[a] = (int32_t)std::floor(ci - ri - hw - 2.0);
+        hi[a] = (int32_t)std::ceil(ci + ri + hw + 2.0);
+    }
+    long long nl[3];
+    for (int a = 0; a < 3; ++a) nl[a] = (long long)(hi[a] >> 3) - (lo[a] >> 3) + 1;
+    long long n_cand = nl[0] * nl[1] * nl[2];
+    if (n_cand > (1ll << 26)) return set_error(ctx, VLR_ERR_CAPACITY, "sphere bounding box too large");
+    int rc = setup_common(ctx, ls, m, vel, lo, hi);
+    if (rc) return rc;
+    size_t vb = (ls->precision == VLR_PREC_F16) ? 2 : 4;
+    int4* o_tmp = nullptr;
+    uint64_t* m_tmp = nullptr;
+    void* v_tmp = nullptr;
+    int* touched = nullptr;
+    int* pos = nullptr;
+    VLR_CUDA(ctx, cudaMalloc(&o_tmp, sizeof(int4) * n_cand));
+    VLR_CUDA(ctx, cudaMalloc(&m_tmp, 64ull * n_cand));
+    VLR_CUDA(ctx, cudaMalloc(&v_tmp, vb * kLeafVoxels * n_cand));
+    VLR_CUDA(ctx, cudaMalloc(&touched, sizeof(int) * (n_cand + 1)));
+    VLR_CUDA(ctx, cudaMalloc(&pos, sizeof(int) * (n_cand + 1)));
+    int blocks = std::min<long long>(n_cand, (long long)ctx->sm_count * 16);
+    if (ls->precision == VLR_PREC_F16)
+        k_m_sphere<__half><<<blocks, 256, 0, ctx->stream>>>(lo[0] >> 3, lo[1] >> 3, lo[2] >> 3, (int)nl[1], (int)nl[2],
+                                                            (int)n_cand, radius, c[0], c[1], c[2], vs, w0[0], w0[1],
+                                                            w0[2], hw, o_tmp, m_tmp, (__half*)v_tmp, touched);
+    else
+        k_m_sphere<float><<<blocks, 256, 0, ctx->stream>>>(lo[0] >> 3, lo[1] >> 3, lo[2] >> 3, (int)nl[1], (int)nl[2],
+                                                           (int)n_cand, radius, c[0], c[1], c[2], vs, w0[0], w0[1],
+                                                           w0[2], hw, o_tmp, m_tmp, (float*)v_tmp, touched);
+    VLR_CUDA(ctx, cudaGetLastError());
+    rc = scan_exclusive(ctx, touched, pos, (int)n_cand, pos + n_cand);
+    if (rc) return rc;
+    int n = 0;
+    rc = read_int(ctx, pos + n_cand, &n);
+    if (rc) return rc;
+    int cap = m->capacity ? (int)std::min<size_t>(m->capacity, (size_t)1 << 30) : 2 * n + 4096;
+    if (cap < n) return set_error(ctx, VLR_ERR_CAPACITY, "capacity below the initial leaf count");
+    rc = ls_alloc(ctx, ls, cap);
+    if (rc) return rc;
+    if (ls->precision == VLR_PREC_F16)
+        k_pick<__half><<<blocks, 256, 0, ctx->stream>>>(touched, pos, (int)n_cand, o_tmp, m_tmp, (const __half*)v_tmp,
+                                                        ls->origin, ls->mask, (__half*)ls->vals[0]);
+    else
+        k_pick<float><<<blocks, 256, 0, ctx->stream>>>(touched, pos, (int)n_cand, o_tmp, m_tmp, (const float*)v_tmp,
+                                                       ls->origin, ls->mask, (float*)ls->vals[0]);
+    VLR_CUDA(ctx, cudaGetLastError());
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(o_tmp);
+    cudaFree(m_tmp);
+    cudaFree(v_tmp);
+    cudaFree(touched);
+    cudaFree(pos);
+    return init_lists(ctx, ls, n);
+}
+
+// Replace the state with n host leaves (origins i32[3], masks, phi f32 voxel
+// units), staged through one pinned-free device buffer.
+__global__ void k_unpack_upload(const int32_t* o3, int n, int4* origin) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        origin[i] = make_int4(o3[3 * i], o3[3 * i + 1], o3[3 * i + 2], 0);
+}
+
+int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                size_t n, bool reset_step) {
+    if (n > (size_t)ls->cap) return set_error(ctx, VLR_ERR_CAPACITY, "more leaves than the level set's capacity");
+    for (size_t i = 0; i < 3 * n; ++i)
+        if (origins[i] & 7) return set_error(ctx, VLR_ERR_INVALID, "leaf origin not a multiple of 8");
+    size_t vbytes = sizeof(float) * kLeafVoxels * n;
+    void* stg = nullptr;
+    int rc = ls_staging(ctx, ls, vbytes + 12 * n + 16, &stg);
+    if (rc) return rc;
+    float* tmp = (float*)stg;
+    int32_t* o3 = (int32_t*)((char*)stg + vbytes);
+    VLR_CUDA(ctx, cudaMemcpyAsync(o3, origins, 12 * n, cudaMemcpyHostToDevice, ctx->stream));
+    VLR_CUDA(ctx, cudaMemcpyAsync(ls->mask, masks, 64 * n, cudaMemcpyHostToDevice, ctx->stream));
+    k_unpack_upload<<<ls->grid_blocks, 256, 0, ctx->stream>>>(o3, (int)n, ls->origin);
+    if (ls->precision == VLR_PREC_F16) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(tmp, phi, vbytes, cudaMemcpyHostToDevice, ctx->stream));
+        k_from_f32<__half><<<ls->grid_blocks, 256, 0, ctx->stream>>>(tmp, (__half*)ls->vals[0], kLeafVoxels * n);
+    } else {
+        VLR_CUDA(ctx, cudaMemcpyAsync(ls->vals[0], phi, vbytes, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    return init_lists(ctx, ls, (int)n, reset_step);
+}
+
+int create_leaves_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* vel,
+                       const int32_t* origins, const uint64_t* masks, const float* phi, size_t n) {
+    if (n == 0) return set_error(ctx, VLR_ERR_INVALID, "no leaves");
+    int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    for (size_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            if (origins[3 * i + a] & 7) return set_error(ctx, VLR_ERR_INVALID, "leaf origin not a multiple of 8");
+            lo[a] = std::min(lo[a], origins[3 * i + a]);
+            hi[a] = std::max(hi[a], origins[3 * i + a] + 7);
+        }
+    for (int a = 0; a < 3; ++a)
+        if (((long long)hi[a] - lo[a]) >> 3 >= (1ll << (ls->key_bits - 1)) - 4)
+            return set_error(ctx, VLR_ERR_EXTENT, "grid spans more than 2^24 voxels along an axis");
+    int rc = setup_common(ctx, ls, m, vel, lo, hi);
+    if (rc) return rc;
+    int cap = m->capacity ? (int)std::min<size_t>(m->capacity, (size_t)1 << 30) : 2 * (int)n + 4096;
+    if ((size_t)cap < n) return set_error(ctx, VLR_ERR_CAPACITY, "capacity below the leaf count");
+    rc = ls_alloc(ctx, ls, cap);
+    if (rc) return rc;
+    return upload_impl(ctx, ls, origins, masks, phi, n, true);
+}
+
+int capture_step(vlr_ctx* ctx, vlr_level_set* ls) {
+    if (ls->graph_exec) return VLR_OK;
+    VLR_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = ls_enqueue_step(ctx, ls);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
+    ls->graph = g;
+    VLR_CUDA(ctx, cudaGraphInstantiate(&ls->graph_exec, g, 0));
+    return VLR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlr_ls_create_sphere(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* vel, double radius,
+                         const double center[3], double voxel_size, const double w0[3], vlr_level_set** out) {
+    if (!ctx || !m || !vel || !center || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (!(voxel_size > 0.0) || !(radius > 0.0)) return set_error(ctx, VLR_ERR_INVALID, "radius and voxel_size > 0");
+    *out = nullptr;
+    vlr_level_set* ls = new vlr_level_set();
+    ls->ctx = ctx;
+    ls->precision = m->precision == VLR_PREC_F16 ? VLR_PREC_F16 : VLR_PREC_F32;
+    double zero[3] = {0, 0, 0};
+    int rc = create_sphere_impl(ctx, ls, m, vel, radius, center, voxel_size, w0 ? w0 : zero);
+    if (rc) {
+        vlr_ls_destroy(ls);
+        return rc;
+    }
+    *out = ls;
+    return VLR_OK;
+}
+
+int vlr_ls_create_from_leaves(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* vel,
+                              const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
+                              vlr_level_set** out) {
+    if (!ctx || !m || !vel || !origins || !masks || !phi || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    vlr_level_set* ls = new vlr_level_set();
+    ls->ctx = ctx;
+    ls->precision = m->precision == VLR_PREC_F16 ? VLR_PREC_F16 : VLR_PREC_F32;
+    int rc = create_leaves_impl(ctx, ls, m, vel, origins, masks, phi, n_leaves);
+    if (rc) {
+        vlr_ls_destroy(ls);
+        return rc;
+    }
+    *out = ls;
+    return VLR_OK;
+}
+
+int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    for (int i = 0; i < n_steps; ++i) {
+        if (ctx->timer.enabled) {
+            int rc = ls_enqueue_step(ctx, ls);
+            if (rc) return rc;
+        } else {
+            int rc = capture_step(ctx, ls);
+            if (rc) return rc;
+            VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
+        }
+    }
+    return VLR_OK;
+}
+
+int vlr_ctx_check(vlr_ctx* ctx) {
+    if (!ctx) return VLR_ERR_INVALID;
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return consume_device_errors(ctx, "vlr_ctx_check");
+}
+
+int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    for (int i = 0; i < n_steps; ++i) {
+        if (ctx->timer.enabled) {
+            int rc = ls_enqueue_step(ctx, ls);
+            if (rc) return rc;
+        } else {
+            int rc = capture_step(ctx, ls);
+            if (rc) return rc;
+            VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
+        }
+    }
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return consume_device_errors(ctx, "vlr_ls_step");
+}
+
+int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_t* n_active, double* time) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    int sc[8];
+    VLR_CUDA(ctx, cudaMemcpyAsync(sc, ls->scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (n_leaves) *n_leaves = (size_t)sc[0];
+    if (time) *time = (double)ls->sp.t0 + (double)sc[1] * (double)ls->sp.dt;
+    if (n_active) {
+        unsigned long long* d = (unsigned long long*)ls->d_sum;
+        VLR_CUDA(ctx, cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream));
+        k_count_active<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, ls->scalars, ls->mask, d);
+        unsigned long long h = 0;
+        VLR_CUDA(ctx, cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *n_active = h;
+    }
+    return VLR_OK;
+}
+
+int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uint64_t* masks, float* phi,
+                    size_t cap_leaves) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    size_t n = 0;
+    int rc = vlr_ls_info(ctx, ls, &n, nullptr, nullptr);
+    if (rc) return rc;
+    if (n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    if (!n) return VLR_OK;
+    void* stg = nullptr;
+    size_t vbytes = sizeof(float) * kLeafVoxels * n;
+    rc = ls_staging(ctx, const_cast<vlr_level_set*>(ls), vbytes + 80 * n, &stg);
+    if (rc) return rc;
+    float* v = (float*)stg;
+    int4* o = (int4*)((char*)stg + vbytes);
+    uint64_t* mm = (uint64_t*)((char*)stg + vbytes + 16 * n);
+    int B = (int)std::min<size_t>(n, (size_t)ctx->sm_count * 8);
+    if (ls->precision == VLR_PREC_F16)
+        k_gather_out<__half><<<B, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, ls->mask,
+                                                         (const __half*)ls->vals[0], o, mm, v);
+    else
+        k_gather_out<float><<<B, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, ls->mask,
+                                                        (const float*)ls->vals[0], o, mm, v);
+    std::vector<int4> ho(n);
+    std::vector<uint64_t> hm(8 * n);
+    std::vector<float> hv(kLeafVoxels * n);
+    VLR_CUDA(ctx, cudaMemcpyAsync(ho.data(), o, sizeof(int4) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaMemcpyAsync(hm.data(), mm, 64 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaMemcpyAsync(hv.data(), v, sizeof(float) * kLeafVoxels * n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<size_t> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        const int4 &A = ho[a], &B2 = ho[b];
+        if (A.w != B2.w) return A.w < B2.w;
+        if (A.x != B2.x) return A.x < B2.x;
+        if (A.y != B2.y) return A.y < B2.y;
+        return A.z < B2.z;
+    });
+    for (size_t i = 0; i < n; ++i) {
+        size_t s = order[i];
+        if (origins) {
+            origins[3 * i] = ho[s].x;
+            origins[3 * i + 1] = ho[s].y;
+            origins[3 * i + 2] = ho[s].z;
+        }
+        if (masks) std::memcpy(masks + 8 * i, &hm[8 * s], 64);
+        if (phi) std::memcpy(phi + kLeafVoxels * i, &hv[kLeafVoxels * s], sizeof(float) * kLeafVoxels);
+    }
+    return VLR_OK;
+}
+
+int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                  size_t n_leaves) {
+    if (!ctx || !ls || !origins || !masks || !phi) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "upload replaces single-grid states only");
+    return upload_impl(ctx, ls, origins, masks, phi, n_leaves, false);
+}
+
+int vlr_ls_volume(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* volume) {
+    if (!ctx || !ls || !volume) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    double r[3] = {0, 0, 0};
+    if (ref) std::memcpy(r, ref, sizeof(r));
+    MLeafArrays A = ls->arrays();
+    if (ls->precision == VLR_PREC_F16)
+        VLR_TIMED(ctx, "k_m_volume",
+                  k_m_volume<__half><<<ls->grid_blocks, 256, 0, ctx->stream>>>(A, (const __half*)ls->vals[0],
+                                                                               ls->d_params, r[0], r[1], r[2],
+                                                                               ls->d_partial));
+    else
+        VLR_TIMED(ctx, "k_m_volume",
+                  k_m_volume<float><<<ls->grid_blocks, 256, 0, ctx->stream>>>(A, (const float*)ls->vals[0],
+                                                                              ls->d_params, r[0], r[1], r[2],
+                                                                              ls->d_partial));
+    k_reduce_fixed<<<1, 1024, 0, ctx->stream>>>(ls->d_partial, ls->scalars, ls->d_sum);
+    VLR_CUDA(ctx, cudaGetLastError());
+    VLR_CUDA(ctx, cudaMemcpyAsync(volume, ls->d_sum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
+
+void vlr_ls_destroy(vlr_level_set* ls) {
+    if (!ls) return;
+    if (ls->ctx) cudaStreamSynchronize(ls->ctx->stream);
+    ls_free(ls);
+    delete ls;
+}
+
+}  // extern "C"

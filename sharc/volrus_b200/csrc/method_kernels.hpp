@@ -1,0 +1,36 @@
+// Declarations shared by the method kernels and their host orchestration.
+#pragma once
+#include "method.cuh"
+
+namespace vlr {
+
+// Slot-indexed leaf arrays of a method grid plus its ordered leaf list.
+struct MLeafArrays {
+    const int* list;     // list[i] = slot of the i-th leaf in processing order
+    const int* count;    // device scalar: number of list entries
+    const int* step;     // device scalar: steps taken since creation
+    const int4* origin;  // {x, y, z, grid id}
+    uint64_t* mask;      // activity
+    uint64_t* dmask;     // dilated activity of the current step (written by advect)
+    const int* nbr;      // 27 neighbour slots per slot
+    unsigned* spill;     // 27-bit spill mask per slot (written by reinit)
+    int* nonempty;       // 1 if the slot has an active voxel after the step
+};
+
+template <typename T, int H>
+__global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
+                           const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
+                           unsigned* __restrict__ err);
+template <typename T, int NIT>
+__global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
+                           const MGridParams* __restrict__ params);
+template <typename T>
+__global__ void k_m_volume(MLeafArrays A, const T* __restrict__ vals, const MGridParams* __restrict__ params,
+                           double r0, double r1, double r2, double* __restrict__ partial);
+__global__ void k_reduce_fixed(const double* __restrict__ in, const int* __restrict__ n_ptr, double* __restrict__ out);
+template <typename T>
+__global__ void k_m_sphere(int lx0, int ly0, int lz0, int ny, int nz, int n_cand, double r, double c0, double c1,
+                           double c2, double vs, double w00, double w01, double w02, double hwd, int4* origin,
+                           uint64_t* mask, T* vals, int* touched);
+
+}  // namespace vlr

@@ -1,0 +1,82 @@
+// Host-side state of a method grid (or a batch of grids): slot pool, ordered
+// leaf list, hash index, neighbour table, per-grid parameters, velocity
+// tables and the captured step graph.
+#pragma once
+#include <vector>
+
+#include "method_kernels.hpp"
+#include "vlr_host.hpp"
+
+struct vlr_level_set {
+    vlr_ctx* ctx = nullptr;
+    int precision = 0;       // VLR_PREC_F32 / VLR_PREC_F16
+    int cap = 0;             // slots
+    int n_grids = 1;
+    int key_bits = 21;
+    int halo = 2;
+    int reinit_iters = 2;
+    // slot-indexed arrays
+    int4* origin = nullptr;
+    uint64_t* mask = nullptr;
+    uint64_t* dmask = nullptr;
+    void* vals[2] = {nullptr, nullptr};  // vals[0] holds the state between steps
+    int* nbr = nullptr;
+    unsigned* spill = nullptr;
+    int* nonempty = nullptr;
+    int* keep = nullptr;
+    // list (position-indexed)
+    int* list = nullptr;
+    int* list_new = nullptr;
+    int* owned = nullptr;    // cap + 1: survive + owned count per position, then scanned
+    int* pos = nullptr;      // cap + 1
+    int* free_stack = nullptr;
+    int* scalars = nullptr;  // [0] count, [1] step, [2] free top, [3] new count
+    // hash (key -> slot) and proposal table (key -> min owner direction)
+    uint64_t* hkey = nullptr;
+    int* hval = nullptr;
+    uint64_t* pkey = nullptr;
+    int* pval = nullptr;
+    int hcap = 0;
+    // parameters
+    vlr::MGridParams* d_params = nullptr;
+    std::vector<vlr::MGridParams> h_params;
+    float2* d_tab = nullptr;
+    vlr::MStepParams sp{};
+    // reductions
+    double* d_partial = nullptr;
+    double* d_sum = nullptr;
+    // staging for uploads and downloads (grown on demand)
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    // captured step
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int grid_blocks = 0;     // persistent grid size
+    int scan_levels = 0;
+
+    vlr::MLeafArrays arrays() const {
+        vlr::MLeafArrays A;
+        A.list = list;
+        A.count = scalars;
+        A.step = scalars + 1;
+        A.origin = origin;
+        A.mask = mask;
+        A.dmask = dmask;
+        A.nbr = nbr;
+        A.spill = spill;
+        A.nonempty = nonempty;
+        return A;
+    }
+};
+
+namespace vlr {
+
+int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap);
+void ls_free(vlr_level_set* ls);
+// Enqueue one step (no host synchronisation; capturable).
+int ls_enqueue_step(vlr_ctx* ctx, vlr_level_set* ls);
+// Rebuild hash and neighbour table from the list (enqueued).
+int ls_enqueue_index(vlr_ctx* ctx, vlr_level_set* ls);
+int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls);
+
+}  // namespace vlr
