@@ -177,6 +177,31 @@ int vlr_ls_create_sphere(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_veloc
 int vlr_ls_create_from_leaves(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocity_desc* vel,
                               const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
                               vlr_level_set** out);
+/* A sphere in index units (voxels) of one grid of a batch. */
+typedef struct vlr_sphere {
+    double center[3];
+    double radius;
+} vlr_sphere;
+
+/* One grid of a batch: the union of its spheres (SDF = min over spheres of
+ * |p - c| - r, in voxels) and its own velocity. */
+typedef struct vlr_batch_grid {
+    const vlr_sphere* spheres;
+    int n_spheres;
+    vlr_velocity_desc velocity;
+} vlr_batch_grid;
+
+/* Many independent grids in one leaf pool: every kernel of a step processes
+ * all leaves of all grids in one persistent launch.  Voxel size 1, world =
+ * index.  n_grids <= 512 when n_grids > 1 (each grid spans < 2^21 voxels per
+ * axis); a single grid may span 2^24 voxels per axis. */
+int vlr_ls_create_spheres(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_batch_grid* grids, int n_grids,
+                          vlr_level_set** out);
+/* Leaves of one grid of a batch (sorted (x, y, z)); pass grid = -1 for all
+ * leaves (sorted by grid then (x, y, z)) with grid_ids receiving each leaf's grid. */
+int vlr_ls_download_grid(vlr_ctx* ctx, const vlr_level_set* ls, int grid, int32_t* grid_ids, int32_t* origins,
+                         uint64_t* masks, float* phi, size_t cap_leaves, size_t* n_out);
+
 /* Advance n_steps steps (each one graph replay on the context stream) and
  * wait for them; device-side errors are reported here. */
 int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);

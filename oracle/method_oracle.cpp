@@ -218,6 +218,59 @@ Grid sphere(double radius, const double center[3], double vs, const double w0[3]
     return g;
 }
 
+// Union of spheres in index units (voxel size 1): phi = min_i |p - c_i| - r_i
+// over ALL spheres; leaves kept when their 10^3 box holds a band voxel.
+Grid spheres_union(const double* sph, int n, double hw) {
+    Grid g;
+    g.hw = hw;
+    auto phi_at = [&](int32_t x, int32_t y, int32_t z) {
+        double best = 1e300;
+        for (int i = 0; i < n; ++i) {
+            double dx = (double)x - sph[4 * i], dy = (double)y - sph[4 * i + 1], dz = (double)z - sph[4 * i + 2];
+            best = std::min(best, std::sqrt(dx * dx + dy * dy + dz * dz) - sph[4 * i + 3]);
+        }
+        return best;
+    };
+    std::unordered_map<Key, int, KeyHash> cand;
+    std::vector<Key> order;
+    for (int i = 0; i < n; ++i) {
+        int32_t l0[3], l1[3];
+        for (int a = 0; a < 3; ++a) {
+            l0[a] = ((int32_t)std::floor(sph[4 * i + a] - sph[4 * i + 3] - hw - 2.0)) >> 3;
+            l1[a] = ((int32_t)std::ceil(sph[4 * i + a] + sph[4 * i + 3] + hw + 2.0)) >> 3;
+        }
+        for (int32_t x = l0[0]; x <= l1[0]; ++x)
+            for (int32_t y = l0[1]; y <= l1[1]; ++y)
+                for (int32_t z = l0[2]; z <= l1[2]; ++z)
+                    if (cand.emplace(Key{x, y, z}, 1).second) order.push_back(Key{x, y, z});
+    }
+    for (const Key& k : order) {
+        bool touched = false;
+        for (int x = -1; x <= 8 && !touched; ++x)
+            for (int y = -1; y <= 8 && !touched; ++y)
+                for (int z = -1; z <= 8 && !touched; ++z)
+                    if (std::fabs(phi_at(8 * k.x + x, 8 * k.y + y, 8 * k.z + z)) < hw) touched = true;
+        if (!touched) continue;
+        Leaf L;
+        L.o[0] = 8 * k.x;
+        L.o[1] = 8 * k.y;
+        L.o[2] = 8 * k.z;
+        std::memset(L.m, 0, sizeof(L.m));
+        for (int off = 0; off < 512; ++off) {
+            double p = phi_at(L.o[0] + (off >> 6), L.o[1] + ((off >> 3) & 7), L.o[2] + (off & 7));
+            if (std::fabs(p) < hw) {
+                L.phi[off] = p;
+                L.m[off >> 6] |= 1ull << (off & 63);
+            } else {
+                L.phi[off] = std::copysign(hw, p);
+            }
+        }
+        g.leaves.push_back(L);
+    }
+    g.reindex();
+    return g;
+}
+
 double volume(const Grid& g, const double ref[3]) {
     const double pi = 3.14159265358979323846, eps = 1.5;
     double total = 0.0;
@@ -250,6 +303,9 @@ void* vm_sphere(double radius, const double* center, double vs, const double* w0
 }
 
 void vm_free(void* g) { delete (Grid*)g; }
+
+// spheres: n x (cx, cy, cz, r) in index units
+void* vm_spheres(const double* spheres, int n, double hw) { return new Grid(spheres_union(spheres, n, hw)); }
 
 size_t vm_leaf_count(void* g) { return ((Grid*)g)->leaves.size(); }
 

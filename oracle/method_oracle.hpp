@@ -221,6 +221,9 @@ bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t
 Grid sphere(double radius, const double center[3], double vs, const double w0[3], double hw,
             const int32_t box_lo[3], const int32_t box_hi[3]);
 
+// Union of spheres (index units, voxel size 1): phi = min_i |p - c_i| - r_i.
+Grid spheres_union(const double* sph, int n, double hw);
+
 // Enclosed volume in index units^3 by the smeared-delta surface integral
 // V = (1/3) sum_active delta_eps(phi) (p - ref) . grad phi, eps = 1.5 voxels.
 double volume(const Grid& g, const double ref[3]);

@@ -47,6 +47,7 @@ SIGS = {
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
     "vm_free": (None, [P]),
+    "vm_spheres": (P, [dbl_p, C.c_int, C.c_double]),
     "vm_leaf_count": (C.c_size_t, [P]),
     "vm_export": (None, [P, i32_p, u64_p, dbl_p]),
     "vm_import": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double]),
@@ -242,6 +243,13 @@ class MOGrid:
         c = np.asarray(center, np.float64)
         w = np.asarray(w0, np.float64)
         return cls(lib.vm_sphere(radius, _p(c, C.c_double), voxel_size, _p(w, C.c_double), half_width), half_width)
+
+    @classmethod
+    def spheres(cls, spheres, half_width):
+        """Union of spheres, rows (cx, cy, cz, r) in voxels."""
+        lib = load()
+        s = np.ascontiguousarray(spheres, np.float64).reshape(-1, 4)
+        return cls(lib.vm_spheres(_p(s, C.c_double), len(s), half_width), half_width)
 
     @classmethod
     def from_arrays(cls, origins, masks, phi, half_width):

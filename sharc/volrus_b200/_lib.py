@@ -67,6 +67,14 @@ class vlr_method_desc(C.Structure):
     ]
 
 
+class vlr_sphere(C.Structure):
+    _fields_ = [("center", C.c_double * 3), ("radius", C.c_double)]
+
+
+class vlr_batch_grid(C.Structure):
+    _fields_ = [("spheres", C.POINTER(vlr_sphere)), ("n_spheres", C.c_int), ("velocity", vlr_velocity_desc)]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 dbl_p = C.POINTER(C.c_double)
@@ -101,6 +109,8 @@ SIGNATURES = {
                                        dbl_p, C.c_double, dbl_p, PP]),
     "vlr_ls_create_from_leaves": (C.c_int, [P, C.POINTER(vlr_method_desc), C.POINTER(vlr_velocity_desc), i32_p, u64_p,
                                             flt_p, C.c_size_t, PP]),
+    "vlr_ls_create_spheres": (C.c_int, [P, C.POINTER(vlr_method_desc), C.POINTER(vlr_batch_grid), C.c_int, PP]),
+    "vlr_ls_download_grid": (C.c_int, [P, P, C.c_int, i32_p, i32_p, u64_p, flt_p, C.c_size_t, size_p]),
     "vlr_ls_step": (C.c_int, [P, P, C.c_int]),
     "vlr_ls_enqueue": (C.c_int, [P, P, C.c_int]),
     "vlr_ctx_check": (C.c_int, [P]),

@@ -35,8 +35,17 @@ struct MGridParams {
     int tab_off[kMaxOctaves][3];  // first float2 of family f, axis a
     int tab_lo[3];         // index coordinate of table entry 0 (per axis)
     int tab_len[3];
+    int full_series;       // 1: rotation angles may reach 1 rad (full Taylor series); 0: below 0.05 rad
+    int pad_;
     long long base[3];     // hash key base (leaf coordinates)
 };
+
+// sin and cos of |d| < 0.05 (Taylor to d^5 / d^4, error < 3e-10).
+__device__ __forceinline__ void tiny_sincos(float d, float& s, float& c) {
+    float d2 = d * d;
+    s = d * (1.0f - d2 * (1.0f / 6.0f) * (1.0f - d2 * (1.0f / 20.0f)));
+    c = 1.0f - d2 * 0.5f * (1.0f - d2 * (1.0f / 12.0f));
+}
 
 // Step-wide parameters (shared by all grids of a batch).
 struct MStepParams {

@@ -26,8 +26,10 @@ void ls_free(vlr_level_set* ls) {
     ls->graph = nullptr;
     void* ptrs[] = {ls->origin, ls->mask, ls->dmask, ls->vals[0], ls->vals[1], ls->nbr, ls->spill, ls->nonempty,
                     ls->keep, ls->list, ls->list_new, ls->owned, ls->pos, ls->free_stack, ls->scalars, ls->hkey,
-                    ls->hval, ls->pkey, ls->pval, ls->d_params, ls->d_tab, ls->d_partial, ls->d_sum};
+                    ls->hval, ls->pkey, ls->pval, ls->d_params, ls->d_tab, ls->d_partial, ls->d_sum,
+                    ls->newinfo};
     for (void* p : ptrs) cudaFree(p);
+    ls->newinfo = nullptr;
     cudaFree(ls->staging);
     ls->staging = nullptr;
     ls->staging_bytes = 0;
@@ -61,6 +63,8 @@ int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     VLR_CUDA(ctx, cudaMalloc(&ls->list_new, sizeof(int) * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->owned, sizeof(int) * (cap + 1)));
     VLR_CUDA(ctx, cudaMalloc(&ls->pos, sizeof(int) * (cap + 1 + scan_scratch_ints(cap))));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (cap + 1 + scan_scratch_ints(cap)), ctx->stream));
+    VLR_CUDA(ctx, cudaMalloc(&ls->newinfo, sizeof(int) * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->free_stack, sizeof(int) * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->scalars, sizeof(int) * 8));
     VLR_CUDA(ctx, cudaMalloc(&ls->hkey, sizeof(uint64_t) * ls->hcap));
@@ -75,7 +79,7 @@ int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     // list entries past a failed allocation must still name valid slots
     VLR_CUDA(ctx, cudaMemsetAsync(ls->list_new, 0, sizeof(int) * cap, ctx->stream));
     VLR_CUDA(ctx, cudaMemsetAsync(ls->list, 0, sizeof(int) * cap, ctx->stream));
-    ls->grid_blocks = ctx->sm_count * 8;
+    ls->grid_blocks = ctx->sm_count * 4;  // stencil kernels keep 4 CTAs of 256 threads per SM
     return VLR_OK;
 }
 
@@ -155,36 +159,53 @@ static int grid_params(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_velocit
     return VLR_OK;
 }
 
-static int setup_common(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* v,
-                        const int32_t bb_lo[3], const int32_t bb_hi[3]) {
+// Per-grid parameters and tables for n grids (bounding boxes in index units);
+// all grids of a level set share dt, integrator, reinitialisation and halo.
+int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* const* vels,
+                   const int32_t (*bb_lo)[3], const int32_t (*bb_hi)[3], int n) {
     if (m->integrator < 1 || m->integrator > 3) return set_error(ctx, VLR_ERR_INVALID, "integrator must be 1, 2 or 3");
     if (m->reinit_iters < 0 || m->reinit_iters > 2)
         return set_error(ctx, VLR_ERR_UNSUPPORTED, "reinit_iters must be 0, 1 or 2");
     if (!(m->half_width > 0.0f) || m->half_width > 7.0f)
         return set_error(ctx, VLR_ERR_INVALID, "half_width must be in (0, 7] voxels");
     if (!(m->dt > 0.0)) return set_error(ctx, VLR_ERR_INVALID, "dt must be positive");
-    double disp = speed_bound(v) * m->dt;
+    double disp = 0.0;
+    for (int g = 0; g < n; ++g) disp = std::max(disp, speed_bound(vels[g]) * m->dt);
     if (disp <= 1.0) ls->halo = 2;
     else if (disp <= 2.0) ls->halo = 3;
     else return set_error(ctx, VLR_ERR_REACH, "velocity * dt exceeds 2 voxels per step (CFL); reduce dt");
     ls->reinit_iters = m->reinit_iters;
+    ls->n_grids = n;
     ls->sp.dt = (float)m->dt;
     ls->sp.t0 = (float)m->t0;
     ls->sp.integrator = m->integrator;
-    ls->sp.n_grids = 1;
+    ls->sp.n_grids = n;
     ls->sp.key_bits = ls->key_bits;
-    MGridParams P;
     std::vector<float2> tab;
-    int rc = grid_params(ctx, m, v, bb_lo, bb_hi, ls->key_bits, P, tab);
-    if (rc) return rc;
-    ls->h_params.assign(1, P);
-    VLR_CUDA(ctx, cudaMalloc(&ls->d_params, sizeof(MGridParams)));
-    VLR_CUDA(ctx, cudaMemcpy(ls->d_params, &P, sizeof(MGridParams), cudaMemcpyHostToDevice));
+    ls->h_params.resize(n);
+    for (int g = 0; g < n; ++g) {
+        MGridParams& P = ls->h_params[g];
+        int rc = grid_params(ctx, m, vels[g], bb_lo[g], bb_hi[g], ls->key_bits, P, tab);
+        if (rc) return rc;
+        // rotation angles stay below dphi * disp; the short series is exact to f32 below 0.05 rad
+        double max_angle = 0.0, gdisp = speed_bound(vels[g]) * m->dt;
+        for (int f = 0; f < kMaxOctaves; ++f) max_angle = std::max(max_angle, std::fabs((double)P.dphi[f]) * gdisp);
+        P.full_series = max_angle > 0.05 ? 1 : 0;
+    }
+    VLR_CUDA(ctx, cudaMalloc(&ls->d_params, sizeof(MGridParams) * n));
+    VLR_CUDA(ctx, cudaMemcpy(ls->d_params, ls->h_params.data(), sizeof(MGridParams) * n, cudaMemcpyHostToDevice));
     size_t nt = std::max<size_t>(tab.size(), 1);
     VLR_CUDA(ctx, cudaMalloc(&ls->d_tab, sizeof(float2) * nt));
     if (!tab.empty())
         VLR_CUDA(ctx, cudaMemcpy(ls->d_tab, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice));
     return VLR_OK;
+}
+
+static int setup_common(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* v,
+                        const int32_t bb_lo[3], const int32_t bb_hi[3]) {
+    const vlr_velocity_desc* vs[1] = {v};
+    int32_t lo[1][3] = {{bb_lo[0], bb_lo[1], bb_lo[2]}}, hi[1][3] = {{bb_hi[0], bb_hi[1], bb_hi[2]}};
+    return ls_setup_grids(ctx, ls, m, vs, lo, hi, 1);
 }
 
 __global__ void k_iota(int* a, int n) {
@@ -202,11 +223,11 @@ __global__ void k_init_lists(int* list, int* free_stack, int* scalars, int n, in
         scalars[0] = n;
         if (reset_step) scalars[1] = 0;
         scalars[2] = cap - n;
-        scalars[3] = 0;
+        for (int q = 3; q < 8; ++q) scalars[q] = 0;
     }
 }
 
-static int init_lists(vlr_ctx* ctx, vlr_level_set* ls, int n, bool reset_step = true) {
+int ls_init_lists(vlr_ctx* ctx, vlr_level_set* ls, int n, bool reset_step) {
     k_init_lists<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, ls->free_stack, ls->scalars, n, ls->cap,
                                                            reset_step ? 1 : 0);
     VLR_CUDA(ctx, cudaGetLastError());
@@ -335,7 +356,7 @@ int create_sphere_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m
     cudaFree(v_tmp);
     cudaFree(touched);
     cudaFree(pos);
-    return init_lists(ctx, ls, n);
+    return ls_init_lists(ctx, ls, n, true);
 }
 
 // Replace the state with n host leaves (origins i32[3], masks, phi f32 voxel
@@ -366,7 +387,7 @@ int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const u
         VLR_CUDA(ctx, cudaMemcpyAsync(ls->vals[0], phi, vbytes, cudaMemcpyHostToDevice, ctx->stream));
     }
     VLR_CUDA(ctx, cudaGetLastError());
-    return init_lists(ctx, ls, (int)n, reset_step);
+    return ls_init_lists(ctx, ls, (int)n, reset_step);
 }
 
 int create_leaves_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* vel,
@@ -504,11 +525,18 @@ int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_
 
 int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uint64_t* masks, float* phi,
                     size_t cap_leaves) {
-    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    size_t n_out = 0;
+    return vlr_ls_download_grid(ctx, ls, -1, nullptr, origins, masks, phi, cap_leaves, &n_out);
+}
+
+int vlr_ls_download_grid(vlr_ctx* ctx, const vlr_level_set* ls, int grid, int32_t* grid_ids, int32_t* origins,
+                         uint64_t* masks, float* phi, size_t cap_leaves, size_t* n_out) {
+    if (!ctx || !ls || !n_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *n_out = 0;
     size_t n = 0;
     int rc = vlr_ls_info(ctx, ls, &n, nullptr, nullptr);
     if (rc) return rc;
-    if (n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    if (grid < 0 && n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
     if (!n) return VLR_OK;
     void* stg = nullptr;
     size_t vbytes = sizeof(float) * kLeafVoxels * n;
@@ -540,16 +568,22 @@ int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uin
         if (A.y != B2.y) return A.y < B2.y;
         return A.z < B2.z;
     });
+    size_t k = 0;
     for (size_t i = 0; i < n; ++i) {
         size_t s = order[i];
+        if (grid >= 0 && ho[s].w != grid) continue;
+        if (k >= cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+        if (grid_ids) grid_ids[k] = ho[s].w;
         if (origins) {
-            origins[3 * i] = ho[s].x;
-            origins[3 * i + 1] = ho[s].y;
-            origins[3 * i + 2] = ho[s].z;
+            origins[3 * k] = ho[s].x;
+            origins[3 * k + 1] = ho[s].y;
+            origins[3 * k + 2] = ho[s].z;
         }
-        if (masks) std::memcpy(masks + 8 * i, &hm[8 * s], 64);
-        if (phi) std::memcpy(phi + kLeafVoxels * i, &hv[kLeafVoxels * s], sizeof(float) * kLeafVoxels);
+        if (masks) std::memcpy(masks + 8 * k, &hm[8 * s], 64);
+        if (phi) std::memcpy(phi + kLeafVoxels * k, &hv[kLeafVoxels * s], sizeof(float) * kLeafVoxels);
+        ++k;
     }
+    *n_out = k;
     return VLR_OK;
 }
 

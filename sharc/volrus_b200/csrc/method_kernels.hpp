@@ -17,13 +17,27 @@ struct MLeafArrays {
     int* nonempty;       // 1 if the slot has an active voxel after the step
 };
 
+// Per-step topology state touched by the stencil kernels: advect clears it,
+// reinit records keep flags and new-leaf proposals.
+struct MTopo {
+    int* keep;           // cap: leaf survives this step
+    int cap;
+    uint64_t* pkey;      // proposal table: key -> min owner direction
+    int* pval;
+    uint64_t* hkey;      // leaf hash, rebuilt each step
+    int* hval;
+    int hcap;
+    int* scalars;        // [7] chunk ticket of the look-back scan
+    int key_bits;
+};
+
 template <typename T, int H>
 __global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
-                           unsigned* __restrict__ err);
+                           MTopo topo, unsigned* __restrict__ err);
 template <typename T, int NIT>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                           const MGridParams* __restrict__ params);
+                           const MGridParams* __restrict__ params, MTopo topo, unsigned* __restrict__ err);
 template <typename T>
 __global__ void k_m_volume(MLeafArrays A, const T* __restrict__ vals, const MGridParams* __restrict__ params,
                            double r0, double r1, double r2, double* __restrict__ partial);

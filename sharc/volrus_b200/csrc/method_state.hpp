@@ -27,8 +27,9 @@ struct vlr_level_set {
     // list (position-indexed)
     int* list = nullptr;
     int* list_new = nullptr;
-    int* owned = nullptr;    // cap + 1: survive + owned count per position, then scanned
-    int* pos = nullptr;      // cap + 1
+    int* owned = nullptr;    // cap + 1: slots of leaves dropped this step (recycle list)
+    int* pos = nullptr;      // status words of the look-back scan (zeroed at allocation)
+    int* newinfo = nullptr;  // cap: per new-list position, owner slot * 32 + direction (-1 survivor)
     int* free_stack = nullptr;
     int* scalars = nullptr;  // [0] count, [1] step, [2] free top, [3] new count
     // hash (key -> slot) and proposal table (key -> min owner direction)
@@ -78,5 +79,10 @@ int ls_enqueue_step(vlr_ctx* ctx, vlr_level_set* ls);
 // Rebuild hash and neighbour table from the list (enqueued).
 int ls_enqueue_index(vlr_ctx* ctx, vlr_level_set* ls);
 int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls);
+// Parameters and velocity tables of n grids (bounding boxes in index units).
+int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* const* vels,
+                   const int32_t (*bb_lo)[3], const int32_t (*bb_hi)[3], int n);
+// List = slots 0..n-1, free stack = the rest; rebuilds hash and neighbours (synchronises).
+int ls_init_lists(vlr_ctx* ctx, vlr_level_set* ls, int n, bool reset_step);
 
 }  // namespace vlr

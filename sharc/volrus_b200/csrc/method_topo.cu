@@ -1,16 +1,20 @@
-// Re-tracking of the narrow band after each method step, entirely on the
-// device and without host synchronisation (so the step can be graph-captured):
+// Re-tracking of the narrow band after each method step, on the device and
+// without host synchronisation (the step is one CUDA graph).  The stencil
+// kernels already did two parts: advect cleared the per-step state, reinit
+// set keep flags (a leaf survives if it, or a neighbour within one voxel,
+// has an active voxel: dilate26 of the band) and proposed missing leaves in
+// a hash table where atomicMin keeps the proposer whose direction, seen from
+// the new leaf, comes first.  Three kernels finish the step:
 //
-//   keep      a leaf survives if it has an active voxel or a neighbour's
-//             active voxel lies within one voxel of it (dilate26 of the band)
-//   propose   a missing leaf touched by a neighbour's spill is proposed in a
-//             hash table; atomicMin keeps the proposer that comes first in a
-//             fixed direction order seen from the new leaf, so the owner is
-//             independent of thread timing
-//   relist    survivors keep their list order; each owner's new leaves follow
-//             it (exclusive scan of survive + owned counts); slots come from a
-//             free stack, new values from the owner by the clamped-sign rule
-//   index     hash table and 27-neighbour table rebuilt from the new list
+//   k_t_scanalloc  per list position: survive flag + owned proposals; an
+//                  exclusive scan in list order (single pass, decoupled
+//                  look-back over 256-position chunks taken by ticket) gives
+//                  each survivor its new position, followed by the new leaves
+//                  it owns; new leaves take slots from the free stack, slots
+//                  of dropped leaves go to a recycle list
+//   k_t_finalize   new list, fill of new leaves (clamped-sign rule from the
+//                  owner), hash insertion, recycled slots back on the stack
+//   k_t_nbr        27-neighbour table of every listed leaf; publishes counts
 //
 // The reference's counterparts are dilate (src/tools/morphology.rs:20-35),
 // trim_narrow_band's deactivation (src/tools/level_set_track.rs:53-68) and
@@ -21,20 +25,15 @@
 
 namespace vlr {
 
+// scalars: [0] count  [1] step  [2] free top  [3] spare
+//          [4] new count  [5] recycled count  [6] new free top  [7] chunk ticket
+constexpr int kChunk = 256;
+constexpr long long kSpinLimit = 1ll << 22;
+
 __device__ __forceinline__ void dir_of(int d, int& dx, int& dy, int& dz) {
     dx = d / 9 - 1;
     dy = (d / 3) % 3 - 1;
     dz = d % 3 - 1;
-}
-
-__global__ void k_t_prepare(int* keep, int cap, uint64_t* pkey, int* pval, uint64_t* hkey, int* hval, int hcap) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max(cap, hcap); i += gridDim.x * blockDim.x) {
-        if (i < cap) keep[i] = 0;
-        if (i < hcap) {
-            pkey[i] = kEmptyKey;
-            pval[i] = INT_MAX;
-        }
-    }
 }
 
 __device__ __forceinline__ uint64_t leaf_key(const int4 o, int dx, int dy, int dz, const MGridParams* params,
@@ -43,152 +42,219 @@ __device__ __forceinline__ uint64_t leaf_key(const int4 o, int dx, int dy, int d
     return mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy, (long long)(o.z >> 3) + dz, o.w, P.base, bits);
 }
 
-__global__ void k_t_propose(MLeafArrays A, int* keep, uint64_t* pkey, int* pval, int hcap,
-                            const MGridParams* __restrict__ params, int bits, unsigned* err) {
-    const int count = *A.count;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const int s = A.list[i];
-        if (A.nonempty[s]) keep[s] = 1;
-        unsigned sp = A.spill[s];
-        if (!sp) continue;
-        const int4 o = A.origin[s];
-        while (sp) {
-            int d = __ffs(sp) - 1;
-            sp &= sp - 1;
-            int n = A.nbr[s * kNbr + d];
-            if (n >= 0) {
-                keep[n] = 1;
-                continue;
-            }
-            int dx, dy, dz;
-            dir_of(d, dx, dy, dz);
-            uint64_t key = leaf_key(o, dx, dy, dz, params, bits);
-            if (key == kEmptyKey) {
-                atomicOr(err, kErrExtent);
-                continue;
-            }
-            uint32_t m = (uint32_t)hcap - 1u, p = (uint32_t)mix64(key) & m;
-            bool done = false;
-            for (int probe = 0; probe < hcap; ++probe) {
-                unsigned long long prev = atomicCAS((unsigned long long*)&pkey[p], (unsigned long long)kEmptyKey,
-                                                    (unsigned long long)key);
-                if (prev == kEmptyKey || prev == key) {
-                    atomicMin(&pval[p], kNbr - 1 - d);  // direction of this proposer seen from the new leaf
-                    done = true;
-                    break;
-                }
-                p = (p + 1u) & m;
-            }
-            if (!done) atomicOr(err, kErrHashFull);
-        }
-    }
+// Status word of a scan chunk: [63..34] tag (step + 1), [33..32] flag
+// (1 aggregate, 2 inclusive prefix), [31..0] value.
+__device__ __forceinline__ unsigned long long pack_status(unsigned tag, unsigned flag, unsigned value) {
+    return ((unsigned long long)(tag & 0x3fffffffu) << 34) | ((unsigned long long)flag << 32) | value;
 }
 
-// Is leaf s (origin o) the owner of its missing neighbour in direction d?
-__device__ __forceinline__ bool owns(const int4 o, int d, const uint64_t* pkey, const int* pval, int hcap,
-                                     const MGridParams* params, int bits) {
-    int dx, dy, dz;
-    dir_of(d, dx, dy, dz);
-    uint64_t key = leaf_key(o, dx, dy, dz, params, bits);
-    return hfind(pkey, pval, hcap, key) == kNbr - 1 - d;
-}
-
-__global__ void k_t_count(MLeafArrays A, const int* keep, const uint64_t* pkey, const int* pval, int hcap,
-                          const MGridParams* __restrict__ params, int bits, int cap, int* owned) {
-    const int count = *A.count;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
-        int c = 0;
-        if (i < count) {
-            const int s = A.list[i];
-            c = keep[s] ? 1 : 0;
+__global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* origin, const int* keep,
+                                                       const uint64_t* __restrict__ pkey, const int* __restrict__ pval,
+                                                       int hcap, const MGridParams* __restrict__ params, int bits,
+                                                       int* free_stack, int* recycled, int* list_new,
+                                                       int* newinfo, unsigned long long* status, int* scalars,
+                                                       int cap, unsigned* err) {
+    __shared__ int s_ticket;
+    __shared__ int s_warp[kChunk / 32];
+    __shared__ int s_prefix;
+    const int count = scalars[0];
+    const unsigned tag = (unsigned)scalars[1] + 1u;
+    const int nchunks = (count + kChunk - 1) / kChunk;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = atomicAdd(&scalars[7], 1);
+        __syncthreads();
+        const int chunk = s_ticket;
+        __syncthreads();
+        if (chunk >= nchunks) break;
+        const int p = chunk * kChunk + threadIdx.x;
+        int s = -1, surv = 0, owned = 0;
+        unsigned own_bits = 0;
+        int4 o = make_int4(0, 0, 0, 0);
+        if (p < count) {
+            s = A.list[p];
+            surv = keep[s] ? 1 : 0;
+            if (!surv) recycled[atomicAdd(&scalars[5], 1)] = s;
             unsigned sp = A.spill[s];
-            const int4 o = A.origin[s];
+            o = origin[s];
             while (sp) {
                 int d = __ffs(sp) - 1;
                 sp &= sp - 1;
-                if (A.nbr[s * kNbr + d] < 0 && owns(o, d, pkey, pval, hcap, params, bits)) ++c;
-            }
-        }
-        owned[i] = c;
-    }
-}
-
-__global__ void k_t_free(MLeafArrays A, const int* keep, int* free_stack, int* free_top) {
-    const int count = *A.count;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const int s = A.list[i];
-        if (!keep[s]) free_stack[atomicAdd(free_top, 1)] = s;
-    }
-}
-
-// One block per list position: write survivors and owned new leaves to the
-// new list; initialise new leaves from their owner's values.
-template <typename T>
-__global__ void __launch_bounds__(256) k_t_alloc(MLeafArrays A, int4* origin, const int* keep, const int* pos,
-                                                const uint64_t* pkey, const int* pval, int hcap,
-                                                const MGridParams* __restrict__ params, int bits, int* free_stack,
-                                                int* free_top, int* list_new, T* vals, unsigned* err) {
-    __shared__ int s_slot;
-    const int count = *A.count;
-    for (int i = blockIdx.x; i < count; i += gridDim.x) {
-        const int s = A.list[i];
-        int p = pos[i];
-        if (keep[s]) {
-            if (threadIdx.x == 0) list_new[p] = s;
-            ++p;
-        }
-        unsigned sp = A.spill[s];
-        const int4 o = origin[s];
-        const float hw = params[o.w].hw;
-        while (sp) {
-            int d = __ffs(sp) - 1;
-            sp &= sp - 1;
-            if (A.nbr[s * kNbr + d] >= 0 || !owns(o, d, pkey, pval, hcap, params, bits)) continue;
-            if (threadIdx.x == 0) {
-                int t = atomicSub(free_top, 1) - 1;
-                if (t < 0) {
-                    atomicOr(err, kErrCapacity);
-                    s_slot = -1;
-                } else {
-                    s_slot = free_stack[t];
+                if (A.nbr[s * kNbr + d] >= 0) continue;
+                int dx, dy, dz;
+                dir_of(d, dx, dy, dz);
+                if (hfind(pkey, pval, hcap, leaf_key(o, dx, dy, dz, params, bits)) == kNbr - 1 - d) {
+                    own_bits |= 1u << d;
+                    ++owned;
                 }
             }
-            __syncthreads();
-            const int ns = s_slot;
-            __syncthreads();
-            if (ns < 0) continue;
-            int dx, dy, dz;
-            dir_of(d, dx, dy, dz);
-            if (threadIdx.x == 0) {
-                list_new[p] = ns;
+        }
+        // block-wide inclusive scan of surv + owned
+        int v = surv + owned, x = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) s_warp[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int a = (lane < kChunk / 32) ? s_warp[lane] : 0, ai = a;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, ai, off);
+                if (lane >= off) ai += y;
+            }
+            if (lane < kChunk / 32) s_warp[lane] = ai - a;
+            if (lane == kChunk / 32 - 1) {
+                // publish the aggregate, look back for the chunk's exclusive prefix
+                const unsigned total = (unsigned)ai;
+                unsigned prefix = 0;
+                if (chunk == 0) {
+                    atomicExch(&status[0], pack_status(tag, 2, total));
+                } else {
+                    atomicExch(&status[chunk], pack_status(tag, 1, total));
+                    int q = chunk - 1;
+                    long long spins = 0;
+                    while (q >= 0) {
+                        unsigned long long st = atomicAdd(&status[q], 0ull);
+                        unsigned stag = (unsigned)(st >> 34), flag = (unsigned)(st >> 32) & 3u;
+                        if (stag == (tag & 0x3fffffffu) && flag != 0) {
+                            prefix += (unsigned)st;
+                            if (flag == 2) break;
+                            --q;
+                            continue;
+                        }
+                        if (++spins > kSpinLimit) {  // bounded wait: report and continue
+                            atomicOr(err, kErrTimeout);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                    atomicExch(&status[chunk], pack_status(tag, 2, prefix + total));
+                }
+                s_prefix = (int)prefix;
+                if (chunk == nchunks - 1) scalars[4] = (int)(prefix + total);
+            }
+        }
+        __syncthreads();
+        int pos = s_prefix + s_warp[w] + x - v;
+        if (p < count) {
+            if (surv) {
+                if (pos < cap) {
+                    list_new[pos] = s;
+                    newinfo[pos] = -1;
+                }
+                ++pos;
+            }
+            while (own_bits) {
+                int d = __ffs(own_bits) - 1;
+                own_bits &= own_bits - 1;
+                int t = atomicSub(&scalars[2], 1) - 1;
+                if (t < 0 || pos >= cap) {
+                    atomicOr(err, kErrCapacity);
+                    if (pos < cap) {
+                        newinfo[pos] = -2;  // slot 0 stands in; its values are left alone
+                        list_new[pos] = 0;
+                    }
+                    ++pos;
+                    continue;
+                }
+                int ns = free_stack[t];
+                int dx, dy, dz;
+                dir_of(d, dx, dy, dz);
                 origin[ns] = make_int4(o.x + 8 * dx, o.y + 8 * dy, o.z + 8 * dz, o.w);
+                list_new[pos] = ns;
+                newinfo[pos] = s * 32 + d;  // owner slot and direction
                 A.spill[ns] = 0;
                 A.nonempty[ns] = 0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    A.mask[(size_t)ns * 8 + q] = 0ull;
+                    A.dmask[(size_t)ns * 8 + q] = 0ull;
+                }
+                ++pos;
             }
-            if (threadIdx.x < 8) {
-                A.mask[(size_t)ns * 8 + threadIdx.x] = 0ull;
-                A.dmask[(size_t)ns * 8 + threadIdx.x] = 0ull;
-            }
-            for (int off = threadIdx.x; off < kLeafVoxels; off += blockDim.x) {
-                int x = 8 * dx + (off >> 6), y = 8 * dy + ((off >> 3) & 7), z = 8 * dz + (off & 7);
-                int cx = min(max(x, 0), 7), cy = min(max(y, 0), 7), cz = min(max(z, 0), 7);
-                float v = to_f(vals[(size_t)s * kLeafVoxels + ((cx << 6) | (cy << 3) | cz)]);
-                vals[(size_t)ns * kLeafVoxels + off] = from_f<T>(copysignf(hw, v));
-            }
-            ++p;
         }
     }
 }
 
-__global__ void k_t_finalize(int* scalars, const int* list_new, int* list, int cap) {
-    const int n = scalars[3];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < min(n, cap); i += gridDim.x * blockDim.x)
-        list[i] = list_new[i];
+// One warp per new-list position (grid-stride): copy the list, insert the
+// hash key, fill new leaves from their owner; thread 0 recycles dropped slots.
+template <typename T>
+__global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const int* newinfo, int* list, const int4* origin,
+                                                   T* vals, uint64_t* hkey, int* hval, int hcap,
+                                                   const MGridParams* __restrict__ params, int bits, int* free_stack,
+                                                   const int* recycled, int* scalars, int cap, unsigned* err) {
+    const int n = min(scalars[4], cap);
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int p = warp; p < n; p += nwarps) {
+        const int s = list_new[p];
+        const int info = newinfo[p];
+        if (lane == 0) {
+            list[p] = s;
+            if (info != -2) {
+                uint64_t key = leaf_key(origin[s], 0, 0, 0, params, bits);
+                bool done = false;
+                if (key != kEmptyKey) {
+                    uint32_t m = (uint32_t)hcap - 1u, q = (uint32_t)mix64(key) & m;
+                    for (int probe = 0; probe < hcap; ++probe) {
+                        unsigned long long prev = atomicCAS((unsigned long long*)&hkey[q],
+                                                            (unsigned long long)kEmptyKey, (unsigned long long)key);
+                        if (prev == kEmptyKey) {
+                            hval[q] = s;
+                            done = true;
+                            break;
+                        }
+                        q = (q + 1u) & m;
+                    }
+                }
+                if (!done) atomicOr(err, key == kEmptyKey ? kErrExtent : kErrHashFull);
+            }
+        }
+        if (info >= 0) {
+            const int owner = info >> 5, d = info & 31;
+            int dx, dy, dz;
+            dir_of(d, dx, dy, dz);
+            const float hw = params[origin[owner].w].hw;
+            for (int off = lane; off < kLeafVoxels; off += 32) {
+                int x = 8 * dx + (off >> 6), y = 8 * dy + ((off >> 3) & 7), z = 8 * dz + (off & 7);
+                int cx = min(max(x, 0), 7), cy = min(max(y, 0), 7), cz = min(max(z, 0), 7);
+                float v = to_f(vals[(size_t)owner * kLeafVoxels + ((cx << 6) | (cy << 3) | cz)]);
+                vals[(size_t)s * kLeafVoxels + off] = from_f<T>(copysignf(hw, v));
+            }
+        }
+    }
+    // dropped slots go back on the free stack above the remaining free slots
+    const int top = max(scalars[2], 0);
+    const int nrec = scalars[5];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrec; i += gridDim.x * blockDim.x)
+        if (top + i < cap) free_stack[top + i] = recycled[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) scalars[6] = min(top + nrec, cap);
+}
+
+__global__ void k_t_nbr(const int* list, int* scalars, const int4* origin, const uint64_t* hkey, const int* hval,
+                        int hcap, const MGridParams* __restrict__ params, int bits, int* nbr, int cap) {
+    const int count = min(scalars[4], cap);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)count * kNbr;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / kNbr), d = (int)(t % kNbr);
+        const int s = list[i];
+        int dx, dy, dz;
+        dir_of(d, dx, dy, dz);
+        nbr[s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        scalars[0] = min(n, cap);
+        scalars[0] = count;
         scalars[1] += 1;
+        scalars[2] = scalars[6];
+        scalars[5] = 0;
     }
 }
+
+// ---------------------------------------------- full index (creation/upload)
 
 __global__ void k_h_clear(uint64_t* hkey, int* hval, int hcap) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < hcap; i += gridDim.x * blockDim.x) {
@@ -236,67 +302,23 @@ __global__ void k_nbr(const int* list, const int* count_ptr, const int4* origin,
     }
 }
 
-// ------------------------------------------------------- scan (prealloc)
-
-__global__ void __launch_bounds__(1024) k_scan_blk(const int* in, int* out, int n, int* block_sums) {
-    __shared__ int ws[32];
-    int i = blockIdx.x * 1024 + threadIdx.x;
-    int v = (i < n) ? in[i] : 0;
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) ws[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int s = ws[lane], si = s;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, si, o);
-            if (lane >= o) si += y;
-        }
-        ws[lane] = si - s;
-        if (lane == 31) block_sums[blockIdx.x] = si;
-    }
-    __syncthreads();
-    if (i < n) out[i] = x - v + ws[w];
-}
-
-__global__ void k_scan_addb(int* out, int n, const int* offs) {
-    int i = blockIdx.x * 1024 + threadIdx.x;
-    if (i < n) out[i] += offs[blockIdx.x];
-}
-
-__global__ void k_scan_tot(const int* in, const int* out, int n, int* total) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *total = out[n - 1] + in[n - 1];
-}
-
-// Exclusive scan of n ints with scratch laid out level by level.
-static void scan_levels(cudaStream_t st, const int* in, int* out, int n, int* total, int* scratch) {
-    int nb = (n + 1023) / 1024;
-    int* sums = scratch;
-    int* sums_scan = scratch + nb;
-    k_scan_blk<<<nb, 1024, 0, st>>>(in, out, n, sums);
-    if (nb > 1) {
-        scan_levels(st, sums, sums_scan, nb, sums_scan + nb, sums_scan + nb + 1);
-        k_scan_addb<<<nb, 1024, 0, st>>>(out, n, sums_scan);
-    }
-    k_scan_tot<<<1, 32, 0, st>>>(in, out, n, total);
-}
-
-size_t scan_scratch_ints(int n) {
-    size_t s = 0;
-    while (true) {
-        int nb = (n + 1023) / 1024;
-        s += 2 * (size_t)nb + 2;
-        if (nb <= 1) break;
-        n = nb;
-    }
-    return s + 16;
-}
+size_t scan_scratch_ints(int n) { return (size_t)((n + kChunk - 1) / kChunk) * 2 + 16; }
 
 // ----------------------------------------------------------- orchestration
+
+MTopo topo_of(vlr_level_set* ls) {
+    MTopo t;
+    t.keep = ls->keep;
+    t.cap = ls->cap;
+    t.pkey = ls->pkey;
+    t.pval = ls->pval;
+    t.hkey = ls->hkey;
+    t.hval = ls->hval;
+    t.hcap = ls->hcap;
+    t.scalars = ls->scalars;
+    t.key_bits = ls->key_bits;
+    return t;
+}
 
 int ls_enqueue_index(vlr_ctx* ctx, vlr_level_set* ls) {
     cudaStream_t st = ctx->stream;
@@ -314,25 +336,29 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
     cudaStream_t st = ctx->stream;
     const int B = ls->grid_blocks;
     MLeafArrays A = ls->arrays();
-    k_t_prepare<<<B, 256, 0, st>>>(ls->keep, ls->cap, ls->pkey, ls->pval, ls->hkey, ls->hval, ls->hcap);
-    VLR_TIMED(ctx, "k_t_propose",
-              k_t_propose<<<B, 256, 0, st>>>(A, ls->keep, ls->pkey, ls->pval, ls->hcap, ls->d_params, ls->key_bits,
-                                             ctx->d_errword));
-    k_t_count<<<B, 256, 0, st>>>(A, ls->keep, ls->pkey, ls->pval, ls->hcap, ls->d_params, ls->key_bits, ls->cap,
-                                 ls->owned);
-    scan_levels(st, ls->owned, ls->pos, ls->cap, ls->scalars + 3, ls->pos + ls->cap + 1);
-    k_t_free<<<B, 256, 0, st>>>(A, ls->keep, ls->free_stack, ls->scalars + 2);
+    // status words of the look-back scan live after the scan positions in `pos`
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(ls->pos);
+    VLR_TIMED(ctx, "k_t_scanalloc",
+              k_t_scanalloc<<<B, kChunk, 0, st>>>(A, ls->origin, ls->keep, ls->pkey, ls->pval, ls->hcap, ls->d_params,
+                                                  ls->key_bits, ls->free_stack, ls->owned, ls->list_new,
+                                                  ls->newinfo, status, ls->scalars, ls->cap, ctx->d_errword));
     if (ls->precision == VLR_PREC_F16)
-        k_t_alloc<__half><<<B, 256, 0, st>>>(A, ls->origin, ls->keep, ls->pos, ls->pkey, ls->pval, ls->hcap,
-                                            ls->d_params, ls->key_bits, ls->free_stack, ls->scalars + 2,
-                                            ls->list_new, (__half*)ls->vals[0], ctx->d_errword);
+        VLR_TIMED(ctx, "k_t_finalize",
+                  k_t_finalize<__half><<<B, 256, 0, st>>>(ls->list_new, ls->newinfo, ls->list, ls->origin,
+                                                         (__half*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
+                                                         ls->d_params, ls->key_bits, ls->free_stack, ls->owned,
+                                                         ls->scalars, ls->cap, ctx->d_errword));
     else
-        k_t_alloc<float><<<B, 256, 0, st>>>(A, ls->origin, ls->keep, ls->pos, ls->pkey, ls->pval, ls->hcap,
-                                           ls->d_params, ls->key_bits, ls->free_stack, ls->scalars + 2,
-                                           ls->list_new, (float*)ls->vals[0], ctx->d_errword);
-    k_t_finalize<<<B, 256, 0, st>>>(ls->scalars, ls->list_new, ls->list, ls->cap);
+        VLR_TIMED(ctx, "k_t_finalize",
+                  k_t_finalize<float><<<B, 256, 0, st>>>(ls->list_new, ls->newinfo, ls->list, ls->origin,
+                                                        (float*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
+                                                        ls->d_params, ls->key_bits, ls->free_stack, ls->owned,
+                                                        ls->scalars, ls->cap, ctx->d_errword));
+    VLR_TIMED(ctx, "k_t_nbr",
+              k_t_nbr<<<B, 256, 0, st>>>(ls->list, ls->scalars, ls->origin, ls->hkey, ls->hval, ls->hcap,
+                                         ls->d_params, ls->key_bits, ls->nbr, ls->cap));
     VLR_CUDA(ctx, cudaGetLastError());
-    return ls_enqueue_index(ctx, ls);
+    return VLR_OK;
 }
 
 template <typename T>
@@ -340,24 +366,30 @@ static int enqueue_stencils(vlr_ctx* ctx, vlr_level_set* ls) {
     cudaStream_t st = ctx->stream;
     const int B = ls->grid_blocks;
     MLeafArrays A = ls->arrays();
+    MTopo topo = topo_of(ls);
     const T* v0 = (const T*)ls->vals[0];
     T* v1 = (T*)ls->vals[1];
     if (ls->halo == 2)
         VLR_TIMED(ctx, "k_m_advect",
-                  k_m_advect<T, 2><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, ctx->d_errword));
+                  k_m_advect<T, 2><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, topo,
+                                                      ctx->d_errword));
     else
         VLR_TIMED(ctx, "k_m_advect",
-                  k_m_advect<T, 3><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, ctx->d_errword));
+                  k_m_advect<T, 3><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, topo,
+                                                      ctx->d_errword));
     T* w0 = (T*)ls->vals[0];
     switch (ls->reinit_iters) {
         case 0:
-            VLR_TIMED(ctx, "k_m_reinit", k_m_reinit<T, 0><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params));
+            VLR_TIMED(ctx, "k_m_reinit",
+                      k_m_reinit<T, 0><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
             break;
         case 1:
-            VLR_TIMED(ctx, "k_m_reinit", k_m_reinit<T, 1><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params));
+            VLR_TIMED(ctx, "k_m_reinit",
+                      k_m_reinit<T, 1><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
             break;
         default:
-            VLR_TIMED(ctx, "k_m_reinit", k_m_reinit<T, 2><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params));
+            VLR_TIMED(ctx, "k_m_reinit",
+                      k_m_reinit<T, 2><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
             break;
     }
     VLR_CUDA(ctx, cudaGetLastError());

@@ -81,6 +81,26 @@ def curl_noise(seed: int, extent: float, amplitude: float = 1.0, octaves: int = 
     return {"kind": "curl", "octaves": octs}
 
 
+def random_sphere_grids(n_grids: int, seed: int, extent_log2=(6.0, 10.0), spheres=(1, 64), radius=(4.0, 24.0),
+                        amplitude: float = 1.0, octaves: int = 3):
+    """Seeded batch of uneven grids: each grid has a cubic extent 2^U(extent_log2)
+    voxels (log-uniform), 1-64 spheres with radii U(radius) and centres uniform in
+    the extent, and its own curl-noise velocity (amplitude voxels per unit time).
+    Returns [(spheres (n, 4), velocity dict, extent)]."""
+    out = []
+    for g in range(n_grids):
+        rng = np.random.default_rng([seed, g])
+        extent = float(2.0 ** rng.uniform(*extent_log2))
+        ns = int(rng.integers(spheres[0], spheres[1] + 1))
+        r = rng.uniform(radius[0], radius[1], ns)
+        c = rng.uniform(0.0, extent, (ns, 3))
+        vel = curl_noise(int(rng.integers(1 << 30)), extent, amplitude, octaves)
+        m = 256  # sampling margin: bands may drift ~amplitude voxels per step
+        vel["domain"] = ((-m, -m, -m), (int(extent) + m, int(extent) + m, int(extent) + m))
+        out.append((np.column_stack([c, r]), vel, extent))
+    return out
+
+
 class LevelSet:
     """A narrow-band level set (method grid) resident on the GPU."""
 
@@ -118,6 +138,46 @@ class LevelSet:
                                                ptr(c, C.c_double), C.c_double(voxel_size), ptr(w, C.c_double),
                                                C.byref(h)), "vlr_ls_create_sphere")
         return cls(ctx, h, half_width, precision, dt, voxel_size)
+
+    @classmethod
+    def spheres(cls, grids, dt: float, half_width: float = 3.0, precision: int = F16, integrator: int = 3,
+                reinit_iters: int = 2, t0: float = 0.0, capacity: int = 0, ctx: Context | None = None) -> "LevelSet":
+        """One or many grids, each a union of spheres with its own velocity.
+
+        ``grids``: list of (spheres, velocity) with spheres an (n, 4) array of
+        (cx, cy, cz, r) in voxels (voxel size 1, world = index)."""
+        ctx = ctx or Context.default()
+        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity)
+        n = len(grids)
+        arr = (_lib.vlr_batch_grid * n)()
+        keep = []
+        for g, (sph, vel) in enumerate(grids):
+            s = np.ascontiguousarray(sph, np.float64).reshape(-1, 4)
+            cs = (_lib.vlr_sphere * len(s))()
+            for i, row in enumerate(s):
+                cs[i].center[0], cs[i].center[1], cs[i].center[2] = row[0], row[1], row[2]
+                cs[i].radius = row[3]
+            keep.append(cs)
+            arr[g].spheres = cs
+            arr[g].n_spheres = len(s)
+            arr[g].velocity = velocity_desc(vel)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.vlr_ls_create_spheres(ctx.handle, C.byref(m), arr, n, C.byref(h)), "vlr_ls_create_spheres")
+        ls = cls(ctx, h, half_width, precision, dt)
+        ls.n_grids = n
+        return ls
+
+    def grid_arrays(self, grid: int):
+        """(origins, masks, phi) of one grid of a batch, sorted (x, y, z)."""
+        n = self.info()[0]
+        o = np.zeros((n, 3), np.int32)
+        m = np.zeros((n, 8), np.uint64)
+        v = np.zeros((n, 512), np.float32)
+        k = C.c_size_t()
+        self.ctx.check(self.ctx.lib.vlr_ls_download_grid(self.ctx.handle, self.handle, grid, None, ptr(o, C.c_int32),
+                                                         ptr(m, C.c_uint64), ptr(v, C.c_float), n, C.byref(k)),
+                       "vlr_ls_download_grid")
+        return o[: k.value], m[: k.value], v[: k.value]
 
     @classmethod
     def from_leaves(cls, origins, masks, phi, velocity: dict, dt: float, half_width: float = 3.0,

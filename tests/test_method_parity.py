@@ -77,6 +77,28 @@ def test_curl_noise_rk3(oracle, precision, tol):
         assert s["max_err"] < tol, s
 
 
+@pytest.mark.parametrize("precision,tol", [(0, TOL_F32), (1, TOL_F16)])
+def test_batched_uneven_grids_rk3(oracle, precision, tol):
+    """Several grids of unions of spheres with their own curl noise in one pool:
+    every grid matches its own FP64 oracle run."""
+    from sharc.volrus_b200.method import LevelSet, random_sphere_grids
+    grids = random_sphere_grids(5, seed=11, extent_log2=(5.0, 6.5), spheres=(1, 6), radius=(3.0, 9.0))
+    ls = LevelSet.spheres([(s, v) for s, v, _ in grids], 1.0, precision=precision, integrator=3)
+    og = [oracle.MOGrid.spheres(s, 3.0) for s, _, _ in grids]
+    for g, (_, v, _) in enumerate(grids):
+        st = compare(ls.grid_arrays(g), og[g].arrays(), 3.0)
+        assert st["only_gpu"] == 0 and st["only_oracle"] == 0 and st["mask_flips"] == 0, (g, st)
+    for step in range(6):
+        ls.step(1)
+        for g, (_, v, _) in enumerate(grids):
+            assert og[g].step(v, 3, 2, float(step), 1.0, 8)
+    for g in range(len(grids)):
+        st = compare(ls.grid_arrays(g), og[g].arrays(), 3.0)
+        assert st["only_gpu"] == 0 and st["only_oracle"] == 0, (g, st)
+        assert st["unexplained_flips"] == 0, (g, st)
+        assert st["max_err"] < tol, (g, st)
+
+
 def test_volume_fp64(oracle):
     from sharc.volrus_b200.method import F32, LevelSet
     vel = {"kind": "constant", "c": (0.3, 0.2, 0.1)}
