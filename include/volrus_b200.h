@@ -223,6 +223,32 @@ int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uin
 int vlr_ls_volume(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* volume);
 void vlr_ls_destroy(vlr_level_set* ls);
 
+/* ---- differentiable advection (no counterpart in the reference) ---------
+ *
+ * Frozen-band semi-Lagrangian advection phi_{k+1}(x) = trilinear(phi_k)(x -
+ * dt cos(pi t_{k+1} / T) u(x)) over the active voxels of the given leaves
+ * (values in voxel units, inactive values +-half_width), with u the trilinear
+ * upsample of a staggered field V: 3 components of n^3 cells of `stag_cell`
+ * voxels, component a on the faces normal to axis a, index ((i*n)+j)*n+k.
+ * forward/backward follow the autograd-Function contract: forward(phi_0, V)
+ * -> phi_K, backward(dL/dphi_K) -> (dL/dphi_0, dL/dV).  The backward pass
+ * recomputes states from checkpoints taken every `checkpoint_every` steps and
+ * scatters trilinear weights by stable radix sort + segmented sum (no float
+ * atomics; deterministic).  Band arrays follow vlr_adj_band's order. */
+typedef struct vlr_adjoint vlr_adjoint;
+
+int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
+                   float half_width, const float* vel, int n_stag, double stag_cell, double dt, double period,
+                   double t0, int steps, int checkpoint_every, vlr_adjoint** out);
+/* Band voxel coordinates (int32[n][3]); coords may be null to query n. */
+int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap, size_t* n);
+/* Replace phi_0 on the band and/or the staggered field (either may be null). */
+int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, const float* vel);
+int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band);
+int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
+                     float* grad_vel);
+void vlr_adj_destroy(vlr_adjoint* a);
+
 #ifdef __cplusplus
 }
 #endif

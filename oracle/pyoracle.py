@@ -48,6 +48,12 @@ SIGS = {
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
     "vm_free": (None, [P]),
     "vm_spheres": (P, [dbl_p, C.c_int, C.c_double]),
+    "va_create": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double, dbl_p, C.c_int, C.c_double, C.c_double,
+                      C.c_double, C.c_double, C.c_int]),
+    "va_free": (None, [P]),
+    "va_nband": (C.c_int, [P]),
+    "va_forward": (None, [P, dbl_p, dbl_p, dbl_p]),
+    "va_backward": (None, [P, dbl_p, dbl_p, dbl_p]),
     "vm_leaf_count": (C.c_size_t, [P]),
     "vm_export": (None, [P, i32_p, u64_p, dbl_p]),
     "vm_import": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double]),

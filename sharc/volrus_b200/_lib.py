@@ -111,6 +111,13 @@ SIGNATURES = {
                                             flt_p, C.c_size_t, PP]),
     "vlr_ls_create_spheres": (C.c_int, [P, C.POINTER(vlr_method_desc), C.POINTER(vlr_batch_grid), C.c_int, PP]),
     "vlr_ls_download_grid": (C.c_int, [P, P, C.c_int, i32_p, i32_p, u64_p, flt_p, C.c_size_t, size_p]),
+    "vlr_adj_create": (C.c_int, [P, i32_p, u64_p, flt_p, C.c_size_t, C.c_float, flt_p, C.c_int, C.c_double,
+                                 C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, PP]),
+    "vlr_adj_band": (C.c_int, [P, P, i32_p, C.c_size_t, size_p]),
+    "vlr_adj_set_inputs": (C.c_int, [P, P, flt_p, flt_p]),
+    "vlr_adj_forward": (C.c_int, [P, P, flt_p]),
+    "vlr_adj_backward": (C.c_int, [P, P, flt_p, flt_p, flt_p]),
+    "vlr_adj_destroy": (None, [P]),
     "vlr_ls_step": (C.c_int, [P, P, C.c_int]),
     "vlr_ls_enqueue": (C.c_int, [P, P, C.c_int]),
     "vlr_ctx_check": (C.c_int, [P]),

@@ -1,0 +1,547 @@
+// Differentiable advection: frozen-band semi-Lagrangian steps through a dense
+// staggered velocity field, with a hand-written adjoint.
+//
+// Forward, K steps (t_k = t0 + k dt, c_k = cos(pi t_{k+1} / T)):
+//   phi_{k+1}(x) = trilinear(phi_k)(x - dt c_k u(x))        for band voxels x
+// where u(x) is the trilinear upsample of a staggered (MAC) field V of n^3
+// cells of H voxels (component a lives on the faces normal to axis a) and
+// every non-band voxel keeps its initial value (+-hw; unallocated leaves read
+// the clamped-sign rule).  The map phi_0 -> phi_K is affine on the band, so
+// the gradient is exact (up to rounding) wherever floor() does not jump.
+//
+// Backward, given lambda_K = dL/dphi_K on the band:
+//   lambda_k(c) = sum_x lambda_{k+1}(x) w_c(p_k(x))     (transpose of the blend)
+//   G(x)      += lambda_{k+1}(x) (-dt c_k) grad trilinear(phi_k)(p_k(x))
+//   dL/dphi_0 = lambda_0,  dL/dV = upsample^T G
+// Both scatters (lambda and upsample^T) go through a stable radix sort and a
+// segmented sum: no float atomics, deterministic results.  phi_k for the
+// backward pass is recomputed from checkpoints taken every C steps (sqrt(K)).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "method_state.hpp"
+#include "sort_reduce.hpp"
+
+struct vlr_adjoint {
+    vlr_ctx* ctx = nullptr;
+    int n_leaves = 0;
+    int n_band = 0;
+    float hw = 3.0f;
+    int4* origin = nullptr;
+    int* nbr = nullptr;
+    uint64_t* hkey = nullptr;
+    int* hval = nullptr;
+    int hcap = 0;
+    long long base[3] = {0, 0, 0};
+    float* phi[2] = {nullptr, nullptr};  // leaf-major, 512 per leaf; phi[0] holds phi_0 layout template
+    float* phi_init = nullptr;           // initial full leaves (non-band values are constants)
+    int* bidx = nullptr;                 // slot*512 + off -> band index or -1
+    int* bvox = nullptr;                 // band index -> slot*512 + off
+    float3* ub = nullptr;                // upsampled velocity at band voxels
+    float* vel = nullptr;                // staggered field 3 x n^3
+    int n_stag = 0;
+    double H = 1.0;                      // staggered cell size in voxels
+    double dt = 0.0, t0 = 0.0, period = 1.0;
+    int steps = 0, chk_every = 1;
+    float* checkpoints = nullptr;        // (steps / chk_every + 1) x n_band
+    float* segment = nullptr;            // chk_every x n_band (recomputed states)
+    float* lam[2] = {nullptr, nullptr};
+    float* gvel = nullptr;               // dL/dV, 3 x n^3
+    float3* G = nullptr;
+    unsigned* keys = nullptr;
+    float* pvals = nullptr;
+    void* scratch = nullptr;
+    size_t n_pairs_cap = 0;
+};
+
+namespace vlr {
+
+__device__ __forceinline__ int nbx(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
+
+// phi at local coordinate (x, y, z) of leaf `slot` (may leave the leaf by one voxel).
+__device__ __forceinline__ float adj_read(const float* __restrict__ phi, const int* __restrict__ nbr, int slot, int x,
+                                          int y, int z, float hw) {
+    int s = nbr[slot * kNbr + nbx(x) * 9 + nbx(y) * 3 + nbx(z)];
+    if (s >= 0) return phi[(size_t)s * kLeafVoxels + voxel_off(x, y, z)];
+    int cx = min(max(x, 0), 7), cy = min(max(y, 0), 7), cz = min(max(z, 0), 7);
+    return copysignf(hw, phi[(size_t)slot * kLeafVoxels + ((cx << 6) | (cy << 3) | cz)]);
+}
+
+// Trilinear upsample of component a of the staggered field at voxel point p.
+__device__ __forceinline__ float stag_sample(const float* __restrict__ V, int n, float H, int a, float px, float py,
+                                             float pz) {
+    float g[3] = {px / H, py / H, pz / H};
+    for (int q = 0; q < 3; ++q)
+        if (q != a) g[q] -= 0.5f;
+    int i0[3];
+    float w[3];
+    for (int q = 0; q < 3; ++q) {
+        float f = floorf(g[q]);
+        i0[q] = (int)f;
+        w[q] = g[q] - f;
+    }
+    auto at = [&](int i, int j, int k) {
+        i = min(max(i, 0), n - 1);
+        j = min(max(j, 0), n - 1);
+        k = min(max(k, 0), n - 1);
+        return V[(size_t)a * n * n * n + ((size_t)i * n + j) * n + k];
+    };
+    float c00 = at(i0[0], i0[1], i0[2]) * (1 - w[0]) + at(i0[0] + 1, i0[1], i0[2]) * w[0];
+    float c01 = at(i0[0], i0[1], i0[2] + 1) * (1 - w[0]) + at(i0[0] + 1, i0[1], i0[2] + 1) * w[0];
+    float c10 = at(i0[0], i0[1] + 1, i0[2]) * (1 - w[0]) + at(i0[0] + 1, i0[1] + 1, i0[2]) * w[0];
+    float c11 = at(i0[0], i0[1] + 1, i0[2] + 1) * (1 - w[0]) + at(i0[0] + 1, i0[1] + 1, i0[2] + 1) * w[0];
+    float c0 = c00 * (1 - w[1]) + c10 * w[1], c1 = c01 * (1 - w[1]) + c11 * w[1];
+    return c0 * (1 - w[2]) + c1 * w[2];
+}
+
+__global__ void k_adj_upsample(const int* __restrict__ bvox, const int4* __restrict__ origin, int nb,
+                               const float* __restrict__ V, int n, float H, float3* __restrict__ ub) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        int sv = bvox[b], s = sv >> 9, off = sv & 511;
+        int4 o = origin[s];
+        float px = (float)(o.x + (off >> 6)), py = (float)(o.y + ((off >> 3) & 7)), pz = (float)(o.z + (off & 7));
+        ub[b] = make_float3(stag_sample(V, n, H, 0, px, py, pz), stag_sample(V, n, H, 1, px, py, pz),
+                            stag_sample(V, n, H, 2, px, py, pz));
+    }
+}
+
+// Foot offset, floor and weights of band voxel b at step k.
+struct Foot {
+    int fx, fy, fz;     // floor of the foot, relative to the voxel
+    float wx, wy, wz;   // fractions
+};
+__device__ __forceinline__ Foot foot_of(float3 u, float s) {
+    float ox = s * u.x, oy = s * u.y, oz = s * u.z;  // s = -dt c_k
+    Foot f;
+    float bx = floorf(ox), by = floorf(oy), bz = floorf(oz);
+    f.fx = (int)bx;
+    f.fy = (int)by;
+    f.fz = (int)bz;
+    f.wx = ox - bx;
+    f.wy = oy - by;
+    f.wz = oz - bz;
+    return f;
+}
+
+// One forward step over all band voxels (non-band voxels are copied).
+__global__ void k_adj_forward(const int4* __restrict__ origin, const int* __restrict__ nbr,
+                              const int* __restrict__ bidx, const float3* __restrict__ ub,
+                              const float* __restrict__ src, float* __restrict__ dst, int n_leaves, float s, float hw,
+                              unsigned* err) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_leaves * kLeafVoxels; t += gridDim.x * blockDim.x) {
+        const int slot = t >> 9, off = t & 511;
+        const int b = bidx[t];
+        if (b < 0) {
+            dst[t] = src[t];
+            continue;
+        }
+        Foot f = foot_of(ub[b], s);
+        int x = (off >> 6) + f.fx, y = ((off >> 3) & 7) + f.fy, z = (off & 7) + f.fz;
+        if (x < -8 || y < -8 || z < -8 || x > 14 || y > 14 || z > 14) {
+            atomicOr(err, kErrReach);
+            dst[t] = src[t];
+            continue;
+        }
+        float c000 = adj_read(src, nbr, slot, x, y, z, hw), c100 = adj_read(src, nbr, slot, x + 1, y, z, hw);
+        float c010 = adj_read(src, nbr, slot, x, y + 1, z, hw), c110 = adj_read(src, nbr, slot, x + 1, y + 1, z, hw);
+        float c001 = adj_read(src, nbr, slot, x, y, z + 1, hw), c101 = adj_read(src, nbr, slot, x + 1, y, z + 1, hw);
+        float c011 = adj_read(src, nbr, slot, x, y + 1, z + 1, hw),
+              c111 = adj_read(src, nbr, slot, x + 1, y + 1, z + 1, hw);
+        float c00 = c000 * (1 - f.wx) + c100 * f.wx, c01 = c001 * (1 - f.wx) + c101 * f.wx;
+        float c10 = c010 * (1 - f.wx) + c110 * f.wx, c11 = c011 * (1 - f.wx) + c111 * f.wx;
+        float c0 = c00 * (1 - f.wy) + c10 * f.wy, c1 = c01 * (1 - f.wy) + c11 * f.wy;
+        dst[t] = c0 * (1 - f.wz) + c1 * f.wz;
+    }
+}
+
+__global__ void k_adj_gather_band(const int* __restrict__ bvox, int nb, const float* __restrict__ phi,
+                                  float* __restrict__ out) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) out[b] = phi[bvox[b]];
+}
+
+__global__ void k_adj_scatter_band(const int* __restrict__ bvox, int nb, const float* __restrict__ in,
+                                   float* __restrict__ phi) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) phi[bvox[b]] = in[b];
+}
+
+// Band index of the voxel at local (x, y, z) of leaf slot, or n_band (dropped key).
+__device__ __forceinline__ unsigned band_key(const int* __restrict__ nbr, const int* __restrict__ bidx, int slot, int x,
+                                             int y, int z, unsigned nb) {
+    int s = nbr[slot * kNbr + nbx(x) * 9 + nbx(y) * 3 + nbx(z)];
+    if (s < 0) return nb;
+    int b = bidx[(size_t)s * kLeafVoxels + voxel_off(x, y, z)];
+    return b < 0 ? nb : (unsigned)b;
+}
+
+// Adjoint of step k: emit 8 (corner band index, lambda * weight) pairs per band
+// voxel (in band order, corners in a fixed order) and accumulate the velocity
+// sensitivity G(x) += lambda (-dt c_k) grad trilinear(phi_k)(p).
+__global__ void k_adj_emit(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
+                           const int* __restrict__ bidx, const float3* __restrict__ ub,
+                           const float* __restrict__ phi_k, const float* __restrict__ lam, float s, float hw,
+                           unsigned* __restrict__ keys, float* __restrict__ vals, float3* __restrict__ G) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
+        const float l = lam[b];
+        Foot f = foot_of(ub[b], s);
+        const int x = (off >> 6) + f.fx, y = ((off >> 3) & 7) + f.fy, z = (off & 7) + f.fz;
+        const float wx[2] = {1 - f.wx, f.wx}, wy[2] = {1 - f.wy, f.wy}, wz[2] = {1 - f.wz, f.wz};
+        float c[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
+            keys[(size_t)b * 8 + q] = band_key(nbr, bidx, slot, x + i, y + j, z + k, (unsigned)nb);
+            vals[(size_t)b * 8 + q] = l * wx[i] * wy[j] * wz[k];
+            c[q] = adj_read(phi_k, nbr, slot, x + i, y + j, z + k, hw);
+        }
+        // c[q] with q = i*4 + j*2 + k
+        float gx = wy[0] * wz[0] * (c[4] - c[0]) + wy[1] * wz[0] * (c[6] - c[2]) + wy[0] * wz[1] * (c[5] - c[1]) +
+                   wy[1] * wz[1] * (c[7] - c[3]);
+        float gy = wx[0] * wz[0] * (c[2] - c[0]) + wx[1] * wz[0] * (c[6] - c[4]) + wx[0] * wz[1] * (c[3] - c[1]) +
+                   wx[1] * wz[1] * (c[7] - c[5]);
+        float gz = wx[0] * wy[0] * (c[1] - c[0]) + wx[1] * wy[0] * (c[5] - c[4]) + wx[0] * wy[1] * (c[3] - c[2]) +
+                   wx[1] * wy[1] * (c[7] - c[6]);
+        float3 g = G[b];
+        g.x += l * s * gx;
+        g.y += l * s * gy;
+        g.z += l * s * gz;
+        G[b] = g;
+    }
+}
+
+// Transpose of the upsample: 3 x 8 (node, G_a * weight) pairs per band voxel.
+__global__ void k_adj_emit_vel(const int* __restrict__ bvox, const int4* __restrict__ origin, int nb,
+                               const float3* __restrict__ G, int n, float H, unsigned* __restrict__ keys,
+                               float* __restrict__ vals) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int sv = bvox[b], s = sv >> 9, off = sv & 511;
+        const int4 o = origin[s];
+        const float p[3] = {(float)(o.x + (off >> 6)), (float)(o.y + ((off >> 3) & 7)), (float)(o.z + (off & 7))};
+        const float3 gg = G[b];
+        const float ga[3] = {gg.x, gg.y, gg.z};
+        for (int a = 0; a < 3; ++a) {
+            float g[3] = {p[0] / H, p[1] / H, p[2] / H};
+            for (int q = 0; q < 3; ++q)
+                if (q != a) g[q] -= 0.5f;
+            int i0[3];
+            float w[3];
+            for (int q = 0; q < 3; ++q) {
+                float fl = floorf(g[q]);
+                i0[q] = (int)fl;
+                w[q] = g[q] - fl;
+            }
+            for (int q = 0; q < 8; ++q) {
+                int di = q >> 2, dj = (q >> 1) & 1, dk = q & 1;
+                int i = min(max(i0[0] + di, 0), n - 1), j = min(max(i0[1] + dj, 0), n - 1),
+                    k = min(max(i0[2] + dk, 0), n - 1);
+                float wt = (di ? w[0] : 1 - w[0]) * (dj ? w[1] : 1 - w[1]) * (dk ? w[2] : 1 - w[2]);
+                size_t e = ((size_t)b * 3 + a) * 8 + q;
+                keys[e] = (unsigned)((size_t)a * n * n * n + ((size_t)i * n + j) * n + k);
+                vals[e] = ga[a] * wt;
+            }
+        }
+    }
+}
+
+__global__ void k_zero3(float3* a, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        a[i] = make_float3(0.f, 0.f, 0.f);
+}
+
+__global__ void k_adj_hash_insert(const int4* origin, int n, uint64_t* hkey, int* hval, int hcap, long long b0,
+                                  long long b1, long long b2, unsigned* err);
+__global__ void k_adj_nbr(const int4* origin, int n, const uint64_t* hkey, const int* hval, int hcap, long long b0,
+                          long long b1, long long b2, int* nbr);
+
+__global__ void k_adj_hash_insert(const int4* origin, int n, uint64_t* hkey, int* hval, int hcap, long long b0,
+                                  long long b1, long long b2, unsigned* err) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long base[3] = {b0, b1, b2};
+    int4 o = origin[i];
+    uint64_t key = pack_key(o.x >> 3, o.y >> 3, o.z >> 3, base);
+    uint32_t m = (uint32_t)hcap - 1u, p = (uint32_t)mix64(key) & m;
+    for (int probe = 0; probe < hcap; ++probe) {
+        unsigned long long prev =
+            atomicCAS((unsigned long long*)&hkey[p], (unsigned long long)kEmptyKey, (unsigned long long)key);
+        if (prev == kEmptyKey) {
+            hval[p] = i;
+            return;
+        }
+        p = (p + 1u) & m;
+    }
+    atomicOr(err, kErrHashFull);
+}
+
+__global__ void k_adj_nbr(const int4* origin, int n, const uint64_t* hkey, const int* hval, int hcap, long long b0,
+                          long long b1, long long b2, int* nbr) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * kNbr) return;
+    int i = t / kNbr, d = t % kNbr;
+    HashView h{hkey, hval, hcap, {b0, b1, b2}};
+    int4 o = origin[i];
+    nbr[t] = hash_find_leaf(h, (long long)(o.x >> 3) + d / 9 - 1, (long long)(o.y >> 3) + (d / 3) % 3 - 1,
+                            (long long)(o.z >> 3) + d % 3 - 1);
+}
+
+}  // namespace vlr
+
+using namespace vlr;
+
+namespace {
+
+int blocks_for(vlr_ctx* ctx, long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, ctx->sm_count * 8ll)); }
+
+void adj_free(vlr_adjoint* a) {
+    void* ptrs[] = {a->origin, a->nbr, a->hkey, a->hval, a->phi[0], a->phi[1], a->phi_init, a->bidx, a->bvox,
+                    a->ub, a->vel, a->checkpoints, a->segment, a->lam[0], a->lam[1], a->G, a->keys, a->pvals,
+                    a->scratch, a->gvel};
+    for (void* p : ptrs) cudaFree(p);
+}
+
+float step_factor(const vlr_adjoint* a, int k) {
+    // s_k = -dt cos(pi t_{k+1} / T)
+    const double pi = 3.14159265358979323846;
+    double t1 = a->t0 + (double)(k + 1) * a->dt;
+    return (float)(-a->dt * std::cos(pi * t1 / a->period));
+}
+
+int enqueue_forward_step(vlr_ctx* ctx, vlr_adjoint* a, int k, const float* src, float* dst) {
+    VLR_TIMED(ctx, "k_adj_forward",
+              k_adj_forward<<<blocks_for(ctx, (long long)a->n_leaves * 512), 256, 0, ctx->stream>>>(
+                  a->origin, a->nbr, a->bidx, a->ub, src, dst, a->n_leaves, step_factor(a, k), a->hw,
+                  ctx->d_errword));
+    VLR_CUDA(ctx, cudaGetLastError());
+    return VLR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
+                   float half_width, const float* vel, int n_stag, double stag_cell, double dt, double period,
+                   double t0, int steps, int checkpoint_every, vlr_adjoint** out) {
+    if (!ctx || !origins || !masks || !phi || !vel || !out || n_leaves == 0)
+        return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (n_stag < 2 || steps < 1 || checkpoint_every < 1 || !(stag_cell > 0.0) || !(dt > 0.0))
+        return set_error(ctx, VLR_ERR_INVALID, "bad adjoint parameters");
+    *out = nullptr;
+    vlr_adjoint* a = new vlr_adjoint();
+    a->ctx = ctx;
+    a->n_leaves = (int)n_leaves;
+    a->hw = half_width;
+    a->n_stag = n_stag;
+    a->H = stag_cell;
+    a->dt = dt;
+    a->period = period;
+    a->t0 = t0;
+    a->steps = steps;
+    a->chk_every = checkpoint_every;
+    auto fail = [&](int rc) {
+        adj_free(a);
+        delete a;
+        return rc;
+    };
+    int rc = choose_base(ctx, origins, n_leaves, a->base);
+    if (rc) return fail(rc);
+    // band: active voxels, in leaf order then ZYX
+    std::vector<int> bidx(n_leaves * 512, -1), bvox;
+    for (size_t i = 0; i < n_leaves; ++i)
+        for (int off = 0; off < 512; ++off)
+            if ((masks[8 * i + (off >> 6)] >> (off & 63)) & 1ull) {
+                bidx[i * 512 + off] = (int)bvox.size();
+                bvox.push_back((int)(i * 512 + off));
+            }
+    a->n_band = (int)bvox.size();
+    if (a->n_band == 0) return fail(set_error(ctx, VLR_ERR_INVALID, "empty band"));
+    const size_t nb = (size_t)a->n_band;
+    a->hcap = 64;
+    while ((size_t)a->hcap < 2 * n_leaves) a->hcap <<= 1;
+    std::vector<int4> o4(n_leaves);
+    for (size_t i = 0; i < n_leaves; ++i) o4[i] = make_int4(origins[3 * i], origins[3 * i + 1], origins[3 * i + 2], 0);
+    size_t nvel = 3ull * n_stag * n_stag * n_stag;
+    int n_chk = steps / checkpoint_every + 1;
+    a->n_pairs_cap = std::max(nb * 8, nb * 24);
+#define ADJ_MALLOC(p, bytes) \
+    do { cudaError_t e_ = cudaMalloc(&(p), (bytes)); if (e_ != cudaSuccess) return fail(check_cuda(ctx, e_, "cudaMalloc")); } while (0)
+    ADJ_MALLOC(a->origin, sizeof(int4) * n_leaves);
+    ADJ_MALLOC(a->nbr, sizeof(int) * kNbr * n_leaves);
+    ADJ_MALLOC(a->hkey, sizeof(uint64_t) * a->hcap);
+    ADJ_MALLOC(a->hval, sizeof(int) * a->hcap);
+    ADJ_MALLOC(a->phi[0], sizeof(float) * 512 * n_leaves);
+    ADJ_MALLOC(a->phi[1], sizeof(float) * 512 * n_leaves);
+    ADJ_MALLOC(a->phi_init, sizeof(float) * 512 * n_leaves);
+    ADJ_MALLOC(a->bidx, sizeof(int) * 512 * n_leaves);
+    ADJ_MALLOC(a->bvox, sizeof(int) * nb);
+    ADJ_MALLOC(a->ub, sizeof(float3) * nb);
+    ADJ_MALLOC(a->vel, sizeof(float) * nvel);
+    ADJ_MALLOC(a->checkpoints, sizeof(float) * nb * n_chk);
+    ADJ_MALLOC(a->segment, sizeof(float) * nb * checkpoint_every);
+    ADJ_MALLOC(a->lam[0], sizeof(float) * nb);
+    ADJ_MALLOC(a->lam[1], sizeof(float) * nb);
+    ADJ_MALLOC(a->gvel, sizeof(float) * nvel);
+    ADJ_MALLOC(a->G, sizeof(float3) * nb);
+    ADJ_MALLOC(a->keys, sizeof(unsigned) * a->n_pairs_cap);
+    ADJ_MALLOC(a->pvals, sizeof(float) * a->n_pairs_cap);
+    ADJ_MALLOC(a->scratch, sort_reduce_scratch_bytes((int)a->n_pairs_cap));
+#undef ADJ_MALLOC
+    cudaStream_t st = ctx->stream;
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->origin, o4.data(), sizeof(int4) * n_leaves, cudaMemcpyHostToDevice, st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->phi_init, phi, sizeof(float) * 512 * n_leaves, cudaMemcpyHostToDevice, st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->bidx, bidx.data(), sizeof(int) * 512 * n_leaves, cudaMemcpyHostToDevice, st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->bvox, bvox.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->vel, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
+    std::vector<uint64_t> hk(a->hcap, kEmptyKey);
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->hkey, hk.data(), sizeof(uint64_t) * a->hcap, cudaMemcpyHostToDevice, st));
+    k_adj_hash_insert<<<(int)((n_leaves + 255) / 256), 256, 0, st>>>(a->origin, (int)n_leaves, a->hkey, a->hval,
+                                                                     a->hcap, a->base[0], a->base[1], a->base[2],
+                                                                     ctx->d_errword);
+    k_adj_nbr<<<(int)((n_leaves * kNbr + 255) / 256), 256, 0, st>>>(a->origin, (int)n_leaves, a->hkey, a->hval, a->hcap,
+                                                                    a->base[0], a->base[1], a->base[2], a->nbr);
+    k_adj_upsample<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, a->origin, (int)nb, a->vel, n_stag, (float)stag_cell,
+                                                        a->ub);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(check_cuda(ctx, e, "adjoint setup"));
+    rc = consume_device_errors(ctx, "vlr_adj_create");
+    if (rc) return fail(rc);
+    *out = a;
+    return VLR_OK;
+}
+
+int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap, size_t* n) {
+    if (!ctx || !a || !n) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *n = (size_t)a->n_band;
+    if (!coords) return VLR_OK;
+    if (cap < *n) return set_error(ctx, VLR_ERR_CAPACITY, "coordinate buffer too small");
+    std::vector<int> bvox(a->n_band);
+    std::vector<int4> o4(a->n_leaves);
+    VLR_CUDA(ctx, cudaMemcpy(bvox.data(), a->bvox, sizeof(int) * a->n_band, cudaMemcpyDeviceToHost));
+    VLR_CUDA(ctx, cudaMemcpy(o4.data(), a->origin, sizeof(int4) * a->n_leaves, cudaMemcpyDeviceToHost));
+    for (int b = 0; b < a->n_band; ++b) {
+        int s = bvox[b] >> 9, off = bvox[b] & 511;
+        coords[3 * b] = o4[s].x + (off >> 6);
+        coords[3 * b + 1] = o4[s].y + ((off >> 3) & 7);
+        coords[3 * b + 2] = o4[s].z + (off & 7);
+    }
+    return VLR_OK;
+}
+
+int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, const float* vel) {
+    if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    cudaStream_t st = ctx->stream;
+    if (phi0_band) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->lam[1], phi0_band, sizeof(float) * a->n_band, cudaMemcpyHostToDevice, st));
+        k_adj_scatter_band<<<blocks_for(ctx, a->n_band), 256, 0, st>>>(a->bvox, a->n_band, a->lam[1], a->phi_init);
+    }
+    if (vel) {
+        size_t nvel = 3ull * a->n_stag * a->n_stag * a->n_stag;
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->vel, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
+        k_adj_upsample<<<blocks_for(ctx, a->n_band), 256, 0, st>>>(a->bvox, a->origin, a->n_band, a->vel, a->n_stag,
+                                                                   (float)a->H, a->ub);
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+    return VLR_OK;
+}
+
+// Forward K steps from the initial state; checkpoints every C steps; writes
+// phi_K on the band (host, n_band floats) when phi_k_band is not null.
+int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band) {
+    if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)a->n_band;
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves, cudaMemcpyDeviceToDevice,
+                                  st));
+    int cur = 0;
+    for (int k = 0; k < a->steps; ++k) {
+        if (k % a->chk_every == 0)
+            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
+                                                                   a->checkpoints + (size_t)(k / a->chk_every) * nb);
+        int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
+        if (rc) return rc;
+        cur = 1 - cur;
+    }
+    k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur], a->lam[1]);
+    VLR_CUDA(ctx, cudaGetLastError());
+    if (phi_k_band)
+        VLR_CUDA(ctx, cudaMemcpyAsync(phi_k_band, a->lam[1], sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+    return consume_device_errors(ctx, "vlr_adj_forward");
+}
+
+// Backward pass (vlr_adj_forward must have run): grad_phik_band = dL/dphi_K
+// on the band; writes dL/dphi_0 (n_band) and dL/dV (3 n^3), host buffers.
+int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
+                     float* grad_vel) {
+    if (!ctx || !a || !grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)a->n_band;
+    float* lam = a->lam[1];
+    VLR_CUDA(ctx, cudaMemcpyAsync(lam, grad_phik_band, sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+    k_zero3<<<blocks_for(ctx, nb), 256, 0, st>>>(a->G, (int)nb);
+    const int C = a->chk_every;
+    for (int seg = (a->steps - 1) / C; seg >= 0; --seg) {
+        const int k0 = seg * C, k1 = std::min(a->steps, k0 + C);
+        // recompute phi_k0 .. phi_{k1-1} from the checkpoint
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves,
+                                      cudaMemcpyDeviceToDevice, st));
+        k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->checkpoints + (size_t)seg * nb,
+                                                                a->phi[0]);
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[1], a->phi[0], sizeof(float) * 512 * a->n_leaves,
+                                      cudaMemcpyDeviceToDevice, st));
+        int cur = 0;
+        for (int k = k0; k < k1; ++k) {
+            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
+                                                                   a->segment + (size_t)(k - k0) * nb);
+            if (k + 1 < k1) {
+                int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
+                if (rc) return rc;
+                cur = 1 - cur;
+            }
+        }
+        // adjoint steps k1-1 .. k0: phi_k from the segment (scattered into a full pool)
+        for (int k = k1 - 1; k >= k0; --k) {
+            k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb,
+                                                                    a->segment + (size_t)(k - k0) * nb, a->phi[0]);
+            VLR_TIMED(ctx, "k_adj_emit",
+                      k_adj_emit<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->bidx, a->ub,
+                                                                      a->phi[0], lam, step_factor(a, k), a->hw,
+                                                                      a->keys, a->pvals, a->G));
+            float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
+            int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 8), (unsigned)nb + 1, lam_out, (unsigned)nb,
+                                 a->scratch);
+            if (rc) return rc;
+            lam = lam_out;
+        }
+        (void)cur;
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    if (grad_phi0_band)
+        VLR_CUDA(ctx, cudaMemcpyAsync(grad_phi0_band, lam, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    if (grad_vel) {
+        size_t nvel = 3ull * a->n_stag * a->n_stag * a->n_stag;
+        float* gv = a->gvel;
+        VLR_TIMED(ctx, "k_adj_emit_vel",
+                  k_adj_emit_vel<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, a->origin, (int)nb, a->G, a->n_stag,
+                                                                      (float)a->H, a->keys, a->pvals));
+        int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 24), (unsigned)nvel + 1, gv, (unsigned)nvel,
+                             a->scratch);
+        if (rc) return rc;
+        VLR_CUDA(ctx, cudaMemcpyAsync(grad_vel, gv, sizeof(float) * nvel, cudaMemcpyDeviceToHost, st));
+    }
+    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+    return consume_device_errors(ctx, "vlr_adj_backward");
+}
+
+void vlr_adj_destroy(vlr_adjoint* a) {
+    if (!a) return;
+    if (a->ctx) cudaStreamSynchronize(a->ctx->stream);
+    adj_free(a);
+    delete a;
+}
+
+}  // extern "C"
