@@ -46,6 +46,7 @@ METRIC = "active voxels/s per advection step"
 DEFORM = dict(radius=0.15, center=(0.35, 0.35, 0.35), voxel_size=1.0 / 512.0, half_width=3.0, period=3.0)
 REF_SPHERE = dict(radius=32.0, center=(64.0, 64.0, 64.0), voxel_size=1.0, half_width=3.0)
 REF_VEL = (1.0, 0.5, 0.25)
+BATCH = dict(grids=256, seed=3)
 
 
 def measured_peaks():
@@ -59,29 +60,41 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled while the GPU is timed.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    The sampler starts before the warm-up and waits for its first sample; the
+    timed regions are marked with ``mark()``; ``summary()`` keeps the samples
+    whose timestamps fall inside a marked region widened by the sampling
+    period (a timed region of a few milliseconds is shorter than one period).
+    """
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 50
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = Path(tempfile.gettempdir()) / f"vlr_clocks_{os.getpid()}.csv"
+        self.windows = []
+        self.path = Path(tempfile.gettempdir()) / f"vlr_clocks_{os.getpid()}_{device}.csv"
 
     def __enter__(self):
         try:
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+                 "-lms", str(self.PERIOD_MS)], stdout=self.out, stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 10.0 and self.path.stat().st_size == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(2.0 * self.PERIOD_MS / 1000.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -92,17 +105,39 @@ class ClockSampler:
         except Exception:
             pass
 
+    def mark(self):
+        """Context manager around one timed region."""
+        sampler = self
+
+        class _W:
+            def __enter__(self):
+                self.t0 = time.time()
+
+            def __exit__(self, *a):
+                sampler.windows.append((self.t0, time.time()))
+
+        return _W()
+
     def summary(self):
+        import datetime
         rows = []
         try:
             for line in open(self.path):
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+                if len(parts) >= 10:
+                    try:
+                        ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        continue
+                    rows.append((ts, parts[1:]))
         except Exception:
             pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        pad = 1.5 * self.PERIOD_MS / 1000.0
+        sel = [r for ts, r in rows if any(a - pad <= ts <= b + pad for a, b in self.windows)]
+        timed_s = sum(b - a for a, b in self.windows)
+        if not sel:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "samples_total": len(rows), "timed_s": timed_s}
 
         def num(x):
             try:
@@ -110,12 +145,14 @@ class ClockSampler:
             except ValueError:
                 return None
 
-        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
-        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
+        sm = [v for v in (num(r[1]) for r in sel) if v is not None]
+        mx = [v for v in (num(r[2]) for r in sel) if v is not None]
+        pw = [v for v in (num(r[3]) for r in sel) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in sel for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(sel),
+                "period_ms": self.PERIOD_MS, "timed_s": timed_s}
 
 
 # ---------------------------------------------------------------- CPU legs
@@ -165,6 +202,22 @@ def cpu_reference_algorithm(sphere: dict, velocity_world, dt: float, sample_voxe
 
 # ---------------------------------------------------------------- GPU legs
 
+STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_t_nbr")
+
+
+# DRAM bytes (read + write) per leaf of one launch, from ncu captures of the
+# bench's own commands (dram__bytes_read.sum + dram__bytes_write.sum divided by
+# the leaves of that launch); keyed by (workload, kernel, value bytes).
+# profiles/stencils_deformation512_full.md (2,853 leaves) and
+# profiles/stencils_batched256_dram.md (151,238 leaves).
+TRAFFIC_PER_LEAF: dict = {
+    ("deformation512", "k_m_advect", 2): 3540736 / 2853,
+    ("deformation512", "k_m_reinit", 2): 3512576 / 2853,
+    ("batched256", "k_m_advect", 2): (193480704 + 160735744) / 151238,
+    ("batched256", "k_m_reinit", 2): (185007616 + 129400320) / 151238,
+}
+
+
 def method_bytes_per_leaf(value_bytes: int):
     """Algorithmic bytes per leaf and launch.
     advect: read values 512*s, mask 64, origin 16, neighbour row 108; write values 512*s, dilated mask 64.
@@ -174,24 +227,22 @@ def method_bytes_per_leaf(value_bytes: int):
     return {"k_m_advect": 1024 * s + 64 + 16 + 108 + 64, "k_m_reinit": 1024 * s + 64 + 16 + 108 + 64 + 8}
 
 
-def run_method(args, ctx, precision, flush, stream, clock=None):
-    import numpy as np
+def time_steps(args, ctx, ls, flush, stream, clock=None, steps=None, warmup=None):
+    """Warm up, then time `steps` graph replays of a method level set, each
+    bracketed by CUDA events on the library stream with the L2 flushed before
+    it (outside the events); then per-kernel durations from the same steps
+    enqueued without the graph (events around each kernel, L2 flushed between
+    steps)."""
     import torch
 
-    from sharc.volrus_b200.method import LevelSet
-
-    vs = DEFORM["voxel_size"]
-    vel = {"kind": "vortex", "vs": vs, "period": DEFORM["period"]}
-    dt = 0.5 * vs / 2.0
-    ls = LevelSet.sphere(DEFORM["radius"], DEFORM["center"], vs, vel, dt, half_width=DEFORM["half_width"],
-                         precision=precision, integrator=2, reinit_iters=2, ctx=ctx)
-    ls.step(args.warmup)
+    steps = steps or args.steps
+    warmup = args.warmup if warmup is None else warmup
+    ls.step(warmup)
     n0, a0, _ = ls.info()
-    times = []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    sampler = clock or _Null()
-    with sampler:
-        for k in range(args.steps):
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize(args.device)
+    with (clock.mark() if clock is not None else _Null()):
+        for k in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(float(k))
                 ev[k][0].record(stream)
@@ -199,20 +250,44 @@ def run_method(args, ctx, precision, flush, stream, clock=None):
             with torch.cuda.stream(stream):
                 ev[k][1].record(stream)
         ctx.check_device()
-    times = [a.elapsed_time(b) for a, b in ev]
+    times = [x.elapsed_time(y) for x, y in ev]
     n1, a1, _ = ls.info()
     ms = sum(times) / len(times)
     active = 0.5 * (a0 + a1)
     leaves = 0.5 * (n0 + n1)
-    # per-kernel durations: the same steps enqueued without the graph, with events
     ctx.profile(True)
-    ls.step(max(3, min(args.steps, 10)))
-    kern = {k: ctx.kernel_time(k) for k in ("k_m_advect", "k_m_reinit", "k_t_propose")}
+    with (clock.mark() if clock is not None else _Null()):
+        for k in range(max(3, min(steps, 10))):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            ls.step(1)
+    kern = {k: ctx.kernel_time(k) for k in STEP_KERNELS}
     ctx.profile(False)
-    n2, a2, _ = ls.info()
-    res = {"ms_per_step": ms, "value": active / (ms * 1e-3), "leaves": leaves, "active": active,
-           "kernels": {k: v[0] / max(v[1], 1) for k, v in kern.items()}, "ls": ls}
-    return res
+    return {"ms_per_step": ms, "value": active / (ms * 1e-3), "leaves": leaves, "active": active,
+            "kernels": {k: v[0] / max(v[1], 1) for k, v in kern.items()}, "ls": ls}
+
+
+def run_method(args, ctx, precision, flush, stream, clock=None):
+    from sharc.volrus_b200.method import LevelSet
+
+    vs = DEFORM["voxel_size"]
+    vel = {"kind": "vortex", "vs": vs, "period": DEFORM["period"]}
+    dt = 0.5 * vs / 2.0
+    ls = LevelSet.sphere(DEFORM["radius"], DEFORM["center"], vs, vel, dt, half_width=DEFORM["half_width"],
+                         precision=precision, integrator=2, reinit_iters=2, ctx=ctx)
+    return time_steps(args, ctx, ls, flush, stream, clock)
+
+
+def run_batched(args, ctx, precision, flush, stream, clock=None, steps=None):
+    """256 uneven grids (unions of 1-64 random spheres, extents 64^3-1024^3
+    log-uniform, curl-noise velocity, RK3), one persistent launch per kernel."""
+    from sharc.volrus_b200.method import LevelSet, random_sphere_grids
+
+    gr = random_sphere_grids(args.grids, seed=BATCH["seed"])
+    ls = LevelSet.spheres([(sph, vel) for sph, vel, _ in gr], 1.0, half_width=3.0, precision=precision,
+                          integrator=3, reinit_iters=2, ctx=ctx)
+    r = time_steps(args, ctx, ls, flush, stream, clock, steps=steps)
+    return r
 
 
 class _Null:
@@ -221,9 +296,6 @@ class _Null:
 
     def __exit__(self, *a):
         pass
-
-    def summary(self):
-        return None
 
 
 def e2e_method(args, ctx, ls, precision):
@@ -269,6 +341,54 @@ def e2e_method(args, ctx, ls, precision):
             "path": "vlr_ls_upload + vlr_ls_step + vlr_ls_download, pinned host buffers"}
 
 
+def roofline_of(r, value_bytes, peak, peak_kind, workload):
+    """Roofline of the dominant stencil kernel of a timed level set."""
+    per = method_bytes_per_leaf(value_bytes)
+    dom = max(("k_m_advect", "k_m_reinit"), key=lambda k: r["kernels"][k])
+    dom_ms = r["kernels"][dom]
+    achieved = per[dom] * r["leaves"] / (dom_ms * 1e-3) / 1e9
+    tr = TRAFFIC_PER_LEAF.get((workload, dom, value_bytes))
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": None if tr is None else tr * r["leaves"],
+            "algorithmic_bytes": per[dom] * r["leaves"], "algorithmic_bytes_per_leaf": per[dom],
+            "launch_ms": dom_ms}
+
+
+def bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=None):
+    from sharc.volrus_b200.method import F16, F32
+    out = {}
+    for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
+        r = run_batched(args, ctx, prec, flush, stream, clk, steps=steps)
+        out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves": r["leaves"],
+                     "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"],
+                     "roofline": roofline_of(r, nb, peak, peak_kind, "batched256")}
+        r["ls"].close()
+    out["fp16_over_fp32"] = out["f16"]["value"] / out["f32"]["value"]
+    out["config"] = {"workload": "batched256", "grids": args.grids, "seed": BATCH["seed"],
+                     "extent": "2^U(6,10) voxels per axis", "spheres": "1-64 per grid, r~U(4,24)",
+                     "velocity": "curl noise, 3 octaves, 1 voxel/step", "integrator": "SSP-RK3", "dt": 1.0,
+                     "half_width": 3, "reinit_iters": 2, "l2": "inputs larger than L2 and flushed between steps"}
+    return out
+
+
+def bench_batched_line(args, ctx, peak, peak_kind):
+    """The batched workload on its own: FP16 line with FP32 beside it."""
+    import torch
+    dev = torch.device("cuda", args.device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    with ClockSampler(args.device) as clk:
+        b = bench_batched(args, ctx, peak, peak_kind, flush, stream, clk)
+    f = b["f16"]
+    return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
+            "dtype": "f16 storage, f32 arithmetic", "config": dict(b["config"], active_voxels=f["active_voxels"],
+                                                                  leaves=f["leaves"]),
+            "fp32": b["f32"], "fp16_over_fp32": b["fp16_over_fp32"], "roofline": f["roofline"],
+            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "e2e": None, "clocks": clk.summary(),
+            "gpu_launches": len(STEP_KERNELS) * args.steps}
+
+
 def bench_deformation(args, ctx, peak, peak_kind):
     import torch
     from sharc.volrus_b200.method import F16, F32
@@ -276,16 +396,15 @@ def bench_deformation(args, ctx, peak, peak_kind):
     dev = torch.device("cuda", args.device)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    clk = ClockSampler(args.device)
-    r16 = run_method(args, ctx, F16, flush, stream, clk)
-    r32 = run_method(args, ctx, F32, flush, stream)
-    per16 = method_bytes_per_leaf(2)
-    dom = max(("k_m_advect", "k_m_reinit"), key=lambda k: r16["kernels"][k])
-    dom_ms = r16["kernels"][dom]
-    achieved = per16[dom] * r16["leaves"] / (dom_ms * 1e-3) / 1e9
+    batched = None
+    with ClockSampler(args.device) as clk:
+        r16 = run_method(args, ctx, F16, flush, stream, clk)
+        r32 = run_method(args, ctx, F32, flush, stream, clk)
+        if not args.no_batched:
+            batched = bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=min(args.steps, 10))
     e2e = e2e_method(args, ctx, r16["ls"], F16)
-    launches_per_step = 2 + 17  # stencils + re-track/index kernels (one graph)
-    return {
+    launches_per_step = len(STEP_KERNELS)  # one CUDA graph per step
+    line = {
         "metric": METRIC, "value": r16["value"], "unit": "voxels/s", "ms_per_step": r16["ms_per_step"],
         "dtype": "f16 storage, f32 arithmetic",
         "config": {"workload": "deformation512", "domain": "unit cube at 512^3", "sphere": "r=0.15 at (0.35,0.35,0.35)",
@@ -295,14 +414,15 @@ def bench_deformation(args, ctx, peak, peak_kind):
                    "step": "advect + 2x Godunov reinit + trim + re-track, one CUDA graph"},
         "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "kernels_ms": r32["kernels"]},
         "fp16_over_fp32": r16["value"] / r32["value"],
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_leaf": per16[dom], "launch_ms": dom_ms},
+        "roofline": roofline_of(r16, 2, peak, peak_kind, "deformation512"),
         "kernels_ms_per_launch": r16["kernels"],
         "e2e": e2e,
         "clocks": clk.summary(),
         "gpu_launches": launches_per_step * args.steps,
     }
+    if batched is not None:
+        line["batched256"] = batched
+    return line
 
 
 def bench_ref_sphere(args, ctx, peak, peak_kind):
@@ -333,8 +453,7 @@ def bench_ref_sphere(args, ctx, peak, peak_kind):
     ctx.synchronize()
     ctx.profile(True)
     times = []
-    clk = ClockSampler(args.device)
-    with clk:
+    with ClockSampler(args.device) as clk, clk.mark():
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
@@ -407,8 +526,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["deformation512", "reference-sphere128"], default="deformation512")
+    ap.add_argument("--workload", choices=["deformation512", "batched256", "reference-sphere128"],
+                    default="deformation512")
+    ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-grid batched measurement")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)
@@ -455,8 +577,12 @@ def main():
     from sharc.volrus_b200 import Context
     ctx = Context.default(local)
     peak, peak_kind = measured_peaks()
-    res = bench_deformation(args, ctx, peak, peak_kind) if args.workload == "deformation512" else \
-        bench_ref_sphere(args, ctx, peak, peak_kind)
+    if args.workload == "deformation512":
+        res = bench_deformation(args, ctx, peak, peak_kind)
+    elif args.workload == "batched256":
+        res = bench_batched_line(args, ctx, peak, peak_kind)
+    else:
+        res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]
     ms = res["ms_per_step"]
     if world > 1:
@@ -472,7 +598,7 @@ def main():
             if args.workload == "deformation512":
                 v, cores, desc = cpu_method_oracle()
                 cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": desc}
-            else:
+            elif args.workload == "reference-sphere128":
                 v, desc = cpu_reference_algorithm(sphere, vel_world, ref_dt)
                 cpu = {"value": v, "unit": "voxels/s", "cores": 1, "kind": "port", "sample": desc}
         line = {"metric": res["metric"], "value": value, "unit": res["unit"], "n_gpus": world, "steps": args.steps,
@@ -481,7 +607,7 @@ def main():
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("fp32", "fp16_over_fp32"):
+        for k in ("fp32", "fp16_over_fp32", "batched256"):
             if k in res:
                 line[k] = res[k]
         print(json.dumps(line))
