@@ -118,6 +118,15 @@ __device__ __forceinline__ float3 velocity(const MGridParams& P, const float2* _
     return u;
 }
 
+// Programmatic dependent launch: the kernels of a step are launched with
+// programmatic stream serialization, so a kernel's CTAs may be scheduled while
+// the previous kernel drains.  dep_wait() blocks until the previous kernel has
+// completed and its writes are visible (a no-op for an ordinary launch);
+// dep_launch() lets the next kernel's CTAs be scheduled as this kernel's CTAs
+// retire.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Hash lookup of a leaf coordinate within a grid (key packs the grid id).
 __device__ __forceinline__ uint64_t mkey(long long lx, long long ly, long long lz, int gid, const long long* base,
                                          int bits) {

@@ -176,6 +176,9 @@ int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, co
     else return set_error(ctx, VLR_ERR_REACH, "velocity * dt exceeds 2 voxels per step (CFL); reduce dt");
     ls->reinit_iters = m->reinit_iters;
     ls->n_grids = n;
+    ls->vel_kind = n > 0 ? vels[0]->kind : -1;
+    for (int g = 1; g < n; ++g)
+        if (vels[g]->kind != ls->vel_kind) ls->vel_kind = -1;
     ls->sp.dt = (float)m->dt;
     ls->sp.t0 = (float)m->t0;
     ls->sp.integrator = m->integrator;

@@ -13,7 +13,7 @@ struct MLeafArrays {
     uint64_t* mask;      // activity
     uint64_t* dmask;     // dilated activity of the current step (written by advect)
     const int* nbr;      // 27 neighbour slots per slot
-    unsigned* spill;     // 27-bit spill mask per slot (written by reinit)
+    unsigned* spill;     // 27-bit mask per slot of absent neighbours the band spills into (written by reinit)
     int* nonempty;       // 1 if the slot has an active voxel after the step
 };
 
@@ -31,10 +31,14 @@ struct MTopo {
     int key_bits;
 };
 
-template <typename T, int H>
+// VK: velocity kind of every grid (MVEL_*), or -1 when a batch mixes kinds.
+template <typename T, int H, int VK>
 __global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
                            MTopo topo, unsigned* __restrict__ err);
+// Dynamic shared memory of the stencil kernels (bytes).
+size_t advect_smem_bytes(int precision_f16, int halo);
+size_t reinit_smem_bytes(int precision_f16);
 template <typename T, int NIT>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, MTopo topo, unsigned* __restrict__ err);

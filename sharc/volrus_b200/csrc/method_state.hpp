@@ -52,7 +52,10 @@ struct vlr_level_set {
     // captured step
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    int grid_blocks = 0;     // persistent grid size
+    int grid_blocks = 0;     // persistent grid size of the index and topology kernels
+    int vel_kind = -1;       // velocity kind shared by every grid (MVEL_*), -1 if mixed
+    int adv_blocks = 0;      // persistent grid sizes of the stencil kernels (0: not chosen yet)
+    int re_blocks = 0;
     int scan_levels = 0;
 
     vlr::MLeafArrays arrays() const {

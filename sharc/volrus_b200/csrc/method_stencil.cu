@@ -10,12 +10,24 @@
 //                on the 10^3 box around the leaf so that the second needs no
 //                exchange), trim to |phi| < hw, new mask, spill mask
 //
-// Instruction economy (both kernels are issue-bound at small leaf counts):
-// the halo is staged one z-row per thread with 16-byte vector loads, grid
-// parameters and the leaf's 8 sin/cos table entries per axis are copied to
-// shared memory once per leaf, dilated voxels are compacted into a list so
-// warps only run backtraces, and results leave through shared memory in
-// 16-byte stores.
+// Staging: the halo tile's rows (8 middle values plus the z-halo pieces of the
+// leaves below and above, per (x, y) row) and the masks of the 27-leaf
+// neighbourhood arrive in shared memory by asynchronous copies (cp.async, all
+// threads, one commit group per leaf) issued one leaf ahead: while the CTA
+// computes leaf i, the copies of leaf i+1 are in flight.  The list entry,
+// origin and neighbour row of the leaves ahead are loaded into registers one
+// or two iterations before they are used, so a leaf costs no dependent global
+// round trip.  The float tile is then built from shared memory.  Measured
+// alternatives: whole-leaf cp.async.bulk copies of the 27 neighbours (one
+// warp issuing 54 bulk copies took ~2,200 cycles per leaf, longer than the
+// leaf's compute) and whole-leaf 16-byte cp.async (8x the bytes the tile
+// needs; the copies' issue took ~2,000 cycles per leaf).
+//
+// Instruction economy (both kernels are issue-bound once latency is hidden):
+// the velocity kind is a template parameter with its constants in registers,
+// dilated voxels are compacted into a list so warps only run backtraces (and
+// the first reinitialisation iteration only the voxels of D), and results
+// leave through shared memory in 16-byte stores.
 #include "method_kernels.hpp"
 
 namespace vlr {
@@ -24,6 +36,80 @@ constexpr int kT = 256;
 
 __device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
 
+// ------------------------------------------------------------ async staging
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Asynchronous global -> shared copy of 4, 8 or 16 bytes (both addresses
+// aligned to the size).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES)
+                     : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Row-packed halo staging of an (8+2H)^2 x (8+2H) tile: tile row (x, y)
+// (local leaf coordinates in [-H, 8+H)) holds the whole z-rows (8 values) of
+// the leaves below, at and above it in z, so element 8 + z is voxel z of the
+// row for z in [-8, 16).  Whole 16-byte rows keep the copies coalesced (a
+// copy per (x, y) row of only the H halo values of the z-neighbours costs one
+// L1 wavefront per lane); only the tile's rows cross from L2, not whole
+// neighbour leaves.
+template <typename T, int H>
+struct RowStage {
+    static constexpr int E = 8 + 2 * H;
+    static constexpr int RP = 24;  // elements per staged row
+    static constexpr size_t bytes = (size_t)E * E * RP * sizeof(T);
+};
+
+// All threads: start the asynchronous copies of one leaf's tile rows and of
+// the 64-byte masks of its 27 neighbours (masks of absent neighbours are
+// zeroed; rows of absent leaves are left for the tile build to fill).
+// `s_nb` holds the 27 neighbour slots.  Called after a CTA barrier that ended
+// every read of the previous stage; stage_ready() completes it.
+template <typename T, int H>
+__device__ __forceinline__ void stage_async(const int* s_nb, const T* __restrict__ vals,
+                                            const uint64_t* __restrict__ masks, T* s_rows, uint64_t* s_m) {
+    using R = RowStage<T, H>;
+    constexpr int E = R::E, RP = R::RP;
+    constexpr int CPR = 8 * (int)sizeof(T) / 16;  // 16-byte chunks per leaf row
+    for (int r = threadIdx.x; r < E * E; r += kT) {
+        const int x = r / E - H, y = r % E - H;
+        const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
+        const int rowoff = ((x & 7) << 6) | ((y & 7) << 3);
+        T* d = s_rows + r * RP;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int sl = s_nb[base + k];
+            if (sl >= 0) {
+                const T* p = vals + (size_t)sl * kLeafVoxels + rowoff;
+#pragma unroll
+                for (int c = 0; c < CPR; ++c) cp_async<16>(d + 8 * k + c * (16 / sizeof(T)), p + c * (16 / sizeof(T)));
+            }
+        }
+    }
+    if (threadIdx.x < kNbr * 4) {
+        const int d = threadIdx.x >> 2, q = threadIdx.x & 3;
+        const int sl = s_nb[d];
+        if (sl >= 0) cp_async<16>(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
+        else *reinterpret_cast<uint4*>(s_m + d * 8 + 2 * q) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    cp_async_commit();
+}
+
+// All threads: wait for this thread's copies, then a CTA barrier.
+__device__ __forceinline__ void stage_ready() {
+    cp_async_wait_all();
+    __syncthreads();
+}
+
 // Copy one grid's parameters into shared memory (all threads call; caller syncs).
 __device__ __forceinline__ void load_params(const MGridParams* __restrict__ params, int gid, MGridParams* s_P) {
     const int* src = (const int*)(params + gid);
@@ -31,12 +117,8 @@ __device__ __forceinline__ void load_params(const MGridParams* __restrict__ para
     for (int i = threadIdx.x; i < (int)(sizeof(MGridParams) / 4); i += blockDim.x) dst[i] = src[i];
 }
 
-// Stage one z-row (E values) of the halo tile.  Row (sx, sy) of the tile maps
-// to local (x, y) = (sx - H, sy - H); z runs over [-H, 8 + H).  Missing
-// neighbour leaves are filled by `fill(zc)` given the clamped z of the centre
-// leaf row.
-template <typename T, int H>
-__device__ __forceinline__ void load_row8(const T* __restrict__ p, float* out) {
+template <typename T>
+__device__ __forceinline__ void lds_row8(const T* p, float* out) {
     if constexpr (sizeof(T) == 2) {
         uint4 u = *reinterpret_cast<const uint4*>(p);
         const __half2* h = reinterpret_cast<const __half2*>(&u);
@@ -54,38 +136,57 @@ __device__ __forceinline__ void load_row8(const T* __restrict__ p, float* out) {
     }
 }
 
-// Fill `row` (E floats) for tile row (x, y) in local leaf coordinates.
-// missing_mode 0: copysign(hw, centre value at clamped position); 1: NaN.
-template <typename T, int H, int MISSING>
-__device__ __forceinline__ void stage_row(const T* __restrict__ vals, const int* s_nbr, const T* __restrict__ centre,
-                                          int x, int y, float hw, float* row) {
-    constexpr int E = 8 + 2 * H;
+// Build tile row (x, y) (local leaf coordinates, z over [-H, 8 + H)) from the
+// row-packed stage.  Absent leaves: kNaN ? NaN : copysign(hw, centre value at
+// the clamped position).
+template <typename T, int H, bool kNaN>
+__device__ __forceinline__ void build_row(const T* s_rows, const int* s_nbr, int x, int y, float hw, float* row) {
+    using R = RowStage<T, H>;
+    constexpr int E = R::E, RP = R::RP;
     const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
-    const int rowoff = ((x & 7) << 6) | ((y & 7) << 3);
-    const int crow = (min(max(x, 0), 7) << 6) | (min(max(y, 0), 7) << 3);
-    const int s0 = s_nbr[base], s1 = s_nbr[base + 1], s2 = s_nbr[base + 2];
+    const T* d = s_rows + ((x + H) * E + (y + H)) * RP;
+    const T* c = s_rows + ((min(max(x, 0), 7) + H) * E + (min(max(y, 0), 7) + H)) * RP + 8;  // centre leaf row
+    const float nan = __int_as_float(0x7fc00000);
     float mid[8];
-    if (s1 >= 0) {
-        load_row8<T, H>(vals + (size_t)s1 * kLeafVoxels + rowoff, mid);
-    } else if (MISSING == 0) {
-        load_row8<T, H>(centre + crow, mid);
+    if (s_nbr[base + 1] >= 0) {
+        lds_row8<T>(d + 8, mid);
+    } else if (!kNaN) {
+        lds_row8<T>(c, mid);
 #pragma unroll
         for (int i = 0; i < 8; ++i) mid[i] = copysignf(hw, mid[i]);
     } else {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) mid[i] = __int_as_float(0x7fc00000);
+        for (int i = 0; i < 8; ++i) mid[i] = nan;
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) row[H + i] = mid[i];
+    if (s_nbr[base] >= 0) {
 #pragma unroll
-    for (int i = 0; i < H; ++i) {
-        float lo, hi;
-        if (s0 >= 0) lo = to_f(vals[(size_t)s0 * kLeafVoxels + rowoff + 8 - H + i]);
-        else lo = (MISSING == 0) ? copysignf(hw, to_f(centre[crow])) : __int_as_float(0x7fc00000);
-        if (s2 >= 0) hi = to_f(vals[(size_t)s2 * kLeafVoxels + rowoff + i]);
-        else hi = (MISSING == 0) ? copysignf(hw, to_f(centre[crow + 7])) : __int_as_float(0x7fc00000);
-        row[i] = lo;
-        row[H + 8 + i] = hi;
+        for (int i = 0; i < H; ++i) row[i] = to_f(d[8 - H + i]);
+    } else {
+        const float f = kNaN ? nan : copysignf(hw, to_f(c[0]));
+#pragma unroll
+        for (int i = 0; i < H; ++i) row[i] = f;
+    }
+    if (s_nbr[base + 2] >= 0) {
+#pragma unroll
+        for (int i = 0; i < H; ++i) row[H + 8 + i] = to_f(d[16 + i]);
+    } else {
+        const float f = kNaN ? nan : copysignf(hw, to_f(c[7]));
+#pragma unroll
+        for (int i = 0; i < H; ++i) row[H + 8 + i] = f;
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void store_row(float* dst, const float* row) {
+    if constexpr (E % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < E / 4; ++i)
+            reinterpret_cast<float4*>(dst)[i] = make_float4(row[4 * i], row[4 * i + 1], row[4 * i + 2], row[4 * i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < E / 2; ++i) reinterpret_cast<float2*>(dst)[i] = make_float2(row[2 * i], row[2 * i + 1]);
     }
 }
 
@@ -105,54 +206,161 @@ __device__ __forceinline__ void store_leaf(T* __restrict__ dst, const float* s_o
     }
 }
 
-__device__ __forceinline__ float2 rotate(float2 t, float d, int full) {
+// ------------------------------------------------------------- velocity
+
+// Per-grid velocity constants held in registers for a leaf.
+struct VelConst {
+    int kind;
+    int octaves;
+    float c[3];
+    float scale;                  // vortex: vel_scale
+    float dphi[kMaxOctaves];
+    float ak[kMaxOctaves];
+    float e[kMaxOctaves][3];
+};
+
+__device__ __forceinline__ VelConst vel_const(const MGridParams& P) {
+    VelConst V;
+    V.kind = P.vel_kind;
+    V.octaves = P.octaves;
+    V.scale = P.vel_scale;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) V.c[a] = P.c[a];
+#pragma unroll
+    for (int o = 0; o < kMaxOctaves; ++o) {
+        V.dphi[o] = P.dphi[o];
+        V.ak[o] = P.ak[o];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) V.e[o][a] = P.e[o][a];
+    }
+    return V;
+}
+
+template <bool FULL>
+__device__ __forceinline__ float2 rotate(float2 t, float d) {
     float sd, cd;
-    if (full) small_sincos(d, sd, cd);
+    if (FULL) small_sincos(d, sd, cd);
     else tiny_sincos(d, sd, cd);
     return make_float2(t.x * cd + t.y * sd, t.y * cd - t.x * sd);
 }
 
 // Velocity (voxels per unit time) at local voxel (lx, ly, lz) + offset, from
-// the leaf's staged tables.  kOff = false: no offset (voxel centre).
-template <bool kOff>
-__device__ __forceinline__ float3 leaf_velocity(const MGridParams& P, const float2 (*tab)[3][8], int lx, int ly, int lz,
+// the leaf's staged sin/cos tables.  kOff = false: no offset (voxel centre).
+template <int VK, bool kOff, bool FULL>
+__device__ __forceinline__ float3 leaf_velocity(const VelConst& V, const float2 (*tab)[3][8], int lx, int ly, int lz,
                                                 float ox, float oy, float oz, float ct) {
-    if (P.vel_kind == MVEL_CONSTANT) return make_float3(P.c[0], P.c[1], P.c[2]);
-    if (P.vel_kind == MVEL_VORTEX) {
+    const int kind = (VK >= 0) ? VK : V.kind;
+    if (kind == MVEL_CONSTANT) return make_float3(V.c[0], V.c[1], V.c[2]);
+    if (kind == MVEL_VORTEX) {
         float2 X = tab[0][0][lx], Y = tab[0][1][ly], Z = tab[0][2][lz];
         if (kOff) {
-            X = rotate(X, P.dphi[0] * ox, P.full_series);
-            Y = rotate(Y, P.dphi[0] * oy, P.full_series);
-            Z = rotate(Z, P.dphi[0] * oz, P.full_series);
+            X = rotate<FULL>(X, V.dphi[0] * ox);
+            Y = rotate<FULL>(Y, V.dphi[0] * oy);
+            Z = rotate<FULL>(Z, V.dphi[0] * oz);
         }
-        float k = P.vel_scale * ct;
+        // u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z), v = -sin(2 pi x) sin^2(pi y) sin(2 pi z),
+        // w = -sin(2 pi x) sin(2 pi y) sin^2(pi z), times cos(pi t / T), world units / voxel size
+        float k = V.scale * ct;
         float sycy = Y.x * Y.y, szcz = Z.x * Z.y, sxcx = X.x * X.y;
         return make_float3(8.0f * k * X.x * X.x * sycy * szcz, -4.0f * k * sxcx * Y.x * Y.x * szcz,
                            -4.0f * k * sxcx * sycy * Z.x * Z.x);
     }
     float3 u = make_float3(0.f, 0.f, 0.f);
-    for (int o = 0; o < P.octaves; ++o) {
-        float2 X = tab[o][0][lx], Y = tab[o][1][ly], Z = tab[o][2][lz];
-        if (kOff) {
-            X = rotate(X, P.dphi[o] * ox, P.full_series);
-            Y = rotate(Y, P.dphi[o] * oy, P.full_series);
-            Z = rotate(Z, P.dphi[o] * oz, P.full_series);
+#pragma unroll
+    for (int o = 0; o < kMaxOctaves; ++o) {
+        if (o < V.octaves) {
+            float2 X = tab[o][0][lx], Y = tab[o][1][ly], Z = tab[o][2][lz];
+            if (kOff) {
+                X = rotate<FULL>(X, V.dphi[o] * ox);
+                Y = rotate<FULL>(Y, V.dphi[o] * oy);
+                Z = rotate<FULL>(Z, V.dphi[o] * oz);
+            }
+            // grad f_o = a (cos x sin y sin z, sin x cos y sin z, sin x sin y cos z); v += grad f_o x e_o
+            const float a = V.ak[o];
+            const float syz = Y.x * Z.x, sxa = a * X.x;
+            const float gx = a * X.y * syz, gy = sxa * Y.y * Z.x, gz = sxa * Y.x * Z.y;
+            u.x += gy * V.e[o][2] - gz * V.e[o][1];
+            u.y += gz * V.e[o][0] - gx * V.e[o][2];
+            u.z += gx * V.e[o][1] - gy * V.e[o][0];
         }
-        float a = P.ak[o];
-        float gx = a * X.y * Y.x * Z.x, gy = a * X.x * Y.y * Z.x, gz = a * X.x * Y.x * Z.y;
-        u.x += gy * P.e[o][2] - gz * P.e[o][1];
-        u.y += gz * P.e[o][0] - gx * P.e[o][2];
-        u.z += gx * P.e[o][1] - gy * P.e[o][0];
     }
     return u;
 }
 
+// Backtrace and trilinear sample of the compacted voxels of D.
+template <int VK, bool FULL, int H>
+__device__ __forceinline__ void advect_voxels(const VelConst& V, const float2 (*s_tab)[3][8], const unsigned short* s_list,
+                                              int nD, const float* s_tile, float* s_out, float dt, int integrator,
+                                              float ct1, float ct2, float ct3, unsigned& bad) {
+    constexpr int E = 8 + 2 * H;
+    for (int i = threadIdx.x; i < nD; i += kT) {
+        const int off = s_list[i];
+        const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
+        float fx, fy, fz;
+        const float3 k1 = leaf_velocity<VK, false, FULL>(V, s_tab, x, y, z, 0.f, 0.f, 0.f, ct1);
+        if (integrator == 1) {
+            fx = -dt * k1.x;
+            fy = -dt * k1.y;
+            fz = -dt * k1.z;
+        } else if (integrator == 2) {
+            const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, -0.5f * dt * k1.x, -0.5f * dt * k1.y,
+                                                            -0.5f * dt * k1.z, ct2);
+            fx = -dt * k2.x;
+            fy = -dt * k2.y;
+            fz = -dt * k2.z;
+        } else {
+            const float h = -dt;
+            const float ax = h * k1.x, ay = h * k1.y, az = h * k1.z;
+            const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, ax, ay, az, ct3);
+            const float bx = 0.25f * (ax + h * k2.x), by = 0.25f * (ay + h * k2.y), bz = 0.25f * (az + h * k2.z);
+            const float3 k3 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, bx, by, bz, ct2);
+            fx = (2.0f / 3.0f) * (bx + h * k3.x);
+            fy = (2.0f / 3.0f) * (by + h * k3.y);
+            fz = (2.0f / 3.0f) * (bz + h * k3.z);
+        }
+        const float px = (float)(x + H) + fx, py = (float)(y + H) + fy, pz = (float)(z + H) + fz;
+        const float bxf = floorf(px), byf = floorf(py), bzf = floorf(pz);
+        float wx = px - bxf, wy = py - byf, wz = pz - bzf;
+        int ii = (int)bxf, jj = (int)byf, kk = (int)bzf;
+        if (ii < 0 || jj < 0 || kk < 0 || ii > E - 2 || jj > E - 2 || kk > E - 2 || !(px == px) || !(py == py) ||
+            !(pz == pz)) {
+            bad = 1u;
+            ii = min(max(ii, 0), E - 2);
+            jj = min(max(jj, 0), E - 2);
+            kk = min(max(kk, 0), E - 2);
+            wx = fminf(fmaxf(wx, 0.f), 1.f);
+            wy = fminf(fmaxf(wy, 0.f), 1.f);
+            wz = fminf(fmaxf(wz, 0.f), 1.f);
+        }
+        const float* q = &s_tile[(ii * E + jj) * E + kk];
+        const float c000 = q[0], c001 = q[1], c010 = q[E], c011 = q[E + 1];
+        const float c100 = q[E * E], c101 = q[E * E + 1], c110 = q[E * E + E], c111 = q[E * E + E + 1];
+        const float c00 = c000 * (1.f - wx) + c100 * wx, c01 = c001 * (1.f - wx) + c101 * wx;
+        const float c10 = c010 * (1.f - wx) + c110 * wx, c11 = c011 * (1.f - wx) + c111 * wx;
+        const float c0 = c00 * (1.f - wy) + c10 * wy, c1 = c01 * (1.f - wy) + c11 * wy;
+        s_out[off] = c0 * (1.f - wz) + c1 * wz;
+    }
+}
+
+// Dynamic shared memory of the advect kernel.
+template <typename T, int H>
+struct AdvectSmem {
+    static constexpr int E = 8 + 2 * H;
+    static constexpr size_t raw = RowStage<T, H>::bytes;
+    static constexpr size_t masks = (size_t)kNbr * 64;
+    static constexpr size_t tile = (size_t)E * E * E * 4;
+    static constexpr size_t out = (size_t)kLeafVoxels * 4;
+    static constexpr size_t bytes = raw + masks + tile + out;
+};
+
 // --------------------------------------------------------------- advect
 
-template <typename T, int H>
+template <typename T, int H, int VK>
 __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                                                 const MGridParams* __restrict__ params, const float2* __restrict__ tab,
                                                 MStepParams sp, MTopo topo, unsigned* __restrict__ err) {
+    dep_wait();
+    dep_launch();
     // clear this step's re-tracking state (keep flags, proposal table, leaf hash)
     for (int i = blockIdx.x * kT + threadIdx.x; i < max(topo.cap, topo.hcap); i += gridDim.x * kT) {
         if (i < topo.cap) topo.keep[i] = 0;
@@ -167,95 +375,124 @@ __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __re
         topo.scalars[4] = 0;  // new count (set by the last scan chunk)
         topo.scalars[7] = 0;  // scan chunk ticket
     }
-    constexpr int E = 8 + 2 * H;
+    using L = AdvectSmem<T, H>;
+    constexpr int E = L::E;
     constexpr int NROW = E * E;
     constexpr int NTAB = kMaxOctaves * 3 * 8;
-    __shared__ __align__(16) float s_tile[E * E * E];
-    __shared__ __align__(16) float s_out[kLeafVoxels];
-    __shared__ __align__(16) uint64_t s_m[kNbr * 8];
-    __shared__ __align__(16) uint64_t s_D[8];
-    __shared__ int s_nbr[kNbr];
+    extern __shared__ __align__(128) unsigned char smem[];
+    T* s_raw = reinterpret_cast<T*>(smem);
+    uint64_t* s_m = reinterpret_cast<uint64_t*>(smem + L::raw);
+    float* s_tile = reinterpret_cast<float*>(smem + L::raw + L::masks);
+    float* s_out = reinterpret_cast<float*>(smem + L::raw + L::masks + L::tile);
+    __shared__ __align__(16) uint64_t s_D[2][8];
+    __shared__ int s_nbr[2][32];
     __shared__ unsigned short s_list[kLeafVoxels];
     __shared__ __align__(16) MGridParams s_P;
     __shared__ float2 s_tab[kMaxOctaves][3][8];
+
     const int count = *A.count;
+    const int G = gridDim.x;
+    int li = blockIdx.x;
+    if (li >= count) return;
     const int step = *A.step;
     const float t1 = sp.t0 + (float)(step + 1) * sp.dt;
     const float dt = sp.dt;
+    const int lane = threadIdx.x & 31;
+    const bool w0 = threadIdx.x < 32;
     unsigned bad = 0;
+
+    // prologue: first leaf staged, next leaf's list entry in flight
+    int slot = A.list[li];
+    int4 o = A.origin[slot];
+    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
+    __syncthreads();
+    stage_async<T, H>(s_nbr[0], src, A.mask, s_raw, s_m);
+    int slot_n = (li + G < count) ? A.list[li + G] : -1;
+
     int cur_gid = -1;
+    VelConst V{};
     float ct1 = 1.f, ct2 = 1.f, ct3 = 1.f;  // vortex time factors cos(pi t / T) at t1, t1 - dt/2, t1 - dt
-    for (int li = blockIdx.x; li < count; li += gridDim.x) {
-        const int slot = A.list[li];
-        const int4 o = A.origin[slot];
+    float hw = 0.f;
+    int fullser = 0;
+    for (unsigned it = 0;; ++it) {
+        const int cur = it & 1;
+        // loads for the leaves ahead (consumed one iteration later)
+        int4 o_n = make_int4(0, 0, 0, -1);
+        if (slot_n >= 0) o_n = A.origin[slot_n];
+        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[slot_n * kNbr + lane] : -1;
+        const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
         if (o.w != cur_gid) {
+            __syncthreads();
             load_params(params, o.w, &s_P);
+            __syncthreads();
             cur_gid = o.w;
-            const MGridParams& G = params[o.w];
-            if (G.vel_kind == MVEL_VORTEX) {
-                ct1 = cosf(G.pi_over_T * t1);
-                ct2 = cosf(G.pi_over_T * (t1 - 0.5f * dt));
-                ct3 = cosf(G.pi_over_T * (t1 - dt));
+            V = vel_const(s_P);
+            hw = s_P.hw;
+            fullser = s_P.full_series;
+            if (V.kind == MVEL_VORTEX) {
+                ct1 = cosf(s_P.pi_over_T * t1);
+                ct2 = cosf(s_P.pi_over_T * (t1 - 0.5f * dt));
+                ct3 = cosf(s_P.pi_over_T * (t1 - dt));
             }
         }
-        if (threadIdx.x < kNbr * 8) {
-            int d = threadIdx.x >> 3;
-            int s = A.nbr[slot * kNbr + d];
-            if ((threadIdx.x & 7) == 0) s_nbr[d] = s;
-            s_m[threadIdx.x] = (s < 0) ? 0ull : A.mask[(size_t)s * 8 + (threadIdx.x & 7)];
-        }
-        __syncthreads();
-        const float hw = s_P.hw;
-        const T* centre = src + (size_t)slot * kLeafVoxels;
-        for (int t = threadIdx.x; t < NROW + NTAB + 64; t += kT) {
-            if (t < NROW) {
-                float row[E];
-                stage_row<T, H, 0>(src, s_nbr, centre, t / E - H, t % E - H, hw, row);
-                float* dstrow = s_tile + t * E;
-#pragma unroll
-                for (int i = 0; i < E; ++i) dstrow[i] = row[i];
-            } else if (t < NROW + NTAB) {
-                int q = t - NROW;
-                int f = q / 24, a = (q / 8) % 3, l = q % 8;
-                if (s_P.vel_kind != MVEL_CONSTANT && (s_P.vel_kind == MVEL_CURL ? f < s_P.octaves : f == 0)) {
-                    int oc = (a == 0 ? o.x : (a == 1 ? o.y : o.z)) + l - s_P.tab_lo[a];
-                    if (oc < 0 || oc >= s_P.tab_len[a]) {
-                        bad = 1u;
-                        oc = min(max(oc, 0), s_P.tab_len[a] - 1);
-                    }
-                    s_tab[f][a][l] = __ldg(&tab[s_P.tab_off[f][a] + oc]);
+        // this leaf's sin/cos table entries, stored after the tile is built
+        float2 tv = make_float2(0.f, 0.f);
+        bool tvalid = false;
+        if (threadIdx.x < NTAB) {
+            const int q = threadIdx.x;
+            const int f = q / 24, a = (q / 8) % 3, l = q % 8;
+            if (V.kind != MVEL_CONSTANT && (V.kind == MVEL_CURL ? f < V.octaves : f == 0)) {
+                int oc = (a == 0 ? o.x : (a == 1 ? o.y : o.z)) + l - s_P.tab_lo[a];
+                if (oc < 0 || oc >= s_P.tab_len[a]) {
+                    bad = 1u;
+                    oc = min(max(oc, 0), s_P.tab_len[a] - 1);
                 }
-            } else {
-                // dilation: one thread per z-row, 10-bit rows z = -1..8
-                int r = t - NROW - NTAB;
-                int x = r >> 3, y = r & 7;
-                unsigned acc = 0;
-#pragma unroll
-                for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll
-                    for (int dy = -1; dy <= 1; ++dy) {
-                        int xx = x + dx, yy = y + dy;
-                        int base = nb_axis(xx) * 9 + nb_axis(yy) * 3;
-                        int bi = ((xx & 7) << 3) | (yy & 7);
-                        const unsigned char* m = (const unsigned char*)s_m;
-                        acc |= ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
-                               (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
-                    }
-                ((unsigned char*)s_D)[r] = (unsigned char)(((acc | (acc << 1) | (acc >> 1)) >> 1) & 0xffu);
+                tv = __ldg(&tab[s_P.tab_off[f][a] + oc]);
+                tvalid = true;
             }
         }
+        stage_ready();
+        const int* nbr = s_nbr[cur];
+        for (int t = threadIdx.x; t < NROW + 64; t += kT) {  // one pass for H = 2
+          if (t < NROW) {
+            float row[E];
+            build_row<T, H, false>(s_raw, nbr, t / E - H, t % E - H, hw, row);
+            store_row<E>(s_tile + t * E, row);
+          } else {
+            // dilation: one thread per z-row, 10-bit rows z = -1..8
+            const int r = t - NROW;
+            const int x = r >> 3, y = r & 7;
+            unsigned acc = 0;
+            const unsigned char* m = (const unsigned char*)s_m;
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int xx = x + dx, yy = y + dy;
+                    const int base = nb_axis(xx) * 9 + nb_axis(yy) * 3;
+                    const int bi = ((xx & 7) << 3) | (yy & 7);
+                    acc |= ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
+                           (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
+                }
+            ((unsigned char*)s_D[cur])[r] = (unsigned char)(((acc | (acc << 1) | (acc >> 1)) >> 1) & 0xffu);
+          }
+        }
+        if (w0) s_nbr[cur ^ 1][lane] = nb_n;
         __syncthreads();
+        // the staging buffers are free: stage the next leaf
+        if (slot_n >= 0) stage_async<T, H>(s_nbr[cur ^ 1], src, A.mask, s_raw, s_m);
+        if (tvalid) (&s_tab[0][0][0])[threadIdx.x] = tv;
         // compact D; voxels outside D keep the sign of their previous value
         int nD = 0, pre = 0;
-        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int w = threadIdx.x >> 5;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            int c = __popcll(s_D[q]);
+            const int c = __popcll(s_D[cur][q]);
             if (q < w) pre += c;
             nD += c;
         }
         {
-            const uint64_t word = s_D[w];
+            const uint64_t word = s_D[cur][w];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int bit = lane + 32 * h;
@@ -268,57 +505,18 @@ __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __re
             }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < nD; i += kT) {
-            const int off = s_list[i];
-            const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
-            float fx, fy, fz;
-            float3 k1 = leaf_velocity<false>(s_P, s_tab, x, y, z, 0.f, 0.f, 0.f, ct1);
-            if (sp.integrator == 1) {
-                fx = -dt * k1.x;
-                fy = -dt * k1.y;
-                fz = -dt * k1.z;
-            } else if (sp.integrator == 2) {
-                float3 k2 = leaf_velocity<true>(s_P, s_tab, x, y, z, -0.5f * dt * k1.x, -0.5f * dt * k1.y,
-                                                -0.5f * dt * k1.z, ct2);
-                fx = -dt * k2.x;
-                fy = -dt * k2.y;
-                fz = -dt * k2.z;
-            } else {
-                const float h = -dt;
-                float ax = h * k1.x, ay = h * k1.y, az = h * k1.z;
-                float3 k2 = leaf_velocity<true>(s_P, s_tab, x, y, z, ax, ay, az, ct3);
-                float bx = 0.25f * (ax + h * k2.x), by = 0.25f * (ay + h * k2.y), bz = 0.25f * (az + h * k2.z);
-                float3 k3 = leaf_velocity<true>(s_P, s_tab, x, y, z, bx, by, bz, ct2);
-                fx = (2.0f / 3.0f) * (bx + h * k3.x);
-                fy = (2.0f / 3.0f) * (by + h * k3.y);
-                fz = (2.0f / 3.0f) * (bz + h * k3.z);
-            }
-            float px = (float)(x + H) + fx, py = (float)(y + H) + fy, pz = (float)(z + H) + fz;
-            float bxf = floorf(px), byf = floorf(py), bzf = floorf(pz);
-            float wx = px - bxf, wy = py - byf, wz = pz - bzf;
-            int ii = (int)bxf, jj = (int)byf, kk = (int)bzf;
-            if (ii < 0 || jj < 0 || kk < 0 || ii > E - 2 || jj > E - 2 || kk > E - 2 || !(px == px) ||
-                !(py == py) || !(pz == pz)) {
-                bad = 1u;
-                ii = min(max(ii, 0), E - 2);
-                jj = min(max(jj, 0), E - 2);
-                kk = min(max(kk, 0), E - 2);
-                wx = fminf(fmaxf(wx, 0.f), 1.f);
-                wy = fminf(fmaxf(wy, 0.f), 1.f);
-                wz = fminf(fmaxf(wz, 0.f), 1.f);
-            }
-            const float* q = &s_tile[(ii * E + jj) * E + kk];
-            float c000 = q[0], c001 = q[1], c010 = q[E], c011 = q[E + 1];
-            float c100 = q[E * E], c101 = q[E * E + 1], c110 = q[E * E + E], c111 = q[E * E + E + 1];
-            float c00 = c000 * (1.f - wx) + c100 * wx, c01 = c001 * (1.f - wx) + c101 * wx;
-            float c10 = c010 * (1.f - wx) + c110 * wx, c11 = c011 * (1.f - wx) + c111 * wx;
-            float c0 = c00 * (1.f - wy) + c10 * wy, c1 = c01 * (1.f - wy) + c11 * wy;
-            s_out[off] = c0 * (1.f - wz) + c1 * wz;
-        }
+        if (fullser)
+            advect_voxels<VK, true, H>(V, s_tab, s_list, nD, s_tile, s_out, dt, sp.integrator, ct1, ct2, ct3, bad);
+        else
+            advect_voxels<VK, false, H>(V, s_tab, s_list, nD, s_tile, s_out, dt, sp.integrator, ct1, ct2, ct3, bad);
         __syncthreads();
         store_leaf<T>(dst + (size_t)slot * kLeafVoxels, s_out);
-        if (threadIdx.x < 8) A.dmask[(size_t)slot * 8 + threadIdx.x] = s_D[threadIdx.x];
-        __syncthreads();
+        if (threadIdx.x < 8) A.dmask[(size_t)slot * 8 + threadIdx.x] = s_D[cur][threadIdx.x];
+        if (slot_n < 0) break;
+        li += G;
+        slot = slot_n;
+        o = o_n;
+        slot_n = slot_nn;
     }
     if (bad) atomicOr(err, kErrReach);
 }
@@ -352,58 +550,124 @@ __device__ __forceinline__ float reinit_update(const float* c, float p, float s,
     return p - 0.5f * s * (G - 1.0f);
 }
 
+template <typename T>
+struct ReinitSmem {
+    static constexpr size_t raw = RowStage<T, 2>::bytes;
+    static constexpr size_t masks = (size_t)kNbr * 64;
+    static constexpr size_t p1 = 12 * 12 * 12 * 4;  // phi1 tile: leaf + 2-voxel ring
+    static constexpr size_t p2 = 10 * 10 * 10 * 4;  // phi2 tile: leaf + 1-voxel ring
+    static constexpr size_t out = (size_t)kLeafVoxels * 4;
+    static constexpr size_t bytes = raw + masks + p1 + p2 + out;
+};
+
 template <typename T, int NIT>
-__global__ void __launch_bounds__(kT) k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                                                const MGridParams* __restrict__ params, MTopo topo,
-                                                unsigned* __restrict__ err) {
+__global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
+                                                   const MGridParams* __restrict__ params, MTopo topo,
+                                                   unsigned* __restrict__ err) {
+    dep_wait();
+    dep_launch();
     constexpr int E = 12;  // phi1 tile: leaf + 2-voxel ring
     constexpr int F = 10;  // phi2 tile and D rows: leaf + 1-voxel ring
-    __shared__ __align__(16) float s_p1[E * E * E];
-    __shared__ __align__(16) float s_p2[F * F * F];
-    __shared__ __align__(16) float s_out[kLeafVoxels];
-    __shared__ __align__(16) uint64_t s_dm[kNbr * 8];
+    using L = ReinitSmem<T>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    T* s_raw = reinterpret_cast<T*>(smem);
+    uint64_t* s_dm = reinterpret_cast<uint64_t*>(smem + L::raw);
+    float* s_p1 = reinterpret_cast<float*>(smem + L::raw + L::masks);
+    float* s_p2 = reinterpret_cast<float*>(smem + L::raw + L::masks + L::p1);
+    float* s_out = reinterpret_cast<float*>(smem + L::raw + L::masks + L::p1 + L::p2);
     __shared__ unsigned short s_D[F * F];
-    __shared__ int s_nbr[kNbr];
+    __shared__ unsigned short s_list[F * F * F];
+    __shared__ int s_rowpre[F * F];
+    __shared__ int s_wsum[4];
+    __shared__ int s_nbr[2][32];
     __shared__ __align__(16) unsigned s_M[16];
+
     const int count = *A.count;
-    for (int li = blockIdx.x; li < count; li += gridDim.x) {
-        const int slot = A.list[li];
-        const int4 o = A.origin[slot];
-        const float hw = params[o.w].hw;
-        if (threadIdx.x < kNbr * 8) {
-            int d = threadIdx.x >> 3;
-            int s = A.nbr[slot * kNbr + d];
-            if ((threadIdx.x & 7) == 0) s_nbr[d] = s;
-            s_dm[threadIdx.x] = (s < 0) ? 0ull : A.dmask[(size_t)s * 8 + (threadIdx.x & 7)];
-        }
-        __syncthreads();
+    const int G = gridDim.x;
+    int li = blockIdx.x;
+    if (li >= count) return;
+    const int lane = threadIdx.x & 31;
+    const bool w0 = threadIdx.x < 32;
+
+    int slot = A.list[li];
+    int4 o = A.origin[slot];
+    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
+    __syncthreads();
+    stage_async<T, 2>(s_nbr[0], src, A.dmask, s_raw, s_dm);
+    int slot_n = (li + G < count) ? A.list[li + G] : -1;
+    float hw = params[o.w].hw;
+
+    for (unsigned it = 0;; ++it) {
+        const int cur = it & 1;
+        int4 o_n = make_int4(0, 0, 0, -1);
+        if (slot_n >= 0) o_n = A.origin[slot_n];
+        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[slot_n * kNbr + lane] : -1;
+        const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
+        stage_ready();
+        const int* nbr = s_nbr[cur];
         for (int t = threadIdx.x; t < E * E + F * F; t += kT) {
             if (t < E * E) {
                 float row[E];
-                stage_row<T, 2, 1>(src, s_nbr, nullptr, t / E - 2, t % E - 2, hw, row);
-                float4* d4 = reinterpret_cast<float4*>(s_p1 + t * E);
-                d4[0] = make_float4(row[0], row[1], row[2], row[3]);
-                d4[1] = make_float4(row[4], row[5], row[6], row[7]);
-                d4[2] = make_float4(row[8], row[9], row[10], row[11]);
+                const int x = t / E - 2, y = t % E - 2;
+                build_row<T, 2, true>(s_raw, nbr, x, y, hw, row);
+                store_row<E>(s_p1 + t * E, row);
+                if (NIT == 2 && x >= -1 && x <= 8 && y >= -1 && y <= 8) {
+                    // phi2 starts as phi1 on the 10^3 box; iteration 1 overwrites the voxels of D
+                    float* d2 = s_p2 + ((x + 1) * F + (y + 1)) * F;
+#pragma unroll
+                    for (int i = 0; i < F; ++i) d2[i] = row[i + 1];
+                }
             } else {
-                int r = t - E * E;
-                int x = r / F - 1, y = r % F - 1;
-                int base = nb_axis(x) * 9 + nb_axis(y) * 3;
-                int bi = ((x & 7) << 3) | (y & 7);
+                const int r = t - E * E;
+                const int x = r / F - 1, y = r % F - 1;
+                const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
+                const int bi = ((x & 7) << 3) | (y & 7);
                 const unsigned char* m = (const unsigned char*)s_dm;
-                s_D[r] = (unsigned short)(((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
-                                          (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9));
+                const unsigned row = ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
+                                     (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
+                s_D[r] = (unsigned short)row;
+                if (NIT == 2) s_rowpre[r] = __popc(row);
             }
         }
+        if (w0) s_nbr[cur ^ 1][lane] = nb_n;
         __syncthreads();
+        if (slot_n >= 0) stage_async<T, 2>(s_nbr[cur ^ 1], src, A.dmask, s_raw, s_dm);
         if (NIT == 2) {
-            for (int t = threadIdx.x; t < F * F * F; t += kT) {
-                int xr = t / (F * F), yr = (t / F) % F, zr = t % F;
+            // compact the voxels of D in the 10^3 box (row-major (x, y, z))
+            int nD = 0;
+            {
+                const int w = threadIdx.x >> 5;
+                int v = (threadIdx.x < F * F) ? s_rowpre[threadIdx.x] : 0, x = v;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, off);
+                    if (lane >= off) x += y;
+                }
+                if (w < 4 && lane == 31) s_wsum[w] = x;
+                __syncthreads();
+                int wpre = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (q < w) wpre += s_wsum[q];
+                    nD += s_wsum[q];
+                }
+                if (threadIdx.x < F * F) {
+                    int pos = wpre + x - v;
+                    unsigned row = s_D[threadIdx.x];
+                    while (row) {
+                        const int z = __ffs(row) - 1;
+                        row &= row - 1u;
+                        s_list[pos++] = (unsigned short)(threadIdx.x * F + z);
+                    }
+                }
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < nD; i += kT) {
+                const int t = s_list[i];
+                const int xr = t / (F * F), yr = (t / F) % F, zr = t % F;
                 const float* c = &s_p1[((xr + 1) * E + (yr + 1)) * E + (zr + 1)];
-                float p = c[0];
-                float q = p;
-                if ((s_D[xr * F + yr] >> zr) & 1u) q = reinit_update<E>(c, p, p * rsqrtf(p * p + 1.0f), hw);
-                s_p2[t] = q;
+                const float p = c[0];
+                s_p2[t] = reinit_update<E>(c, p, p * rsqrtf(p * p + 1.0f), hw);
             }
             __syncthreads();
         }
@@ -422,36 +686,40 @@ __global__ void __launch_bounds__(kT) k_m_reinit(MLeafArrays A, const T* __restr
                 v = inD ? reinit_update<E>(c1, p1, p1 * rsqrtf(p1 * p1 + 1.0f), hw) : p1;
             } else {
                 const float* c2 = &s_p2[((x + 1) * F + (y + 1)) * F + (z + 1)];
-                float p2 = c2[0];
+                const float p2 = c2[0];
                 v = inD ? reinit_update<F>(c2, p2, p1 * rsqrtf(p1 * p1 + 1.0f), hw) : p2;
             }
             const bool on = inD && fabsf(v) < hw;
             if (!on) v = copysignf(hw, v);
             s_out[off] = v;
-            unsigned b = __ballot_sync(0xffffffffu, on);
-            if ((threadIdx.x & 31) == 0) s_M[off >> 5] = b;
+            const unsigned b = __ballot_sync(0xffffffffu, on);
+            if (lane == 0) s_M[off >> 5] = b;
             any |= on;
         }
         __syncthreads();
         store_leaf<T>(dst + (size_t)slot * kLeafVoxels, s_out);
         if (threadIdx.x < 16) reinterpret_cast<unsigned*>(A.mask + (size_t)slot * 8)[threadIdx.x] = s_M[threadIdx.x];
-        if (threadIdx.x < 32) {
+        if (threadIdx.x >= 32 && threadIdx.x < 64) {
             // spill mask from 64-bit (x*8+y) plane masks of z = 0, z = 7 and any z
-            const int lane = threadIdx.x;
             const unsigned char* B = (const unsigned char*)s_M;
-            unsigned b0 = B[lane], b1 = B[lane + 32];
-            uint64_t z0 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 1u) | ((uint64_t)__ballot_sync(0xffffffffu, b1 & 1u) << 32);
-            uint64_t z7 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 0x80u) | ((uint64_t)__ballot_sync(0xffffffffu, b1 & 0x80u) << 32);
-            uint64_t za = (uint64_t)__ballot_sync(0xffffffffu, b0 != 0u) | ((uint64_t)__ballot_sync(0xffffffffu, b1 != 0u) << 32);
+            const unsigned b0 = B[lane], b1 = B[lane + 32];
+            const uint64_t z0 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 1u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 1u) << 32);
+            const uint64_t z7 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 0x80u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 0x80u) << 32);
+            const uint64_t za = (uint64_t)__ballot_sync(0xffffffffu, b0 != 0u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 != 0u) << 32);
             bool spl = false;
             if (lane < kNbr && lane != 13) {
-                int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-                uint64_t plane = dz < 0 ? z0 : (dz > 0 ? z7 : za);
-                uint64_t xs = dx < 0 ? 0xFFull : (dx > 0 ? (0xFFull << 56) : ~0ull);
-                uint64_t ys = dy < 0 ? 0x0101010101010101ull : (dy > 0 ? 0x8080808080808080ull : ~0ull);
+                const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+                const uint64_t plane = dz < 0 ? z0 : (dz > 0 ? z7 : za);
+                const uint64_t xs = dx < 0 ? 0xFFull : (dx > 0 ? (0xFFull << 56) : ~0ull);
+                const uint64_t ys = dy < 0 ? 0x0101010101010101ull : (dy > 0 ? 0x8080808080808080ull : ~0ull);
                 spl = (plane & xs & ys) != 0ull;
             }
-            unsigned bits = __ballot_sync(0xffffffffu, spl);
+            // spill toward absent neighbours only: those are the proposals the
+            // allocation scan resolves (present ones are kept right here)
+            const unsigned bits = __ballot_sync(0xffffffffu, spl && nbr[lane] < 0);
             if (lane == 0) {
                 A.spill[slot] = bits;
                 A.nonempty[slot] = (za != 0ull) ? 1 : 0;
@@ -461,20 +729,21 @@ __global__ void __launch_bounds__(kT) k_m_reinit(MLeafArrays A, const T* __restr
             // survives; a missing one is proposed, keeping the proposer whose
             // direction seen from the new leaf comes first (atomicMin).
             if (spl) {
-                const int n = s_nbr[lane];
+                const int n = nbr[lane];
                 if (n >= 0) {
                     topo.keep[n] = 1;
                 } else {
-                    int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+                    const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
                     const MGridParams& P = params[o.w];
-                    uint64_t key = mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy,
-                                        (long long)(o.z >> 3) + dz, o.w, P.base, topo.key_bits);
+                    const uint64_t key = mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy,
+                                              (long long)(o.z >> 3) + dz, o.w, P.base, topo.key_bits);
                     bool done = false;
                     if (key != kEmptyKey) {
                         uint32_t m = (uint32_t)topo.hcap - 1u, p = (uint32_t)mix64(key) & m;
                         for (int probe = 0; probe < topo.hcap; ++probe) {
-                            unsigned long long prev = atomicCAS((unsigned long long*)&topo.pkey[p],
-                                                                (unsigned long long)kEmptyKey, (unsigned long long)key);
+                            const unsigned long long prev = atomicCAS((unsigned long long*)&topo.pkey[p],
+                                                                      (unsigned long long)kEmptyKey,
+                                                                      (unsigned long long)key);
                             if (prev == kEmptyKey || prev == key) {
                                 atomicMin(&topo.pval[p], kNbr - 1 - lane);
                                 done = true;
@@ -487,19 +756,43 @@ __global__ void __launch_bounds__(kT) k_m_reinit(MLeafArrays A, const T* __restr
                 }
             }
         }
-        __syncthreads();
+        (void)any;
+        if (slot_n < 0) break;
+        li += G;
+        slot = slot_n;
+        if (o_n.w != o.w) hw = params[o_n.w].hw;
+        o = o_n;
+        slot_n = slot_nn;
     }
 }
 
-#define VLR_INST_STENCIL(T)                                                                                      \
-    template __global__ void k_m_advect<T, 2>(MLeafArrays, const T*, T*, const MGridParams*, const float2*,        \
-                                              MStepParams, MTopo, unsigned*);                                    \
-    template __global__ void k_m_advect<T, 3>(MLeafArrays, const T*, T*, const MGridParams*, const float2*,        \
-                                              MStepParams, MTopo, unsigned*);                                    \
+#define VLR_INST_ADVECT(T, H)                                                                                    \
+    template __global__ void k_m_advect<T, H, -1>(MLeafArrays, const T*, T*, const MGridParams*, const float2*,    \
+                                                  MStepParams, MTopo, unsigned*);                                \
+    template __global__ void k_m_advect<T, H, MVEL_CONSTANT>(MLeafArrays, const T*, T*, const MGridParams*,        \
+                                                             const float2*, MStepParams, MTopo, unsigned*);      \
+    template __global__ void k_m_advect<T, H, MVEL_VORTEX>(MLeafArrays, const T*, T*, const MGridParams*,          \
+                                                           const float2*, MStepParams, MTopo, unsigned*);        \
+    template __global__ void k_m_advect<T, H, MVEL_CURL>(MLeafArrays, const T*, T*, const MGridParams*,            \
+                                                         const float2*, MStepParams, MTopo, unsigned*);
+#define VLR_INST_REINIT(T)                                                                                       \
     template __global__ void k_m_reinit<T, 0>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);    \
     template __global__ void k_m_reinit<T, 1>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);    \
     template __global__ void k_m_reinit<T, 2>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);
-VLR_INST_STENCIL(float)
-VLR_INST_STENCIL(__half)
+VLR_INST_ADVECT(float, 2)
+VLR_INST_ADVECT(float, 3)
+VLR_INST_ADVECT(__half, 2)
+VLR_INST_ADVECT(__half, 3)
+VLR_INST_REINIT(float)
+VLR_INST_REINIT(__half)
+
+size_t advect_smem_bytes(int precision_f16, int halo) {
+    if (precision_f16) return halo == 2 ? AdvectSmem<__half, 2>::bytes : AdvectSmem<__half, 3>::bytes;
+    return halo == 2 ? AdvectSmem<float, 2>::bytes : AdvectSmem<float, 3>::bytes;
+}
+
+size_t reinit_smem_bytes(int precision_f16) {
+    return precision_f16 ? ReinitSmem<__half>::bytes : ReinitSmem<float>::bytes;
+}
 
 }  // namespace vlr

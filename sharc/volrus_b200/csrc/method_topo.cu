@@ -54,6 +54,8 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
                                                        int* free_stack, int* recycled, int* list_new,
                                                        int* newinfo, unsigned long long* status, int* scalars,
                                                        int cap, unsigned* err) {
+    dep_wait();
+    dep_launch();
     __shared__ int s_ticket;
     __shared__ int s_warp[kChunk / 32];
     __shared__ int s_prefix;
@@ -77,10 +79,9 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
             if (!surv) recycled[atomicAdd(&scalars[5], 1)] = s;
             unsigned sp = A.spill[s];
             o = origin[s];
-            while (sp) {
+            while (sp) {  // absent neighbours only (reinit masked the present ones out)
                 int d = __ffs(sp) - 1;
                 sp &= sp - 1;
-                if (A.nbr[s * kNbr + d] >= 0) continue;
                 int dx, dy, dz;
                 dir_of(d, dx, dy, dz);
                 if (hfind(pkey, pval, hcap, leaf_key(o, dx, dy, dz, params, bits)) == kNbr - 1 - d) {
@@ -106,33 +107,49 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
                 if (lane >= off) ai += y;
             }
             if (lane < kChunk / 32) s_warp[lane] = ai - a;
-            if (lane == kChunk / 32 - 1) {
-                // publish the aggregate, look back for the chunk's exclusive prefix
-                const unsigned total = (unsigned)ai;
-                unsigned prefix = 0;
-                if (chunk == 0) {
-                    atomicExch(&status[0], pack_status(tag, 2, total));
-                } else {
-                    atomicExch(&status[chunk], pack_status(tag, 1, total));
-                    int q = chunk - 1;
-                    long long spins = 0;
-                    while (q >= 0) {
-                        unsigned long long st = atomicAdd(&status[q], 0ull);
-                        unsigned stag = (unsigned)(st >> 34), flag = (unsigned)(st >> 32) & 3u;
-                        if (stag == (tag & 0x3fffffffu) && flag != 0) {
-                            prefix += (unsigned)st;
-                            if (flag == 2) break;
-                            --q;
-                            continue;
-                        }
+            // publish the aggregate, then look back 32 chunks at a time: lane j
+            // reads the status of chunk q - j; the walk stops at the nearest
+            // chunk holding an inclusive prefix (a virtual one before chunk 0)
+            const unsigned total = (unsigned)__shfl_sync(0xffffffffu, ai, kChunk / 32 - 1);
+            const unsigned wtag = tag & 0x3fffffffu;
+            unsigned prefix = 0;
+            if (chunk == 0) {
+                if (lane == 0) atomicExch(&status[0], pack_status(tag, 2, total));
+            } else {
+                if (lane == 0) atomicExch(&status[chunk], pack_status(tag, 1, total));
+                int q = chunk - 1;
+                long long spins = 0;
+                for (;;) {
+                    const int idx = q - lane;
+                    unsigned flag = 2, val = 0;
+                    if (idx >= 0) {
+                        const unsigned long long st = *reinterpret_cast<volatile unsigned long long*>(&status[idx]);
+                        const bool cur = (unsigned)(st >> 34) == wtag;
+                        flag = cur ? (unsigned)(st >> 32) & 3u : 0u;
+                        val = (unsigned)st;
+                    }
+                    const unsigned pmask = __ballot_sync(0xffffffffu, flag == 2);
+                    const unsigned invalid = __ballot_sync(0xffffffffu, flag == 0);
+                    const int first_p = pmask ? __ffs(pmask) - 1 : 32;
+                    const unsigned upto = first_p >= 31 ? 0xffffffffu : ((2u << first_p) - 1u);
+                    if (invalid & upto) {
                         if (++spins > kSpinLimit) {  // bounded wait: report and continue
-                            atomicOr(err, kErrTimeout);
+                            if (lane == 0) atomicOr(err, kErrTimeout);
                             break;
                         }
-                        __nanosleep(64);
+                        __nanosleep(32);
+                        continue;
                     }
-                    atomicExch(&status[chunk], pack_status(tag, 2, prefix + total));
+                    unsigned add = ((upto >> lane) & 1u) ? val : 0u;
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) add += __shfl_xor_sync(0xffffffffu, add, off);
+                    prefix += add;
+                    if (first_p < 32) break;
+                    q -= 32;
                 }
+                if (lane == 0) atomicExch(&status[chunk], pack_status(tag, 2, prefix + total));
+            }
+            if (lane == 0) {
                 s_prefix = (int)prefix;
                 if (chunk == nchunks - 1) scalars[4] = (int)(prefix + total);
             }
@@ -186,6 +203,8 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
                                                    T* vals, uint64_t* hkey, int* hval, int hcap,
                                                    const MGridParams* __restrict__ params, int bits, int* free_stack,
                                                    const int* recycled, int* scalars, int cap, unsigned* err) {
+    dep_wait();
+    dep_launch();
     const int n = min(scalars[4], cap);
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -237,6 +256,8 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
 
 __global__ void k_t_nbr(const int* list, int* scalars, const int4* origin, const uint64_t* hkey, const int* hval,
                         int hcap, const MGridParams* __restrict__ params, int bits, int* nbr, int cap) {
+    dep_wait();
+    dep_launch();
     const int count = min(scalars[4], cap);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)count * kNbr;
          t += (long long)gridDim.x * blockDim.x) {
@@ -306,6 +327,25 @@ size_t scan_scratch_ints(int n) { return (size_t)((n + kChunk - 1) / kChunk) * 2
 
 // ----------------------------------------------------------- orchestration
 
+// Launch one kernel of the step with programmatic stream serialization (its
+// CTAs may be scheduled while the previous kernel drains; the kernel itself
+// waits for that kernel's results with dep_wait()).
+template <typename... KArgs, typename... Args>
+static cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 MTopo topo_of(vlr_level_set* ls) {
     MTopo t;
     t.keep = ls->keep;
@@ -339,59 +379,94 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
     // status words of the look-back scan live after the scan positions in `pos`
     unsigned long long* status = reinterpret_cast<unsigned long long*>(ls->pos);
     VLR_TIMED(ctx, "k_t_scanalloc",
-              k_t_scanalloc<<<B, kChunk, 0, st>>>(A, ls->origin, ls->keep, ls->pkey, ls->pval, ls->hcap, ls->d_params,
-                                                  ls->key_bits, ls->free_stack, ls->owned, ls->list_new,
-                                                  ls->newinfo, status, ls->scalars, ls->cap, ctx->d_errword));
+              VLR_CUDA(ctx, pdl_launch(k_t_scanalloc, B, kChunk, 0, st, A, ls->origin, (const int*)ls->keep,
+                                       (const uint64_t*)ls->pkey, (const int*)ls->pval, ls->hcap,
+                                       (const MGridParams*)ls->d_params, ls->key_bits, ls->free_stack, ls->owned,
+                                       ls->list_new, ls->newinfo, status, ls->scalars, ls->cap, ctx->d_errword)));
     if (ls->precision == VLR_PREC_F16)
         VLR_TIMED(ctx, "k_t_finalize",
-                  k_t_finalize<__half><<<B, 256, 0, st>>>(ls->list_new, ls->newinfo, ls->list, ls->origin,
-                                                         (__half*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
-                                                         ls->d_params, ls->key_bits, ls->free_stack, ls->owned,
-                                                         ls->scalars, ls->cap, ctx->d_errword));
+                  VLR_CUDA(ctx, pdl_launch(k_t_finalize<__half>, B, 256, 0, st, (const int*)ls->list_new,
+                                           (const int*)ls->newinfo, ls->list, (const int4*)ls->origin,
+                                           (__half*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
+                                           (const MGridParams*)ls->d_params, ls->key_bits, ls->free_stack,
+                                           (const int*)ls->owned, ls->scalars, ls->cap, ctx->d_errword)));
     else
         VLR_TIMED(ctx, "k_t_finalize",
-                  k_t_finalize<float><<<B, 256, 0, st>>>(ls->list_new, ls->newinfo, ls->list, ls->origin,
-                                                        (float*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
-                                                        ls->d_params, ls->key_bits, ls->free_stack, ls->owned,
-                                                        ls->scalars, ls->cap, ctx->d_errword));
+                  VLR_CUDA(ctx, pdl_launch(k_t_finalize<float>, B, 256, 0, st, (const int*)ls->list_new,
+                                           (const int*)ls->newinfo, ls->list, (const int4*)ls->origin,
+                                           (float*)ls->vals[0], ls->hkey, ls->hval, ls->hcap,
+                                           (const MGridParams*)ls->d_params, ls->key_bits, ls->free_stack,
+                                           (const int*)ls->owned, ls->scalars, ls->cap, ctx->d_errword)));
     VLR_TIMED(ctx, "k_t_nbr",
-              k_t_nbr<<<B, 256, 0, st>>>(ls->list, ls->scalars, ls->origin, ls->hkey, ls->hval, ls->hcap,
-                                         ls->d_params, ls->key_bits, ls->nbr, ls->cap));
+              VLR_CUDA(ctx, pdl_launch(k_t_nbr, B, 256, 0, st, (const int*)ls->list, ls->scalars,
+                                       (const int4*)ls->origin, (const uint64_t*)ls->hkey, (const int*)ls->hval,
+                                       ls->hcap, (const MGridParams*)ls->d_params, ls->key_bits, ls->nbr, ls->cap)));
     VLR_CUDA(ctx, cudaGetLastError());
+    return VLR_OK;
+}
+
+// Persistent grid of a stencil kernel: every SM filled to the occupancy its
+// registers and shared memory allow (dynamic shared memory opted in once).
+template <typename K>
+static int stencil_blocks(vlr_ctx* ctx, K kernel, size_t smem, int* out) {
+    VLR_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
+    if (per_sm < 1) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
+    *out = per_sm * ctx->sm_count;
+    return VLR_OK;
+}
+
+template <typename T, int H, int VK>
+static int launch_advect(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+    const size_t smem = advect_smem_bytes(sizeof(T) == 2, H);
+    if (!ls->adv_blocks) {
+        int rc = stencil_blocks(ctx, k_m_advect<T, H, VK>, smem, &ls->adv_blocks);
+        if (rc) return rc;
+    }
+    VLR_TIMED(ctx, "k_m_advect",
+              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK>, ls->adv_blocks, 256, smem, ctx->stream, A,
+                                       (const T*)ls->vals[0], (T*)ls->vals[1], (const MGridParams*)ls->d_params,
+                                       (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword)));
+    return VLR_OK;
+}
+
+template <typename T, int H>
+static int launch_advect_vk(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+    switch (ls->vel_kind) {
+        case MVEL_CONSTANT: return launch_advect<T, H, MVEL_CONSTANT>(ctx, ls, A, topo);
+        case MVEL_VORTEX: return launch_advect<T, H, MVEL_VORTEX>(ctx, ls, A, topo);
+        case MVEL_CURL: return launch_advect<T, H, MVEL_CURL>(ctx, ls, A, topo);
+        default: return launch_advect<T, H, -1>(ctx, ls, A, topo);
+    }
+}
+
+template <typename T, int NIT>
+static int launch_reinit(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+    const size_t smem = reinit_smem_bytes(sizeof(T) == 2);
+    if (!ls->re_blocks) {
+        int rc = stencil_blocks(ctx, k_m_reinit<T, NIT>, smem, &ls->re_blocks);
+        if (rc) return rc;
+    }
+    VLR_TIMED(ctx, "k_m_reinit",
+              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT>, ls->re_blocks, 256, smem, ctx->stream, A,
+                                       (const T*)ls->vals[1], (T*)ls->vals[0], (const MGridParams*)ls->d_params,
+                                       topo, ctx->d_errword)));
     return VLR_OK;
 }
 
 template <typename T>
 static int enqueue_stencils(vlr_ctx* ctx, vlr_level_set* ls) {
-    cudaStream_t st = ctx->stream;
-    const int B = ls->grid_blocks;
     MLeafArrays A = ls->arrays();
     MTopo topo = topo_of(ls);
-    const T* v0 = (const T*)ls->vals[0];
-    T* v1 = (T*)ls->vals[1];
-    if (ls->halo == 2)
-        VLR_TIMED(ctx, "k_m_advect",
-                  k_m_advect<T, 2><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, topo,
-                                                      ctx->d_errword));
-    else
-        VLR_TIMED(ctx, "k_m_advect",
-                  k_m_advect<T, 3><<<B, 256, 0, st>>>(A, v0, v1, ls->d_params, ls->d_tab, ls->sp, topo,
-                                                      ctx->d_errword));
-    T* w0 = (T*)ls->vals[0];
+    int rc = (ls->halo == 2) ? launch_advect_vk<T, 2>(ctx, ls, A, topo) : launch_advect_vk<T, 3>(ctx, ls, A, topo);
+    if (rc) return rc;
     switch (ls->reinit_iters) {
-        case 0:
-            VLR_TIMED(ctx, "k_m_reinit",
-                      k_m_reinit<T, 0><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
-            break;
-        case 1:
-            VLR_TIMED(ctx, "k_m_reinit",
-                      k_m_reinit<T, 1><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
-            break;
-        default:
-            VLR_TIMED(ctx, "k_m_reinit",
-                      k_m_reinit<T, 2><<<B, 256, 0, st>>>(A, v1, w0, ls->d_params, topo, ctx->d_errword));
-            break;
+        case 0: rc = launch_reinit<T, 0>(ctx, ls, A, topo); break;
+        case 1: rc = launch_reinit<T, 1>(ctx, ls, A, topo); break;
+        default: rc = launch_reinit<T, 2>(ctx, ls, A, topo); break;
     }
+    if (rc) return rc;
     VLR_CUDA(ctx, cudaGetLastError());
     return VLR_OK;
 }
