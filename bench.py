@@ -237,6 +237,9 @@ def time_steps(args, ctx, ls, flush, stream, clock=None, steps=None, warmup=None
 
     steps = steps or args.steps
     warmup = args.warmup if warmup is None else warmup
+    if args.launch_shape:
+        v = [int(x) for x in args.launch_shape.split(",")]
+        ls.set_launch_shape((v[0], v[1]), (v[2], v[3]))
     ls.step(warmup)
     n0, a0, _ = ls.info()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -264,7 +267,7 @@ def time_steps(args, ctx, ls, flush, stream, clock=None, steps=None, warmup=None
     kern = {k: ctx.kernel_time(k) for k in STEP_KERNELS}
     ctx.profile(False)
     return {"ms_per_step": ms, "value": active / (ms * 1e-3), "leaves": leaves, "active": active,
-            "kernels": {k: v[0] / max(v[1], 1) for k, v in kern.items()}, "ls": ls}
+            "kernels": {k: v[0] / max(v[1], 1) for k, v in kern.items()}, "ls": ls, "launch": ls.launch_shape()}
 
 
 def run_method(args, ctx, precision, flush, stream, clock=None):
@@ -412,7 +415,9 @@ def bench_deformation(args, ctx, peak, peak_kind):
                    "cfl": 0.5, "reinit_iters": 2, "leaves": r16["leaves"], "active_voxels": r16["active"],
                    "l2": "flushed between steps (256 MiB write outside the step events)",
                    "step": "advect + 2x Godunov reinit + trim + re-track, one CUDA graph"},
-        "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "kernels_ms": r32["kernels"]},
+        "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "kernels_ms": r32["kernels"],
+                 "launch_shape": r32["launch"]},
+        "launch_shape": r16["launch"],
         "fp16_over_fp32": r16["value"] / r32["value"],
         "roofline": roofline_of(r16, 2, peak, peak_kind, "deformation512"),
         "kernels_ms_per_launch": r16["kernels"],
@@ -531,6 +536,8 @@ def main():
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-grid batched measurement")
+    ap.add_argument("--launch-shape", default="",
+                    help="advect threads,CTAs,reinit threads,CTAs of the stencil kernels (default: autotuned)")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)
@@ -607,7 +614,7 @@ def main():
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("fp32", "fp16_over_fp32", "batched256"):
+        for k in ("fp32", "fp16_over_fp32", "launch_shape", "batched256"):
             if k in res:
                 line[k] = res[k]
         print(json.dumps(line))

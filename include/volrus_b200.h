@@ -203,11 +203,29 @@ int vlr_ls_download_grid(vlr_ctx* ctx, const vlr_level_set* ls, int grid, int32_
                          uint64_t* masks, float* phi, size_t cap_leaves, size_t* n_out);
 
 /* Advance n_steps steps (each one graph replay on the context stream) and
- * wait for them; device-side errors are reported here. */
+ * wait for them; device-side errors are reported here.  The first step of a
+ * level set also chooses the launch shapes of its two stencil kernels (see
+ * vlr_ls_set_launch_shape): it launches each kernel at every candidate shape
+ * on the same inputs, times them and keeps the fastest, which synchronises
+ * the stream; its result is that of an ordinary step. */
 int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
-/* Enqueue n_steps steps on the context stream and return without waiting;
- * vlr_ctx_check() later waits and reports device-side errors. */
+/* Enqueue n_steps steps on the context stream and return without waiting
+ * (apart from the first step's launch tuning); vlr_ctx_check() later waits and
+ * reports device-side errors. */
 int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
+/* Launch shapes of the advect and reinitialisation kernels: threads per CTA
+ * (128 or 256) and persistent CTAs (> 0).  Fixing them turns the first-step
+ * autotuning off; advect_threads = 0 turns it back on for the next step.
+ * Results never depend on the shape.  No counterpart in the reference (its
+ * step is serial Rust). */
+int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int reinit_threads,
+                            int reinit_ctas);
+/* shape[0..3] = advect threads, advect CTAs, reinit threads, reinit CTAs (0
+ * before the first step); *n_timed = candidates the autotuner timed, and if
+ * `log` is non-null, up to cap_log rows of (kernel 0/1, threads, CTAs,
+ * microseconds) for them. */
+int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[4], int* n_timed, float* log,
+                            int cap_log);
 int vlr_ctx_check(vlr_ctx* ctx);
 int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_t* n_active, double* time);
 /* Replace the state of a single-grid level set with host leaves (same layout

@@ -36,7 +36,7 @@ struct MGridParams {
     int tab_lo[3];         // index coordinate of table entry 0 (per axis)
     int tab_len[3];
     int full_series;       // 1: rotation angles may reach 1 rad (full Taylor series); 0: below 0.05 rad
-    int pad_;
+    int doubling;          // curl: dphi[o] = 2^o dphi[0] exactly (rotations by double-angle formulas)
     long long base[3];     // hash key base (leaf coordinates)
 };
 

@@ -190,9 +190,15 @@ int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, co
         MGridParams& P = ls->h_params[g];
         int rc = grid_params(ctx, m, vels[g], bb_lo[g], bb_hi[g], ls->key_bits, P, tab);
         if (rc) return rc;
+        // curl octaves whose table angles double from one octave to the next
+        // rotate by double-angle formulas from octave 0's series
+        P.doubling = (P.vel_kind == MVEL_CURL && P.octaves >= 2) ? 1 : 0;
+        for (int o = 1; o < P.octaves && P.doubling; ++o)
+            if (P.dphi[o] != 2.0f * P.dphi[o - 1]) P.doubling = 0;
         // rotation angles stay below dphi * disp; the short series is exact to f32 below 0.05 rad
         double max_angle = 0.0, gdisp = speed_bound(vels[g]) * m->dt;
-        for (int f = 0; f < kMaxOctaves; ++f) max_angle = std::max(max_angle, std::fabs((double)P.dphi[f]) * gdisp);
+        for (int f = 0; f < (P.doubling ? 1 : kMaxOctaves); ++f)
+            max_angle = std::max(max_angle, std::fabs((double)P.dphi[f]) * gdisp);
         P.full_series = max_angle > 0.05 ? 1 : 0;
     }
     VLR_CUDA(ctx, cudaMalloc(&ls->d_params, sizeof(MGridParams) * n));
@@ -431,6 +437,32 @@ int capture_step(vlr_ctx* ctx, vlr_level_set* ls) {
     return VLR_OK;
 }
 
+void drop_graph(vlr_level_set* ls) {
+    if (ls->graph_exec) cudaGraphExecDestroy(ls->graph_exec);
+    if (ls->graph) cudaGraphDestroy(ls->graph);
+    ls->graph_exec = nullptr;
+    ls->graph = nullptr;
+}
+
+// One step: the autotuning step first (launch shapes not chosen yet, run with
+// the kernel timers paused), then graph replays (direct launches while the
+// per-kernel timers are on).
+int enqueue_one_step(vlr_ctx* ctx, vlr_level_set* ls) {
+    if (ls->autotune && !ls->tuned) {
+        const bool timing = ctx->timer.enabled;
+        ctx->timer.enabled = false;
+        drop_graph(ls);
+        int rc = ls_autotune_step(ctx, ls);
+        ctx->timer.enabled = timing;
+        return rc;
+    }
+    if (ctx->timer.enabled) return ls_enqueue_step(ctx, ls);
+    int rc = capture_step(ctx, ls);
+    if (rc) return rc;
+    VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
+    return VLR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -473,14 +505,8 @@ int vlr_ls_create_from_leaves(vlr_ctx* ctx, const vlr_method_desc* m, const vlr_
 int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
     if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     for (int i = 0; i < n_steps; ++i) {
-        if (ctx->timer.enabled) {
-            int rc = ls_enqueue_step(ctx, ls);
-            if (rc) return rc;
-        } else {
-            int rc = capture_step(ctx, ls);
-            if (rc) return rc;
-            VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
-        }
+        int rc = enqueue_one_step(ctx, ls);
+        if (rc) return rc;
     }
     return VLR_OK;
 }
@@ -494,17 +520,52 @@ int vlr_ctx_check(vlr_ctx* ctx) {
 int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
     if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     for (int i = 0; i < n_steps; ++i) {
-        if (ctx->timer.enabled) {
-            int rc = ls_enqueue_step(ctx, ls);
-            if (rc) return rc;
-        } else {
-            int rc = capture_step(ctx, ls);
-            if (rc) return rc;
-            VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
-        }
+        int rc = enqueue_one_step(ctx, ls);
+        if (rc) return rc;
     }
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return consume_device_errors(ctx, "vlr_ls_step");
+}
+
+int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas,
+                            int reinit_threads, int reinit_ctas) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    drop_graph(ls);
+    if (advect_threads == 0) {
+        ls->autotune = true;
+        ls->tuned = false;
+        return VLR_OK;
+    }
+    auto ok_nt = [](int t) { return t == 128 || t == 256; };
+    if (!ok_nt(advect_threads) || !ok_nt(reinit_threads) || advect_ctas < 1 || reinit_ctas < 1)
+        return set_error(ctx, VLR_ERR_INVALID, "launch shape: threads must be 128 or 256 and CTAs > 0");
+    ls->adv_shape = StencilShape{advect_threads, advect_ctas};
+    ls->re_shape = StencilShape{reinit_threads, reinit_ctas};
+    ls->autotune = false;
+    ls->tuned = true;
+    return VLR_OK;
+}
+
+int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[4], int* n_timed, float* log,
+                            int cap_log) {
+    if (!ctx || !ls || !shape) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    shape[0] = ls->adv_shape.nt;
+    shape[1] = ls->adv_shape.blocks;
+    shape[2] = ls->re_shape.nt;
+    shape[3] = ls->re_shape.blocks;
+    int k = 0;
+    for (int w = 0; w < 2; ++w)
+        for (const TuneEntry& e : ls->tune_log[w]) {
+            if (log && k < cap_log) {
+                log[4 * k] = (float)w;
+                log[4 * k + 1] = (float)e.shape.nt;
+                log[4 * k + 2] = (float)e.shape.blocks;
+                log[4 * k + 3] = e.ms * 1000.0f;
+            }
+            ++k;
+        }
+    if (n_timed) *n_timed = k;
+    return VLR_OK;
 }
 
 int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_t* n_active, double* time) {

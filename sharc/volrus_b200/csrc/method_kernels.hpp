@@ -32,14 +32,16 @@ struct MTopo {
 };
 
 // VK: velocity kind of every grid (MVEL_*), or -1 when a batch mixes kinds.
-template <typename T, int H, int VK>
+// NT: threads per CTA (128 or 256); the result does not depend on NT or on
+// the grid size.
+template <typename T, int H, int VK, int NT>
 __global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
                            MTopo topo, unsigned* __restrict__ err);
 // Dynamic shared memory of the stencil kernels (bytes).
 size_t advect_smem_bytes(int precision_f16, int halo);
 size_t reinit_smem_bytes(int precision_f16);
-template <typename T, int NIT>
+template <typename T, int NIT, int NT>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, MTopo topo, unsigned* __restrict__ err);
 template <typename T>

@@ -7,6 +7,18 @@
 #include "method_kernels.hpp"
 #include "vlr_host.hpp"
 
+// Launch shape of a stencil kernel: threads per CTA and persistent CTAs.
+struct StencilShape {
+    int nt = 0;       // 128 or 256 (0: not chosen)
+    int blocks = 0;   // grid size (CTAs per SM x SMs)
+};
+
+// One timed candidate of the launch autotuner.
+struct TuneEntry {
+    StencilShape shape;
+    float ms;
+};
+
 struct vlr_level_set {
     vlr_ctx* ctx = nullptr;
     int precision = 0;       // VLR_PREC_F32 / VLR_PREC_F16
@@ -54,8 +66,11 @@ struct vlr_level_set {
     cudaGraphExec_t graph_exec = nullptr;
     int grid_blocks = 0;     // persistent grid size of the index and topology kernels
     int vel_kind = -1;       // velocity kind shared by every grid (MVEL_*), -1 if mixed
-    int adv_blocks = 0;      // persistent grid sizes of the stencil kernels (0: not chosen yet)
-    int re_blocks = 0;
+    StencilShape adv_shape;  // launch shapes of the stencil kernels
+    StencilShape re_shape;
+    bool tuned = false;      // shapes chosen (by the autotuner or the caller)
+    bool autotune = true;    // choose the shapes on the first step
+    std::vector<TuneEntry> tune_log[2];  // candidates timed by the autotuner (advect, reinit)
     int scan_levels = 0;
 
     vlr::MLeafArrays arrays() const {
@@ -82,6 +97,10 @@ int ls_enqueue_step(vlr_ctx* ctx, vlr_level_set* ls);
 // Rebuild hash and neighbour table from the list (enqueued).
 int ls_enqueue_index(vlr_ctx* ctx, vlr_level_set* ls);
 int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls);
+// One step whose stencil kernels are launched at every candidate shape (timed,
+// synchronising); keeps the fastest shape of each kernel.  The step's result
+// is the same as ls_enqueue_step's.
+int ls_autotune_step(vlr_ctx* ctx, vlr_level_set* ls);
 // Parameters and velocity tables of n grids (bounding boxes in index units).
 int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* const* vels,
                    const int32_t (*bb_lo)[3], const int32_t (*bb_hi)[3], int n);

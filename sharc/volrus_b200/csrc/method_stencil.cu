@@ -1,5 +1,6 @@
-// The two stencil kernels of the METHOD step.  One CTA (256 threads) works on
-// one 8^3 leaf at a time and strides over the ordered leaf list (persistent).
+// The two stencil kernels of the METHOD step.  One CTA (NT = 128 or 256
+// threads, chosen by the launch autotuner) works on one 8^3 leaf at a time and
+// strides over the ordered leaf list (persistent).
 //
 //   k_m_advect   26-neighbourhood dilation D of the activity mask, then the
 //                semi-Lagrangian backtrace (Euler / RK2 midpoint / SSP-RK3) of
@@ -17,22 +18,24 @@
 // computes leaf i, the copies of leaf i+1 are in flight.  The list entry,
 // origin and neighbour row of the leaves ahead are loaded into registers one
 // or two iterations before they are used, so a leaf costs no dependent global
-// round trip.  The float tile is then built from shared memory.  Measured
-// alternatives: whole-leaf cp.async.bulk copies of the 27 neighbours (one
-// warp issuing 54 bulk copies took ~2,200 cycles per leaf, longer than the
-// leaf's compute) and whole-leaf 16-byte cp.async (8x the bytes the tile
-// needs; the copies' issue took ~2,000 cycles per leaf).
+// round trip.  The float tile is then built from shared memory.
 //
-// Instruction economy (both kernels are issue-bound once latency is hidden):
-// the velocity kind is a template parameter with its constants in registers,
-// dilated voxels are compacted into a list so warps only run backtraces (and
-// the first reinitialisation iteration only the voxels of D), and results
-// leave through shared memory in 16-byte stores.
+// Both kernels are latency- and issue-bound (a leaf moves 2-4 KB but runs a few
+// thousand instructions in phases separated by CTA barriers), so a leaf passes
+// as few barriers as its data flow allows (advect 3, reinit 4), results leave
+// from registers straight to global memory (each warp's stores fall in one
+// leaf), and 128-thread CTAs keep eight leaves in flight per SM.  The first
+// reinitialisation iteration compacts its voxels per warp (ballot + scan), so
+// it needs no CTA barrier of its own.
+//
+// Launch-shape independence: every leaf is computed by one CTA with the same
+// arithmetic whatever NT and the grid size are, and the kernels' side effects
+// on shared per-step state are idempotent (flags set to 1, atomicMin of
+// proposals, clears), so the autotuner may launch a kernel several times on
+// the same inputs within a step and the step's result is unchanged.
 #include "method_kernels.hpp"
 
 namespace vlr {
-
-constexpr int kT = 256;
 
 __device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
 
@@ -40,15 +43,9 @@ __device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Asynchronous global -> shared copy of 4, 8 or 16 bytes (both addresses
-// aligned to the size).
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* dst, const void* src) {
-    if constexpr (BYTES == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES)
-                     : "memory");
+// Asynchronous global -> shared copy of 16 bytes (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -58,10 +55,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Row-packed halo staging of an (8+2H)^2 x (8+2H) tile: tile row (x, y)
 // (local leaf coordinates in [-H, 8+H)) holds the whole z-rows (8 values) of
 // the leaves below, at and above it in z, so element 8 + z is voxel z of the
-// row for z in [-8, 16).  Whole 16-byte rows keep the copies coalesced (a
-// copy per (x, y) row of only the H halo values of the z-neighbours costs one
-// L1 wavefront per lane); only the tile's rows cross from L2, not whole
-// neighbour leaves.
+// row for z in [-8, 16).  Whole 16-byte rows keep the copies coalesced; only
+// the tile's rows cross from L2, not whole neighbour leaves.
 template <typename T, int H>
 struct RowStage {
     static constexpr int E = 8 + 2 * H;
@@ -69,36 +64,70 @@ struct RowStage {
     static constexpr size_t bytes = (size_t)E * E * RP * sizeof(T);
 };
 
-// All threads: start the asynchronous copies of one leaf's tile rows and of
-// the 64-byte masks of its 27 neighbours (masks of absent neighbours are
-// zeroed; rows of absent leaves are left for the tile build to fill).
-// `s_nb` holds the 27 neighbour slots.  Called after a CTA barrier that ended
-// every read of the previous stage; stage_ready() completes it.
+// Copy descriptors of the staged pieces: piece p = (row r, z-piece k) of the
+// row-packed stage, k = 0 / 1 / 2 for the leaves below / at / above in z.
+// They depend only on the piece, so each CTA builds the table once:
+//   bits 0-4   neighbour index d of the leaf that holds the piece
+//   bits 5-13  element offset of the copied 16 bytes within that leaf
+//   bits 14-26 element offset of the destination within the stage
+//   bit 27     a second 16-byte copy follows (f32 rows of the centre z-leaf)
+// For f32 a z-halo piece copies only the 16-byte half that holds the H <= 4
+// values the tile uses (k = 0: z in [8-H, 8), upper half; k = 2: z in [0, H)).
 template <typename T, int H>
-__device__ __forceinline__ void stage_async(const int* s_nb, const T* __restrict__ vals,
-                                            const uint64_t* __restrict__ masks, T* s_rows, uint64_t* s_m) {
+struct StageDesc {
+    static constexpr int E = 8 + 2 * H;
+    static constexpr int NP = E * E * 3;
+};
+
+template <typename T, int H, int NT>
+__device__ __forceinline__ void build_stage_desc(unsigned* s_desc) {
     using R = RowStage<T, H>;
     constexpr int E = R::E, RP = R::RP;
-    constexpr int CPR = 8 * (int)sizeof(T) / 16;  // 16-byte chunks per leaf row
-    for (int r = threadIdx.x; r < E * E; r += kT) {
-        const int x = r / E - H, y = r % E - H;
-        const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
-        const int rowoff = ((x & 7) << 6) | ((y & 7) << 3);
-        T* d = s_rows + r * RP;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int sl = s_nb[base + k];
-            if (sl >= 0) {
-                const T* p = vals + (size_t)sl * kLeafVoxels + rowoff;
-#pragma unroll
-                for (int c = 0; c < CPR; ++c) cp_async<16>(d + 8 * k + c * (16 / sizeof(T)), p + c * (16 / sizeof(T)));
+    constexpr int HALF = 16 / (int)sizeof(T);  // elements in 16 bytes
+    static_assert(E * E * RP < (1 << 13), "stage offset fits 13 bits");
+    for (int p = threadIdx.x; p < StageDesc<T, H>::NP; p += NT) {
+        const int r = p / 3, k = p - 3 * r;
+        const int rx = r / E;
+        const int x = rx - H, y = r - rx * E - H;
+        const unsigned d = (unsigned)(nb_axis(x) * 9 + nb_axis(y) * 3 + k);
+        unsigned goff = (unsigned)(((x & 7) << 6) | ((y & 7) << 3));
+        unsigned soff = (unsigned)(r * RP + 8 * k);
+        unsigned two = 0;
+        if constexpr (sizeof(T) == 4) {
+            if (k == 0) {
+                goff += HALF;
+                soff += HALF;
+            } else if (k == 1) {
+                two = 1;
             }
+        }
+        s_desc[p] = d | (goff << 5) | (soff << 14) | (two << 27);
+    }
+}
+
+// All threads: start the asynchronous copies of one leaf's tile rows and of
+// the 64-byte masks of its 27 neighbours (masks of absent neighbours are
+// zeroed; rows of absent leaves are left for the tile build to fill).  `s_nb`
+// holds the 27 neighbour slots.  Called after a CTA barrier that ended every
+// read of the previous stage; stage_ready() completes it.
+template <typename T, int H, int NT>
+__device__ __forceinline__ void stage_async(const unsigned* s_desc, const int* s_nb, const T* __restrict__ vals,
+                                            const uint64_t* __restrict__ masks, T* s_rows, uint64_t* s_m) {
+    constexpr int HALF = 16 / (int)sizeof(T);
+    for (int p = threadIdx.x; p < StageDesc<T, H>::NP; p += NT) {
+        const unsigned dsc = s_desc[p];
+        const int sl = s_nb[dsc & 31u];
+        if (sl >= 0) {
+            const T* src = vals + (size_t)sl * kLeafVoxels + ((dsc >> 5) & 511u);
+            T* d = s_rows + ((dsc >> 14) & 8191u);
+            cp_async16(d, src);
+            if (sizeof(T) == 4 && (dsc >> 27)) cp_async16(d + HALF, src + HALF);
         }
     }
     if (threadIdx.x < kNbr * 4) {
         const int d = threadIdx.x >> 2, q = threadIdx.x & 3;
         const int sl = s_nb[d];
-        if (sl >= 0) cp_async<16>(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
+        if (sl >= 0) cp_async16(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
         else *reinterpret_cast<uint4*>(s_m + d * 8 + 2 * q) = make_uint4(0u, 0u, 0u, 0u);
     }
     cp_async_commit();
@@ -190,28 +219,13 @@ __device__ __forceinline__ void store_row(float* dst, const float* row) {
     }
 }
 
-template <typename T>
-__device__ __forceinline__ void store_leaf(T* __restrict__ dst, const float* s_out) {
-    if constexpr (sizeof(T) == 2) {
-        if (threadIdx.x < 64) {
-            const float4* q = reinterpret_cast<const float4*>(s_out + 8 * threadIdx.x);
-            float4 a = q[0], b = q[1];
-            __half2 h[4] = {__floats2half2_rn(a.x, a.y), __floats2half2_rn(a.z, a.w), __floats2half2_rn(b.x, b.y),
-                            __floats2half2_rn(b.z, b.w)};
-            *reinterpret_cast<uint4*>(dst + 8 * threadIdx.x) = *reinterpret_cast<uint4*>(h);
-        }
-    } else {
-        if (threadIdx.x < 128)
-            reinterpret_cast<float4*>(dst)[threadIdx.x] = reinterpret_cast<const float4*>(s_out)[threadIdx.x];
-    }
-}
-
 // ------------------------------------------------------------- velocity
 
 // Per-grid velocity constants held in registers for a leaf.
 struct VelConst {
     int kind;
     int octaves;
+    int doubling;                 // curl: octave o's table angle per voxel is 2^o times octave 0's
     float c[3];
     float scale;                  // vortex: vel_scale
     float dphi[kMaxOctaves];
@@ -223,6 +237,7 @@ __device__ __forceinline__ VelConst vel_const(const MGridParams& P) {
     VelConst V;
     V.kind = P.vel_kind;
     V.octaves = P.octaves;
+    V.doubling = P.doubling;
     V.scale = P.vel_scale;
 #pragma unroll
     for (int a = 0; a < 3; ++a) V.c[a] = P.c[a];
@@ -237,11 +252,34 @@ __device__ __forceinline__ VelConst vel_const(const MGridParams& P) {
 }
 
 template <bool FULL>
-__device__ __forceinline__ float2 rotate(float2 t, float d) {
-    float sd, cd;
+__device__ __forceinline__ void series_sincos(float d, float& sd, float& cd) {
     if (FULL) small_sincos(d, sd, cd);
     else tiny_sincos(d, sd, cd);
+}
+
+// (sin, cos) of (table angle - rotation angle) from the table pair and the
+// rotation's sine and cosine.
+__device__ __forceinline__ float2 rot(float2 t, float sd, float cd) {
     return make_float2(t.x * cd + t.y * sd, t.y * cd - t.x * sd);
+}
+
+template <bool FULL>
+__device__ __forceinline__ float2 rotate(float2 t, float d) {
+    float sd, cd;
+    series_sincos<FULL>(d, sd, cd);
+    return rot(t, sd, cd);
+}
+
+// Curl-noise octave o's contribution grad f_o x e_o, from its rotated
+// (sin, cos) pairs per axis.
+__device__ __forceinline__ void curl_octave(const VelConst& V, int o, float2 X, float2 Y, float2 Z, float3& u) {
+    // grad f_o = a (cos x sin y sin z, sin x cos y sin z, sin x sin y cos z); v += grad f_o x e_o
+    const float a = V.ak[o];
+    const float syz = Y.x * Z.x, sxa = a * X.x;
+    const float gx = a * X.y * syz, gy = sxa * Y.y * Z.x, gz = sxa * Y.x * Z.y;
+    u.x += gy * V.e[o][2] - gz * V.e[o][1];
+    u.y += gz * V.e[o][0] - gx * V.e[o][2];
+    u.z += gx * V.e[o][1] - gy * V.e[o][0];
 }
 
 // Velocity (voxels per unit time) at local voxel (lx, ly, lz) + offset, from
@@ -266,6 +304,31 @@ __device__ __forceinline__ float3 leaf_velocity(const VelConst& V, const float2 
                            -4.0f * k * sxcx * sycy * Z.x * Z.x);
     }
     float3 u = make_float3(0.f, 0.f, 0.f);
+    if (kOff && V.doubling) {
+        // octave o rotates by 2^o times octave 0's angle: one series per axis,
+        // then the double-angle formulas sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a
+        float sx, cx, sy, cy, sz, cz;
+        series_sincos<FULL>(V.dphi[0] * ox, sx, cx);
+        series_sincos<FULL>(V.dphi[0] * oy, sy, cy);
+        series_sincos<FULL>(V.dphi[0] * oz, sz, cz);
+#pragma unroll
+        for (int o = 0; o < kMaxOctaves; ++o) {
+            if (o < V.octaves) {
+                curl_octave(V, o, rot(tab[o][0][lx], sx, cx), rot(tab[o][1][ly], sy, cy), rot(tab[o][2][lz], sz, cz),
+                            u);
+                float t = sx + sx;
+                sx = t * cx;
+                cx = 1.0f - t * (t * 0.5f);
+                t = sy + sy;
+                sy = t * cy;
+                cy = 1.0f - t * (t * 0.5f);
+                t = sz + sz;
+                sz = t * cz;
+                cz = 1.0f - t * (t * 0.5f);
+            }
+        }
+        return u;
+    }
 #pragma unroll
     for (int o = 0; o < kMaxOctaves; ++o) {
         if (o < V.octaves) {
@@ -275,25 +338,20 @@ __device__ __forceinline__ float3 leaf_velocity(const VelConst& V, const float2 
                 Y = rotate<FULL>(Y, V.dphi[o] * oy);
                 Z = rotate<FULL>(Z, V.dphi[o] * oz);
             }
-            // grad f_o = a (cos x sin y sin z, sin x cos y sin z, sin x sin y cos z); v += grad f_o x e_o
-            const float a = V.ak[o];
-            const float syz = Y.x * Z.x, sxa = a * X.x;
-            const float gx = a * X.y * syz, gy = sxa * Y.y * Z.x, gz = sxa * Y.x * Z.y;
-            u.x += gy * V.e[o][2] - gz * V.e[o][1];
-            u.y += gz * V.e[o][0] - gx * V.e[o][2];
-            u.z += gx * V.e[o][1] - gy * V.e[o][0];
+            curl_octave(V, o, X, Y, Z, u);
         }
     }
     return u;
 }
 
-// Backtrace and trilinear sample of the compacted voxels of D.
-template <int VK, bool FULL, int H>
+// Backtrace and trilinear sample of the compacted voxels of D; each result is
+// stored straight to the leaf's values in global memory.
+template <typename T, int VK, bool FULL, int H, int NT>
 __device__ __forceinline__ void advect_voxels(const VelConst& V, const float2 (*s_tab)[3][8], const unsigned short* s_list,
-                                              int nD, const float* s_tile, float* s_out, float dt, int integrator,
-                                              float ct1, float ct2, float ct3, unsigned& bad) {
+                                              int nD, const float* s_tile, T* __restrict__ out, float dt,
+                                              int integrator, float ct1, float ct2, float ct3, unsigned& bad) {
     constexpr int E = 8 + 2 * H;
-    for (int i = threadIdx.x; i < nD; i += kT) {
+    for (int i = threadIdx.x; i < nD; i += NT) {
         const int off = s_list[i];
         const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
         float fx, fy, fz;
@@ -338,7 +396,7 @@ __device__ __forceinline__ void advect_voxels(const VelConst& V, const float2 (*
         const float c00 = c000 * (1.f - wx) + c100 * wx, c01 = c001 * (1.f - wx) + c101 * wx;
         const float c10 = c010 * (1.f - wx) + c110 * wx, c11 = c011 * (1.f - wx) + c111 * wx;
         const float c0 = c00 * (1.f - wy) + c10 * wy, c1 = c01 * (1.f - wy) + c11 * wy;
-        s_out[off] = c0 * (1.f - wz) + c1 * wz;
+        out[off] = from_f<T>(c0 * (1.f - wz) + c1 * wz);
     }
 }
 
@@ -349,20 +407,22 @@ struct AdvectSmem {
     static constexpr size_t raw = RowStage<T, H>::bytes;
     static constexpr size_t masks = (size_t)kNbr * 64;
     static constexpr size_t tile = (size_t)E * E * E * 4;
-    static constexpr size_t out = (size_t)kLeafVoxels * 4;
-    static constexpr size_t bytes = raw + masks + tile + out;
+    static constexpr size_t bytes = raw + masks + tile;
 };
 
 // --------------------------------------------------------------- advect
 
-template <typename T, int H, int VK>
-__global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                                                const MGridParams* __restrict__ params, const float2* __restrict__ tab,
-                                                MStepParams sp, MTopo topo, unsigned* __restrict__ err) {
+template <typename T, int H, int VK, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const T* __restrict__ src,
+                                                           T* __restrict__ dst, const MGridParams* __restrict__ params,
+                                                           const float2* __restrict__ tab, MStepParams sp, MTopo topo,
+                                                           unsigned* __restrict__ err) {
+    static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
+    constexpr int VPT = kLeafVoxels / NT;  // voxels per thread in whole-leaf passes
     dep_wait();
     dep_launch();
     // clear this step's re-tracking state (keep flags, proposal table, leaf hash)
-    for (int i = blockIdx.x * kT + threadIdx.x; i < max(topo.cap, topo.hcap); i += gridDim.x * kT) {
+    for (int i = blockIdx.x * NT + threadIdx.x; i < max(topo.cap, topo.hcap); i += gridDim.x * NT) {
         if (i < topo.cap) topo.keep[i] = 0;
         if (i < topo.hcap) {
             topo.pkey[i] = kEmptyKey;
@@ -379,16 +439,17 @@ __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __re
     constexpr int E = L::E;
     constexpr int NROW = E * E;
     constexpr int NTAB = kMaxOctaves * 3 * 8;
+    static_assert(NTAB <= NT, "one table entry per thread");
     extern __shared__ __align__(128) unsigned char smem[];
     T* s_raw = reinterpret_cast<T*>(smem);
     uint64_t* s_m = reinterpret_cast<uint64_t*>(smem + L::raw);
     float* s_tile = reinterpret_cast<float*>(smem + L::raw + L::masks);
-    float* s_out = reinterpret_cast<float*>(smem + L::raw + L::masks + L::tile);
-    __shared__ __align__(16) uint64_t s_D[2][8];
+    __shared__ __align__(16) uint64_t s_D[8];
     __shared__ int s_nbr[2][32];
     __shared__ unsigned short s_list[kLeafVoxels];
     __shared__ __align__(16) MGridParams s_P;
     __shared__ float2 s_tab[kMaxOctaves][3][8];
+    __shared__ unsigned s_desc[StageDesc<T, H>::NP];
 
     const int count = *A.count;
     const int G = gridDim.x;
@@ -404,9 +465,10 @@ __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __re
     // prologue: first leaf staged, next leaf's list entry in flight
     int slot = A.list[li];
     int4 o = A.origin[slot];
+    build_stage_desc<T, H, NT>(s_desc);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
     __syncthreads();
-    stage_async<T, H>(s_nbr[0], src, A.mask, s_raw, s_m);
+    stage_async<T, H, NT>(s_desc, s_nbr[0], src, A.mask, s_raw, s_m);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
 
     int cur_gid = -1;
@@ -451,67 +513,81 @@ __global__ void __launch_bounds__(kT, 4) k_m_advect(MLeafArrays A, const T* __re
                 tvalid = true;
             }
         }
-        stage_ready();
+        stage_ready();  // barrier 1: this leaf's rows and masks are in shared memory
         const int* nbr = s_nbr[cur];
-        for (int t = threadIdx.x; t < NROW + 64; t += kT) {  // one pass for H = 2
-          if (t < NROW) {
-            float row[E];
-            build_row<T, H, false>(s_raw, nbr, t / E - H, t % E - H, hw, row);
-            store_row<E>(s_tile + t * E, row);
-          } else {
-            // dilation: one thread per z-row, 10-bit rows z = -1..8
-            const int r = t - NROW;
-            const int x = r >> 3, y = r & 7;
-            unsigned acc = 0;
-            const unsigned char* m = (const unsigned char*)s_m;
+        for (int t = threadIdx.x; t < NROW + 64; t += NT) {
+            if (t < NROW) {
+                float row[E];
+                build_row<T, H, false>(s_raw, nbr, t / E - H, t % E - H, hw, row);
+                store_row<E>(s_tile + t * E, row);
+            } else {
+                // dilation: one thread per z-row, 10-bit rows z = -1..8
+                const int r = t - NROW;
+                const int x = r >> 3, y = r & 7;
+                unsigned acc = 0;
+                const unsigned char* m = (const unsigned char*)s_m;
 #pragma unroll
-            for (int dx = -1; dx <= 1; ++dx)
+                for (int dx = -1; dx <= 1; ++dx)
 #pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int xx = x + dx, yy = y + dy;
-                    const int base = nb_axis(xx) * 9 + nb_axis(yy) * 3;
-                    const int bi = ((xx & 7) << 3) | (yy & 7);
-                    acc |= ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
-                           (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
-                }
-            ((unsigned char*)s_D[cur])[r] = (unsigned char)(((acc | (acc << 1) | (acc >> 1)) >> 1) & 0xffu);
-          }
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const int xx = x + dx, yy = y + dy;
+                        const int base = nb_axis(xx) * 9 + nb_axis(yy) * 3;
+                        const int bi = ((xx & 7) << 3) | (yy & 7);
+                        acc |= ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
+                               (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
+                    }
+                ((unsigned char*)s_D)[r] = (unsigned char)(((acc | (acc << 1) | (acc >> 1)) >> 1) & 0xffu);
+            }
         }
         if (w0) s_nbr[cur ^ 1][lane] = nb_n;
-        __syncthreads();
-        // the staging buffers are free: stage the next leaf
-        if (slot_n >= 0) stage_async<T, H>(s_nbr[cur ^ 1], src, A.mask, s_raw, s_m);
+        __syncthreads();  // barrier 2: tile and D are built; the staging buffers are free
+        if (slot_n >= 0) stage_async<T, H, NT>(s_desc, s_nbr[cur ^ 1], src, A.mask, s_raw, s_m);
         if (tvalid) (&s_tab[0][0][0])[threadIdx.x] = tv;
-        // compact D; voxels outside D keep the sign of their previous value
-        int nD = 0, pre = 0;
-        const int w = threadIdx.x >> 5;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int c = __popcll(s_D[cur][q]);
-            if (q < w) pre += c;
-            nD += c;
-        }
+        // compact D; voxels outside D keep the sign of their previous value and
+        // are stored here
+        T* out = dst + (size_t)slot * kLeafVoxels;
+        int nD, pre_w[8 / (NT / 32)];
         {
-            const uint64_t word = s_D[cur][w];
+            // prefix of the popcounts of the 8 words of D (x planes) over lanes 0..7
+            const int c = (lane < 8) ? __popcll(s_D[lane]) : 0;
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 8; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            nD = __shfl_sync(0xffffffffu, incl, 7);
+#pragma unroll
+            for (int j = 0; j < 8 / (NT / 32); ++j) {
+                const int q = (threadIdx.x >> 5) + (NT / 32) * j;
+                pre_w[j] = __shfl_sync(0xffffffffu, incl - c, q);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 8 / (NT / 32); ++j) {
+            // warp w compacts words w, w + NW, ...: lane l handles bits l and l + 32
+            const int q = (threadIdx.x >> 5) + (NT / 32) * j;
+            const uint64_t word = s_D[q];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int bit = lane + 32 * h;
-                const int off = w * 64 + bit;
-                const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
-                if ((word >> bit) & 1ull)
-                    s_list[pre + __popcll(word & ((1ull << bit) - 1ull))] = (unsigned short)off;
-                else
-                    s_out[off] = copysignf(hw, s_tile[((x + H) * E + (y + H)) * E + (z + H)]);
+                const int off = q * 64 + bit;
+                if ((word >> bit) & 1ull) {
+                    s_list[pre_w[j] + __popcll(word & ((1ull << bit) - 1ull))] = (unsigned short)off;
+                } else {
+                    const int y = (off >> 3) & 7, z = off & 7;
+                    out[off] = from_f<T>(copysignf(hw, s_tile[((q + H) * E + (y + H)) * E + (z + H)]));
+                }
             }
         }
-        __syncthreads();
+        __syncthreads();  // barrier 3: list and velocity tables are ready
         if (fullser)
-            advect_voxels<VK, true, H>(V, s_tab, s_list, nD, s_tile, s_out, dt, sp.integrator, ct1, ct2, ct3, bad);
+            advect_voxels<T, VK, true, H, NT>(V, s_tab, s_list, nD, s_tile, out, dt, sp.integrator, ct1, ct2, ct3,
+                                              bad);
         else
-            advect_voxels<VK, false, H>(V, s_tab, s_list, nD, s_tile, s_out, dt, sp.integrator, ct1, ct2, ct3, bad);
-        __syncthreads();
-        store_leaf<T>(dst + (size_t)slot * kLeafVoxels, s_out);
-        if (threadIdx.x < 8) A.dmask[(size_t)slot * 8 + threadIdx.x] = s_D[cur][threadIdx.x];
+            advect_voxels<T, VK, false, H, NT>(V, s_tab, s_list, nD, s_tile, out, dt, sp.integrator, ct1, ct2, ct3,
+                                               bad);
+        if (threadIdx.x < 8) A.dmask[(size_t)slot * 8 + threadIdx.x] = s_D[threadIdx.x];
         if (slot_n < 0) break;
         li += G;
         slot = slot_n;
@@ -550,50 +626,55 @@ __device__ __forceinline__ float reinit_update(const float* c, float p, float s,
     return p - 0.5f * s * (G - 1.0f);
 }
 
+
 template <typename T>
 struct ReinitSmem {
     static constexpr size_t raw = RowStage<T, 2>::bytes;
     static constexpr size_t masks = (size_t)kNbr * 64;
     static constexpr size_t p1 = 12 * 12 * 12 * 4;  // phi1 tile: leaf + 2-voxel ring
     static constexpr size_t p2 = 10 * 10 * 10 * 4;  // phi2 tile: leaf + 1-voxel ring
-    static constexpr size_t out = (size_t)kLeafVoxels * 4;
-    static constexpr size_t bytes = raw + masks + p1 + p2 + out;
+    static constexpr size_t bytes = raw + masks + p1 + p2;
 };
 
-template <typename T, int NIT>
-__global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                                                   const MGridParams* __restrict__ params, MTopo topo,
-                                                   unsigned* __restrict__ err) {
+template <typename T, int NIT, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const T* __restrict__ src,
+                                                           T* __restrict__ dst, const MGridParams* __restrict__ params,
+                                                           MTopo topo, unsigned* __restrict__ err) {
+    static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     dep_wait();
     dep_launch();
     constexpr int E = 12;  // phi1 tile: leaf + 2-voxel ring
     constexpr int F = 10;  // phi2 tile and D rows: leaf + 1-voxel ring
+    constexpr int NW = NT / 32;
+    constexpr int VPT = kLeafVoxels / NT;
+    constexpr int RPW = (F * F + NW - 1) / NW;  // D rows per warp (rows r = lane * NW + warp)
+    static_assert(32 * NW >= F * F, "one D row per lane");
     using L = ReinitSmem<T>;
     extern __shared__ __align__(128) unsigned char smem[];
     T* s_raw = reinterpret_cast<T*>(smem);
     uint64_t* s_dm = reinterpret_cast<uint64_t*>(smem + L::raw);
     float* s_p1 = reinterpret_cast<float*>(smem + L::raw + L::masks);
     float* s_p2 = reinterpret_cast<float*>(smem + L::raw + L::masks + L::p1);
-    float* s_out = reinterpret_cast<float*>(smem + L::raw + L::masks + L::p1 + L::p2);
     __shared__ unsigned short s_D[F * F];
-    __shared__ unsigned short s_list[F * F * F];
-    __shared__ int s_rowpre[F * F];
-    __shared__ int s_wsum[4];
+    __shared__ unsigned short s_list[NW][RPW * F];
     __shared__ int s_nbr[2][32];
     __shared__ __align__(16) unsigned s_M[16];
+    __shared__ unsigned s_desc[StageDesc<T, 2>::NP];
 
     const int count = *A.count;
     const int G = gridDim.x;
     int li = blockIdx.x;
     if (li >= count) return;
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const bool w0 = threadIdx.x < 32;
 
     int slot = A.list[li];
     int4 o = A.origin[slot];
+    build_stage_desc<T, 2, NT>(s_desc);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
     __syncthreads();
-    stage_async<T, 2>(s_nbr[0], src, A.dmask, s_raw, s_dm);
+    stage_async<T, 2, NT>(s_desc, s_nbr[0], src, A.dmask, s_raw, s_dm);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
     float hw = params[o.w].hw;
 
@@ -603,9 +684,9 @@ __global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __re
         if (slot_n >= 0) o_n = A.origin[slot_n];
         const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[slot_n * kNbr + lane] : -1;
         const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
-        stage_ready();
+        stage_ready();  // barrier 1
         const int* nbr = s_nbr[cur];
-        for (int t = threadIdx.x; t < E * E + F * F; t += kT) {
+        for (int t = threadIdx.x; t < E * E + F * F; t += NT) {
             if (t < E * E) {
                 float row[E];
                 const int x = t / E - 2, y = t % E - 2;
@@ -626,55 +707,46 @@ __global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __re
                 const unsigned row = ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
                                      (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
                 s_D[r] = (unsigned short)row;
-                if (NIT == 2) s_rowpre[r] = __popc(row);
             }
         }
         if (w0) s_nbr[cur ^ 1][lane] = nb_n;
-        __syncthreads();
-        if (slot_n >= 0) stage_async<T, 2>(s_nbr[cur ^ 1], src, A.dmask, s_raw, s_dm);
+        __syncthreads();  // barrier 2: tiles and D rows built; staging buffers free
+        if (slot_n >= 0) stage_async<T, 2, NT>(s_desc, s_nbr[cur ^ 1], src, A.dmask, s_raw, s_dm);
         if (NIT == 2) {
-            // compact the voxels of D in the 10^3 box (row-major (x, y, z))
-            int nD = 0;
-            {
-                const int w = threadIdx.x >> 5;
-                int v = (threadIdx.x < F * F) ? s_rowpre[threadIdx.x] : 0, x = v;
+            // iteration 1 on the voxels of D in the 10^3 box, compacted per warp:
+            // lane l of warp w owns D row r = l * NW + w
+            const int r = lane * NW + warp;
+            unsigned row = (r < F * F) ? s_D[r] : 0u;
+            const int c = __popc(row);
+            int incl = c;
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, x, off);
-                    if (lane >= off) x += y;
-                }
-                if (w < 4 && lane == 31) s_wsum[w] = x;
-                __syncthreads();
-                int wpre = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (q < w) wpre += s_wsum[q];
-                    nD += s_wsum[q];
-                }
-                if (threadIdx.x < F * F) {
-                    int pos = wpre + x - v;
-                    unsigned row = s_D[threadIdx.x];
-                    while (row) {
-                        const int z = __ffs(row) - 1;
-                        row &= row - 1u;
-                        s_list[pos++] = (unsigned short)(threadIdx.x * F + z);
-                    }
-                }
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
             }
-            __syncthreads();
-            for (int i = threadIdx.x; i < nD; i += kT) {
-                const int t = s_list[i];
+            const int nW = __shfl_sync(0xffffffffu, incl, 31);
+            int pos = incl - c;
+            unsigned short* wl = s_list[warp];
+            while (row) {
+                const int z = __ffs(row) - 1;
+                row &= row - 1u;
+                wl[pos++] = (unsigned short)(r * F + z);
+            }
+            __syncwarp();
+            for (int i = lane; i < nW; i += 32) {
+                const int t = wl[i];
                 const int xr = t / (F * F), yr = (t / F) % F, zr = t % F;
-                const float* c = &s_p1[((xr + 1) * E + (yr + 1)) * E + (zr + 1)];
-                const float p = c[0];
-                s_p2[t] = reinit_update<E>(c, p, p * rsqrtf(p * p + 1.0f), hw);
+                const float* c1 = &s_p1[((xr + 1) * E + (yr + 1)) * E + (zr + 1)];
+                const float p = c1[0];
+                s_p2[t] = reinit_update<E>(c1, p, p * rsqrtf(p * p + 1.0f), hw);
             }
-            __syncthreads();
+            __syncthreads();  // barrier 3: phi2 complete on the 10^3 box
         }
+        T* out = dst + (size_t)slot * kLeafVoxels;
         bool any = false;
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int off = threadIdx.x + kT * r;
+        for (int r = 0; r < VPT; ++r) {
+            const int off = threadIdx.x + NT * r;
             const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
             const bool inD = (s_D[(x + 1) * F + (y + 1)] >> (z + 1)) & 1u;
             const float* c1 = &s_p1[((x + 2) * E + (y + 2)) * E + (z + 2)];
@@ -691,13 +763,12 @@ __global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __re
             }
             const bool on = inD && fabsf(v) < hw;
             if (!on) v = copysignf(hw, v);
-            s_out[off] = v;
+            out[off] = from_f<T>(v);
             const unsigned b = __ballot_sync(0xffffffffu, on);
             if (lane == 0) s_M[off >> 5] = b;
             any |= on;
         }
-        __syncthreads();
-        store_leaf<T>(dst + (size_t)slot * kLeafVoxels, s_out);
+        __syncthreads();  // barrier 4: the new mask words are in shared memory
         if (threadIdx.x < 16) reinterpret_cast<unsigned*>(A.mask + (size_t)slot * 8)[threadIdx.x] = s_M[threadIdx.x];
         if (threadIdx.x >= 32 && threadIdx.x < 64) {
             // spill mask from 64-bit (x*8+y) plane masks of z = 0, z = 7 and any z
@@ -766,19 +837,21 @@ __global__ void __launch_bounds__(kT, 4) k_m_reinit(MLeafArrays A, const T* __re
     }
 }
 
-#define VLR_INST_ADVECT(T, H)                                                                                    \
-    template __global__ void k_m_advect<T, H, -1>(MLeafArrays, const T*, T*, const MGridParams*, const float2*,    \
-                                                  MStepParams, MTopo, unsigned*);                                \
-    template __global__ void k_m_advect<T, H, MVEL_CONSTANT>(MLeafArrays, const T*, T*, const MGridParams*,        \
-                                                             const float2*, MStepParams, MTopo, unsigned*);      \
-    template __global__ void k_m_advect<T, H, MVEL_VORTEX>(MLeafArrays, const T*, T*, const MGridParams*,          \
-                                                           const float2*, MStepParams, MTopo, unsigned*);        \
-    template __global__ void k_m_advect<T, H, MVEL_CURL>(MLeafArrays, const T*, T*, const MGridParams*,            \
-                                                         const float2*, MStepParams, MTopo, unsigned*);
-#define VLR_INST_REINIT(T)                                                                                       \
-    template __global__ void k_m_reinit<T, 0>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);    \
-    template __global__ void k_m_reinit<T, 1>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);    \
-    template __global__ void k_m_reinit<T, 2>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);
+#define VLR_INST_ADVECT_NT(T, H, NT)                                                                               \
+    template __global__ void k_m_advect<T, H, -1, NT>(MLeafArrays, const T*, T*, const MGridParams*,               \
+                                                      const float2*, MStepParams, MTopo, unsigned*);               \
+    template __global__ void k_m_advect<T, H, MVEL_CONSTANT, NT>(MLeafArrays, const T*, T*, const MGridParams*,    \
+                                                                 const float2*, MStepParams, MTopo, unsigned*);    \
+    template __global__ void k_m_advect<T, H, MVEL_VORTEX, NT>(MLeafArrays, const T*, T*, const MGridParams*,      \
+                                                               const float2*, MStepParams, MTopo, unsigned*);      \
+    template __global__ void k_m_advect<T, H, MVEL_CURL, NT>(MLeafArrays, const T*, T*, const MGridParams*,        \
+                                                             const float2*, MStepParams, MTopo, unsigned*);
+#define VLR_INST_ADVECT(T, H) VLR_INST_ADVECT_NT(T, H, 128) VLR_INST_ADVECT_NT(T, H, 256)
+#define VLR_INST_REINIT_NT(T, NT)                                                                                  \
+    template __global__ void k_m_reinit<T, 0, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*); \
+    template __global__ void k_m_reinit<T, 1, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*); \
+    template __global__ void k_m_reinit<T, 2, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);
+#define VLR_INST_REINIT(T) VLR_INST_REINIT_NT(T, 128) VLR_INST_REINIT_NT(T, 256)
 VLR_INST_ADVECT(float, 2)
 VLR_INST_ADVECT(float, 3)
 VLR_INST_ADVECT(__half, 2)

@@ -405,70 +405,212 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
     return VLR_OK;
 }
 
-// Persistent grid of a stencil kernel: every SM filled to the occupancy its
-// registers and shared memory allow (dynamic shared memory opted in once).
-template <typename K>
-static int stencil_blocks(vlr_ctx* ctx, K kernel, size_t smem, int* out) {
-    VLR_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
-    if (per_sm < 1) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
-    *out = per_sm * ctx->sm_count;
-    return VLR_OK;
-}
+// ------------------------------------------------------ stencil launches
 
-template <typename T, int H, int VK>
-static int launch_advect(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+// The launch shape of a stencil kernel (threads per CTA, persistent CTAs per
+// SM) is chosen by ls_autotune_step; until then the kernels run at 256
+// threads with every SM filled to the occupancy limit.
+template <typename T, int H, int VK, int NT>
+static int launch_advect_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
     const size_t smem = advect_smem_bytes(sizeof(T) == 2, H);
-    if (!ls->adv_blocks) {
-        int rc = stencil_blocks(ctx, k_m_advect<T, H, VK>, smem, &ls->adv_blocks);
-        if (rc) return rc;
-    }
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, H, VK, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
     VLR_TIMED(ctx, "k_m_advect",
-              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK>, ls->adv_blocks, 256, smem, ctx->stream, A,
+              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK, NT>, blocks, NT, smem, ctx->stream, A,
                                        (const T*)ls->vals[0], (T*)ls->vals[1], (const MGridParams*)ls->d_params,
                                        (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword)));
     return VLR_OK;
 }
 
+template <typename T, int H, int VK>
+static int launch_advect_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
+                               StencilShape sh) {
+    return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128>(ctx, ls, A, topo, sh.blocks)
+                        : launch_advect_nt<T, H, VK, 256>(ctx, ls, A, topo, sh.blocks);
+}
+
 template <typename T, int H>
-static int launch_advect_vk(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+static int launch_advect_vk(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
+                            StencilShape sh) {
     switch (ls->vel_kind) {
-        case MVEL_CONSTANT: return launch_advect<T, H, MVEL_CONSTANT>(ctx, ls, A, topo);
-        case MVEL_VORTEX: return launch_advect<T, H, MVEL_VORTEX>(ctx, ls, A, topo);
-        case MVEL_CURL: return launch_advect<T, H, MVEL_CURL>(ctx, ls, A, topo);
-        default: return launch_advect<T, H, -1>(ctx, ls, A, topo);
+        case MVEL_CONSTANT: return launch_advect_shape<T, H, MVEL_CONSTANT>(ctx, ls, A, topo, sh);
+        case MVEL_VORTEX: return launch_advect_shape<T, H, MVEL_VORTEX>(ctx, ls, A, topo, sh);
+        case MVEL_CURL: return launch_advect_shape<T, H, MVEL_CURL>(ctx, ls, A, topo, sh);
+        default: return launch_advect_shape<T, H, -1>(ctx, ls, A, topo, sh);
     }
 }
 
-template <typename T, int NIT>
-static int launch_reinit(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo) {
+template <typename T>
+static int launch_advect(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
+    MLeafArrays A = ls->arrays();
+    MTopo topo = topo_of(ls);
+    return ls->halo == 2 ? launch_advect_vk<T, 2>(ctx, ls, A, topo, sh) : launch_advect_vk<T, 3>(ctx, ls, A, topo, sh);
+}
+
+template <typename T, int NIT, int NT>
+static int launch_reinit_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
     const size_t smem = reinit_smem_bytes(sizeof(T) == 2);
-    if (!ls->re_blocks) {
-        int rc = stencil_blocks(ctx, k_m_reinit<T, NIT>, smem, &ls->re_blocks);
-        if (rc) return rc;
-    }
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, NIT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
     VLR_TIMED(ctx, "k_m_reinit",
-              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT>, ls->re_blocks, 256, smem, ctx->stream, A,
+              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, NT>, blocks, NT, smem, ctx->stream, A,
                                        (const T*)ls->vals[1], (T*)ls->vals[0], (const MGridParams*)ls->d_params,
                                        topo, ctx->d_errword)));
     return VLR_OK;
 }
 
+template <typename T, int NIT>
+static int launch_reinit_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
+                               StencilShape sh) {
+    return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128>(ctx, ls, A, topo, sh.blocks)
+                        : launch_reinit_nt<T, NIT, 256>(ctx, ls, A, topo, sh.blocks);
+}
+
 template <typename T>
-static int enqueue_stencils(vlr_ctx* ctx, vlr_level_set* ls) {
+static int launch_reinit(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
     MLeafArrays A = ls->arrays();
     MTopo topo = topo_of(ls);
-    int rc = (ls->halo == 2) ? launch_advect_vk<T, 2>(ctx, ls, A, topo) : launch_advect_vk<T, 3>(ctx, ls, A, topo);
-    if (rc) return rc;
     switch (ls->reinit_iters) {
-        case 0: rc = launch_reinit<T, 0>(ctx, ls, A, topo); break;
-        case 1: rc = launch_reinit<T, 1>(ctx, ls, A, topo); break;
-        default: rc = launch_reinit<T, 2>(ctx, ls, A, topo); break;
+        case 0: return launch_reinit_shape<T, 0>(ctx, ls, A, topo, sh);
+        case 1: return launch_reinit_shape<T, 1>(ctx, ls, A, topo, sh);
+        default: return launch_reinit_shape<T, 2>(ctx, ls, A, topo, sh);
     }
+}
+
+// Occupancy limit (CTAs per SM) of the stencil kernel of `which` (0 advect,
+// 1 reinit) at NT threads.
+template <typename T, int NT>
+static int stencil_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int which, int* per_sm) {
+    *per_sm = 0;
+    if (which == 0) {
+        const size_t smem = advect_smem_bytes(sizeof(T) == 2, ls->halo);
+        // every velocity kind instantiates the same staging and tile, so the
+        // constant-velocity kernel stands for the register and smem footprint
+        if (ls->halo == 2) {
+            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 2, -1, NT>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 2, -1, NT>, NT, smem));
+        } else {
+            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 3, -1, NT>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 3, -1, NT>, NT, smem));
+        }
+    } else {
+        const size_t smem = reinit_smem_bytes(sizeof(T) == 2);
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, NT>, NT, smem));
+    }
+    return VLR_OK;
+}
+
+template <typename T>
+static int stencil_candidates(vlr_ctx* ctx, vlr_level_set* ls, int which, std::vector<StencilShape>& out) {
+    out.clear();
+    for (int nt : {128, 256}) {
+        int occ = 0;
+        int rc = nt == 128 ? stencil_occupancy<T, 128>(ctx, ls, which, &occ)
+                           : stencil_occupancy<T, 256>(ctx, ls, which, &occ);
+        if (rc) return rc;
+        if (occ < 1) continue;
+        int prev = -1;
+        for (int per_sm : {occ, (3 * occ + 3) / 4, (occ + 1) / 2}) {
+            if (per_sm < 1 || per_sm == prev) continue;
+            prev = per_sm;
+            out.push_back(StencilShape{nt, per_sm * ctx->sm_count});
+        }
+    }
+    if (out.empty()) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
+    return VLR_OK;
+}
+
+// The shape used when none has been chosen: 256 threads, occupancy-limited.
+template <typename T>
+static int default_shape(vlr_ctx* ctx, vlr_level_set* ls, int which, StencilShape* sh) {
+    int occ = 0;
+    int rc = stencil_occupancy<T, 256>(ctx, ls, which, &occ);
+    if (rc) return rc;
+    if (occ < 1) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
+    *sh = StencilShape{256, occ * ctx->sm_count};
+    return VLR_OK;
+}
+
+template <typename T>
+static int enqueue_stencils(vlr_ctx* ctx, vlr_level_set* ls) {
+    if (!ls->adv_shape.nt) {
+        int rc = default_shape<T>(ctx, ls, 0, &ls->adv_shape);
+        if (rc) return rc;
+    }
+    if (!ls->re_shape.nt) {
+        int rc = default_shape<T>(ctx, ls, 1, &ls->re_shape);
+        if (rc) return rc;
+    }
+    int rc = launch_advect<T>(ctx, ls, ls->adv_shape);
+    if (rc) return rc;
+    rc = launch_reinit<T>(ctx, ls, ls->re_shape);
     if (rc) return rc;
     VLR_CUDA(ctx, cudaGetLastError());
     return VLR_OK;
+}
+
+// Times every candidate shape of one stencil kernel on the current inputs
+// (two rounds; the second round's time counts, so the first round warms the
+// caches for all candidates alike) and keeps the fastest.
+template <typename T>
+static int tune_one(vlr_ctx* ctx, vlr_level_set* ls, int which, StencilShape* best) {
+    std::vector<StencilShape> cand;
+    int rc = stencil_candidates<T>(ctx, ls, which, cand);
+    if (rc) return rc;
+    const int n = (int)cand.size();
+    std::vector<cudaEvent_t> ev(2 * n);
+    for (auto& e : ev) VLR_CUDA(ctx, cudaEventCreate(&e));
+    ls->tune_log[which].clear();
+    for (int round = 0; round < 2 && !rc; ++round)
+        for (int i = 0; i < n && !rc; ++i) {
+            if (round) VLR_CUDA(ctx, cudaEventRecord(ev[2 * i], ctx->stream));
+            rc = which == 0 ? launch_advect<T>(ctx, ls, cand[i]) : launch_reinit<T>(ctx, ls, cand[i]);
+            if (round && !rc) VLR_CUDA(ctx, cudaEventRecord(ev[2 * i + 1], ctx->stream));
+        }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = check_cuda(ctx, e, "autotune");
+    }
+    float best_ms = 0.f;
+    for (int i = 0; i < n && !rc; ++i) {
+        float ms = 0.f;
+        cudaError_t e = cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+        if (e != cudaSuccess) {
+            rc = check_cuda(ctx, e, "autotune timing");
+            break;
+        }
+        ls->tune_log[which].push_back(TuneEntry{cand[i], ms});
+        if (i == 0 || ms < best_ms) {
+            best_ms = ms;
+            *best = cand[i];
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+template <typename T>
+static int autotune_stencils(vlr_ctx* ctx, vlr_level_set* ls) {
+    StencilShape a{}, r{};
+    int rc = tune_one<T>(ctx, ls, 0, &a);
+    if (rc) return rc;
+    // the inputs of the last advect launch stand (every candidate wrote the same)
+    ls->adv_shape = a;
+    rc = tune_one<T>(ctx, ls, 1, &r);
+    if (rc) return rc;
+    ls->re_shape = r;
+    return VLR_OK;
+}
+
+int ls_autotune_step(vlr_ctx* ctx, vlr_level_set* ls) {
+    int rc = (ls->precision == VLR_PREC_F16) ? autotune_stencils<__half>(ctx, ls) : autotune_stencils<float>(ctx, ls);
+    if (rc) return rc;
+    ls->tuned = true;
+    return ls_enqueue_retrack(ctx, ls);
 }
 
 int ls_enqueue_step(vlr_ctx* ctx, vlr_level_set* ls) {
