@@ -283,13 +283,24 @@ def run_method(args, ctx, precision, flush, stream, clock=None):
 
 def run_batched(args, ctx, precision, flush, stream, clock=None, steps=None):
     """256 uneven grids (unions of 1-64 random spheres, extents 64^3-1024^3
-    log-uniform, curl-noise velocity, RK3), one persistent launch per kernel."""
+    log-uniform, curl-noise velocity, RK3), one persistent launch per kernel.
+    With N ranks each rank runs its LPT share of the grids (no data-path
+    collective); the whole-job rate is the summed active voxels over the
+    slowest rank's step time."""
     from sharc.volrus_b200.method import LevelSet, random_sphere_grids
+    from sharc.volrus_b200.shard import reduce_totals, shard_of
 
     gr = random_sphere_grids(args.grids, seed=BATCH["seed"])
+    gr, idx = shard_of(gr, args.rank, args.world)
     ls = LevelSet.spheres([(sph, vel) for sph, vel, _ in gr], 1.0, half_width=3.0, precision=precision,
                           integrator=3, reinit_iters=2, ctx=ctx)
     r = time_steps(args, ctx, ls, flush, stream, clock, steps=steps)
+    r["grids_this_rank"] = len(idx)
+    r["active_this_rank"] = r["active"]
+    if args.world > 1:
+        import torch
+        total, ms = reduce_totals(r["active"], r["ms_per_step"], torch.device("cuda", args.device))
+        r["active"], r["ms_per_step"], r["value"] = total, ms, total / (ms * 1e-3)
     return r
 
 
@@ -341,6 +352,7 @@ def e2e_method(args, ctx, ls, precision):
         call()
     e2e_s = (time.perf_counter() - t0) / args.steps
     return {"value": a / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "seconds_per_step": e2e_s,
             "path": "vlr_ls_upload + vlr_ls_step + vlr_ls_download, pinned host buffers"}
 
 
@@ -363,12 +375,15 @@ def bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=None):
     out = {}
     for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
         r = run_batched(args, ctx, prec, flush, stream, clk, steps=steps)
-        out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves": r["leaves"],
-                     "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"],
+        out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves_this_rank": r["leaves"],
+                     "active_voxels": r["active"], "grids_this_rank": r["grids_this_rank"], "kernels_ms_per_launch": r["kernels"],
                      "roofline": roofline_of(r, nb, peak, peak_kind, "batched256")}
         r["ls"].close()
     out["fp16_over_fp32"] = out["f16"]["value"] / out["f32"]["value"]
+    out["scaling"] = "strong"
+    out["n_gpus"] = args.world
     out["config"] = {"workload": "batched256", "grids": args.grids, "seed": BATCH["seed"],
+                     "sharding": "whole grids per rank, greedy LPT on estimated band voxels; no data-path collective",
                      "extent": "2^U(6,10) voxels per axis", "spheres": "1-64 per grid, r~U(4,24)",
                      "velocity": "curl noise, 3 octaves, 1 voxel/step", "integrator": "SSP-RK3", "dt": 1.0,
                      "half_width": 3, "reinit_iters": 2, "l2": "inputs larger than L2 and flushed between steps"}
@@ -386,10 +401,98 @@ def bench_batched_line(args, ctx, peak, peak_kind):
     f = b["f16"]
     return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
             "dtype": "f16 storage, f32 arithmetic", "config": dict(b["config"], active_voxels=f["active_voxels"],
-                                                                  leaves=f["leaves"]),
+                                                                  leaves_this_rank=f["leaves_this_rank"]),
             "fp32": b["f32"], "fp16_over_fp32": b["fp16_over_fp32"], "roofline": f["roofline"],
             "kernels_ms_per_launch": f["kernels_ms_per_launch"], "e2e": None, "clocks": clk.summary(),
             "gpu_launches": len(STEP_KERNELS) * args.steps}
+
+
+def leaf_voxel_coords(origins, masks):
+    """Index coordinates (n_active, 3) and (leaf, offset) of the active voxels."""
+    import numpy as np
+    off = np.arange(512)
+    rel = np.stack([off >> 6, (off >> 3) & 7, off & 7], axis=1)
+    bits = np.unpackbits(masks.view(np.uint8).reshape(-1, 64), axis=1, bitorder="little").astype(bool)
+    li, vi = np.nonzero(bits)
+    return origins[li].astype(np.int64) + rel[vi], li, vi
+
+
+def full_period(args, ctx, precision, reinit_mode=0):
+    """One full period of the deformation test (T = 3, dt = vs / 4: 6,144 steps
+    at 512^3): the shape returns to the start sphere, so the error of phi on the
+    interface (active voxels with |phi_exact| <= 1 voxel) against the exact
+    signed distance, and the relative change of the FP64 enclosed volume, measure
+    the method's accuracy at this resolution."""
+    import numpy as np
+    from sharc.volrus_b200.method import LevelSet
+    vs, T = DEFORM["voxel_size"], DEFORM["period"]
+    dt = 0.5 * vs / 2.0
+    steps = int(round(T / dt))
+    # the stretched sheet at t = T/2 holds many times the sphere's leaves
+    ls = LevelSet.sphere(DEFORM["radius"], DEFORM["center"], vs, {"kind": "vortex", "vs": vs, "period": T}, dt,
+                         half_width=DEFORM["half_width"], precision=precision, integrator=2, reinit_iters=2,
+                         capacity=200_000, reinit_mode=reinit_mode, ctx=ctx)
+    v0 = ls.volume()
+    n0 = ls.leaf_count()
+    peak = n0
+    for _ in range(16):
+        ls.step(steps // 16)
+        peak = max(peak, ls.leaf_count())
+    ls.step(steps - 16 * (steps // 16))
+    v1 = ls.volume()
+    o, m, p = ls.arrays()
+    ls.close()
+    xyz, li, vi = leaf_voxel_coords(o, m)
+    c = np.asarray(DEFORM["center"]) / vs
+    exact = np.sqrt(((xyz - c) ** 2).sum(axis=1)) - DEFORM["radius"] / vs
+    sel = np.abs(exact) <= 1.0
+    err = p[li, vi][sel] - exact[sel]
+    exact_vol = 4.0 / 3.0 * math.pi * (DEFORM["radius"] / vs) ** 3
+    far = int((np.abs(exact) > 2.0 * DEFORM["half_width"]).sum())
+    return {"steps": steps, "reinit_mode": reinit_mode, "leaves_start": n0, "leaves_peak_sampled": peak, "leaves_end": int(len(o)),
+            "active_far_from_start_shape": far,
+            "interface_voxels": int(sel.sum()), "max_err_vox": float(np.abs(err).max()),
+            "rms_err_vox": float(np.sqrt(np.mean(err ** 2))), "volume_change_rel": (v1 - v0) / v0,
+            "volume_start_vs_exact_rel": (v0 - exact_vol) / exact_vol,
+            "against": "exact signed distance of the start sphere (the flow returns to it after one period)"}
+
+
+def bench_adjoint(args, ctx):
+    """The adjoint configuration: sphere r = 32 centred in 256^3, FP32, K = 64
+    steps of the deformation field (T = 2), checkpoints every 8 steps, a 128^3
+    staggered velocity; forward then backward, timed with CUDA events on the
+    library stream.  Rate = band voxels x K / (forward + backward)."""
+    import numpy as np
+    import torch
+    from sharc.volrus_b200.adjoint import AdvectionFunction, sphere_band, staggered_vortex
+    domain, radius, n, steps, chk = 256, 32.0, 128, 64, 8
+    cell, vs = domain / n, 1.0 / domain
+    dt = 0.5 / (2.0 / vs)
+    o, m, p = sphere_band(radius, (128.0, 128.0, 128.0), domain, ctx=ctx)
+    V = staggered_vortex(n, cell, vs)
+    fn = AdvectionFunction(o, m, p, V, cell, dt, 2.0, steps, chk, ctx=ctx)
+    band = fn.band()
+    target = (np.sqrt(((band - np.array([136.0, 128.0, 128.0])) ** 2).sum(axis=1)) - radius).astype(np.float32)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", args.device))
+    fw, bw = [], []
+    for k in range(args.warmup + max(3, min(args.steps, 10))):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        phik = fn.forward()
+        e[1].record(stream)
+        fn.backward(2.0 * (phik - target))
+        e[2].record(stream)
+        torch.cuda.synchronize(args.device)
+        if k >= args.warmup:
+            fw.append(e[0].elapsed_time(e[1]))
+            bw.append(e[1].elapsed_time(e[2]))
+    nb = fn.n_band
+    fn.close()
+    f, b = statistics.median(fw), statistics.median(bw)
+    return {"workload": "adjoint256: sphere r=32 in 256^3, K=64, checkpoint 8, 128^3 staggered velocity, FP32",
+            "band_voxels": nb, "forward_ms": f, "backward_ms": b,
+            "value": nb * steps / ((f + b) * 1e-3), "unit": "band voxel-steps/s (forward + backward)",
+            "forward_voxels_per_s": nb * steps / (f * 1e-3)}
 
 
 def bench_deformation(args, ctx, peak, peak_kind):
@@ -406,6 +509,9 @@ def bench_deformation(args, ctx, peak, peak_kind):
         if not args.no_batched:
             batched = bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=min(args.steps, 10))
     e2e = e2e_method(args, ctx, r16["ls"], F16)
+    accuracy = None if args.no_accuracy else {"f16": full_period(args, ctx, F16), "f32": full_period(args, ctx, F32),
+                                              "f16_subcell_fix": full_period(args, ctx, F16, reinit_mode=1)}
+    adjoint = None if args.no_adjoint else bench_adjoint(args, ctx)
     launches_per_step = len(STEP_KERNELS)  # one CUDA graph per step
     line = {
         "metric": METRIC, "value": r16["value"], "unit": "voxels/s", "ms_per_step": r16["ms_per_step"],
@@ -427,6 +533,10 @@ def bench_deformation(args, ctx, peak, peak_kind):
     }
     if batched is not None:
         line["batched256"] = batched
+    if accuracy is not None:
+        line["full_period"] = accuracy
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     return line
 
 
@@ -536,6 +646,8 @@ def main():
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-grid batched measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the full-period accuracy run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--launch-shape", default="",
                     help="advect threads,CTAs,reinit threads,CTAs of the stencil kernels (default: autotuned)")
     args = ap.parse_args()
@@ -546,6 +658,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     args.device = local
+    args.rank, args.world = rank, world
 
     if args.workload == "deformation512":
         sphere = dict(radius=DEFORM["radius"], center=DEFORM["center"], voxel_size=DEFORM["voxel_size"],
@@ -592,12 +705,20 @@ def main():
         res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]
     ms = res["ms_per_step"]
+    # batched: ranks hold disjoint grids and the totals are already whole-job;
+    # deformation: one replica per rank (a single grid does not shard)
+    scaling = "strong" if args.workload == "batched256" else "weak"
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        value = world * res["config"]["active_voxels"] / (ms * 1e-3)
+        if args.workload != "batched256":
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            value = world * res["config"]["active_voxels"] / (ms * 1e-3)
+            if res.get("e2e"):
+                e = torch.tensor([res["e2e"]["seconds_per_step"]], device="cuda")
+                dist.all_reduce(e, op=dist.ReduceOp.MAX)
+                res["e2e"]["value"] = world * res["config"]["active_voxels"] / float(e.item())
         dist.barrier()
     if rank == 0:
         cpu = None
@@ -609,12 +730,12 @@ def main():
                 v, desc = cpu_reference_algorithm(sphere, vel_world, ref_dt)
                 cpu = {"value": v, "unit": "voxels/s", "cores": 1, "kind": "port", "sample": desc}
         line = {"metric": res["metric"], "value": value, "unit": res["unit"], "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": scaling,
                 "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic", "config": res["config"],
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("fp32", "fp16_over_fp32", "launch_shape", "batched256"):
+        for k in ("fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint"):
             if k in res:
                 line[k] = res[k]
         print(json.dumps(line))

@@ -167,6 +167,10 @@ typedef struct vlr_method_desc {
     double dt;                     /* time step */
     double t0;                     /* time of the initial state */
     size_t capacity;               /* leaf slots; 0 = 2 x initial + 4096 */
+    int reinit_mode;               /* 0: plain Godunov (default); 1: Godunov with the
+                                      Russo-Smereka subcell fix at cut voxels (keeps
+                                      the interface in place, but its sign test makes
+                                      long runs sensitive to rounding) */
 } vlr_method_desc;
 
 /* Sphere of `radius` (world units) at `center` (world), voxel size vs, world = w0 + vs * index. */

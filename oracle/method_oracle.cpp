@@ -54,7 +54,8 @@ bool spills(const Leaf& L, const int* d) {
 
 }  // namespace
 
-bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t, double dt, int nthreads) {
+bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t, double dt, int nthreads,
+          int reinit_mode) {
     const int n = (int)g.leaves.size();
     const double hw = g.hw;
     std::vector<std::vector<char>> Dm(n, std::vector<char>(512));
@@ -84,7 +85,18 @@ bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t
             L1[i].phi[off] = trilinear(g, g.leaves, i, f);
         }
     });
-    // 3. reinit (Jacobi), S0 from the advected field
+    // 3. reinit (Jacobi), S0 from the advected field.  Mode 1 (subcell fix):
+    //    voxels whose 6-neighbourhood in the advected field crosses zero relax
+    //    toward the distance estimated from that field instead of taking the
+    //    Godunov update, so reinitialisation does not move the interface.
+    std::vector<std::vector<double>> dist;
+    if (reinit_iters > 0 && reinit_mode == 1) {
+        dist.assign(n, std::vector<double>(512, kNoCut));
+        parallel_for(n, nthreads, [&](int i) {
+            for (int off = 0; off < 512; ++off)
+                if (Dm[i][off]) dist[i][off] = cut_distance(g, L1, i, off);
+        });
+    }
     std::vector<Leaf> cur = L1, nxt = L1;
     for (int it = 0; it < reinit_iters; ++it) {
         parallel_for(n, nthreads, [&](int i) {
@@ -95,6 +107,10 @@ bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t
                     continue;
                 }
                 double p1 = L1[i].phi[off];
+                if (reinit_mode == 1 && dist[i][off] != kNoCut) {
+                    nxt[i].phi[off] = p - 0.5 * (std::copysign(std::fabs(p), p1) - dist[i][off]);
+                    continue;
+                }
                 double s = p1 / std::sqrt(p1 * p1 + 1.0);
                 double G = godunov(g, cur, i, off, s);
                 nxt[i].phi[off] = p - 0.5 * s * (G - 1.0);
@@ -370,10 +386,11 @@ static Velocity unpack_vel(int kind, const double* p) {
     return v;
 }
 
-int vm_step(void* g, int vel_kind, const double* vel_params, int integrator, int reinit_iters, double t, double dt,
+int vm_step(void* g, int vel_kind, const double* vel_params, int integrator, int reinit_iters, int reinit_mode,
+            double t, double dt,
             int nthreads) {
     Velocity v = unpack_vel(vel_kind, vel_params);
-    return step(*(Grid*)g, v, integrator, reinit_iters, t, dt, nthreads) ? 1 : 0;
+    return step(*(Grid*)g, v, integrator, reinit_iters, t, dt, nthreads, reinit_mode) ? 1 : 0;
 }
 
 void vm_velocity(int vel_kind, const double* vel_params, const double* p, double t, double* u) {

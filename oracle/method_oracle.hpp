@@ -20,7 +20,10 @@
 //             x not in D -> copysign(hw, phi0(x))
 //     foot: Euler x - dt u(x, t1); RK2 midpoint; SSP-RK3 (Shu-Osher), t1 = t + dt
 //  3. reinit (N iterations, Jacobi, dtau = 0.5): S0 = phi1/sqrt(phi1^2 + 1);
-//     phi <- phi - dtau S0 (G(phi) - 1) on D, G = Godunov |grad phi|
+//     phi <- phi - dtau S0 (G(phi) - 1) on D, G = Godunov |grad phi|; in mode
+//     1 cut voxels (a 6-neighbour of opposite sign in phi1) instead relax
+//     toward the distance d = phi1 / |grad phi1|:
+//     phi <- phi - dtau (sign(phi1) |phi| - d)   (cut_distance below)
 //  4. trim: active = D and |phi| < hw; others become copysign(hw, phi)
 //  5. re-track: keep leaves touched by dilate26(active); allocate missing ones,
 //     filled from the first proposing neighbour (fixed direction order) by the
@@ -214,8 +217,37 @@ inline double godunov(const Grid& g, const std::vector<Leaf>& L, int c, int off,
     return std::sqrt(g2);
 }
 
+// Subcell fix of the reinitialisation (Russo & Smereka, J. Comput. Phys. 163,
+// 2000): a voxel whose 6-neighbourhood in phi0 (the field before
+// reinitialisation) changes sign is a cut voxel; its distance to the interface
+// is estimated as phi0 / |grad phi0| with, per axis, the largest of the
+// central and the two one-sided differences (at least 1e-6), and the
+// iteration relaxes it toward that distance,
+//   phi <- phi - 1/2 (sign(phi0) |phi| - d),
+// instead of taking the Godunov update.  Returns kNoCut for other voxels.
+constexpr double kNoCut = 1e300;
+inline double cut_distance(const Grid& g, const std::vector<Leaf>& L0, int c, int off) {
+    const Leaf& C = L0[c];
+    int x = C.o[0] + (off >> 6), y = C.o[1] + ((off >> 3) & 7), z = C.o[2] + (off & 7);
+    double p = C.phi[off];
+    double nb[6] = {g.read(L0, c, x - 1, y, z), g.read(L0, c, x + 1, y, z), g.read(L0, c, x, y - 1, z),
+                    g.read(L0, c, x, y + 1, z), g.read(L0, c, x, y, z - 1), g.read(L0, c, x, y, z + 1)};
+    bool cut = false;
+    for (int k = 0; k < 6; ++k) cut |= (p * nb[k] < 0.0);
+    if (!cut) return kNoCut;
+    double d2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        double m = std::max(std::max(std::fabs(nb[2 * a + 1] - nb[2 * a]) * 0.5, std::fabs(nb[2 * a + 1] - p)),
+                            std::max(std::fabs(p - nb[2 * a]), 1e-6));
+        d2 += m * m;
+    }
+    return p / std::sqrt(d2);
+}
+
 // One method step; returns false if a foot left the 27-leaf neighbourhood.
-bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t, double dt, int nthreads);
+// reinit_mode 0: plain Godunov; 1: Godunov with the subcell fix at cut voxels.
+bool step(Grid& g, const Velocity& v, int integrator, int reinit_iters, double t, double dt, int nthreads,
+          int reinit_mode = 0);
 
 // Initial state from the sphere SDF (index units): phi = (|p*vs + w0 - c| - r)/vs.
 Grid sphere(double radius, const double center[3], double vs, const double w0[3], double hw,

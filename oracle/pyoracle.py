@@ -57,7 +57,7 @@ SIGS = {
     "vm_leaf_count": (C.c_size_t, [P]),
     "vm_export": (None, [P, i32_p, u64_p, dbl_p]),
     "vm_import": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double]),
-    "vm_step": (C.c_int, [P, C.c_int, dbl_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
+    "vm_step": (C.c_int, [P, C.c_int, dbl_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
     "vm_velocity": (None, [C.c_int, dbl_p, dbl_p, C.c_double, dbl_p]),
     "vm_volume": (C.c_double, [P, dbl_p]),
 }
@@ -278,9 +278,11 @@ class MOGrid:
     def leaf_count(self):
         return self.lib.vm_leaf_count(self.h)
 
-    def step(self, vel: dict, integrator: int, reinit_iters: int, t: float, dt: float, nthreads: int = 8) -> bool:
+    def step(self, vel: dict, integrator: int, reinit_iters: int, t: float, dt: float, nthreads: int = 8,
+             reinit_mode: int = 0) -> bool:
         kind, p = pack_velocity(vel)
-        return bool(self.lib.vm_step(self.h, kind, _p(p, C.c_double), integrator, reinit_iters, t, dt, nthreads))
+        return bool(self.lib.vm_step(self.h, kind, _p(p, C.c_double), integrator, reinit_iters, reinit_mode, t, dt,
+                                     nthreads))
 
     def volume(self, ref=(0.0, 0.0, 0.0)):
         r = np.asarray(ref, np.float64)

@@ -64,6 +64,7 @@ class vlr_method_desc(C.Structure):
         ("dt", C.c_double),
         ("t0", C.c_double),
         ("capacity", C.c_size_t),
+        ("reinit_mode", C.c_int),
     ]
 
 

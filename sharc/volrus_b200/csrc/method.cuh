@@ -54,6 +54,7 @@ struct MStepParams {
     int integrator;        // 1 Euler, 2 RK2 midpoint, 3 SSP-RK3
     int n_grids;
     int key_bits;          // bits per axis in a hash key (21 for one grid, 18 for batches)
+    int reinit_mode;       // 0 plain Godunov, 1 Godunov with the subcell fix at cut voxels
 };
 
 __device__ __forceinline__ float to_f(float v) { return v; }

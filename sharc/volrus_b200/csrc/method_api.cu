@@ -184,6 +184,9 @@ int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, co
     ls->sp.integrator = m->integrator;
     ls->sp.n_grids = n;
     ls->sp.key_bits = ls->key_bits;
+    if (m->reinit_mode != 0 && m->reinit_mode != 1)
+        return set_error(ctx, VLR_ERR_INVALID, "reinit_mode must be 0 (plain Godunov) or 1 (subcell fix)");
+    ls->sp.reinit_mode = m->reinit_mode;
     std::vector<float2> tab;
     ls->h_params.resize(n);
     for (int g = 0; g < n; ++g) {

@@ -43,7 +43,7 @@ size_t advect_smem_bytes(int precision_f16, int halo);
 size_t reinit_smem_bytes(int precision_f16);
 template <typename T, int NIT, int NT>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                           const MGridParams* __restrict__ params, MTopo topo, unsigned* __restrict__ err);
+                           const MGridParams* __restrict__ params, MTopo topo, int mode, unsigned* __restrict__ err);
 template <typename T>
 __global__ void k_m_volume(MLeafArrays A, const T* __restrict__ vals, const MGridParams* __restrict__ params,
                            double r0, double r1, double r2, double* __restrict__ partial);

@@ -619,11 +619,47 @@ __device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym
 // copysign(hw, phi(centre)).
 __device__ __forceinline__ float nbv(float v, float centre, float hw) { return (v != v) ? copysignf(hw, centre) : v; }
 
+// The 6 neighbours of a tile voxel (row pitch S), missing-leaf NaNs resolved
+// against the centre value p.
+struct Nb6 {
+    float xm, xp, ym, yp, zm, zp;
+};
+
+template <int S>
+__device__ __forceinline__ Nb6 load_nb6(const float* c, float p, float hw) {
+    return Nb6{nbv(c[-S * S], p, hw), nbv(c[S * S], p, hw), nbv(c[-S], p, hw),
+               nbv(c[S], p, hw),      nbv(c[-1], p, hw),    nbv(c[1], p, hw)};
+}
+
+__device__ __forceinline__ float godunov_update(float p, const Nb6& n, float s) {
+    const float G = godunov_g(p, n.xm, n.xp, n.ym, n.yp, n.zm, n.zp, s);
+    return p - 0.5f * s * (G - 1.0f);
+}
+
 template <int S>
 __device__ __forceinline__ float reinit_update(const float* c, float p, float s, float hw) {
-    float G = godunov_g(p, nbv(c[-S * S], p, hw), nbv(c[S * S], p, hw), nbv(c[-S], p, hw), nbv(c[S], p, hw),
-                        nbv(c[-1], p, hw), nbv(c[1], p, hw), s);
-    return p - 0.5f * s * (G - 1.0f);
+    return godunov_update(p, load_nb6<S>(c, p, hw), s);
+}
+
+// Subcell fix of the reinitialisation (Russo & Smereka, J. Comput. Phys. 163,
+// 2000): if the 6-neighbourhood of phi0 (the field before reinitialisation)
+// changes sign at this voxel, the distance to the interface estimated as
+// phi0 / |grad phi0| (per axis the largest of the central and the two
+// one-sided differences, at least 1e-6); NaN otherwise.  Cut voxels relax
+// toward it, phi <- phi - 1/2 (sign(phi0) |phi| - d), instead of taking the
+// Godunov update, so reinitialisation does not move the interface.
+__device__ __forceinline__ float cut_distance(float p, const Nb6& n) {
+    const bool cut = (p * n.xm < 0.f) | (p * n.xp < 0.f) | (p * n.ym < 0.f) | (p * n.yp < 0.f) |
+                     (p * n.zm < 0.f) | (p * n.zp < 0.f);
+    if (!cut) return __int_as_float(0x7fc00000);
+    const float mx = fmaxf(fmaxf(fabsf(n.xp - n.xm) * 0.5f, fabsf(n.xp - p)), fmaxf(fabsf(p - n.xm), 1e-6f));
+    const float my = fmaxf(fmaxf(fabsf(n.yp - n.ym) * 0.5f, fabsf(n.yp - p)), fmaxf(fabsf(p - n.ym), 1e-6f));
+    const float mz = fmaxf(fmaxf(fabsf(n.zp - n.zm) * 0.5f, fabsf(n.zp - p)), fmaxf(fabsf(p - n.zm), 1e-6f));
+    return p / sqrtf(mx * mx + my * my + mz * mz);
+}
+
+__device__ __forceinline__ float cut_relax(float phi, float phi0, float d) {
+    return phi - 0.5f * (copysignf(fabsf(phi), phi0) - d);
 }
 
 
@@ -639,7 +675,7 @@ struct ReinitSmem {
 template <typename T, int NIT, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const T* __restrict__ src,
                                                            T* __restrict__ dst, const MGridParams* __restrict__ params,
-                                                           MTopo topo, unsigned* __restrict__ err) {
+                                                           MTopo topo, int mode, unsigned* __restrict__ err) {
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     dep_wait();
     dep_launch();
@@ -660,6 +696,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     __shared__ int s_nbr[2][32];
     __shared__ __align__(16) unsigned s_M[16];
     __shared__ unsigned s_desc[StageDesc<T, 2>::NP];
+    __shared__ float s_dist[NIT == 2 ? F * F * F : 1];  // cut-voxel distances of the 10^3 box (NaN: not cut)
 
     const int count = *A.count;
     const int G = gridDim.x;
@@ -667,6 +704,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     if (li >= count) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    const bool fix = (mode == 1);
     const bool w0 = threadIdx.x < 32;
 
     int slot = A.list[li];
@@ -738,7 +776,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
                 const int xr = t / (F * F), yr = (t / F) % F, zr = t % F;
                 const float* c1 = &s_p1[((xr + 1) * E + (yr + 1)) * E + (zr + 1)];
                 const float p = c1[0];
-                s_p2[t] = reinit_update<E>(c1, p, p * rsqrtf(p * p + 1.0f), hw);
+                const Nb6 n = load_nb6<E>(c1, p, hw);
+                const float d = fix ? cut_distance(p, n) : __int_as_float(0x7fc00000);
+                s_dist[t] = d;
+                s_p2[t] = (d == d) ? cut_relax(p, p, d) : godunov_update(p, n, p * rsqrtf(p * p + 1.0f));
             }
             __syncthreads();  // barrier 3: phi2 complete on the 10^3 box
         }
@@ -755,11 +796,21 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
             if (NIT == 0) {
                 v = p1;
             } else if (NIT == 1) {
-                v = inD ? reinit_update<E>(c1, p1, p1 * rsqrtf(p1 * p1 + 1.0f), hw) : p1;
+                v = p1;
+                if (inD) {
+                    const Nb6 n = load_nb6<E>(c1, p1, hw);
+                    const float d = fix ? cut_distance(p1, n) : __int_as_float(0x7fc00000);
+                    v = (d == d) ? cut_relax(p1, p1, d) : godunov_update(p1, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                }
             } else {
-                const float* c2 = &s_p2[((x + 1) * F + (y + 1)) * F + (z + 1)];
+                const int t10 = ((x + 1) * F + (y + 1)) * F + (z + 1);
+                const float* c2 = &s_p2[t10];
                 const float p2 = c2[0];
-                v = inD ? reinit_update<F>(c2, p2, p1 * rsqrtf(p1 * p1 + 1.0f), hw) : p2;
+                v = p2;
+                if (inD) {
+                    const float d = fix ? s_dist[t10] : __int_as_float(0x7fc00000);
+                    v = (d == d) ? cut_relax(p2, p1, d) : reinit_update<F>(c2, p2, p1 * rsqrtf(p1 * p1 + 1.0f), hw);
+                }
             }
             const bool on = inD && fabsf(v) < hw;
             if (!on) v = copysignf(hw, v);
@@ -848,9 +899,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
                                                              const float2*, MStepParams, MTopo, unsigned*);
 #define VLR_INST_ADVECT(T, H) VLR_INST_ADVECT_NT(T, H, 128) VLR_INST_ADVECT_NT(T, H, 256)
 #define VLR_INST_REINIT_NT(T, NT)                                                                                  \
-    template __global__ void k_m_reinit<T, 0, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*); \
-    template __global__ void k_m_reinit<T, 1, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*); \
-    template __global__ void k_m_reinit<T, 2, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*);
+    template __global__ void k_m_reinit<T, 0, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
+                                                  unsigned*);                                                      \
+    template __global__ void k_m_reinit<T, 1, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
+                                                  unsigned*);                                                      \
+    template __global__ void k_m_reinit<T, 2, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
+                                                  unsigned*);
 #define VLR_INST_REINIT(T) VLR_INST_REINIT_NT(T, 128) VLR_INST_REINIT_NT(T, 256)
 VLR_INST_ADVECT(float, 2)
 VLR_INST_ADVECT(float, 3)

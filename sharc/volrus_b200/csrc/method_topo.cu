@@ -455,7 +455,7 @@ static int launch_reinit_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& 
     VLR_TIMED(ctx, "k_m_reinit",
               VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, NT>, blocks, NT, smem, ctx->stream, A,
                                        (const T*)ls->vals[1], (T*)ls->vals[0], (const MGridParams*)ls->d_params,
-                                       topo, ctx->d_errword)));
+                                       topo, ls->sp.reinit_mode, ctx->d_errword)));
     return VLR_OK;
 }
 

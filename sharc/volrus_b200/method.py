@@ -113,7 +113,7 @@ class LevelSet:
         self.voxel_size = voxel_size
 
     @staticmethod
-    def _method(precision, half_width, integrator, reinit_iters, dt, t0, capacity):
+    def _method(precision, half_width, integrator, reinit_iters, dt, t0, capacity, reinit_mode=0):
         m = _lib.vlr_method_desc()
         m.precision = precision
         m.half_width = half_width
@@ -122,14 +122,18 @@ class LevelSet:
         m.dt = dt
         m.t0 = t0
         m.capacity = capacity
+        m.reinit_mode = reinit_mode
         return m
 
     @classmethod
     def sphere(cls, radius, center, voxel_size, velocity: dict, dt: float, half_width: float = 3.0,
                precision: int = F32, integrator: int = 2, reinit_iters: int = 2, t0: float = 0.0, w0=(0.0, 0.0, 0.0),
-               capacity: int = 0, ctx: Context | None = None) -> "LevelSet":
+               capacity: int = 0, reinit_mode: int = 0, ctx: Context | None = None) -> "LevelSet":
+        """``reinit_mode`` 0: plain Godunov reinitialisation; 1: Godunov with the
+        subcell fix at cut voxels (the interface does not move, but the fix's
+        sign test makes long runs sensitive to rounding)."""
         ctx = ctx or Context.default()
-        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity)
+        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity, reinit_mode)
         v = velocity_desc(velocity)
         c = np.asarray(center, np.float64)
         w = np.asarray(w0, np.float64)
@@ -141,13 +145,14 @@ class LevelSet:
 
     @classmethod
     def spheres(cls, grids, dt: float, half_width: float = 3.0, precision: int = F16, integrator: int = 3,
-                reinit_iters: int = 2, t0: float = 0.0, capacity: int = 0, ctx: Context | None = None) -> "LevelSet":
+                reinit_iters: int = 2, t0: float = 0.0, capacity: int = 0, reinit_mode: int = 0,
+                ctx: Context | None = None) -> "LevelSet":
         """One or many grids, each a union of spheres with its own velocity.
 
         ``grids``: list of (spheres, velocity) with spheres an (n, 4) array of
         (cx, cy, cz, r) in voxels (voxel size 1, world = index)."""
         ctx = ctx or Context.default()
-        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity)
+        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity, reinit_mode)
         n = len(grids)
         arr = (_lib.vlr_batch_grid * n)()
         keep = []
@@ -182,9 +187,9 @@ class LevelSet:
     @classmethod
     def from_leaves(cls, origins, masks, phi, velocity: dict, dt: float, half_width: float = 3.0,
                     precision: int = F32, integrator: int = 2, reinit_iters: int = 2, t0: float = 0.0,
-                    capacity: int = 0, ctx: Context | None = None) -> "LevelSet":
+                    capacity: int = 0, reinit_mode: int = 0, ctx: Context | None = None) -> "LevelSet":
         ctx = ctx or Context.default()
-        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity)
+        m = cls._method(precision, half_width, integrator, reinit_iters, dt, t0, capacity, reinit_mode)
         v = velocity_desc(velocity)
         o = np.ascontiguousarray(origins, np.int32)
         mk = np.ascontiguousarray(masks, np.uint64)

@@ -41,4 +41,5 @@ def compare(gpu_arrays, oracle_arrays, hw, tol_threshold=1e-3):
         "leaves_gpu": len(go), "leaves_oracle": len(oo), "only_gpu": len(only_gpu), "only_oracle": len(only_oracle),
         "active_gpu": int(gb.sum()), "active_oracle": int(ob.sum()), "mask_flips": flips,
         "unexplained_flips": unexplained, "max_err": float(e.max()), "rms_err": float(np.sqrt((e ** 2).mean())),
+        "frac_over_1e-2": float((e > 1e-2).mean()),
     }
