@@ -209,12 +209,12 @@ STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_
 # bench's own commands (dram__bytes_read.sum + dram__bytes_write.sum divided by
 # the leaves of that launch); keyed by (workload, kernel, value bytes).
 # profiles/stencils_deformation512_full.md (2,853 leaves) and
-# profiles/stencils_batched256_dram.md (151,238 leaves).
+# profiles/stencils_batched256_subset48_full.md (151,238 leaves).
 TRAFFIC_PER_LEAF: dict = {
-    ("deformation512", "k_m_advect", 2): 3540736 / 2853,
-    ("deformation512", "k_m_reinit", 2): 3512576 / 2853,
-    ("batched256", "k_m_advect", 2): (193480704 + 160735744) / 151238,
-    ("batched256", "k_m_reinit", 2): (185007616 + 129400320) / 151238,
+    ("deformation512", "k_m_advect", 2): 3531264 / 2850,
+    ("deformation512", "k_m_reinit", 2): 3519744 / 2850,
+    ("batched256", "k_m_advect", 2): (192670464 + 161785856) / 151238,
+    ("batched256", "k_m_reinit", 2): (194985984 + 136462080) / 151238,
 }
 
 
@@ -495,6 +495,18 @@ def bench_adjoint(args, ctx):
             "forward_voxels_per_s": nb * steps / (f * 1e-3)}
 
 
+def bench_adjoint_line(args, ctx):
+    """The adjoint configuration on its own (forward + backward per step)."""
+    with ClockSampler(args.device) as clk, clk.mark():
+        a = bench_adjoint(args, ctx)
+    return {"metric": "band voxel-steps/s of the adjoint (forward + backward)", "value": a["value"],
+            "unit": "voxels/s", "ms_per_step": (a["forward_ms"] + a["backward_ms"]) / 64.0, "dtype": "f32",
+            "config": {"workload": "adjoint256", "active_voxels": a["band_voxels"], "steps": 64,
+                       "checkpoint_every": 8, "velocity": "128^3 staggered, trilinear upsample"},
+            "roofline": None, "e2e": None, "clocks": clk.summary(), "gpu_launches": None,
+            "kernels_ms_per_launch": {}, "adjoint": a}
+
+
 def bench_deformation(args, ctx, peak, peak_kind):
     import torch
     from sharc.volrus_b200.method import F16, F32
@@ -641,7 +653,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["deformation512", "batched256", "reference-sphere128"],
+    ap.add_argument("--workload", choices=["deformation512", "batched256", "adjoint256", "reference-sphere128"],
                     default="deformation512")
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -701,6 +713,8 @@ def main():
         res = bench_deformation(args, ctx, peak, peak_kind)
     elif args.workload == "batched256":
         res = bench_batched_line(args, ctx, peak, peak_kind)
+    elif args.workload == "adjoint256":
+        res = bench_adjoint_line(args, ctx)
     else:
         res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]
@@ -736,6 +750,8 @@ def main():
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
         for k in ("fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint"):
+            if k in res and res[k] is None:
+                continue
             if k in res:
                 line[k] = res[k]
         print(json.dumps(line))

@@ -13,8 +13,10 @@
 //   lambda_k(c) = sum_x lambda_{k+1}(x) w_c(p_k(x))     (transpose of the blend)
 //   G(x)      += lambda_{k+1}(x) (-dt c_k) grad trilinear(phi_k)(p_k(x))
 //   dL/dphi_0 = lambda_0,  dL/dV = upsample^T G
-// Both scatters (lambda and upsample^T) go through a stable radix sort and a
-// segmented sum: no float atomics, deterministic results.  phi_k for the
+// The lambda transpose is a gather over the band voxels whose foot cell can
+// hold the corner (a window of (2R+2)^3 voxels, R the per-step reach), summed
+// in a fixed order; upsample^T goes through a stable radix sort and a
+// segmented sum.  No float atomics: deterministic results.  phi_k for the
 // backward pass is recomputed from checkpoints taken every C steps (sqrt(K)).
 #include <algorithm>
 #include <cmath>
@@ -51,6 +53,7 @@ struct vlr_adjoint {
     float* lam[2] = {nullptr, nullptr};
     float* gvel = nullptr;               // dL/dV, 3 x n^3
     float3* G = nullptr;
+    int reach = 1;                       // displacement bound per step, voxels (ceil of dt max|V|)
     unsigned* keys = nullptr;
     float* pvals = nullptr;
     void* scratch = nullptr;
@@ -176,39 +179,63 @@ __device__ __forceinline__ unsigned band_key(const int* __restrict__ nbr, const 
     return b < 0 ? nb : (unsigned)b;
 }
 
-// Adjoint of step k: emit 8 (corner band index, lambda * weight) pairs per band
-// voxel (in band order, corners in a fixed order) and accumulate the velocity
-// sensitivity G(x) += lambda (-dt c_k) grad trilinear(phi_k)(p).
-__global__ void k_adj_emit(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
-                           const int* __restrict__ bidx, const float3* __restrict__ ub,
-                           const float* __restrict__ phi_k, const float* __restrict__ lam, float s, float hw,
-                           unsigned* __restrict__ keys, float* __restrict__ vals, float3* __restrict__ G) {
+// Adjoint of step k as a gather, one band voxel b per thread:
+//   G(b)      += lambda(b) s grad trilinear(phi_k)(p(b))      (b's own foot)
+//   lambda'(b) = sum over band voxels x of lambda(x) w_b(p(x))  (b as a corner)
+// A step moves a voxel by at most R = reach voxels per axis, so b is a corner
+// of x's foot cell only if x lies in b + [-1-R, R]^3; those candidates are
+// visited in a fixed order (x, then y, then z ascending), each x's foot taken
+// from the same foot_of() as the forward step, so the transpose is exact and
+// the sum order is fixed: deterministic, with no sort and no float atomics.
+__global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
+                             const int* __restrict__ bidx, const float3* __restrict__ ub,
+                             const float* __restrict__ phi_k, const float* __restrict__ lam, float s, float hw, int R,
+                             float* __restrict__ lam_out, float3* __restrict__ G) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
+        const int cx = off >> 6, cy = (off >> 3) & 7, cz = off & 7;
         const float l = lam[b];
-        Foot f = foot_of(ub[b], s);
-        const int x = (off >> 6) + f.fx, y = ((off >> 3) & 7) + f.fy, z = (off & 7) + f.fz;
-        const float wx[2] = {1 - f.wx, f.wx}, wy[2] = {1 - f.wy, f.wy}, wz[2] = {1 - f.wz, f.wz};
-        float c[8];
+        {
+            const Foot f = foot_of(ub[b], s);
+            const int x = cx + f.fx, y = cy + f.fy, z = cz + f.fz;
+            const float wx[2] = {1 - f.wx, f.wx}, wy[2] = {1 - f.wy, f.wy}, wz[2] = {1 - f.wz, f.wz};
+            float c[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
-            keys[(size_t)b * 8 + q] = band_key(nbr, bidx, slot, x + i, y + j, z + k, (unsigned)nb);
-            vals[(size_t)b * 8 + q] = l * wx[i] * wy[j] * wz[k];
-            c[q] = adj_read(phi_k, nbr, slot, x + i, y + j, z + k, hw);
+            for (int q = 0; q < 8; ++q) c[q] = adj_read(phi_k, nbr, slot, x + (q >> 2), y + ((q >> 1) & 1), z + (q & 1), hw);
+            // c[q] with q = i*4 + j*2 + k
+            float gx = wy[0] * wz[0] * (c[4] - c[0]) + wy[1] * wz[0] * (c[6] - c[2]) + wy[0] * wz[1] * (c[5] - c[1]) +
+                       wy[1] * wz[1] * (c[7] - c[3]);
+            float gy = wx[0] * wz[0] * (c[2] - c[0]) + wx[1] * wz[0] * (c[6] - c[4]) + wx[0] * wz[1] * (c[3] - c[1]) +
+                       wx[1] * wz[1] * (c[7] - c[5]);
+            float gz = wx[0] * wy[0] * (c[1] - c[0]) + wx[1] * wy[0] * (c[5] - c[4]) + wx[0] * wy[1] * (c[3] - c[2]) +
+                       wx[1] * wy[1] * (c[7] - c[6]);
+            float3 g = G[b];
+            g.x += l * s * gx;
+            g.y += l * s * gy;
+            g.z += l * s * gz;
+            G[b] = g;
         }
-        // c[q] with q = i*4 + j*2 + k
-        float gx = wy[0] * wz[0] * (c[4] - c[0]) + wy[1] * wz[0] * (c[6] - c[2]) + wy[0] * wz[1] * (c[5] - c[1]) +
-                   wy[1] * wz[1] * (c[7] - c[3]);
-        float gy = wx[0] * wz[0] * (c[2] - c[0]) + wx[1] * wz[0] * (c[6] - c[4]) + wx[0] * wz[1] * (c[3] - c[1]) +
-                   wx[1] * wz[1] * (c[7] - c[5]);
-        float gz = wx[0] * wy[0] * (c[1] - c[0]) + wx[1] * wy[0] * (c[5] - c[4]) + wx[0] * wy[1] * (c[3] - c[2]) +
-                   wx[1] * wy[1] * (c[7] - c[6]);
-        float3 g = G[b];
-        g.x += l * s * gx;
-        g.y += l * s * gy;
-        g.z += l * s * gz;
-        G[b] = g;
+        float acc = 0.f;
+        for (int dx = -1 - R; dx <= R; ++dx) {
+            const int x = cx + dx;
+            for (int dy = -1 - R; dy <= R; ++dy) {
+                const int y = cy + dy;
+                for (int dz = -1 - R; dz <= R; ++dz) {
+                    const int z = cz + dz;
+                    const int ns = nbr[slot * kNbr + nbx(x) * 9 + nbx(y) * 3 + nbx(z)];
+                    if (ns < 0) continue;
+                    const int bx = bidx[(size_t)ns * kLeafVoxels + voxel_off(x, y, z)];
+                    if (bx < 0) continue;
+                    const Foot f = foot_of(ub[bx], s);
+                    // corner index of b in x's foot cell: b - (x + floor(offset))
+                    const int i = -(dx + f.fx), j = -(dy + f.fy), k = -(dz + f.fz);
+                    if ((unsigned)i > 1u || (unsigned)j > 1u || (unsigned)k > 1u) continue;
+                    const float wx = i ? f.wx : 1 - f.wx, wy = j ? f.wy : 1 - f.wy, wz = k ? f.wz : 1 - f.wz;
+                    acc += lam[bx] * wx * wy * wz;
+                }
+            }
+        }
+        lam_out[b] = acc;
     }
 }
 
@@ -300,6 +327,14 @@ void adj_free(vlr_adjoint* a) {
                     a->ub, a->vel, a->checkpoints, a->segment, a->lam[0], a->lam[1], a->G, a->keys, a->pvals,
                     a->scratch, a->gvel};
     for (void* p : ptrs) cudaFree(p);
+}
+
+// Per-axis displacement bound of one step in whole voxels: |s_k u| <= dt max|V|
+// (the upsample is a convex combination of V and |cos| <= 1).
+int reach_of(const float* vel, size_t nvel, double dt) {
+    double m = 0.0;
+    for (size_t i = 0; i < nvel; ++i) m = std::max(m, (double)std::fabs(vel[i]));
+    return std::max(1, (int)std::ceil(dt * m * (1.0 + 1e-6)));
 }
 
 float step_factor(const vlr_adjoint* a, int k) {
@@ -394,6 +429,8 @@ int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, 
     VLR_CUDA(ctx, cudaMemcpyAsync(a->phi_init, phi, sizeof(float) * 512 * n_leaves, cudaMemcpyHostToDevice, st));
     VLR_CUDA(ctx, cudaMemcpyAsync(a->bidx, bidx.data(), sizeof(int) * 512 * n_leaves, cudaMemcpyHostToDevice, st));
     VLR_CUDA(ctx, cudaMemcpyAsync(a->bvox, bvox.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+    a->reach = reach_of(vel, nvel, dt);
+    if (a->reach > 6) return fail(set_error(ctx, VLR_ERR_REACH, "dt * max|V| exceeds 6 voxels per step"));
     VLR_CUDA(ctx, cudaMemcpyAsync(a->vel, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
     std::vector<uint64_t> hk(a->hcap, kEmptyKey);
     VLR_CUDA(ctx, cudaMemcpyAsync(a->hkey, hk.data(), sizeof(uint64_t) * a->hcap, cudaMemcpyHostToDevice, st));
@@ -439,6 +476,9 @@ int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, con
     }
     if (vel) {
         size_t nvel = 3ull * a->n_stag * a->n_stag * a->n_stag;
+        const int reach = reach_of(vel, nvel, a->dt);
+        if (reach > 6) return set_error(ctx, VLR_ERR_REACH, "dt * max|V| exceeds 6 voxels per step");
+        a->reach = reach;
         VLR_CUDA(ctx, cudaMemcpyAsync(a->vel, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
         k_adj_upsample<<<blocks_for(ctx, a->n_band), 256, 0, st>>>(a->bvox, a->origin, a->n_band, a->vel, a->n_stag,
                                                                    (float)a->H, a->ub);
@@ -507,14 +547,11 @@ int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, 
         for (int k = k1 - 1; k >= k0; --k) {
             k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb,
                                                                     a->segment + (size_t)(k - k0) * nb, a->phi[0]);
-            VLR_TIMED(ctx, "k_adj_emit",
-                      k_adj_emit<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->bidx, a->ub,
-                                                                      a->phi[0], lam, step_factor(a, k), a->hw,
-                                                                      a->keys, a->pvals, a->G));
             float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
-            int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 8), (unsigned)nb + 1, lam_out, (unsigned)nb,
-                                 a->scratch);
-            if (rc) return rc;
+            VLR_TIMED(ctx, "k_adj_lambda",
+                      k_adj_lambda<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->bidx, a->ub,
+                                                                        a->phi[0], lam, step_factor(a, k), a->hw,
+                                                                        a->reach, lam_out, a->G));
             lam = lam_out;
         }
         (void)cur;
