@@ -473,26 +473,55 @@ def bench_adjoint(args, ctx):
     fn = AdvectionFunction(o, m, p, V, cell, dt, 2.0, steps, chk, ctx=ctx)
     band = fn.band()
     target = (np.sqrt(((band - np.array([136.0, 128.0, 128.0])) ** 2).sum(axis=1)) - radius).astype(np.float32)
-    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", args.device))
+    dev = torch.device("cuda", args.device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    # device-resident passes (buffers in HBM; what a GPU training loop calls)
+    d_phik = torch.empty(fn.n_band, dtype=torch.float32, device=dev)
+    d_lam = torch.empty(fn.n_band, dtype=torch.float32, device=dev)
+    d_g0 = torch.empty(fn.n_band, dtype=torch.float32, device=dev)
+    d_gv = torch.empty(3 * n ** 3, dtype=torch.float32, device=dev)
+    d_target = torch.from_numpy(target).to(dev)
     fw, bw = [], []
     for k in range(args.warmup + max(3, min(args.steps, 10))):
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record(stream)
-        phik = fn.forward()
-        e[1].record(stream)
-        fn.backward(2.0 * (phik - target))
-        e[2].record(stream)
-        torch.cuda.synchronize(args.device)
+        with torch.cuda.stream(stream):
+            e[0].record(stream)
+            fn.forward_device(d_phik.data_ptr())
+            e[1].record(stream)
+            torch.sub(d_phik, d_target, out=d_lam)
+            d_lam.mul_(2.0)
+            fn.backward_device(d_lam.data_ptr(), d_g0.data_ptr(), d_gv.data_ptr())
+            e[2].record(stream)
+        ctx.check_device()
         if k >= args.warmup:
             fw.append(e[0].elapsed_time(e[1]))
             bw.append(e[1].elapsed_time(e[2]))
+    # host-resident passes through the C ABI (inputs and outputs in host memory)
+    hw_, t0 = [], time.perf_counter()
+    for k in range(3):
+        t0 = time.perf_counter()
+        phik = fn.forward()
+        fn.backward(2.0 * (phik - target))
+        hw_.append(time.perf_counter() - t0)
+    ctx.profile(True)
+    phik = fn.forward()
+    fn.backward(2.0 * (phik - target))
+    kern = {k: ctx.kernel_time(k) for k in ("k_adj_forward", "k_adj_pack", "k_adj_lambda", "k_adj_emit_vel")}
+    ctx.profile(False)
     nb = fn.n_band
     fn.close()
     f, b = statistics.median(fw), statistics.median(bw)
+    he = statistics.median(hw_)
     return {"workload": "adjoint256: sphere r=32 in 256^3, K=64, checkpoint 8, 128^3 staggered velocity, FP32",
             "band_voxels": nb, "forward_ms": f, "backward_ms": b,
             "value": nb * steps / ((f + b) * 1e-3), "unit": "band voxel-steps/s (forward + backward)",
-            "forward_voxels_per_s": nb * steps / (f * 1e-3)}
+            "timing": "device buffers, CUDA events on the library stream (forward_device + backward_device)",
+            "e2e": {"value": nb * steps / he, "unit": "band voxel-steps/s",
+                    "path": "vlr_adj_forward + vlr_adj_backward with host buffers (dL/dV: 25 MB to the host)",
+                    "h2d_bytes_per_step": nb * 4, "d2h_bytes_per_step": nb * 8 + 3 * n ** 3 * 4},
+            "forward_voxels_per_s": nb * steps / (f * 1e-3),
+            "kernels_ms_total_per_pass": {k: v[0] for k, v in kern.items()},
+            "kernels_launches_per_pass": {k: v[1] for k, v in kern.items()}}
 
 
 def bench_adjoint_line(args, ctx):

@@ -269,6 +269,13 @@ int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, con
 int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band);
 int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
                      float* grad_vel);
+/* Device-resident forms for GPU training loops: the same passes with device
+ * buffers (band arrays of n_band floats, grad_vel of 3 n^3), enqueued on the
+ * context stream without waiting; vlr_ctx_check() waits and reports
+ * device-side errors.  Output pointers may be null to skip that output. */
+int vlr_adj_forward_device(vlr_ctx* ctx, vlr_adjoint* a, float* d_phi_k_band);
+int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_phik_band, float* d_grad_phi0_band,
+                            float* d_grad_vel);
 void vlr_adj_destroy(vlr_adjoint* a);
 
 #ifdef __cplusplus

@@ -118,6 +118,8 @@ SIGNATURES = {
     "vlr_adj_set_inputs": (C.c_int, [P, P, flt_p, flt_p]),
     "vlr_adj_forward": (C.c_int, [P, P, flt_p]),
     "vlr_adj_backward": (C.c_int, [P, P, flt_p, flt_p, flt_p]),
+    "vlr_adj_forward_device": (C.c_int, [P, P, P]),
+    "vlr_adj_backward_device": (C.c_int, [P, P, P, P, P]),
     "vlr_adj_destroy": (None, [P]),
     "vlr_ls_step": (C.c_int, [P, P, C.c_int]),
     "vlr_ls_enqueue": (C.c_int, [P, P, C.c_int]),

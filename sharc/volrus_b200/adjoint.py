@@ -90,6 +90,20 @@ class AdvectionFunction:
                                                      ptr(g0, C.c_float), ptr(gv, C.c_float)), "vlr_adj_backward")
         return g0, gv
 
+    def forward_device(self, phik_ptr: int = 0):
+        """Forward pass into a device buffer of n_band floats (raw pointer, or 0
+        to keep phi_K only internally); enqueued on the context stream, no wait."""
+        self.ctx.check(self.ctx.lib.vlr_adj_forward_device(self.ctx.handle, self.handle, phik_ptr or None),
+                       "vlr_adj_forward_device")
+
+    def backward_device(self, grad_phik_ptr: int, grad_phi0_ptr: int = 0, grad_vel_ptr: int = 0):
+        """Backward pass on device buffers (raw pointers: n_band floats in,
+        n_band and 3 n^3 floats out, 0 to skip an output); enqueued on the
+        context stream, no wait (``Context.check_device`` reports errors)."""
+        self.ctx.check(self.ctx.lib.vlr_adj_backward_device(self.ctx.handle, self.handle, grad_phik_ptr,
+                                                            grad_phi0_ptr or None, grad_vel_ptr or None),
+                       "vlr_adj_backward_device")
+
     def close(self):
         if self.handle:
             self.ctx.lib.vlr_adj_destroy(self.handle)

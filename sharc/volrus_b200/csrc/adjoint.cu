@@ -51,9 +51,12 @@ struct vlr_adjoint {
     float* checkpoints = nullptr;        // (steps / chk_every + 1) x n_band
     float* segment = nullptr;            // chk_every x n_band (recomputed states)
     float* lam[2] = {nullptr, nullptr};
+    float* lam_final = nullptr;          // lam buffer holding dL/dphi_0 after the last backward pass
     float* gvel = nullptr;               // dL/dV, 3 x n^3
     float3* G = nullptr;
     int reach = 1;                       // displacement bound per step, voxels (ceil of dt max|V|)
+    unsigned* foot_pk = nullptr;         // per pool voxel: packed foot offsets of band voxels, 0 elsewhere
+    float4* foot_w = nullptr;            // per pool voxel: (wx, wy, wz, lambda) of band voxels
     unsigned* keys = nullptr;
     float* pvals = nullptr;
     void* scratch = nullptr;
@@ -179,26 +182,47 @@ __device__ __forceinline__ unsigned band_key(const int* __restrict__ nbr, const 
     return b < 0 ? nb : (unsigned)b;
 }
 
+// Per step k, for every band voxel x: its foot (floor offsets packed as three
+// biased bytes, bit 31 marking a band voxel) and (wx, wy, wz, lambda(x)) in
+// pool order, so the gather below reads one word per candidate instead of a
+// chain of band-index, velocity and lambda lookups.
+__global__ void k_adj_pack(const int* __restrict__ bvox, int nb, const float3* __restrict__ ub,
+                           const float* __restrict__ lam, float s, unsigned* __restrict__ foot_pk,
+                           float4* __restrict__ foot_w) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const Foot f = foot_of(ub[b], s);
+        const int sv = bvox[b];
+        foot_pk[sv] = 0x80000000u | ((unsigned)(f.fx + 64) << 14) | ((unsigned)(f.fy + 64) << 7) |
+                      (unsigned)(f.fz + 64);
+        foot_w[sv] = make_float4(f.wx, f.wy, f.wz, lam[b]);
+    }
+}
+
 // Adjoint of step k as a gather, one band voxel b per thread:
 //   G(b)      += lambda(b) s grad trilinear(phi_k)(p(b))      (b's own foot)
 //   lambda'(b) = sum over band voxels x of lambda(x) w_b(p(x))  (b as a corner)
 // A step moves a voxel by at most R = reach voxels per axis, so b is a corner
 // of x's foot cell only if x lies in b + [-1-R, R]^3; those candidates are
 // visited in a fixed order (x, then y, then z ascending), each x's foot taken
-// from the same foot_of() as the forward step, so the transpose is exact and
-// the sum order is fixed: deterministic, with no sort and no float atomics.
+// from the same foot_of() as the forward step (through k_adj_pack), so the
+// transpose is exact and the sum order is fixed: deterministic, with no sort
+// and no float atomics.  RT > 0 fixes R at compile time (unrolled window).
+template <int RT>
 __global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
-                             const int* __restrict__ bidx, const float3* __restrict__ ub,
-                             const float* __restrict__ phi_k, const float* __restrict__ lam, float s, float hw, int R,
+                             const float* __restrict__ phi_k, const unsigned* __restrict__ foot_pk,
+                             const float4* __restrict__ foot_w, float s, float hw, int R_run,
                              float* __restrict__ lam_out, float3* __restrict__ G) {
+    const int R = RT > 0 ? RT : R_run;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
         const int cx = off >> 6, cy = (off >> 3) & 7, cz = off & 7;
-        const float l = lam[b];
         {
-            const Foot f = foot_of(ub[b], s);
-            const int x = cx + f.fx, y = cy + f.fy, z = cz + f.fz;
-            const float wx[2] = {1 - f.wx, f.wx}, wy[2] = {1 - f.wy, f.wy}, wz[2] = {1 - f.wz, f.wz};
+            const unsigned pk = foot_pk[sv];
+            const float4 w4 = foot_w[sv];
+            const float l = w4.w;
+            const int x = cx + (int)((pk >> 14) & 127u) - 64, y = cy + (int)((pk >> 7) & 127u) - 64,
+                      z = cz + (int)(pk & 127u) - 64;
+            const float wx[2] = {1 - w4.x, w4.x}, wy[2] = {1 - w4.y, w4.y}, wz[2] = {1 - w4.z, w4.z};
             float c[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) c[q] = adj_read(phi_k, nbr, slot, x + (q >> 2), y + ((q >> 1) & 1), z + (q & 1), hw);
@@ -215,23 +239,29 @@ __global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __
             g.z += l * s * gz;
             G[b] = g;
         }
+        const int* nrow = nbr + slot * kNbr;
         float acc = 0.f;
+#pragma unroll
         for (int dx = -1 - R; dx <= R; ++dx) {
             const int x = cx + dx;
+#pragma unroll
             for (int dy = -1 - R; dy <= R; ++dy) {
                 const int y = cy + dy;
+                const int nb2 = nbx(x) * 9 + nbx(y) * 3;
+#pragma unroll
                 for (int dz = -1 - R; dz <= R; ++dz) {
                     const int z = cz + dz;
-                    const int ns = nbr[slot * kNbr + nbx(x) * 9 + nbx(y) * 3 + nbx(z)];
+                    const int ns = __ldg(&nrow[nb2 + nbx(z)]);
                     if (ns < 0) continue;
-                    const int bx = bidx[(size_t)ns * kLeafVoxels + voxel_off(x, y, z)];
-                    if (bx < 0) continue;
-                    const Foot f = foot_of(ub[bx], s);
+                    const size_t e = (size_t)ns * kLeafVoxels + voxel_off(x, y, z);
+                    const unsigned pk = __ldg(&foot_pk[e]);
                     // corner index of b in x's foot cell: b - (x + floor(offset))
-                    const int i = -(dx + f.fx), j = -(dy + f.fy), k = -(dz + f.fz);
-                    if ((unsigned)i > 1u || (unsigned)j > 1u || (unsigned)k > 1u) continue;
-                    const float wx = i ? f.wx : 1 - f.wx, wy = j ? f.wy : 1 - f.wy, wz = k ? f.wz : 1 - f.wz;
-                    acc += lam[bx] * wx * wy * wz;
+                    const int i = 64 - dx - (int)((pk >> 14) & 127u), j = 64 - dy - (int)((pk >> 7) & 127u),
+                              k = 64 - dz - (int)(pk & 127u);
+                    if (!(pk >> 31) || (unsigned)i > 1u || (unsigned)j > 1u || (unsigned)k > 1u) continue;
+                    const float4 w4 = __ldg(&foot_w[e]);
+                    const float wx = i ? w4.x : 1 - w4.x, wy = j ? w4.y : 1 - w4.y, wz = k ? w4.z : 1 - w4.z;
+                    acc += w4.w * wx * wy * wz;
                 }
             }
         }
@@ -325,7 +355,7 @@ int blocks_for(vlr_ctx* ctx, long long n) { return (int)std::max<long long>(1, s
 void adj_free(vlr_adjoint* a) {
     void* ptrs[] = {a->origin, a->nbr, a->hkey, a->hval, a->phi[0], a->phi[1], a->phi_init, a->bidx, a->bvox,
                     a->ub, a->vel, a->checkpoints, a->segment, a->lam[0], a->lam[1], a->G, a->keys, a->pvals,
-                    a->scratch, a->gvel};
+                    a->scratch, a->gvel, a->foot_pk, a->foot_w};
     for (void* p : ptrs) cudaFree(p);
 }
 
@@ -419,6 +449,9 @@ int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, 
     ADJ_MALLOC(a->lam[0], sizeof(float) * nb);
     ADJ_MALLOC(a->lam[1], sizeof(float) * nb);
     ADJ_MALLOC(a->gvel, sizeof(float) * nvel);
+    ADJ_MALLOC(a->foot_pk, sizeof(unsigned) * 512 * n_leaves);
+    ADJ_MALLOC(a->foot_w, sizeof(float4) * 512 * n_leaves);
+    VLR_CUDA(ctx, cudaMemsetAsync(a->foot_pk, 0, sizeof(unsigned) * 512 * n_leaves, ctx->stream));
     ADJ_MALLOC(a->G, sizeof(float3) * nb);
     ADJ_MALLOC(a->keys, sizeof(unsigned) * a->n_pairs_cap);
     ADJ_MALLOC(a->pvals, sizeof(float) * a->n_pairs_cap);
@@ -490,7 +523,7 @@ int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, con
 
 // Forward K steps from the initial state; checkpoints every C steps; writes
 // phi_K on the band (host, n_band floats) when phi_k_band is not null.
-int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band) {
+int vlr_adj_forward_device(vlr_ctx* ctx, vlr_adjoint* a, float* d_phi_k_band) {
     if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
@@ -507,21 +540,31 @@ int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band) {
     }
     k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur], a->lam[1]);
     VLR_CUDA(ctx, cudaGetLastError());
+    if (d_phi_k_band)
+        VLR_CUDA(ctx, cudaMemcpyAsync(d_phi_k_band, a->lam[1], sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
+    return VLR_OK;
+}
+
+int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band) {
+    int rc = vlr_adj_forward_device(ctx, a, nullptr);
+    if (rc) return rc;
     if (phi_k_band)
-        VLR_CUDA(ctx, cudaMemcpyAsync(phi_k_band, a->lam[1], sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
-    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+        VLR_CUDA(ctx, cudaMemcpyAsync(phi_k_band, a->lam[1], sizeof(float) * a->n_band, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return consume_device_errors(ctx, "vlr_adj_forward");
 }
 
 // Backward pass (vlr_adj_forward must have run): grad_phik_band = dL/dphi_K
 // on the band; writes dL/dphi_0 (n_band) and dL/dV (3 n^3), host buffers.
-int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
-                     float* grad_vel) {
-    if (!ctx || !a || !grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_phik_band, float* d_grad_phi0_band,
+                            float* d_grad_vel) {
+    if (!ctx || !a || !d_grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
     float* lam = a->lam[1];
-    VLR_CUDA(ctx, cudaMemcpyAsync(lam, grad_phik_band, sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+    if (d_grad_phik_band != lam)
+        VLR_CUDA(ctx, cudaMemcpyAsync(lam, d_grad_phik_band, sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
     k_zero3<<<blocks_for(ctx, nb), 256, 0, st>>>(a->G, (int)nb);
     const int C = a->chk_every;
     for (int seg = (a->steps - 1) / C; seg >= 0; --seg) {
@@ -548,28 +591,56 @@ int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, 
             k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb,
                                                                     a->segment + (size_t)(k - k0) * nb, a->phi[0]);
             float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
-            VLR_TIMED(ctx, "k_adj_lambda",
-                      k_adj_lambda<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->bidx, a->ub,
-                                                                        a->phi[0], lam, step_factor(a, k), a->hw,
-                                                                        a->reach, lam_out, a->G));
+            const float sk = step_factor(a, k);
+            VLR_TIMED(ctx, "k_adj_pack",
+                      k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk, a->foot_pk,
+                                                                      a->foot_w));
+            const int gb = blocks_for(ctx, nb);
+            if (a->reach == 1)
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<1><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, 1, lam_out, a->G));
+            else if (a->reach == 2)
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<2><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, 2, lam_out, a->G));
+            else
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<0><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, a->reach, lam_out, a->G));
             lam = lam_out;
         }
         (void)cur;
     }
     VLR_CUDA(ctx, cudaGetLastError());
-    if (grad_phi0_band)
-        VLR_CUDA(ctx, cudaMemcpyAsync(grad_phi0_band, lam, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
-    if (grad_vel) {
+    a->lam_final = lam;
+    if (d_grad_phi0_band)
+        VLR_CUDA(ctx, cudaMemcpyAsync(d_grad_phi0_band, lam, sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
+    if (d_grad_vel) {
         size_t nvel = 3ull * a->n_stag * a->n_stag * a->n_stag;
-        float* gv = a->gvel;
         VLR_TIMED(ctx, "k_adj_emit_vel",
                   k_adj_emit_vel<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, a->origin, (int)nb, a->G, a->n_stag,
                                                                       (float)a->H, a->keys, a->pvals));
-        int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 24), (unsigned)nvel + 1, gv, (unsigned)nvel,
+        int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 24), (unsigned)nvel + 1, d_grad_vel, (unsigned)nvel,
                              a->scratch);
         if (rc) return rc;
-        VLR_CUDA(ctx, cudaMemcpyAsync(grad_vel, gv, sizeof(float) * nvel, cudaMemcpyDeviceToHost, st));
     }
+    return VLR_OK;
+}
+
+int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
+                     float* grad_vel) {
+    if (!ctx || !a || !grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)a->n_band;
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->lam[1], grad_phik_band, sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+    int rc = vlr_adj_backward_device(ctx, a, a->lam[1], nullptr, grad_vel ? a->gvel : nullptr);
+    if (rc) return rc;
+    if (grad_phi0_band)
+        VLR_CUDA(ctx, cudaMemcpyAsync(grad_phi0_band, a->lam_final, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+    if (grad_vel)
+        VLR_CUDA(ctx, cudaMemcpyAsync(grad_vel, a->gvel, sizeof(float) * 3ull * a->n_stag * a->n_stag * a->n_stag,
+                                      cudaMemcpyDeviceToHost, st));
     VLR_CUDA(ctx, cudaStreamSynchronize(st));
     return consume_device_errors(ctx, "vlr_adj_backward");
 }
