@@ -75,6 +75,30 @@ int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, con
 /* Leaf count, active voxel count, background and transform of a grid. */
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf);
+/* ---- serialised formats ------------------------------------------------
+ * .vol byte image (src/io/vol_format.rs:1-160) <-> device grid.  Replaces
+ * read_vol (:85-150): validates magic, version, grid class and length
+ * (VLR_ERR_FORMAT), keeps the last record of a repeated leaf, builds
+ * Grid::new(background, voxel_size) semantics (uniform transform); the leaf
+ * block crosses to the device in one copy.  *grid_class receives the class. */
+int vlr_grid_from_vol(vlr_ctx* ctx, const void* bytes, size_t n_bytes, vlr_grid** out, int* grid_class);
+/* Replaces write_vol (src/io/vol_format.rs:53-83); leaves in (x, y, z) order
+ * of origin.  grid_class -1 writes the grid's own class.  out = NULL queries
+ * *n_bytes only. */
+int vlr_grid_to_vol(vlr_ctx* ctx, const vlr_grid* g, int grid_class, void* out, size_t cap, size_t* n_bytes);
+/* NanoGrid byte image (src/nano/layout.rs:13-286) <-> device grid.  Replaces
+ * NanoGrid::from_bytes (:208-252) + to_grid (:255-286): validates magic,
+ * version, length and strictly sorted leaves (VLR_ERR_FORMAT), keeps active
+ * voxels only (leaves without active voxels dropped, inactive voxels =
+ * background), with_affine transform from the header's forward matrix. */
+int vlr_grid_from_nano(vlr_ctx* ctx, const void* bytes, size_t n_bytes, vlr_grid** out, int* grid_class);
+/* Replaces NanoGrid::from_grid (:89-170): header with the active bounding
+ * box and the forward/inverse matrices, leaves sorted by origin with all 512
+ * values.  affine_inv (rows 0..2 of the inverse 4x4) may be NULL: the inverse
+ * the grid was read with, else 1 / voxel size on the diagonal. */
+int vlr_grid_to_nano(vlr_ctx* ctx, const vlr_grid* g, int grid_class, const double* affine_inv, void* out,
+                     size_t cap, size_t* n_bytes);
+
 /* Copy a grid back into caller buffers sized for at least vlr_grid_info's leaf
  * count, sorted (x, y, z) like NanoGrid (src/nano/layout.rs:81-106). */
 int vlr_grid_download(vlr_ctx* ctx, const vlr_grid* g, int32_t* origins, uint64_t* masks, float* values,

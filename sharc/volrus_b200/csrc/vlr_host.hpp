@@ -56,6 +56,10 @@ struct vlr_grid {
     uint64_t* hkey = nullptr;
     int* hval = nullptr;
     int hcap = 0;
+    // metadata carried for the serialised formats (src/io/vol_format.rs, src/nano/layout.rs)
+    int grid_class = 0;          // 0 unknown, 1 level set, 2 fog volume
+    int has_inv = 0;             // affine_inv holds the inverse map the grid was read with
+    double affine_inv[12] = {0}; // rows 0..2 of the inverse 4x4 (world -> index)
 };
 
 namespace vlr {
