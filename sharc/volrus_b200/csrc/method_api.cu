@@ -282,12 +282,17 @@ __global__ void k_from_f32(const float* in, T* out, size_t n) {
         out[i] = from_f<T>(in[i]);
 }
 
+__global__ void k_gather_origins(const int* list, int n, const int4* origin, int4* o_out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o_out[i] = origin[list[i]];
+}
+
+// Masks and f32 values of the leaves at list positions sel[0..k) in that
+// order (output order), one CTA per leaf.
 template <typename T>
-__global__ void k_gather_out(const int* list, int n, const int4* origin, const uint64_t* mask, const T* vals,
-                             int4* o_out, uint64_t* m_out, float* v_out) {
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
-        int s = list[i];
-        if (threadIdx.x == 0) o_out[i] = origin[s];
+__global__ void k_gather_sel(const int* list, const int* sel, int k, const uint64_t* mask, const T* vals,
+                             uint64_t* m_out, float* v_out) {
+    for (int i = blockIdx.x; i < k; i += gridDim.x) {
+        const int s = list[sel[i]];
         if (threadIdx.x < 8) m_out[(size_t)i * 8 + threadIdx.x] = mask[(size_t)s * 8 + threadIdx.x];
         for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
             v_out[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
@@ -605,50 +610,60 @@ int vlr_ls_download_grid(vlr_ctx* ctx, const vlr_level_set* ls, int grid, int32_
     if (rc) return rc;
     if (grid < 0 && n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
     if (!n) return VLR_OK;
+    // origins in list order -> host, output order sorted by (grid, x, y, z)
+    // there; masks and values are then gathered on the device in that order
+    // and copied once, straight into the caller's buffers
     void* stg = nullptr;
     size_t vbytes = sizeof(float) * kLeafVoxels * n;
-    rc = ls_staging(ctx, const_cast<vlr_level_set*>(ls), vbytes + 80 * n, &stg);
+    rc = ls_staging(ctx, const_cast<vlr_level_set*>(ls), vbytes + 84 * n + 256, &stg);
     if (rc) return rc;
     float* v = (float*)stg;
     int4* o = (int4*)((char*)stg + vbytes);
     uint64_t* mm = (uint64_t*)((char*)stg + vbytes + 16 * n);
-    int B = (int)std::min<size_t>(n, (size_t)ctx->sm_count * 8);
-    if (ls->precision == VLR_PREC_F16)
-        k_gather_out<__half><<<B, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, ls->mask,
-                                                         (const __half*)ls->vals[0], o, mm, v);
-    else
-        k_gather_out<float><<<B, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, ls->mask,
-                                                        (const float*)ls->vals[0], o, mm, v);
+    int* dsel = (int*)((char*)stg + vbytes + 80 * n);
+    k_gather_origins<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, o);
     std::vector<int4> ho(n);
-    std::vector<uint64_t> hm(8 * n);
-    std::vector<float> hv(kLeafVoxels * n);
     VLR_CUDA(ctx, cudaMemcpyAsync(ho.data(), o, sizeof(int4) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    VLR_CUDA(ctx, cudaMemcpyAsync(hm.data(), mm, 64 * n, cudaMemcpyDeviceToHost, ctx->stream));
-    VLR_CUDA(ctx, cudaMemcpyAsync(hv.data(), v, sizeof(float) * kLeafVoxels * n, cudaMemcpyDeviceToHost, ctx->stream));
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    std::vector<size_t> order(n);
+    std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
         const int4 &A = ho[a], &B2 = ho[b];
         if (A.w != B2.w) return A.w < B2.w;
         if (A.x != B2.x) return A.x < B2.x;
         if (A.y != B2.y) return A.y < B2.y;
         return A.z < B2.z;
     });
-    size_t k = 0;
-    for (size_t i = 0; i < n; ++i) {
-        size_t s = order[i];
-        if (grid >= 0 && ho[s].w != grid) continue;
-        if (k >= cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
-        if (grid_ids) grid_ids[k] = ho[s].w;
+    std::vector<int> sel;
+    sel.reserve(n);
+    for (size_t i = 0; i < n; ++i)
+        if (grid < 0 || ho[order[i]].w == grid) sel.push_back(order[i]);
+    const size_t k = sel.size();
+    if (k > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    for (size_t i = 0; i < k; ++i) {
+        const int4 q = ho[sel[i]];
+        if (grid_ids) grid_ids[i] = q.w;
         if (origins) {
-            origins[3 * k] = ho[s].x;
-            origins[3 * k + 1] = ho[s].y;
-            origins[3 * k + 2] = ho[s].z;
+            origins[3 * i] = q.x;
+            origins[3 * i + 1] = q.y;
+            origins[3 * i + 2] = q.z;
         }
-        if (masks) std::memcpy(masks + 8 * k, &hm[8 * s], 64);
-        if (phi) std::memcpy(phi + kLeafVoxels * k, &hv[kLeafVoxels * s], sizeof(float) * kLeafVoxels);
-        ++k;
+    }
+    if (k && (masks || phi)) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(dsel, sel.data(), sizeof(int) * k, cudaMemcpyHostToDevice, ctx->stream));
+        const int B = (int)std::min<size_t>(k, (size_t)ctx->sm_count * 8);
+        if (ls->precision == VLR_PREC_F16)
+            k_gather_sel<__half><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
+                                                             (const __half*)ls->vals[0], mm, v);
+        else
+            k_gather_sel<float><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
+                                                            (const float*)ls->vals[0], mm, v);
+        VLR_CUDA(ctx, cudaGetLastError());
+        if (masks) VLR_CUDA(ctx, cudaMemcpyAsync(masks, mm, 64 * k, cudaMemcpyDeviceToHost, ctx->stream));
+        if (phi)
+            VLR_CUDA(ctx, cudaMemcpyAsync(phi, v, sizeof(float) * kLeafVoxels * k, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
     *n_out = k;
     return VLR_OK;
