@@ -75,6 +75,13 @@ int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, con
 /* Leaf count, active voxel count, background and transform of a grid. */
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf);
+/* Replaces dilate(&mut Grid<f32>, iterations) (src/tools/morphology.rs:20-35):
+ * every inactive voxel with an active 6-neighbour becomes active with the
+ * value of the neighbour that comes first in the tree's iteration order
+ * (128^3 tiles in ascending origin order, then leaves, then voxels in ZYX
+ * order); missing leaves are allocated at the background. */
+int vlr_dilate(vlr_ctx* ctx, vlr_grid* g, unsigned iterations);
+
 /* ---- serialised formats ------------------------------------------------
  * .vol byte image (src/io/vol_format.rs:1-160) <-> device grid.  Replaces
  * read_vol (:85-150): validates magic, version, grid class and length

@@ -164,10 +164,20 @@ struct Grid {
             for (auto& ch : kv.second->children)
                 if (ch && ch->is_empty()) ch.reset();
     }
-    // leaf iteration (order is irrelevant to every result on this path)
+    // leaf iteration: tiles in ascending (x, y, z) of origin (the crate's
+    // HashMap order is unspecified; dilate's values depend on it and the GPU
+    // uses this order), then children in index order (x*256 + y*16 + z,
+    // src/tree/internal.rs:88-95)
     template <class F> void for_each_leaf(F&& f) const {
-        for (auto& kv : tiles)
-            for (auto& ch : kv.second->children)
+        std::vector<const std::pair<const Coord, std::unique_ptr<Internal>>*> kv;
+        for (auto& t : tiles) kv.push_back(&t);
+        std::sort(kv.begin(), kv.end(), [](auto* a, auto* b) {
+            if (a->first.x != b->first.x) return a->first.x < b->first.x;
+            if (a->first.y != b->first.y) return a->first.y < b->first.y;
+            return a->first.z < b->first.z;
+        });
+        for (auto* t : kv)
+            for (auto& ch : t->second->children)
                 if (ch) f(*ch);
     }
     template <class F> void for_each_leaf_mut(F&& f) {

@@ -10,6 +10,7 @@ it replaces and runs on the B200 through the C ABI:
     trim_narrow_band(grid, half_width)               src/tools/level_set_track.rs:53-68
     rebuild_narrow_band(grid, half_width)            src/tools/level_set_track.rs:80-114
     make_level_set_sphere(r, c, vs, hw) -> Grid      src/tools/sphere.rs:17-59
+    dilate(grid, iterations)                         src/tools/morphology.rs:20-35
 
 Host ``Grid`` arguments are uploaded, processed and downloaded per call (the
 drop-in form); ``DeviceGrid`` arguments stay resident in HBM between calls.
@@ -164,6 +165,18 @@ def rebuild_narrow_band(grid, half_width: float, ctx: Context | None = None):
               "vlr_rebuild_narrow_band")
     if uploaded:
         _replace(grid, g.download())
+
+
+def dilate(grid, iterations: int, ctx: Context | None = None):
+    """``dilate`` (src/tools/morphology.rs:20-35), in place: inactive voxels with
+    an active 6-neighbour become active with that neighbour's value (the first
+    in tree iteration order, 128^3 tiles taken in ascending origin order)."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    d, created = _as_device(grid, ctx)
+    ctx.check(ctx.lib.vlr_dilate(ctx.handle, d.handle, int(iterations)), "vlr_dilate")
+    if created:
+        _replace(grid, d.download())
+        d.close()
 
 
 def make_level_set_sphere(radius: float, center, voxel_size: float, half_width: float, ctx: Context | None = None,

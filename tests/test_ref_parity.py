@@ -198,6 +198,39 @@ def test_trim_bit_exact(oracle, hw):
     assert_same(g, og)
 
 
+def test_dilate_single_voxel_kat(oracle):  # src/tools/morphology.rs:88-111
+    from sharc.volrus_b200 import Grid, dilate
+    g = Grid(0.0, 1.0)
+    g.set((0, 0, 0), 1.0)
+    dilate(g, 1)
+    assert g.active_voxel_count() == 7
+    for c in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+        assert g.is_active(c) and g.get(c) == 1.0
+
+
+@pytest.mark.parametrize("iterations", [1, 3])
+def test_dilate_sphere_bit_exact(oracle, iterations):
+    from sharc.volrus_b200 import dilate, make_level_set_sphere
+    g = make_level_set_sphere(9.0, (0.5, 0.25, -1.0), 1.0, 2.0)
+    og = to_oracle(oracle, g)
+    dilate(g, iterations)
+    og.dilate(iterations)
+    assert_same(g, og)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_dilate_order_dependent_values_bit_exact(oracle, seed):
+    """Sparse voxels with distinct values over several 128^3 tiles (negative
+    coordinates included): a new voxel between active voxels takes the value
+    of the one first in iteration order, so values pin the order."""
+    from sharc.volrus_b200 import dilate
+    g = random_grid(np.random.default_rng(seed), 120, 24, -2.5, fill=0.08)
+    og = to_oracle(oracle, g)
+    dilate(g, 2)
+    og.dilate(2)
+    assert_same(g, og)
+
+
 @pytest.mark.parametrize("hw", [0.0, 1.0, 2.5, 3.0, 7.5, 9.0, 12.0])
 def test_rebuild_bit_exact(oracle, hw):
     """Window path (hw <= 9) and literal O(N x M) path (hw > 9)."""
