@@ -47,6 +47,7 @@ DEFORM = dict(radius=0.15, center=(0.35, 0.35, 0.35), voxel_size=1.0 / 512.0, ha
 REF_SPHERE = dict(radius=32.0, center=(64.0, 64.0, 64.0), voxel_size=1.0, half_width=3.0)
 REF_VEL = (1.0, 0.5, 0.25)
 BATCH = dict(grids=256, seed=3)
+LARGE = dict(spheres=8000, extent=8192.0, radius=(6.0, 40.0), seed=7)
 
 
 def measured_peaks():
@@ -524,6 +525,53 @@ def bench_adjoint(args, ctx):
             "kernels_launches_per_pass": {k: v[1] for k, v in kern.items()}}
 
 
+def large_grid(n_spheres: int, seed: int):
+    """One grid: n seeded random spheres, radii U(6, 40) voxels, centres uniform
+    in an 8192^3 extent, with a 3-octave curl-noise velocity of 1 voxel/step."""
+    import numpy as np
+    from sharc.volrus_b200.method import curl_noise
+    rng = np.random.default_rng(seed)
+    e = LARGE["extent"]
+    sph = np.column_stack([rng.uniform(0.0, e, (n_spheres, 3)), rng.uniform(*LARGE["radius"], n_spheres)])
+    vel = curl_noise(int(rng.integers(1 << 30)), e, 1.0, 3)
+    vel["domain"] = ((-256, -256, -256), (int(e) + 256, int(e) + 256, int(e) + 256))
+    return sph, vel
+
+
+def bench_large_line(args, ctx, peak, peak_kind):
+    """The large single grid: FP16 line with FP32 beside it."""
+    import torch
+    from sharc.volrus_b200.method import F16, F32, LevelSet
+    dev = torch.device("cuda", args.device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sph, vel = large_grid(args.large_spheres, LARGE["seed"])
+    out = {}
+    with ClockSampler(args.device) as clk:
+        for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
+            t0 = time.perf_counter()
+            ls = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=prec, integrator=3, reinit_iters=2,
+                                  ctx=ctx)
+            build_s = time.perf_counter() - t0
+            r = time_steps(args, ctx, ls, flush, stream, clk, steps=min(args.steps, 5))
+            out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves": r["leaves"],
+                         "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"],
+                         "launch_shape": r["launch"], "create_s": build_s,
+                         "roofline": roofline_of(r, nb, peak, peak_kind, "large8192")}
+            ls.close()
+    f = out["f16"]
+    return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
+            "dtype": "f16 storage, f32 arithmetic",
+            "config": {"workload": "large8192", "spheres": args.large_spheres, "extent": "8192^3",
+                       "radius": "U(6, 40)", "velocity": "curl noise, 3 octaves, 1 voxel/step",
+                       "integrator": "SSP-RK3", "half_width": 3, "reinit_iters": 2,
+                       "active_voxels": f["active_voxels"], "leaves": f["leaves"],
+                       "l2": "inputs larger than L2 and flushed between steps"},
+            "fp32": out["f32"], "fp16_over_fp32": f["value"] / out["f32"]["value"], "roofline": f["roofline"],
+            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "launch_shape": f["launch_shape"], "e2e": None,
+            "clocks": clk.summary(), "gpu_launches": len(STEP_KERNELS) * min(args.steps, 5)}
+
+
 def bench_adjoint_line(args, ctx):
     """The adjoint configuration on its own (forward + backward per step)."""
     with ClockSampler(args.device) as clk, clk.mark():
@@ -682,9 +730,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["deformation512", "batched256", "adjoint256", "reference-sphere128"],
+    ap.add_argument("--workload", choices=["deformation512", "batched256", "large8192", "adjoint256",
+                                           "reference-sphere128"],
                     default="deformation512")
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
+    ap.add_argument("--large-spheres", type=int, default=LARGE["spheres"], help="spheres of the large single grid")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-grid batched measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the full-period accuracy run")
@@ -744,6 +794,8 @@ def main():
         res = bench_batched_line(args, ctx, peak, peak_kind)
     elif args.workload == "adjoint256":
         res = bench_adjoint_line(args, ctx)
+    elif args.workload == "large8192":
+        res = bench_large_line(args, ctx, peak, peak_kind)
     else:
         res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]

@@ -138,9 +138,27 @@ int create_spheres_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* 
             if (((long long)bhi[g][a] - blo[g][a]) >> 3 >= (1ll << (ls->key_bits - 1)) - 4)
                 return set_error(ctx, VLR_ERR_EXTENT, "grid spans too many voxels along an axis for its batch");
         }
-        // candidate leaves: 10^3 box meets some sphere's band
-        std::unordered_map<LeafKey, int, LeafKeyHash> seen;
+        // candidate leaves: the 10^3 box meets some sphere's band.  Each
+        // sphere visits the boxes of its own bounding range once and records
+        // (box, sphere) pairs; a box lying deeper than hw inside any sphere is
+        // interior and skipped.  Candidates keep the order in which a band
+        // first reaches them, and each lists its spheres in ascending index
+        // (the spheres whose band-expanded ball meets the box).
+        std::unordered_map<LeafKey, int, LeafKeyHash> kid;   // box -> index in keys
         std::vector<LeafKey> keys;
+        std::vector<int> disc;                               // discovery rank per key, -1 if none
+        std::vector<char> inner;                             // key lies inside some sphere
+        std::vector<std::pair<int, int>> pairs;              // (key index, sphere), sphere-major
+        int n_disc = 0;
+        auto key_index = [&](const LeafKey& k) {
+            auto it = kid.emplace(k, (int)keys.size());
+            if (it.second) {
+                keys.push_back(k);
+                disc.push_back(-1);
+                inner.push_back(0);
+            }
+            return it.first->second;
+        };
         for (int i = 0; i < G.n_spheres; ++i) {
             const vlr_sphere& S = G.spheres[i];
             int32_t l0[3], l1[3];
@@ -154,30 +172,32 @@ int create_spheres_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* 
                         double bl[3] = {8.0 * x - 1, 8.0 * y - 1, 8.0 * z - 1}, bh[3] = {8.0 * x + 8, 8.0 * y + 8, 8.0 * z + 8};
                         double dmin, dmax;
                         box_dist(S.center, bl, bh, dmin, dmax);
-                        if (dmin < S.radius + hw && dmax > S.radius - hw) {
-                            LeafKey k{x, y, z};
-                            if (seen.emplace(k, 1).second) keys.push_back(k);
+                        if (dmax < S.radius - hw) {
+                            inner[key_index(LeafKey{x, y, z})] = 1;
+                        } else if (dmin < S.radius + hw) {
+                            const int j = key_index(LeafKey{x, y, z});
+                            pairs.emplace_back(j, s0 + i);
+                            if (dmax > S.radius - hw && disc[j] < 0) disc[j] = n_disc++;
                         }
                     }
         }
-        for (const LeafKey& k : keys) {
-            double bl[3] = {8.0 * k.x - 1, 8.0 * k.y - 1, 8.0 * k.z - 1}, bh[3] = {8.0 * k.x + 8, 8.0 * k.y + 8, 8.0 * k.z + 8};
-            bool interior = false;
-            size_t mark = sidx.size();
-            for (int i = 0; i < G.n_spheres; ++i) {
-                const vlr_sphere& S = G.spheres[i];
-                double dmin, dmax;
-                box_dist(S.center, bl, bh, dmin, dmax);
-                if (dmax < S.radius - hw) {
-                    interior = true;
-                    break;
-                }
-                if (dmin < S.radius + hw) sidx.push_back(s0 + i);
-            }
-            if (interior) {
-                sidx.resize(mark);
-                continue;
-            }
+        // pairs grouped by key (stable: spheres stay ascending within a key)
+        std::vector<int> start(keys.size() + 1, 0);
+        for (const auto& pr : pairs) ++start[pr.first + 1];
+        for (size_t j = 0; j < keys.size(); ++j) start[j + 1] += start[j];
+        std::vector<int> by_key(pairs.size());
+        {
+            std::vector<int> fill(start.begin(), start.end() - 1);
+            for (const auto& pr : pairs) by_key[fill[pr.first]++] = pr.second;
+        }
+        std::vector<int> order_of(n_disc, -1);
+        for (size_t j = 0; j < keys.size(); ++j)
+            if (disc[j] >= 0) order_of[disc[j]] = (int)j;
+        for (int r = 0; r < n_disc; ++r) {
+            const int j = order_of[r];
+            if (inner[j]) continue;
+            const LeafKey& k = keys[j];
+            sidx.insert(sidx.end(), by_key.begin() + start[j], by_key.begin() + start[j + 1]);
             cand.push_back(make_int4(8 * k.x, 8 * k.y, 8 * k.z, g));
             off.push_back((int)sidx.size());
         }

@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(kThreads) k_m_volume(MLeafArrays A, const T* _
         const int slot = A.list[li];
         const int4 o = A.origin[slot];
         const float hw = params[o.w].hw;
-        if (threadIdx.x < kNbr) s_nbr[threadIdx.x] = A.nbr[slot * kNbr + threadIdx.x];
+        if (threadIdx.x < kNbr) s_nbr[threadIdx.x] = A.nbr[(size_t)slot * kNbr + threadIdx.x];
         __syncthreads();
         double acc = 0.0;
         for (int r = 0; r < 2; ++r) {

@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     int slot = A.list[li];
     int4 o = A.origin[slot];
     build_stage_desc<T, H, NT>(s_desc);
-    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
+    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
     stage_async<T, H, NT>(s_desc, s_nbr[0], src, A.mask, s_raw, s_m);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
         // loads for the leaves ahead (consumed one iteration later)
         int4 o_n = make_int4(0, 0, 0, -1);
         if (slot_n >= 0) o_n = A.origin[slot_n];
-        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[slot_n * kNbr + lane] : -1;
+        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
         const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
         if (o.w != cur_gid) {
             __syncthreads();
@@ -710,7 +710,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     int slot = A.list[li];
     int4 o = A.origin[slot];
     build_stage_desc<T, 2, NT>(s_desc);
-    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[slot * kNbr + lane] : -1;
+    if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
     stage_async<T, 2, NT>(s_desc, s_nbr[0], src, A.dmask, s_raw, s_dm);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         const int cur = it & 1;
         int4 o_n = make_int4(0, 0, 0, -1);
         if (slot_n >= 0) o_n = A.origin[slot_n];
-        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[slot_n * kNbr + lane] : -1;
+        const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
         const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
         stage_ready();  // barrier 1
         const int* nbr = s_nbr[cur];

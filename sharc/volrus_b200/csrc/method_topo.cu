@@ -265,7 +265,7 @@ __global__ void k_t_nbr(const int* list, int* scalars, const int4* origin, const
         const int s = list[i];
         int dx, dy, dz;
         dir_of(d, dx, dy, dz);
-        nbr[s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
+        nbr[(size_t)s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         scalars[0] = count;
@@ -319,7 +319,7 @@ __global__ void k_nbr(const int* list, const int* count_ptr, const int4* origin,
         const int s = list[i];
         int dx, dy, dz;
         dir_of(d, dx, dy, dz);
-        nbr[s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
+        nbr[(size_t)s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
     }
 }
 
