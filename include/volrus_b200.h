@@ -75,6 +75,12 @@ int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, con
 /* Leaf count, active voxel count, background and transform of a grid. */
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf);
+/* Replaces the position update of advect_particles (RK4, rk4 = 1) and
+ * advect_particles_euler (rk4 = 0) (src/tools/advection.rs:58-110): positions
+ * (f64, 3 per particle, world units) move in place through VelocityField
+ * {vx, vy, vz}; re-binning into the point grid's leaves stays with the caller. */
+int vlr_advect_particles(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, const vlr_grid* vz, double* positions,
+                         size_t n, double dt, int rk4);
 /* Replaces dilate(&mut Grid<f32>, iterations) (src/tools/morphology.rs:20-35):
  * every inactive voxel with an active 6-neighbour becomes active with the
  * value of the neighbour that comes first in the tree's iteration order

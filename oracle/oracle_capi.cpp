@@ -86,6 +86,39 @@ void vo_sample_trilinear(void* g, const double* world, size_t n, float* out) {
     for (size_t i = 0; i < n; ++i) out[i] = sample_trilinear(*(Grid*)g, world + 3 * i);
 }
 
+// advect_particles / advect_particles_euler (src/tools/advection.rs:58-110):
+// the position update only, f64, in the reference's evaluation order.
+void vo_advect_particles(void* vx, void* vy, void* vz, double* pos, size_t n, double dt, int rk4) {
+    const Grid &gx = *(Grid*)vx, &gy = *(Grid*)vy, &gz = *(Grid*)vz;
+    auto sample = [&](const double p[3], double v[3]) {
+        v[0] = (double)sample_trilinear(gx, p);
+        v[1] = (double)sample_trilinear(gy, p);
+        v[2] = (double)sample_trilinear(gz, p);
+    };
+    for (size_t i = 0; i < n; ++i) {
+        double* p = pos + 3 * i;
+        double v[3];
+        if (!rk4) {
+            sample(p, v);
+            for (int a = 0; a < 3; ++a) p[a] += dt * v[a];
+            continue;
+        }
+        double k1[3], k2[3], k3[3], k4[3], q[3];
+        sample(p, v);
+        for (int a = 0; a < 3; ++a) k1[a] = dt * v[a];
+        for (int a = 0; a < 3; ++a) q[a] = p[a] + k1[a] * 0.5;
+        sample(q, v);
+        for (int a = 0; a < 3; ++a) k2[a] = dt * v[a];
+        for (int a = 0; a < 3; ++a) q[a] = p[a] + k2[a] * 0.5;
+        sample(q, v);
+        for (int a = 0; a < 3; ++a) k3[a] = dt * v[a];
+        for (int a = 0; a < 3; ++a) q[a] = p[a] + k3[a];
+        sample(q, v);
+        for (int a = 0; a < 3; ++a) k4[a] = dt * v[a];
+        for (int a = 0; a < 3; ++a) p[a] = p[a] + (k1[a] + 2.0 * k2[a] + 2.0 * k3[a] + k4[a]) / 6.0;
+    }
+}
+
 void* vo_advect_level_set(void* g, void* vx, void* vy, void* vz, double dt) {
     return new Grid(advect_level_set(*(Grid*)g, *(Grid*)vx, *(Grid*)vy, *(Grid*)vz, dt));
 }

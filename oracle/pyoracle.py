@@ -43,6 +43,7 @@ SIGS = {
     "vo_trim_narrow_band": (None, [P, C.c_float]),
     "vo_rebuild_narrow_band": (None, [P, C.c_float, C.c_int]),
     "vo_dilate": (None, [P, C.c_uint]),
+    "vo_advect_particles": (None, [P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
     "vo_remove_empty_leaves": (None, [P]),
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
@@ -195,6 +196,14 @@ class OGrid:
                 self.h = None
         except Exception:
             pass
+
+
+def advect_particles(vx, vy, vz, positions, dt, rk4=True):
+    """Positions (n, 3) f64 after one advect_particles (RK4) or
+    advect_particles_euler step through the grids vx, vy, vz."""
+    p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3).copy()
+    load().vo_advect_particles(vx.h, vy.h, vz.h, _p(p, C.c_double), len(p), dt, 1 if rk4 else 0)
+    return p
 
 
 def uniform_velocity(voxel_size, vel, bbox_min=None, bbox_max=None):

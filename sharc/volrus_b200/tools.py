@@ -11,6 +11,8 @@ it replaces and runs on the B200 through the C ABI:
     rebuild_narrow_band(grid, half_width)            src/tools/level_set_track.rs:80-114
     make_level_set_sphere(r, c, vs, hw) -> Grid      src/tools/sphere.rs:17-59
     dilate(grid, iterations)                         src/tools/morphology.rs:20-35
+    advect_particles(positions, velocity, dt)        src/tools/advection.rs:58-95 (positions only)
+    advect_particles_euler(positions, velocity, dt)  src/tools/advection.rs:97-110 (positions only)
 
 Host ``Grid`` arguments are uploaded, processed and downloaded per call (the
 drop-in form); ``DeviceGrid`` arguments stay resident in HBM between calls.
@@ -165,6 +167,33 @@ def rebuild_narrow_band(grid, half_width: float, ctx: Context | None = None):
               "vlr_rebuild_narrow_band")
     if uploaded:
         _replace(grid, g.download())
+
+
+def _particles(positions, velocity: VelocityField, dt: float, rk4: bool, ctx):
+    ctx = ctx or Context.default()
+    p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3).copy()
+    made = [_as_device(g, ctx) for g in (velocity.vx, velocity.vy, velocity.vz)]
+    try:
+        ctx.check(ctx.lib.vlr_advect_particles(ctx.handle, made[0][0].handle, made[1][0].handle, made[2][0].handle,
+                                               ptr(p, C.c_double), len(p), float(dt), 1 if rk4 else 0),
+                  "vlr_advect_particles")
+    finally:
+        for d, created in made:
+            if created:
+                d.close()
+    return p
+
+
+def advect_particles(positions, velocity: VelocityField, dt: float, ctx: Context | None = None) -> np.ndarray:
+    """Position update of ``advect_particles`` (src/tools/advection.rs:58-95):
+    RK4 through the velocity field; (n, 3) world positions in, new ones out.
+    Re-binning into a point grid's leaves is the caller's (``PointDataGrid::rebin``)."""
+    return _particles(positions, velocity, dt, True, ctx)
+
+
+def advect_particles_euler(positions, velocity: VelocityField, dt: float, ctx: Context | None = None) -> np.ndarray:
+    """Position update of ``advect_particles_euler`` (src/tools/advection.rs:97-110)."""
+    return _particles(positions, velocity, dt, False, ctx)
 
 
 def dilate(grid, iterations: int, ctx: Context | None = None):
