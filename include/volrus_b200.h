@@ -75,6 +75,13 @@ int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, con
 /* Leaf count, active voxel count, background and transform of a grid. */
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf);
+/* Replaces extend_velocity(&Grid<f32>, &mut vx, &mut vy, &mut vz, f32)
+ * (src/tools/level_set_track.rs:115-160): band voxels of the SDF copy the
+ * velocity of the nearest interface voxel (ties: first in iteration order,
+ * 128^3 tiles in ascending origin order) and become active in vx, vy, vz,
+ * whose missing leaves are allocated at their backgrounds. */
+int vlr_extend_velocity(vlr_ctx* ctx, const vlr_grid* sdf, vlr_grid* vx, vlr_grid* vy, vlr_grid* vz,
+                        float half_width);
 /* Replaces the position update of advect_particles (RK4, rk4 = 1) and
  * advect_particles_euler (rk4 = 0) (src/tools/advection.rs:58-110): positions
  * (f64, 3 per particle, world units) move in place through VelocityField

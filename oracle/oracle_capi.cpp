@@ -142,6 +142,9 @@ size_t vo_find_zero_crossings(void* g, int32_t* out, size_t cap) {
 void vo_trim_narrow_band(void* g, float hw) { trim_narrow_band(*(Grid*)g, hw); }
 void vo_rebuild_narrow_band(void* g, float hw, int brute) { rebuild_narrow_band(*(Grid*)g, hw, brute != 0); }
 void vo_dilate(void* g, unsigned iterations) { dilate(*(Grid*)g, iterations); }
+void vo_extend_velocity(void* sdf, void* vx, void* vy, void* vz, float hw) {
+    extend_velocity(*(Grid*)sdf, *(Grid*)vx, *(Grid*)vy, *(Grid*)vz, hw);
+}
 void vo_remove_empty_leaves(void* g) { ((Grid*)g)->remove_empty_leaves(); }
 
 // One step of the reference pipeline, timed on this thread: advect_level_set

@@ -44,6 +44,7 @@ SIGS = {
     "vo_rebuild_narrow_band": (None, [P, C.c_float, C.c_int]),
     "vo_dilate": (None, [P, C.c_uint]),
     "vo_advect_particles": (None, [P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
+    "vo_extend_velocity": (None, [P, P, P, P, C.c_float]),
     "vo_remove_empty_leaves": (None, [P]),
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
@@ -185,6 +186,10 @@ class OGrid:
 
     def dilate(self, iterations=1):
         self.lib.vo_dilate(self.h, iterations)
+
+    def extend_velocity(self, vx, vy, vz, half_width):
+        """extend_velocity(self as the SDF, vx, vy, vz, half_width), in place on vx, vy, vz."""
+        self.lib.vo_extend_velocity(self.h, vx.h, vy.h, vz.h, half_width)
 
     def remove_empty_leaves(self):
         self.lib.vo_remove_empty_leaves(self.h)

@@ -371,6 +371,42 @@ inline void rebuild_narrow_band(Grid& g, float half_width, bool brute) {
     g.remove_empty_leaves();
 }
 
+// extend_velocity (src/tools/level_set_track.rs:115-160): band voxels copy
+// the velocity of their nearest interface voxel (first minimum in iteration
+// order, as min_by_key returns it) and become active in each velocity grid.
+inline void extend_velocity(const Grid& sdf, Grid& vx, Grid& vy, Grid& vz, float half_width) {
+    const float vs = (float)sdf.voxel_size;
+    const float band = half_width * vs;
+    std::vector<Coord> iface, bandv;
+    sdf.for_each_active([&](Coord c, float v) {
+        if (std::fabs(v) < vs) iface.push_back(c);
+    });
+    if (iface.empty()) return;
+    sdf.for_each_active([&](Coord c, float v) {
+        const float a = std::fabs(v);
+        if (a >= vs && a < band) bandv.push_back(c);
+    });
+    auto dist_sq = [](const Coord& a, const Coord& b) {
+        const int64_t dx = (int64_t)(a.x - b.x), dy = (int64_t)(a.y - b.y), dz = (int64_t)(a.z - b.z);
+        return dx * dx + dy * dy + dz * dz;
+    };
+    for (const Coord& c : bandv) {
+        size_t best = 0;
+        int64_t bd = dist_sq(c, iface[0]);
+        for (size_t k = 1; k < iface.size(); ++k) {
+            const int64_t d = dist_sq(c, iface[k]);
+            if (d < bd) {
+                bd = d;
+                best = k;
+            }
+        }
+        const Coord& s = iface[best];
+        vx.set(c, vx.get(s));
+        vy.set(c, vy.get(s));
+        vz.set(c, vz.get(s));
+    }
+}
+
 // dilate (src/tools/morphology.rs:20-35): snapshot, then activate inactive
 // 6-neighbours with the current voxel's value.  First writer wins, so the
 // values depend on iteration order; only the topology is order independent.

@@ -96,6 +96,7 @@ SIGNATURES = {
     "vlr_grid_create": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t, PP]),
     "vlr_grid_info": (C.c_int, [P, P, size_p, C.POINTER(C.c_uint64), flt_p, C.POINTER(vlr_transform)]),
     "vlr_grid_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
+    "vlr_extend_velocity": (C.c_int, [P, P, P, P, P, C.c_float]),
     "vlr_advect_particles": (C.c_int, [P, P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
     "vlr_dilate": (C.c_int, [P, P, C.c_uint]),
     "vlr_grid_from_vol": (C.c_int, [P, P, C.c_size_t, PP, C.POINTER(C.c_int)]),

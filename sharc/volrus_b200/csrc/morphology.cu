@@ -26,6 +26,10 @@
 
 using namespace vlr;
 
+namespace vlr {
+int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origins);
+}
+
 namespace {
 
 // neighbour-table index of the 6 face directions -x, +x, -y, +y, -z, +z
@@ -164,16 +168,43 @@ int grow_for_dilation(vlr_ctx* ctx, vlr_grid* g) {
         for (int d = 0; d < 6; ++d)
             if (flags[i] >> d & 1)
                 nw.insert(nw.end(), {org[i].x + kStep[d][0], org[i].y + kStep[d][1], org[i].z + kStep[d][2]});
-    const size_t m0 = nw.size() / 3;
+    return grid_add_leaves(ctx, g, nw);
+}
+
+}  // namespace
+
+namespace vlr {
+
+// Add leaves at the given origins (3 ints each, any order, repeats and
+// origins already present allowed) to a world-unit f32 grid, inactive at the
+// background, keeping the pool in (x, y, z) order of origin; rebuilds the
+// hash and neighbour table when anything was added.
+int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origins) {
+    const int n = g->n;
+    const size_t m0 = origins.size() / 3;
     if (!m0) return VLR_OK;
+    std::vector<int4> org(n);
+    if (n)
+        VLR_CUDA(ctx, cudaMemcpyAsync(org.data(), g->origin, sizeof(int4) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     std::vector<int> ord(m0);
     std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return less3(&nw[3 * a], &nw[3 * b]); });
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return less3(&origins[3 * a], &origins[3 * b]); });
     std::vector<int32_t> uniq;
-    for (size_t k = 0; k < m0; ++k)
-        if (k == 0 || less3(&nw[3 * ord[k - 1]], &nw[3 * ord[k]]))
-            uniq.insert(uniq.end(), &nw[3 * ord[k]], &nw[3 * ord[k]] + 3);
+    for (size_t k = 0; k < m0; ++k) {
+        const int32_t* c = &origins[3 * ord[k]];
+        if (k > 0 && !less3(&origins[3 * ord[k - 1]], c)) continue;
+        // skip origins the grid already holds (the pool is sorted)
+        const int4 key = make_int4(c[0], c[1], c[2], 0);
+        const bool present = std::binary_search(org.begin(), org.end(), key, [](const int4& a, const int4& b) {
+            if (a.x != b.x) return a.x < b.x;
+            if (a.y != b.y) return a.y < b.y;
+            return a.z < b.z;
+        });
+        if (!present) uniq.insert(uniq.end(), c, c + 3);
+    }
     const int m = (int)(uniq.size() / 3);
+    if (!m) return VLR_OK;
     // merged (x, y, z) order of the old leaves (already sorted) and the new ones
     std::vector<int> dst_old(n), dst_new(m);
     std::vector<int4> o_new(m);
@@ -197,7 +228,7 @@ int grow_for_dilation(vlr_ctx* ctx, vlr_grid* g) {
         }
     }
     long long base[3];
-    rc = choose_base(ctx, all.data(), (size_t)(n + m), base);
+    int rc = choose_base(ctx, all.data(), (size_t)(n + m), base);
     if (rc) return rc;
     vlr_grid tmp;
     tmp.ctx = ctx;
@@ -208,7 +239,8 @@ int grow_for_dilation(vlr_ctx* ctx, vlr_grid* g) {
     int4* d_onew = nullptr;
     VLR_CUDA(ctx, cudaMallocAsync(&d_onew, sizeof(int4) * m + sizeof(int) * (n + m), ctx->stream));
     int* d_idx = reinterpret_cast<int*>(d_onew + m);
-    VLR_CUDA(ctx, cudaMemcpyAsync(d_idx, dst_old.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (n)
+        VLR_CUDA(ctx, cudaMemcpyAsync(d_idx, dst_old.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(d_idx + n, dst_new.data(), sizeof(int) * m, cudaMemcpyHostToDevice, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(d_onew, o_new.data(), sizeof(int4) * m, cudaMemcpyHostToDevice, ctx->stream));
     k_dil_merge<<<std::min(n + m, ctx->sm_count * 16), 128, 0, ctx->stream>>>(
@@ -231,7 +263,7 @@ int grow_for_dilation(vlr_ctx* ctx, vlr_grid* g) {
     return grid_index(ctx, g);
 }
 
-}  // namespace
+}  // namespace vlr
 
 extern "C" {
 

@@ -1,5 +1,7 @@
 // Host entry points of the reference-semantics kernels (ref_ops.cu).
 #pragma once
+#include <vector>
+
 #include "vlr_host.hpp"
 
 namespace vlr {
@@ -12,5 +14,7 @@ int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size
 int trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int make_sphere(vlr_ctx* ctx, double radius, const double c[3], double vs, double hw, vlr_grid* out);
+// Add inactive background leaves at `origins` (3 ints each) to a world-unit grid (morphology.cu).
+int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origins);
 
 }  // namespace vlr

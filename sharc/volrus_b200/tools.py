@@ -11,6 +11,7 @@ it replaces and runs on the B200 through the C ABI:
     rebuild_narrow_band(grid, half_width)            src/tools/level_set_track.rs:80-114
     make_level_set_sphere(r, c, vs, hw) -> Grid      src/tools/sphere.rs:17-59
     dilate(grid, iterations)                         src/tools/morphology.rs:20-35
+    extend_velocity(sdf, vx, vy, vz, half_width)     src/tools/level_set_track.rs:115-160
     advect_particles(positions, velocity, dt)        src/tools/advection.rs:58-95 (positions only)
     advect_particles_euler(positions, velocity, dt)  src/tools/advection.rs:97-110 (positions only)
 
@@ -167,6 +168,23 @@ def rebuild_narrow_band(grid, half_width: float, ctx: Context | None = None):
               "vlr_rebuild_narrow_band")
     if uploaded:
         _replace(grid, g.download())
+
+
+def extend_velocity(sdf, vx, vy, vz, half_width: float, ctx: Context | None = None):
+    """``extend_velocity`` (src/tools/level_set_track.rs:115-160), in place on
+    vx, vy, vz (host ``Grid`` or ``DeviceGrid``)."""
+    ctx = ctx or Context.default()
+    made = [_as_device(g, ctx) for g in (sdf, vx, vy, vz)]
+    try:
+        ctx.check(ctx.lib.vlr_extend_velocity(ctx.handle, *(d.handle for d, _ in made), C.c_float(half_width)),
+                  "vlr_extend_velocity")
+        for (d, created), host in zip(made[1:], (vx, vy, vz)):
+            if created:
+                _replace(host, d.download())
+    finally:
+        for d, created in made:
+            if created:
+                d.close()
 
 
 def _particles(positions, velocity: VelocityField, dt: float, rk4: bool, ctx):
