@@ -219,6 +219,32 @@ TRAFFIC_PER_LEAF: dict = {
 }
 
 
+# Warp instructions per leaf of one launch (smsp__inst_executed.sum / leaves)
+# from the same ncu captures, FP16, 128-thread CTAs.
+INST_PER_LEAF: dict = {
+    ("deformation512", "k_m_advect"): 12154621 / 2850,
+    ("deformation512", "k_m_reinit"): 17443240 / 2850,
+    ("batched256", "k_m_advect"): 1063617820 / 151238,
+    ("batched256", "k_m_reinit"): 864912635 / 151238,
+}
+SM_COUNT = 148
+ISSUE_PER_SM_PER_CYCLE = 4  # one warp instruction per scheduler per cycle
+
+
+def issue_roofline(r, workload, sm_mhz):
+    """Instruction-issue roofline of the dominant stencil kernel: warp
+    instructions per launch (ncu count per leaf x leaves) / launch time, against
+    148 SMs x 4 schedulers x the sampled SM clock."""
+    dom = max(("k_m_advect", "k_m_reinit"), key=lambda k: r["kernels"][k])
+    ipl = INST_PER_LEAF.get((workload, dom))
+    if ipl is None or not sm_mhz:
+        return None
+    achieved = ipl * r["leaves"] / (r["kernels"][dom] * 1e-3)
+    peak = SM_COUNT * ISSUE_PER_SM_PER_CYCLE * sm_mhz * 1e6
+    return {"kernel": dom, "achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "inst_per_leaf_ncu": ipl, "sm_mhz": sm_mhz}
+
+
 def method_bytes_per_leaf(value_bytes: int):
     """Algorithmic bytes per leaf and launch.
     advect: read values 512*s, mask 64, origin 16, neighbour row 108; write values 512*s, dilated mask 64.
@@ -376,7 +402,8 @@ def bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=None):
     out = {}
     for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
         r = run_batched(args, ctx, prec, flush, stream, clk, steps=steps)
-        out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves_this_rank": r["leaves"],
+        out[name] = {"_r": {"kernels": r["kernels"], "leaves": r["leaves"]},
+                     "value": r["value"], "ms_per_step": r["ms_per_step"], "leaves_this_rank": r["leaves"],
                      "active_voxels": r["active"], "grids_this_rank": r["grids_this_rank"], "kernels_ms_per_launch": r["kernels"],
                      "roofline": roofline_of(r, nb, peak, peak_kind, "batched256")}
         r["ls"].close()
@@ -400,11 +427,15 @@ def bench_batched_line(args, ctx, peak, peak_kind):
     with ClockSampler(args.device) as clk:
         b = bench_batched(args, ctx, peak, peak_kind, flush, stream, clk)
     f = b["f16"]
+    ck = clk.summary()
+    f["issue_roofline"] = issue_roofline(f.pop("_r"), "batched256", ck.get("sm_mhz"))
+    b["f32"].pop("_r", None)
     return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
             "dtype": "f16 storage, f32 arithmetic", "config": dict(b["config"], active_voxels=f["active_voxels"],
                                                                   leaves_this_rank=f["leaves_this_rank"]),
             "fp32": b["f32"], "fp16_over_fp32": b["fp16_over_fp32"], "roofline": f["roofline"],
-            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "e2e": None, "clocks": clk.summary(),
+            "issue_roofline": f["issue_roofline"],
+            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "e2e": None, "clocks": ck,
             "gpu_launches": len(STEP_KERNELS) * args.steps}
 
 
@@ -615,12 +646,18 @@ def bench_deformation(args, ctx, peak, peak_kind):
         "launch_shape": r16["launch"],
         "fp16_over_fp32": r16["value"] / r32["value"],
         "roofline": roofline_of(r16, 2, peak, peak_kind, "deformation512"),
+        "issue_roofline": None,
         "kernels_ms_per_launch": r16["kernels"],
         "e2e": e2e,
         "clocks": clk.summary(),
         "gpu_launches": launches_per_step * args.steps,
     }
+    ck = line["clocks"]
+    line["issue_roofline"] = issue_roofline(r16, "deformation512", ck.get("sm_mhz"))
     if batched is not None:
+        batched["f16"]["issue_roofline"] = issue_roofline(batched["f16"]["_r"], "batched256", ck.get("sm_mhz"))
+        for k in ("f16", "f32"):
+            batched[k].pop("_r", None)
         line["batched256"] = batched
     if accuracy is not None:
         line["full_period"] = accuracy
@@ -830,7 +867,7 @@ def main():
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint"):
+        for k in ("issue_roofline", "fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint"):
             if k in res and res[k] is None:
                 continue
             if k in res:
