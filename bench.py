@@ -360,14 +360,12 @@ def e2e_method(args, ctx, ls, precision):
 
     def call():
         nonlocal cur, h2d, d2h
-        ctx.check(ctx.lib.vlr_ls_upload(ctx.handle, ls.handle, ptr(pin_o, C.c_int32), ptr(pin_m, C.c_uint64),
-                                        ptr(pin_v, C.c_float), cur), "upload")
-        h2d = cur * (12 + 64 + 2048)
-        ctx.check(ctx.lib.vlr_ls_step(ctx.handle, ls.handle, 1), "step")
         nn = C.c_size_t()
-        ctx.check(ctx.lib.vlr_ls_info(ctx.handle, ls.handle, C.byref(nn), None, None), "info")
-        ctx.check(ctx.lib.vlr_ls_download(ctx.handle, ls.handle, ptr(out_o, C.c_int32), ptr(out_m, C.c_uint64),
-                                          ptr(out_v, C.c_float), cap), "download")
+        ctx.check(ctx.lib.vlr_ls_step_host(ctx.handle, ls.handle, ptr(pin_o, C.c_int32), ptr(pin_m, C.c_uint64),
+                                           ptr(pin_v, C.c_float), cur, 1, ptr(out_o, C.c_int32),
+                                           ptr(out_m, C.c_uint64), ptr(out_v, C.c_float), cap, C.byref(nn)),
+                  "vlr_ls_step_host")
+        h2d = cur * (12 + 64 + 2048)
         d2h = nn.value * (12 + 64 + 2048)
         return nn.value
 
@@ -380,7 +378,7 @@ def e2e_method(args, ctx, ls, precision):
     e2e_s = (time.perf_counter() - t0) / args.steps
     return {"value": a / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "seconds_per_step": e2e_s,
-            "path": "vlr_ls_upload + vlr_ls_step + vlr_ls_download, pinned host buffers"}
+            "path": "vlr_ls_step_host (upload, one step, download), pinned host buffers"}
 
 
 def roofline_of(r, value_bytes, peak, peak_kind, workload):

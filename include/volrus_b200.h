@@ -281,6 +281,14 @@ int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_
  * and allocations: the host-resident form of a step is upload, step, download. */
 int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
                   size_t n_leaves);
+/* The host-resident form of n_steps steps in one call: replace the state with
+ * host leaves (as vlr_ls_upload), step, and write the result (as
+ * vlr_ls_download) into caller buffers of cap_leaves leaves; *n_out = leaves
+ * written.  Waits once for the leaf count and device errors and once for the
+ * copies.  No counterpart in the reference (its step is serial Rust). */
+int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                     size_t n_leaves, int n_steps, int32_t* out_origins, uint64_t* out_masks, float* out_phi,
+                     size_t cap_leaves, size_t* n_out);
 /* Allocated leaves (sorted (x, y, z)), masks, values in voxel units as f32. */
 int vlr_ls_download(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* origins, uint64_t* masks, float* phi,
                     size_t cap_leaves);

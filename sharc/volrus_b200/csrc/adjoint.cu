@@ -52,6 +52,10 @@ struct vlr_adjoint {
     float* segment = nullptr;            // chk_every x n_band (recomputed states)
     float* lam[2] = {nullptr, nullptr};
     float* lam_final = nullptr;          // lam buffer holding dL/dphi_0 after the last backward pass
+    // the forward and backward step loops captured as CUDA graphs (dropped
+    // when the velocity, hence the reach, changes)
+    cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
+    float* bwd_final = nullptr;          // lam buffer the captured backward loop ends in
     float* gvel = nullptr;               // dL/dV, 3 x n^3
     float3* G = nullptr;
     int reach = 1;                       // displacement bound per step, voxels (ceil of dt max|V|)
@@ -352,7 +356,14 @@ namespace {
 
 int blocks_for(vlr_ctx* ctx, long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, ctx->sm_count * 8ll)); }
 
+void adj_drop_graphs(vlr_adjoint* a) {
+    if (a->fwd_exec) cudaGraphExecDestroy(a->fwd_exec);
+    if (a->bwd_exec) cudaGraphExecDestroy(a->bwd_exec);
+    a->fwd_exec = a->bwd_exec = nullptr;
+}
+
 void adj_free(vlr_adjoint* a) {
+    adj_drop_graphs(a);
     void* ptrs[] = {a->origin, a->nbr, a->hkey, a->hval, a->phi[0], a->phi[1], a->phi_init, a->bidx, a->bvox,
                     a->ub, a->vel, a->checkpoints, a->segment, a->lam[0], a->lam[1], a->G, a->keys, a->pvals,
                     a->scratch, a->gvel, a->foot_pk, a->foot_w};
@@ -380,6 +391,109 @@ int enqueue_forward_step(vlr_ctx* ctx, vlr_adjoint* a, int k, const float* src, 
                   a->origin, a->nbr, a->bidx, a->ub, src, dst, a->n_leaves, step_factor(a, k), a->hw,
                   ctx->d_errword));
     VLR_CUDA(ctx, cudaGetLastError());
+    return VLR_OK;
+}
+
+// The forward step loop from the initial state (checkpoints every C steps;
+// phi_K on the band into lam[1]), enqueued without waiting.
+int adj_forward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)a->n_band;
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves, cudaMemcpyDeviceToDevice,
+                                  st));
+    int cur = 0;
+    for (int k = 0; k < a->steps; ++k) {
+        if (k % a->chk_every == 0)
+            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
+                                                                   a->checkpoints + (size_t)(k / a->chk_every) * nb);
+        int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
+        if (rc) return rc;
+        cur = 1 - cur;
+    }
+    k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur], a->lam[1]);
+    VLR_CUDA(ctx, cudaGetLastError());
+    return VLR_OK;
+}
+
+// The backward step loop from lambda_K in lam[1] (recompute from checkpoints,
+// gather transpose, G accumulation), enqueued without waiting; records the
+// lam buffer it ends in.
+int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
+    cudaStream_t st = ctx->stream;
+    const size_t nb = (size_t)a->n_band;
+    float* lam = a->lam[1];
+    k_zero3<<<blocks_for(ctx, nb), 256, 0, st>>>(a->G, (int)nb);
+    const int C = a->chk_every;
+    for (int seg = (a->steps - 1) / C; seg >= 0; --seg) {
+        const int k0 = seg * C, k1 = std::min(a->steps, k0 + C);
+        // recompute phi_k0 .. phi_{k1-1} from the checkpoint
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves,
+                                      cudaMemcpyDeviceToDevice, st));
+        k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->checkpoints + (size_t)seg * nb,
+                                                                a->phi[0]);
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[1], a->phi[0], sizeof(float) * 512 * a->n_leaves,
+                                      cudaMemcpyDeviceToDevice, st));
+        int cur = 0;
+        for (int k = k0; k < k1; ++k) {
+            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
+                                                                   a->segment + (size_t)(k - k0) * nb);
+            if (k + 1 < k1) {
+                int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
+                if (rc) return rc;
+                cur = 1 - cur;
+            }
+        }
+        // adjoint steps k1-1 .. k0: phi_k from the segment (scattered into a full pool)
+        for (int k = k1 - 1; k >= k0; --k) {
+            k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb,
+                                                                    a->segment + (size_t)(k - k0) * nb, a->phi[0]);
+            float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
+            const float sk = step_factor(a, k);
+            VLR_TIMED(ctx, "k_adj_pack",
+                      k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk, a->foot_pk,
+                                                                      a->foot_w));
+            const int gb = blocks_for(ctx, nb);
+            if (a->reach == 1)
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<1><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, 1, lam_out, a->G));
+            else if (a->reach == 2)
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<2><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, 2, lam_out, a->G));
+            else
+                VLR_TIMED(ctx, "k_adj_lambda",
+                          k_adj_lambda<0><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
+                                                              a->foot_w, sk, a->hw, a->reach, lam_out, a->G));
+            lam = lam_out;
+        }
+        (void)cur;
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    a->bwd_final = lam;
+    return VLR_OK;
+}
+
+// Run `enqueue` through a CUDA graph captured on first use (or directly while
+// per-kernel timing is on, which brackets launches with events).
+template <class F>
+int run_captured(vlr_ctx* ctx, cudaGraphExec_t* exec, F&& enqueue) {
+    if (ctx->timer.enabled) return enqueue();
+    if (!*exec) {
+        VLR_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return check_cuda(ctx, e, "cudaStreamEndCapture");
+        const cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) return check_cuda(ctx, e2, "cudaGraphInstantiate");
+    }
+    VLR_CUDA(ctx, cudaGraphLaunch(*exec, ctx->stream));
     return VLR_OK;
 }
 
@@ -511,6 +625,7 @@ int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, con
         size_t nvel = 3ull * a->n_stag * a->n_stag * a->n_stag;
         const int reach = reach_of(vel, nvel, a->dt);
         if (reach > 6) return set_error(ctx, VLR_ERR_REACH, "dt * max|V| exceeds 6 voxels per step");
+        if (reach != a->reach) adj_drop_graphs(a);
         a->reach = reach;
         VLR_CUDA(ctx, cudaMemcpyAsync(a->vel, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
         k_adj_upsample<<<blocks_for(ctx, a->n_band), 256, 0, st>>>(a->bvox, a->origin, a->n_band, a->vel, a->n_stag,
@@ -525,23 +640,11 @@ int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, con
 // phi_K on the band (host, n_band floats) when phi_k_band is not null.
 int vlr_adj_forward_device(vlr_ctx* ctx, vlr_adjoint* a, float* d_phi_k_band) {
     if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
-    cudaStream_t st = ctx->stream;
-    const size_t nb = (size_t)a->n_band;
-    VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves, cudaMemcpyDeviceToDevice,
-                                  st));
-    int cur = 0;
-    for (int k = 0; k < a->steps; ++k) {
-        if (k % a->chk_every == 0)
-            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
-                                                                   a->checkpoints + (size_t)(k / a->chk_every) * nb);
-        int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
-        if (rc) return rc;
-        cur = 1 - cur;
-    }
-    k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur], a->lam[1]);
-    VLR_CUDA(ctx, cudaGetLastError());
+    int rc = run_captured(ctx, &a->fwd_exec, [&]() { return adj_forward_enqueue(ctx, a); });
+    if (rc) return rc;
     if (d_phi_k_band)
-        VLR_CUDA(ctx, cudaMemcpyAsync(d_phi_k_band, a->lam[1], sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
+        VLR_CUDA(ctx, cudaMemcpyAsync(d_phi_k_band, a->lam[1], sizeof(float) * a->n_band, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
     return VLR_OK;
 }
 
@@ -562,57 +665,11 @@ int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_ph
     if (!ctx || !a || !d_grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
-    float* lam = a->lam[1];
-    if (d_grad_phik_band != lam)
-        VLR_CUDA(ctx, cudaMemcpyAsync(lam, d_grad_phik_band, sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
-    k_zero3<<<blocks_for(ctx, nb), 256, 0, st>>>(a->G, (int)nb);
-    const int C = a->chk_every;
-    for (int seg = (a->steps - 1) / C; seg >= 0; --seg) {
-        const int k0 = seg * C, k1 = std::min(a->steps, k0 + C);
-        // recompute phi_k0 .. phi_{k1-1} from the checkpoint
-        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves,
-                                      cudaMemcpyDeviceToDevice, st));
-        k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->checkpoints + (size_t)seg * nb,
-                                                                a->phi[0]);
-        VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[1], a->phi[0], sizeof(float) * 512 * a->n_leaves,
-                                      cudaMemcpyDeviceToDevice, st));
-        int cur = 0;
-        for (int k = k0; k < k1; ++k) {
-            k_adj_gather_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->phi[cur],
-                                                                   a->segment + (size_t)(k - k0) * nb);
-            if (k + 1 < k1) {
-                int rc = enqueue_forward_step(ctx, a, k, a->phi[cur], a->phi[1 - cur]);
-                if (rc) return rc;
-                cur = 1 - cur;
-            }
-        }
-        // adjoint steps k1-1 .. k0: phi_k from the segment (scattered into a full pool)
-        for (int k = k1 - 1; k >= k0; --k) {
-            k_adj_scatter_band<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb,
-                                                                    a->segment + (size_t)(k - k0) * nb, a->phi[0]);
-            float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
-            const float sk = step_factor(a, k);
-            VLR_TIMED(ctx, "k_adj_pack",
-                      k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk, a->foot_pk,
-                                                                      a->foot_w));
-            const int gb = blocks_for(ctx, nb);
-            if (a->reach == 1)
-                VLR_TIMED(ctx, "k_adj_lambda",
-                          k_adj_lambda<1><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, 1, lam_out, a->G));
-            else if (a->reach == 2)
-                VLR_TIMED(ctx, "k_adj_lambda",
-                          k_adj_lambda<2><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, 2, lam_out, a->G));
-            else
-                VLR_TIMED(ctx, "k_adj_lambda",
-                          k_adj_lambda<0><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, a->reach, lam_out, a->G));
-            lam = lam_out;
-        }
-        (void)cur;
-    }
-    VLR_CUDA(ctx, cudaGetLastError());
+    if (d_grad_phik_band != a->lam[1])
+        VLR_CUDA(ctx, cudaMemcpyAsync(a->lam[1], d_grad_phik_band, sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
+    int rc = run_captured(ctx, &a->bwd_exec, [&]() { return adj_backward_enqueue(ctx, a); });
+    if (rc) return rc;
+    float* lam = a->bwd_final;
     a->lam_final = lam;
     if (d_grad_phi0_band)
         VLR_CUDA(ctx, cudaMemcpyAsync(d_grad_phi0_band, lam, sizeof(float) * nb, cudaMemcpyDeviceToDevice, st));
@@ -621,8 +678,8 @@ int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_ph
         VLR_TIMED(ctx, "k_adj_emit_vel",
                   k_adj_emit_vel<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, a->origin, (int)nb, a->G, a->n_stag,
                                                                       (float)a->H, a->keys, a->pvals));
-        int rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 24), (unsigned)nvel + 1, d_grad_vel, (unsigned)nvel,
-                             a->scratch);
+        rc = sort_reduce(ctx, a->keys, a->pvals, (int)(nb * 24), (unsigned)nvel + 1, d_grad_vel, (unsigned)nvel,
+                         a->scratch);
         if (rc) return rc;
     }
     return VLR_OK;

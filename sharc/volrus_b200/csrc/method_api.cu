@@ -383,8 +383,9 @@ __global__ void k_unpack_upload(const int32_t* o3, int n, int4* origin) {
         origin[i] = make_int4(o3[3 * i], o3[3 * i + 1], o3[3 * i + 2], 0);
 }
 
-int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
-                size_t n, bool reset_step) {
+// Enqueue the replacement of a level set's state by host leaves (no wait).
+int upload_enqueue(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                   size_t n, bool reset_step) {
     if (n > (size_t)ls->cap) return set_error(ctx, VLR_ERR_CAPACITY, "more leaves than the level set's capacity");
     for (size_t i = 0; i < 3 * n; ++i)
         if (origins[i] & 7) return set_error(ctx, VLR_ERR_INVALID, "leaf origin not a multiple of 8");
@@ -404,7 +405,18 @@ int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const u
         VLR_CUDA(ctx, cudaMemcpyAsync(ls->vals[0], phi, vbytes, cudaMemcpyHostToDevice, ctx->stream));
     }
     VLR_CUDA(ctx, cudaGetLastError());
-    return ls_init_lists(ctx, ls, (int)n, reset_step);
+    k_init_lists<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, ls->free_stack, ls->scalars, (int)n, ls->cap,
+                                                           reset_step ? 1 : 0);
+    VLR_CUDA(ctx, cudaGetLastError());
+    return ls_enqueue_index(ctx, ls);
+}
+
+int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                size_t n, bool reset_step) {
+    int rc = upload_enqueue(ctx, ls, origins, masks, phi, n, reset_step);
+    if (rc) return rc;
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return consume_device_errors(ctx, "method grid index");
 }
 
 int create_leaves_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, const vlr_velocity_desc* vel,
@@ -468,6 +480,73 @@ int enqueue_one_step(vlr_ctx* ctx, vlr_level_set* ls) {
     int rc = capture_step(ctx, ls);
     if (rc) return rc;
     VLR_CUDA(ctx, cudaGraphLaunch(ls->graph_exec, ctx->stream));
+    return VLR_OK;
+}
+
+// Leaves of one grid (grid < 0: all) of a level set holding n listed leaves,
+// sorted by (grid, x, y, z), into host buffers.
+int download_n(vlr_ctx* ctx, const vlr_level_set* ls, size_t n, int grid, int32_t* grid_ids, int32_t* origins,
+               uint64_t* masks, float* phi, size_t cap_leaves, size_t* n_out) {
+    int rc = VLR_OK;
+    *n_out = 0;
+    if (grid < 0 && n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    if (!n) return VLR_OK;
+    // origins in list order -> host, output order sorted by (grid, x, y, z)
+    // there; masks and values are then gathered on the device in that order
+    // and copied once, straight into the caller's buffers
+    void* stg = nullptr;
+    size_t vbytes = sizeof(float) * kLeafVoxels * n;
+    rc = ls_staging(ctx, const_cast<vlr_level_set*>(ls), vbytes + 84 * n + 256, &stg);
+    if (rc) return rc;
+    float* v = (float*)stg;
+    int4* o = (int4*)((char*)stg + vbytes);
+    uint64_t* mm = (uint64_t*)((char*)stg + vbytes + 16 * n);
+    int* dsel = (int*)((char*)stg + vbytes + 80 * n);
+    k_gather_origins<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, o);
+    std::vector<int4> ho(n);
+    VLR_CUDA(ctx, cudaMemcpyAsync(ho.data(), o, sizeof(int4) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const int4 &A = ho[a], &B2 = ho[b];
+        if (A.w != B2.w) return A.w < B2.w;
+        if (A.x != B2.x) return A.x < B2.x;
+        if (A.y != B2.y) return A.y < B2.y;
+        return A.z < B2.z;
+    });
+    std::vector<int> sel;
+    sel.reserve(n);
+    for (size_t i = 0; i < n; ++i)
+        if (grid < 0 || ho[order[i]].w == grid) sel.push_back(order[i]);
+    const size_t k = sel.size();
+    if (k > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    for (size_t i = 0; i < k; ++i) {
+        const int4 q = ho[sel[i]];
+        if (grid_ids) grid_ids[i] = q.w;
+        if (origins) {
+            origins[3 * i] = q.x;
+            origins[3 * i + 1] = q.y;
+            origins[3 * i + 2] = q.z;
+        }
+    }
+    if (k && (masks || phi)) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(dsel, sel.data(), sizeof(int) * k, cudaMemcpyHostToDevice, ctx->stream));
+        const int B = (int)std::min<size_t>(k, (size_t)ctx->sm_count * 8);
+        if (ls->precision == VLR_PREC_F16)
+            k_gather_sel<__half><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
+                                                             (const __half*)ls->vals[0], mm, v);
+        else
+            k_gather_sel<float><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
+                                                            (const float*)ls->vals[0], mm, v);
+        VLR_CUDA(ctx, cudaGetLastError());
+        if (masks) VLR_CUDA(ctx, cudaMemcpyAsync(masks, mm, 64 * k, cudaMemcpyDeviceToHost, ctx->stream));
+        if (phi)
+            VLR_CUDA(ctx, cudaMemcpyAsync(phi, v, sizeof(float) * kLeafVoxels * k, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    *n_out = k;
     return VLR_OK;
 }
 
@@ -608,65 +687,27 @@ int vlr_ls_download_grid(vlr_ctx* ctx, const vlr_level_set* ls, int grid, int32_
     size_t n = 0;
     int rc = vlr_ls_info(ctx, ls, &n, nullptr, nullptr);
     if (rc) return rc;
-    if (grid < 0 && n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
-    if (!n) return VLR_OK;
-    // origins in list order -> host, output order sorted by (grid, x, y, z)
-    // there; masks and values are then gathered on the device in that order
-    // and copied once, straight into the caller's buffers
-    void* stg = nullptr;
-    size_t vbytes = sizeof(float) * kLeafVoxels * n;
-    rc = ls_staging(ctx, const_cast<vlr_level_set*>(ls), vbytes + 84 * n + 256, &stg);
+    return download_n(ctx, ls, n, grid, grid_ids, origins, masks, phi, cap_leaves, n_out);
+}
+
+int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
+                     size_t n_leaves, int n_steps, int32_t* out_origins, uint64_t* out_masks, float* out_phi,
+                     size_t cap_leaves, size_t* n_out) {
+    if (!ctx || !ls || !origins || !masks || !phi || !n_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "host steps replace single-grid states only");
+    *n_out = 0;
+    int rc = upload_enqueue(ctx, ls, origins, masks, phi, n_leaves, false);
     if (rc) return rc;
-    float* v = (float*)stg;
-    int4* o = (int4*)((char*)stg + vbytes);
-    uint64_t* mm = (uint64_t*)((char*)stg + vbytes + 16 * n);
-    int* dsel = (int*)((char*)stg + vbytes + 80 * n);
-    k_gather_origins<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, (int)n, ls->origin, o);
-    std::vector<int4> ho(n);
-    VLR_CUDA(ctx, cudaMemcpyAsync(ho.data(), o, sizeof(int4) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](int a, int b) {
-        const int4 &A = ho[a], &B2 = ho[b];
-        if (A.w != B2.w) return A.w < B2.w;
-        if (A.x != B2.x) return A.x < B2.x;
-        if (A.y != B2.y) return A.y < B2.y;
-        return A.z < B2.z;
-    });
-    std::vector<int> sel;
-    sel.reserve(n);
-    for (size_t i = 0; i < n; ++i)
-        if (grid < 0 || ho[order[i]].w == grid) sel.push_back(order[i]);
-    const size_t k = sel.size();
-    if (k > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
-    for (size_t i = 0; i < k; ++i) {
-        const int4 q = ho[sel[i]];
-        if (grid_ids) grid_ids[i] = q.w;
-        if (origins) {
-            origins[3 * i] = q.x;
-            origins[3 * i + 1] = q.y;
-            origins[3 * i + 2] = q.z;
-        }
+    for (int i = 0; i < n_steps; ++i) {
+        rc = enqueue_one_step(ctx, ls);
+        if (rc) return rc;
     }
-    if (k && (masks || phi)) {
-        VLR_CUDA(ctx, cudaMemcpyAsync(dsel, sel.data(), sizeof(int) * k, cudaMemcpyHostToDevice, ctx->stream));
-        const int B = (int)std::min<size_t>(k, (size_t)ctx->sm_count * 8);
-        if (ls->precision == VLR_PREC_F16)
-            k_gather_sel<__half><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
-                                                             (const __half*)ls->vals[0], mm, v);
-        else
-            k_gather_sel<float><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, (int)k, ls->mask,
-                                                            (const float*)ls->vals[0], mm, v);
-        VLR_CUDA(ctx, cudaGetLastError());
-        if (masks) VLR_CUDA(ctx, cudaMemcpyAsync(masks, mm, 64 * k, cudaMemcpyDeviceToHost, ctx->stream));
-        if (phi)
-            VLR_CUDA(ctx, cudaMemcpyAsync(phi, v, sizeof(float) * kLeafVoxels * k, cudaMemcpyDeviceToHost,
-                                          ctx->stream));
-        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    }
-    *n_out = k;
-    return VLR_OK;
+    // leaf count and device errors in one round trip
+    int* h = static_cast<int*>(ctx->pinned) + 16;
+    VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    rc = consume_device_errors(ctx, "vlr_ls_step_host");
+    if (rc) return rc;
+    return download_n(ctx, ls, (size_t)h[0], -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
 }
 
 int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,

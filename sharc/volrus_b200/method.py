@@ -254,6 +254,24 @@ class LevelSet:
                                                     ptr(m, C.c_uint64), ptr(v, C.c_float), n), "vlr_ls_download")
         return o, m, v
 
+    def step_host(self, origins, masks, phi, n_steps: int = 1, out=None):
+        """Host-resident steps in one call: state from host leaves, n steps,
+        result into host arrays (``out`` = (origins, masks, phi) buffers to
+        reuse, else new ones sized for twice the input).  Returns the result."""
+        o = np.ascontiguousarray(origins, np.int32)
+        m = np.ascontiguousarray(masks, np.uint64)
+        p = np.ascontiguousarray(phi, np.float32)
+        if out is None:
+            cap = 2 * len(o) + 64
+            out = (np.zeros((cap, 3), np.int32), np.zeros((cap, 8), np.uint64), np.zeros((cap, 512), np.float32))
+        k = C.c_size_t()
+        self.ctx.check(self.ctx.lib.vlr_ls_step_host(self.ctx.handle, self.handle, ptr(o, C.c_int32),
+                                                     ptr(m, C.c_uint64), ptr(p, C.c_float), len(o), int(n_steps),
+                                                     ptr(out[0], C.c_int32), ptr(out[1], C.c_uint64),
+                                                     ptr(out[2], C.c_float), len(out[0]), C.byref(k)),
+                       "vlr_ls_step_host")
+        return out[0][: k.value], out[1][: k.value], out[2][: k.value]
+
     def upload(self, origins, masks, phi):
         """Replace the state with host leaves (voxel units), keeping time and allocations."""
         o = np.ascontiguousarray(origins, np.int32)

@@ -68,3 +68,19 @@ def test_invalid_launch_shape_rejected(ctx):
         with pytest.raises(VolrusError):
             ls.set_launch_shape(*bad)
     ls.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["f32", "f16"])
+def test_host_step_matches_upload_step_download(ctx, precision):
+    """vlr_ls_step_host = vlr_ls_upload + vlr_ls_step + vlr_ls_download."""
+    a = _vortex(precision, None)
+    a.step(2)
+    state = a.arrays()
+    b = _vortex(precision, None)
+    b.step(2)
+    got = b.step_host(*state, n_steps=3)
+    a.upload(*state)
+    a.step(3)
+    _same(got, a.arrays())
+    a.close()
+    b.close()
