@@ -266,7 +266,10 @@ def time_steps(args, ctx, ls, flush, stream, clock=None, steps=None, warmup=None
     warmup = args.warmup if warmup is None else warmup
     if args.launch_shape:
         v = [int(x) for x in args.launch_shape.split(",")]
-        ls.set_launch_shape((v[0], v[1]), (v[2], v[3]))
+        if len(v) == 4:
+            ls.set_launch_shape((v[0], v[1]), (v[2], v[3]))
+        else:
+            ls.set_launch_shape(tuple(v[0:3]), tuple(v[3:6]))
     ls.step(warmup)
     n0, a0, _ = ls.info()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -775,7 +778,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the full-period accuracy run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--launch-shape", default="",
-                    help="advect threads,CTAs,reinit threads,CTAs of the stencil kernels (default: autotuned)")
+                    help="threads,CTAs[,staging] of advect then reinit, e.g. 128,1184,1,128,888,1 (default: "
+                         "autotuned; staging 0 cp.async, 1 TMA)")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)

@@ -262,17 +262,19 @@ int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
  * reports device-side errors. */
 int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
 /* Launch shapes of the advect and reinitialisation kernels: threads per CTA
- * (128 or 256) and persistent CTAs (> 0).  Fixing them turns the first-step
- * autotuning off; advect_threads = 0 turns it back on for the next step.
- * Results never depend on the shape.  No counterpart in the reference (its
- * step is serial Rust). */
-int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int reinit_threads,
-                            int reinit_ctas);
-/* shape[0..3] = advect threads, advect CTAs, reinit threads, reinit CTAs (0
- * before the first step); *n_timed = candidates the autotuner timed, and if
+ * (128 or 256), persistent CTAs (> 0) and the staging of the halo tiles (0:
+ * 16-byte cp.async row copies by every thread; 1: one TMA tensor copy per
+ * present neighbour leaf, completing on an mbarrier).  Fixing them turns the
+ * first-step autotuning off; advect_threads = 0 turns it back on for the next
+ * step.  Results never depend on the shape.  No counterpart in the reference
+ * (its step is serial Rust). */
+int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int advect_staging,
+                            int reinit_threads, int reinit_ctas, int reinit_staging);
+/* shape[0..5] = advect threads, CTAs, staging, reinit threads, CTAs, staging
+ * (0 before the first step); *n_timed = candidates the autotuner timed, and if
  * `log` is non-null, up to cap_log rows of (kernel 0/1, threads, CTAs,
- * microseconds) for them. */
-int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[4], int* n_timed, float* log,
+ * staging, microseconds) for them. */
+int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[6], int* n_timed, float* log,
                             int cap_log);
 int vlr_ctx_check(vlr_ctx* ctx);
 int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_t* n_active, double* time);

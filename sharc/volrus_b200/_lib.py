@@ -130,7 +130,7 @@ SIGNATURES = {
     "vlr_adj_destroy": (None, [P]),
     "vlr_ls_step": (C.c_int, [P, P, C.c_int]),
     "vlr_ls_enqueue": (C.c_int, [P, P, C.c_int]),
-    "vlr_ls_set_launch_shape": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "vlr_ls_set_launch_shape": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "vlr_ls_get_launch_shape": (C.c_int, [P, P, C.POINTER(C.c_int), C.POINTER(C.c_int), flt_p, C.c_int]),
     "vlr_ctx_check": (C.c_int, [P]),
     "vlr_ls_step_host": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t, C.c_int, i32_p, u64_p, flt_p,

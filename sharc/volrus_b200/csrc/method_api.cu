@@ -44,10 +44,12 @@ void ls_free(vlr_level_set* ls) {
     ls->d_params = nullptr;
     ls->d_tab = nullptr;
     ls->d_partial = ls->d_sum = nullptr;
+    ls->maps_h[0] = ls->maps_h[1] = 0;
 }
 
 int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     ls->cap = cap;
+    ls->maps_h[0] = ls->maps_h[1] = 0;  // tensor maps are encoded for the pools allocated here
     size_t vb = (ls->precision == VLR_PREC_F16) ? 2 : 4;
     ls->hcap = next_pow2i(2ll * cap);
     VLR_CUDA(ctx, cudaMalloc(&ls->origin, sizeof(int4) * cap));
@@ -614,8 +616,8 @@ int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
     return consume_device_errors(ctx, "vlr_ls_step");
 }
 
-int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas,
-                            int reinit_threads, int reinit_ctas) {
+int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int advect_staging,
+                            int reinit_threads, int reinit_ctas, int reinit_staging) {
     if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     drop_graph(ls);
     if (advect_threads == 0) {
@@ -624,30 +626,36 @@ int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads,
         return VLR_OK;
     }
     auto ok_nt = [](int t) { return t == 128 || t == 256; };
-    if (!ok_nt(advect_threads) || !ok_nt(reinit_threads) || advect_ctas < 1 || reinit_ctas < 1)
-        return set_error(ctx, VLR_ERR_INVALID, "launch shape: threads must be 128 or 256 and CTAs > 0");
-    ls->adv_shape = StencilShape{advect_threads, advect_ctas};
-    ls->re_shape = StencilShape{reinit_threads, reinit_ctas};
+    auto ok_st = [](int s) { return s == 0 || s == 1; };
+    if (!ok_nt(advect_threads) || !ok_nt(reinit_threads) || advect_ctas < 1 || reinit_ctas < 1 ||
+        !ok_st(advect_staging) || !ok_st(reinit_staging))
+        return set_error(ctx, VLR_ERR_INVALID,
+                         "launch shape: threads must be 128 or 256, CTAs > 0 and staging 0 or 1");
+    ls->adv_shape = StencilShape{advect_threads, advect_ctas, advect_staging};
+    ls->re_shape = StencilShape{reinit_threads, reinit_ctas, reinit_staging};
     ls->autotune = false;
     ls->tuned = true;
     return VLR_OK;
 }
 
-int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[4], int* n_timed, float* log,
+int vlr_ls_get_launch_shape(vlr_ctx* ctx, const vlr_level_set* ls, int shape[6], int* n_timed, float* log,
                             int cap_log) {
     if (!ctx || !ls || !shape) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     shape[0] = ls->adv_shape.nt;
     shape[1] = ls->adv_shape.blocks;
-    shape[2] = ls->re_shape.nt;
-    shape[3] = ls->re_shape.blocks;
+    shape[2] = ls->adv_shape.stage;
+    shape[3] = ls->re_shape.nt;
+    shape[4] = ls->re_shape.blocks;
+    shape[5] = ls->re_shape.stage;
     int k = 0;
     for (int w = 0; w < 2; ++w)
         for (const TuneEntry& e : ls->tune_log[w]) {
             if (log && k < cap_log) {
-                log[4 * k] = (float)w;
-                log[4 * k + 1] = (float)e.shape.nt;
-                log[4 * k + 2] = (float)e.shape.blocks;
-                log[4 * k + 3] = e.ms * 1000.0f;
+                log[5 * k] = (float)w;
+                log[5 * k + 1] = (float)e.shape.nt;
+                log[5 * k + 2] = (float)e.shape.blocks;
+                log[5 * k + 3] = (float)e.shape.stage;
+                log[5 * k + 4] = e.ms * 1000.0f;
             }
             ++k;
         }

@@ -1,5 +1,7 @@
 // Declarations shared by the method kernels and their host orchestration.
 #pragma once
+#include <cuda.h>  // CUtensorMap (a plain 128-byte struct; no driver library is linked)
+
 #include "method.cuh"
 
 namespace vlr {
@@ -31,19 +33,31 @@ struct MTopo {
     int key_bits;
 };
 
+// Tensor maps of a stencil kernel's source value pool for staging mode 1: a
+// 4-D view (z, y, x, slot) of the pool with one box shape per map.  Map i has
+// box extents z = (i & 4 ? 4 : 8), y = (i & 1 ? 8 : H), x = (i & 2 ? 8 : H),
+// slot = 1; f16 pools use maps 0-3, f32 pools 0-7.
+struct StageMaps {
+    CUtensorMap m[8];
+};
+
+// Staging of the stencil kernels' halo tiles (ST): 0 = asynchronous 16-byte
+// copies by every thread (cp.async), 1 = one tensor copy per present
+// neighbour leaf (cp.async.bulk.tensor, TMA) completing on an mbarrier.
 // VK: velocity kind of every grid (MVEL_*), or -1 when a batch mixes kinds.
-// NT: threads per CTA (128 or 256); the result does not depend on NT or on
-// the grid size.
-template <typename T, int H, int VK, int NT>
+// NT: threads per CTA (128 or 256); the result depends neither on NT, on ST
+// nor on the grid size.
+template <typename T, int H, int VK, int NT, int ST>
 __global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
-                           MTopo topo, unsigned* __restrict__ err);
+                           MTopo topo, unsigned* __restrict__ err, const __grid_constant__ StageMaps maps);
 // Dynamic shared memory of the stencil kernels (bytes).
-size_t advect_smem_bytes(int precision_f16, int halo);
-size_t reinit_smem_bytes(int precision_f16);
-template <typename T, int NIT, int NT>
+size_t advect_smem_bytes(int precision_f16, int halo, int stage);
+size_t reinit_smem_bytes(int precision_f16, int stage);
+template <typename T, int NIT, int NT, int ST>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                           const MGridParams* __restrict__ params, MTopo topo, int mode, unsigned* __restrict__ err);
+                           const MGridParams* __restrict__ params, MTopo topo, int mode, unsigned* __restrict__ err,
+                           const __grid_constant__ StageMaps maps);
 template <typename T>
 __global__ void k_m_volume(MLeafArrays A, const T* __restrict__ vals, const MGridParams* __restrict__ params,
                            double r0, double r1, double r2, double* __restrict__ partial);

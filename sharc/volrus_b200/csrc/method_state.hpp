@@ -7,10 +7,12 @@
 #include "method_kernels.hpp"
 #include "vlr_host.hpp"
 
-// Launch shape of a stencil kernel: threads per CTA and persistent CTAs.
+// Launch shape of a stencil kernel: threads per CTA, persistent CTAs and the
+// staging of its halo tiles.
 struct StencilShape {
     int nt = 0;       // 128 or 256 (0: not chosen)
     int blocks = 0;   // grid size (CTAs per SM x SMs)
+    int stage = 0;    // 0: cp.async row copies, 1: TMA tensor copies per neighbour leaf
 };
 
 // One timed candidate of the launch autotuner.
@@ -71,6 +73,10 @@ struct vlr_level_set {
     bool tuned = false;      // shapes chosen (by the autotuner or the caller)
     bool autotune = true;    // choose the shapes on the first step
     std::vector<TuneEntry> tune_log[2];  // candidates timed by the autotuner (advect, reinit)
+    // tensor maps of the stencil kernels' source pools for TMA staging:
+    // [0] advect (vals[0], halo maps_h[0]), [1] reinit (vals[1], halo 2)
+    vlr::StageMaps maps[2];
+    int maps_h[2] = {0, 0};  // halo the maps were encoded for (0: not yet)
     int scan_levels = 0;
 
     vlr::MLeafArrays arrays() const {

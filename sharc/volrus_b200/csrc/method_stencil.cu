@@ -139,6 +139,199 @@ __device__ __forceinline__ void stage_ready() {
     __syncthreads();
 }
 
+// --------------------------------------------------------- TMA staging (ST = 1)
+//
+// The tile pieces held by neighbour leaf d = ax * 9 + ay * 3 + az arrive as
+// ONE tensor copy of the box of that leaf which the tile covers:
+//   x: [8-H, 8) for the leaf below, [0, 8) at, [0, H) above the centre leaf
+//   y: the same
+//   z: the whole row (f16: 8 values = 16 bytes); f32 z-neighbours copy only
+//      the 16-byte half that holds the H <= 4 values the tile uses
+// Each box lands dense (z fastest, then y, then x) at a 128-byte aligned
+// offset of the stage.  The row-offset table (built once per CTA in s_desc)
+// gives, for tile row (x, y) and z-piece k, the element offset p_k such that
+// stage[p_k + z] is voxel z of that row in the leaf below / at / above (k =
+// 0 / 1 / 2).  Up to 27 copies per leaf complete on one mbarrier whose
+// expected byte count is the sum of the issued boxes; the 27 masks still
+// arrive by cp.async.
+template <typename T, int H>
+struct BoxStage {
+    static constexpr int E = 8 + 2 * H;
+    static constexpr int ext(int a) { return a == 1 ? 8 : H; }
+    static constexpr int lo(int a) { return a == 0 ? 8 - H : 0; }
+    static constexpr int ez(int az) { return (sizeof(T) == 4 && az != 1) ? 4 : 8; }
+    static constexpr int z0(int az) { return (sizeof(T) == 4 && az == 0) ? 4 : 0; }
+    static constexpr int box_bytes(int d) { return ez(d % 3) * ext((d / 3) % 3) * ext(d / 9) * (int)sizeof(T); }
+    static constexpr int off(int d) {
+        int s = 0;
+        for (int i = 0; i < d; ++i) s += (box_bytes(i) + 127) & ~127;
+        return s;
+    }
+    // tensor map of box d (see StageMaps)
+    static constexpr int map_of(int d) {
+        return ((d / 9) == 1 ? 2 : 0) | (((d / 3) % 3) == 1 ? 1 : 0) | ((sizeof(T) == 4 && d % 3 != 1) ? 4 : 0);
+    }
+    static constexpr size_t bytes = (size_t)off(kNbr);
+    static_assert(H >= 1 && H <= 4, "the f32 z-halves hold up to 4 values");
+};
+
+template <typename T, int H, int NT>
+__device__ __forceinline__ void build_row_offsets(unsigned* s_desc) {
+    using B = BoxStage<T, H>;
+    constexpr int E = B::E;
+    for (int p = threadIdx.x; p < E * E * 3; p += NT) {
+        const int r = p / 3, k = p - 3 * r;
+        const int rx = r / E;
+        const int x = rx - H, y = r - rx * E - H;
+        const int ax = nb_axis(x), ay = nb_axis(y);
+        const int d = ax * 9 + ay * 3 + k;
+        const int xl = (x & 7) - B::lo(ax), yl = (y & 7) - B::lo(ay);
+        const int start = B::off(d) / (int)sizeof(T) + (xl * B::ext(ay) + yl) * B::ez(k);
+        s_desc[p] = (unsigned)(start - B::z0(k));  // may be negative (f32, k = 0): stored as two's complement
+    }
+}
+
+// Copy descriptor of box d: x = shared address, y = z0 | y0 << 8 | x0 << 16 |
+// map << 24, z = bytes.
+template <typename T, int H>
+__device__ __forceinline__ uint4 tma_piece(uint32_t stage, int d) {
+    using B = BoxStage<T, H>;
+    const int ax = d / 9, ay = (d / 3) % 3, az = d % 3;
+    const unsigned co = (unsigned)B::z0(az) | ((unsigned)B::lo(ay) << 8) | ((unsigned)B::lo(ax) << 16) |
+                        ((unsigned)B::map_of(d) << 24);
+    return make_uint4(stage + (uint32_t)B::off(d), co, (unsigned)B::box_bytes(d), 0u);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx_only(uint32_t bar, unsigned bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+
+// 4-D tiled tensor copy global -> shared (coordinates z, y, x, slot), completing
+// on the mbarrier at `bar`.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+// All threads (same place as stage_async): thread 0 walks the 27 neighbours
+// and, for each present one, raises the mbarrier's expected bytes by its box
+// and issues its tensor copy, then arrives (the phase cannot complete before
+// that arrival, so every expectation is posted in time); the masks follow by
+// cp.async.  One issuing thread keeps the issue out of the register budget of
+// the other warps, which the stencil arithmetic holds at the 64-register cap.
+__device__ __forceinline__ void stage_tma(const uint4* s_tma, const int* s_nb, const StageMaps& maps, uint32_t bar,
+                                          const uint64_t* __restrict__ masks, uint64_t* s_m) {
+    if (threadIdx.x == 0) {
+#pragma unroll 1
+        for (int d = 0; d < kNbr; ++d) {
+            const int sl = s_nb[d];
+            if (sl >= 0) {
+                const uint4 pc = s_tma[d];
+                mbar_expect_tx_only(bar, pc.z);
+                tma_load_4d(pc.x, &maps.m[pc.y >> 24], (int)(pc.y & 255u), (int)((pc.y >> 8) & 255u),
+                            (int)((pc.y >> 16) & 255u), sl, bar);
+            }
+        }
+        mbar_arrive(bar);
+    }
+    if (threadIdx.x < kNbr * 4) {
+        const int d = threadIdx.x >> 2, q = threadIdx.x & 3;
+        const int sl = s_nb[d];
+        if (sl >= 0) cp_async16(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
+        else *reinterpret_cast<uint4*>(s_m + d * 8 + 2 * q) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    cp_async_commit();
+}
+
+// Bounded wait of the tensor copies (about a second at most): every thread
+// polls the phase, then a CTA barrier that also agrees on the outcome.
+// Returns false on every thread if any thread gave up.  The stage of the
+// it-th leaf a CTA processes completes phase it of the mbarrier, so the
+// parity waited for is it & 1.
+constexpr int kStageSpin = 1 << 20;
+__device__ __forceinline__ bool stage_ready_tma(uint32_t bar, unsigned parity) {
+    cp_async_wait_all();
+    bool ok = false;
+    for (int i = 0; i < kStageSpin; ++i)
+        if (mbar_try_wait(bar, parity)) {
+            ok = true;
+            break;
+        }
+    return __syncthreads_or(ok ? 0 : 1) == 0;
+}
+
+// Shared setup of the stage for mode ST: copy descriptors (ST 0) or row
+// offsets, per-neighbour copy descriptors and the mbarrier (ST 1).  Callers
+// follow it with a CTA barrier.
+template <typename T, int H, int NT, int ST>
+__device__ __forceinline__ void stage_setup(unsigned* s_desc, uint4* s_tma, uint64_t* s_bar, const T* s_stage,
+                                            const StageMaps& maps) {
+    if constexpr (ST == 0) {
+        build_stage_desc<T, H, NT>(s_desc);
+    } else {
+        // bring the tensor maps' descriptors on chip before the first copy
+        if (threadIdx.x < (sizeof(T) == 2 ? 4 : 8))
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.m[threadIdx.x]))
+                         : "memory");
+        build_row_offsets<T, H, NT>(s_desc);
+        if (threadIdx.x < kNbr) s_tma[threadIdx.x] = tma_piece<T, H>(smem_addr(s_stage), threadIdx.x);
+        if (threadIdx.x == 0) mbar_init(smem_addr(s_bar), 1u);
+    }
+}
+
+template <typename T, int H, int NT, int ST>
+__device__ __forceinline__ void stage_issue(const unsigned* s_desc, const uint4* s_tma, uint64_t* s_bar,
+                                            const int* s_nb, const T* __restrict__ vals, const StageMaps& maps,
+                                            const uint64_t* __restrict__ masks, T* s_rows, uint64_t* s_m) {
+    if constexpr (ST == 0) stage_async<T, H, NT>(s_desc, s_nb, vals, masks, s_rows, s_m);
+    else stage_tma(s_tma, s_nb, maps, smem_addr(s_bar), masks, s_m);
+}
+
+// Returns false (on every thread) if the tensor copies did not arrive in time.
+template <int ST>
+__device__ __forceinline__ bool stage_wait(uint64_t* s_bar, unsigned parity) {
+    if constexpr (ST == 0) {
+        stage_ready();
+        return true;
+    } else {
+        return stage_ready_tma(smem_addr(s_bar), parity);
+    }
+}
+
+// Start of the stage in dynamic shared memory: the tensor copies want 128-byte
+// aligned destinations, so mode 1 rounds the base up (its size reserves 128
+// bytes for this).
+template <int ST>
+__device__ __forceinline__ unsigned char* stage_base(unsigned char* smem) {
+    if constexpr (ST == 0) return smem;
+    else return smem + ((128u - (smem_addr(smem) & 127u)) & 127u);
+}
+
 // Copy one grid's parameters into shared memory (all threads call; caller syncs).
 __device__ __forceinline__ void load_params(const MGridParams* __restrict__ params, int gid, MGridParams* s_P) {
     const int* src = (const int*)(params + gid);
@@ -166,19 +359,33 @@ __device__ __forceinline__ void lds_row8(const T* p, float* out) {
 }
 
 // Build tile row (x, y) (local leaf coordinates, z over [-H, 8 + H)) from the
-// row-packed stage.  Absent leaves: kNaN ? NaN : copysign(hw, centre value at
-// the clamped position).
-template <typename T, int H, bool kNaN>
-__device__ __forceinline__ void build_row(const T* s_rows, const int* s_nbr, int x, int y, float hw, float* row) {
+// stage: row-packed (ST 0) or boxes located by the row-offset table s_desc
+// (ST 1).  Absent leaves: kNaN ? NaN : copysign(hw, centre value at the
+// clamped position).
+template <typename T, int H, bool kNaN, int ST>
+__device__ __forceinline__ void build_row(const T* s_rows, const unsigned* s_desc, const int* s_nbr, int x, int y,
+                                          float hw, float* row) {
     using R = RowStage<T, H>;
     constexpr int E = R::E, RP = R::RP;
     const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
-    const T* d = s_rows + ((x + H) * E + (y + H)) * RP;
-    const T* c = s_rows + ((min(max(x, 0), 7) + H) * E + (min(max(y, 0), 7) + H)) * RP + 8;  // centre leaf row
+    const int r = (x + H) * E + (y + H);
+    const int rc = (min(max(x, 0), 7) + H) * E + (min(max(y, 0), 7) + H);
+    const T *p0, *p1, *p2, *c;  // z-pieces of the rows below / at / above; centre leaf row
+    if constexpr (ST == 0) {
+        p0 = s_rows + r * RP;
+        p1 = p0 + 8;
+        p2 = p0 + 16;
+        c = s_rows + rc * RP + 8;
+    } else {
+        p0 = s_rows + (int)s_desc[3 * r];
+        p1 = s_rows + (int)s_desc[3 * r + 1];
+        p2 = s_rows + (int)s_desc[3 * r + 2];
+        c = s_rows + (int)s_desc[3 * rc + 1];
+    }
     const float nan = __int_as_float(0x7fc00000);
     float mid[8];
     if (s_nbr[base + 1] >= 0) {
-        lds_row8<T>(d + 8, mid);
+        lds_row8<T>(p1, mid);
     } else if (!kNaN) {
         lds_row8<T>(c, mid);
 #pragma unroll
@@ -191,7 +398,7 @@ __device__ __forceinline__ void build_row(const T* s_rows, const int* s_nbr, int
     for (int i = 0; i < 8; ++i) row[H + i] = mid[i];
     if (s_nbr[base] >= 0) {
 #pragma unroll
-        for (int i = 0; i < H; ++i) row[i] = to_f(d[8 - H + i]);
+        for (int i = 0; i < H; ++i) row[i] = to_f(p0[8 - H + i]);
     } else {
         const float f = kNaN ? nan : copysignf(hw, to_f(c[0]));
 #pragma unroll
@@ -199,7 +406,7 @@ __device__ __forceinline__ void build_row(const T* s_rows, const int* s_nbr, int
     }
     if (s_nbr[base + 2] >= 0) {
 #pragma unroll
-        for (int i = 0; i < H; ++i) row[H + 8 + i] = to_f(d[16 + i]);
+        for (int i = 0; i < H; ++i) row[H + 8 + i] = to_f(p2[i]);
     } else {
         const float f = kNaN ? nan : copysignf(hw, to_f(c[7]));
 #pragma unroll
@@ -400,23 +607,25 @@ __device__ __forceinline__ void advect_voxels(const VelConst& V, const float2 (*
     }
 }
 
-// Dynamic shared memory of the advect kernel.
-template <typename T, int H>
+// Dynamic shared memory of the advect kernel (stage, masks, float tile; mode 1
+// reserves 128 bytes to align the stage).
+template <typename T, int H, int ST>
 struct AdvectSmem {
     static constexpr int E = 8 + 2 * H;
-    static constexpr size_t raw = RowStage<T, H>::bytes;
+    static constexpr size_t raw = ST ? BoxStage<T, H>::bytes : RowStage<T, H>::bytes;
     static constexpr size_t masks = (size_t)kNbr * 64;
     static constexpr size_t tile = (size_t)E * E * E * 4;
-    static constexpr size_t bytes = raw + masks + tile;
+    static constexpr size_t bytes = raw + masks + tile + (ST ? 128 : 0);
 };
 
 // --------------------------------------------------------------- advect
 
-template <typename T, int H, int VK, int NT>
+template <typename T, int H, int VK, int NT, int ST>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const T* __restrict__ src,
                                                            T* __restrict__ dst, const MGridParams* __restrict__ params,
                                                            const float2* __restrict__ tab, MStepParams sp, MTopo topo,
-                                                           unsigned* __restrict__ err) {
+                                                           unsigned* __restrict__ err,
+                                                           const __grid_constant__ StageMaps maps) {
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     constexpr int VPT = kLeafVoxels / NT;  // voxels per thread in whole-leaf passes
     dep_wait();
@@ -435,12 +644,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
         topo.scalars[4] = 0;  // new count (set by the last scan chunk)
         topo.scalars[7] = 0;  // scan chunk ticket
     }
-    using L = AdvectSmem<T, H>;
+    using L = AdvectSmem<T, H, ST>;
     constexpr int E = L::E;
     constexpr int NROW = E * E;
     constexpr int NTAB = kMaxOctaves * 3 * 8;
     static_assert(NTAB <= NT, "one table entry per thread");
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* smem = stage_base<ST>(smem_dyn);
     T* s_raw = reinterpret_cast<T*>(smem);
     uint64_t* s_m = reinterpret_cast<uint64_t*>(smem + L::raw);
     float* s_tile = reinterpret_cast<float*>(smem + L::raw + L::masks);
@@ -450,6 +660,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     __shared__ __align__(16) MGridParams s_P;
     __shared__ float2 s_tab[kMaxOctaves][3][8];
     __shared__ unsigned s_desc[StageDesc<T, H>::NP];
+    __shared__ uint4 s_tma[ST ? kNbr : 1];
+    __shared__ uint64_t s_bar;
 
     const int count = *A.count;
     const int G = gridDim.x;
@@ -465,10 +677,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     // prologue: first leaf staged, next leaf's list entry in flight
     int slot = A.list[li];
     int4 o = A.origin[slot];
-    build_stage_desc<T, H, NT>(s_desc);
+    stage_setup<T, H, NT, ST>(s_desc, s_tma, &s_bar, s_raw, maps);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
-    stage_async<T, H, NT>(s_desc, s_nbr[0], src, A.mask, s_raw, s_m);
+    stage_issue<T, H, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[0], src, maps, A.mask, s_raw, s_m);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
 
     int cur_gid = -1;
@@ -513,12 +725,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
                 tvalid = true;
             }
         }
-        stage_ready();  // barrier 1: this leaf's rows and masks are in shared memory
+        // barrier 1: this leaf's rows and masks are in shared memory
+        if (!stage_wait<ST>(&s_bar, (unsigned)cur)) {
+            if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+            return;
+        }
         const int* nbr = s_nbr[cur];
         for (int t = threadIdx.x; t < NROW + 64; t += NT) {
             if (t < NROW) {
                 float row[E];
-                build_row<T, H, false>(s_raw, nbr, t / E - H, t % E - H, hw, row);
+                build_row<T, H, false, ST>(s_raw, s_desc, nbr, t / E - H, t % E - H, hw, row);
                 store_row<E>(s_tile + t * E, row);
             } else {
                 // dilation: one thread per z-row, 10-bit rows z = -1..8
@@ -541,7 +757,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
         }
         if (w0) s_nbr[cur ^ 1][lane] = nb_n;
         __syncthreads();  // barrier 2: tile and D are built; the staging buffers are free
-        if (slot_n >= 0) stage_async<T, H, NT>(s_desc, s_nbr[cur ^ 1], src, A.mask, s_raw, s_m);
+        if (slot_n >= 0)
+            stage_issue<T, H, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[cur ^ 1], src, maps, A.mask, s_raw, s_m);
         if (tvalid) (&s_tab[0][0][0])[threadIdx.x] = tv;
         // compact D; voxels outside D keep the sign of their previous value and
         // are stored here
@@ -663,19 +880,20 @@ __device__ __forceinline__ float cut_relax(float phi, float phi0, float d) {
 }
 
 
-template <typename T>
+template <typename T, int ST>
 struct ReinitSmem {
-    static constexpr size_t raw = RowStage<T, 2>::bytes;
+    static constexpr size_t raw = ST ? BoxStage<T, 2>::bytes : RowStage<T, 2>::bytes;
     static constexpr size_t masks = (size_t)kNbr * 64;
     static constexpr size_t p1 = 12 * 12 * 12 * 4;  // phi1 tile: leaf + 2-voxel ring
     static constexpr size_t p2 = 10 * 10 * 10 * 4;  // phi2 tile: leaf + 1-voxel ring
-    static constexpr size_t bytes = raw + masks + p1 + p2;
+    static constexpr size_t bytes = raw + masks + p1 + p2 + (ST ? 128 : 0);
 };
 
-template <typename T, int NIT, int NT>
+template <typename T, int NIT, int NT, int ST>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const T* __restrict__ src,
                                                            T* __restrict__ dst, const MGridParams* __restrict__ params,
-                                                           MTopo topo, int mode, unsigned* __restrict__ err) {
+                                                           MTopo topo, int mode, unsigned* __restrict__ err,
+                                                           const __grid_constant__ StageMaps maps) {
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     dep_wait();
     dep_launch();
@@ -685,8 +903,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     constexpr int VPT = kLeafVoxels / NT;
     constexpr int RPW = (F * F + NW - 1) / NW;  // D rows per warp (rows r = lane * NW + warp)
     static_assert(32 * NW >= F * F, "one D row per lane");
-    using L = ReinitSmem<T>;
-    extern __shared__ __align__(128) unsigned char smem[];
+    using L = ReinitSmem<T, ST>;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* smem = stage_base<ST>(smem_dyn);
     T* s_raw = reinterpret_cast<T*>(smem);
     uint64_t* s_dm = reinterpret_cast<uint64_t*>(smem + L::raw);
     float* s_p1 = reinterpret_cast<float*>(smem + L::raw + L::masks);
@@ -696,6 +915,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     __shared__ int s_nbr[2][32];
     __shared__ __align__(16) unsigned s_M[16];
     __shared__ unsigned s_desc[StageDesc<T, 2>::NP];
+    __shared__ uint4 s_tma[ST ? kNbr : 1];
+    __shared__ uint64_t s_bar;
     __shared__ float s_dist[NIT == 2 ? F * F * F : 1];  // cut-voxel distances of the 10^3 box (NaN: not cut)
 
     const int count = *A.count;
@@ -709,10 +930,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
 
     int slot = A.list[li];
     int4 o = A.origin[slot];
-    build_stage_desc<T, 2, NT>(s_desc);
+    stage_setup<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_raw, maps);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
-    stage_async<T, 2, NT>(s_desc, s_nbr[0], src, A.dmask, s_raw, s_dm);
+    stage_issue<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[0], src, maps, A.dmask, s_raw, s_dm);
     int slot_n = (li + G < count) ? A.list[li + G] : -1;
     float hw = params[o.w].hw;
 
@@ -722,13 +943,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         if (slot_n >= 0) o_n = A.origin[slot_n];
         const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
         const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
-        stage_ready();  // barrier 1
+        if (!stage_wait<ST>(&s_bar, (unsigned)cur)) {  // barrier 1
+            if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+            return;
+        }
         const int* nbr = s_nbr[cur];
         for (int t = threadIdx.x; t < E * E + F * F; t += NT) {
             if (t < E * E) {
                 float row[E];
                 const int x = t / E - 2, y = t % E - 2;
-                build_row<T, 2, true>(s_raw, nbr, x, y, hw, row);
+                build_row<T, 2, true, ST>(s_raw, s_desc, nbr, x, y, hw, row);
                 store_row<E>(s_p1 + t * E, row);
                 if (NIT == 2 && x >= -1 && x <= 8 && y >= -1 && y <= 8) {
                     // phi2 starts as phi1 on the 10^3 box; iteration 1 overwrites the voxels of D
@@ -749,7 +973,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         }
         if (w0) s_nbr[cur ^ 1][lane] = nb_n;
         __syncthreads();  // barrier 2: tiles and D rows built; staging buffers free
-        if (slot_n >= 0) stage_async<T, 2, NT>(s_desc, s_nbr[cur ^ 1], src, A.dmask, s_raw, s_dm);
+        if (slot_n >= 0)
+            stage_issue<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[cur ^ 1], src, maps, A.dmask, s_raw, s_dm);
         if (NIT == 2) {
             // iteration 1 on the voxels of D in the 10^3 box, compacted per warp:
             // lane l of warp w owns D row r = l * NW + w
@@ -888,24 +1113,25 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     }
 }
 
-#define VLR_INST_ADVECT_NT(T, H, NT)                                                                               \
-    template __global__ void k_m_advect<T, H, -1, NT>(MLeafArrays, const T*, T*, const MGridParams*,               \
-                                                      const float2*, MStepParams, MTopo, unsigned*);               \
-    template __global__ void k_m_advect<T, H, MVEL_CONSTANT, NT>(MLeafArrays, const T*, T*, const MGridParams*,    \
-                                                                 const float2*, MStepParams, MTopo, unsigned*);    \
-    template __global__ void k_m_advect<T, H, MVEL_VORTEX, NT>(MLeafArrays, const T*, T*, const MGridParams*,      \
-                                                               const float2*, MStepParams, MTopo, unsigned*);      \
-    template __global__ void k_m_advect<T, H, MVEL_CURL, NT>(MLeafArrays, const T*, T*, const MGridParams*,        \
-                                                             const float2*, MStepParams, MTopo, unsigned*);
-#define VLR_INST_ADVECT(T, H) VLR_INST_ADVECT_NT(T, H, 128) VLR_INST_ADVECT_NT(T, H, 256)
-#define VLR_INST_REINIT_NT(T, NT)                                                                                  \
-    template __global__ void k_m_reinit<T, 0, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
-                                                  unsigned*);                                                      \
-    template __global__ void k_m_reinit<T, 1, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
-                                                  unsigned*);                                                      \
-    template __global__ void k_m_reinit<T, 2, NT>(MLeafArrays, const T*, T*, const MGridParams*, MTopo, int,         \
-                                                  unsigned*);
-#define VLR_INST_REINIT(T) VLR_INST_REINIT_NT(T, 128) VLR_INST_REINIT_NT(T, 256)
+#define VLR_ADVECT_ARGS(T)                                                                       \
+    MLeafArrays, const T*, T*, const MGridParams*, const float2*, MStepParams, MTopo, unsigned*, \
+        const __grid_constant__ StageMaps
+#define VLR_INST_ADVECT_ST(T, H, NT, ST)                                                  \
+    template __global__ void k_m_advect<T, H, -1, NT, ST>(VLR_ADVECT_ARGS(T));            \
+    template __global__ void k_m_advect<T, H, MVEL_CONSTANT, NT, ST>(VLR_ADVECT_ARGS(T)); \
+    template __global__ void k_m_advect<T, H, MVEL_VORTEX, NT, ST>(VLR_ADVECT_ARGS(T));   \
+    template __global__ void k_m_advect<T, H, MVEL_CURL, NT, ST>(VLR_ADVECT_ARGS(T));
+#define VLR_INST_ADVECT(T, H)                                                                          \
+    VLR_INST_ADVECT_ST(T, H, 128, 0) VLR_INST_ADVECT_ST(T, H, 256, 0) VLR_INST_ADVECT_ST(T, H, 128, 1) \
+        VLR_INST_ADVECT_ST(T, H, 256, 1)
+#define VLR_REINIT_ARGS(T) \
+    MLeafArrays, const T*, T*, const MGridParams*, MTopo, int, unsigned*, const __grid_constant__ StageMaps
+#define VLR_INST_REINIT_ST(T, NT, ST)                                      \
+    template __global__ void k_m_reinit<T, 0, NT, ST>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 1, NT, ST>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 2, NT, ST>(VLR_REINIT_ARGS(T));
+#define VLR_INST_REINIT(T) \
+    VLR_INST_REINIT_ST(T, 128, 0) VLR_INST_REINIT_ST(T, 256, 0) VLR_INST_REINIT_ST(T, 128, 1) VLR_INST_REINIT_ST(T, 256, 1)
 VLR_INST_ADVECT(float, 2)
 VLR_INST_ADVECT(float, 3)
 VLR_INST_ADVECT(__half, 2)
@@ -913,13 +1139,18 @@ VLR_INST_ADVECT(__half, 3)
 VLR_INST_REINIT(float)
 VLR_INST_REINIT(__half)
 
-size_t advect_smem_bytes(int precision_f16, int halo) {
-    if (precision_f16) return halo == 2 ? AdvectSmem<__half, 2>::bytes : AdvectSmem<__half, 3>::bytes;
-    return halo == 2 ? AdvectSmem<float, 2>::bytes : AdvectSmem<float, 3>::bytes;
+size_t advect_smem_bytes(int precision_f16, int halo, int stage) {
+    if (stage) {
+        if (precision_f16) return halo == 2 ? AdvectSmem<__half, 2, 1>::bytes : AdvectSmem<__half, 3, 1>::bytes;
+        return halo == 2 ? AdvectSmem<float, 2, 1>::bytes : AdvectSmem<float, 3, 1>::bytes;
+    }
+    if (precision_f16) return halo == 2 ? AdvectSmem<__half, 2, 0>::bytes : AdvectSmem<__half, 3, 0>::bytes;
+    return halo == 2 ? AdvectSmem<float, 2, 0>::bytes : AdvectSmem<float, 3, 0>::bytes;
 }
 
-size_t reinit_smem_bytes(int precision_f16) {
-    return precision_f16 ? ReinitSmem<__half>::bytes : ReinitSmem<float>::bytes;
+size_t reinit_smem_bytes(int precision_f16, int stage) {
+    if (stage) return precision_f16 ? ReinitSmem<__half, 1>::bytes : ReinitSmem<float, 1>::bytes;
+    return precision_f16 ? ReinitSmem<__half, 0>::bytes : ReinitSmem<float, 0>::bytes;
 }
 
 }  // namespace vlr

@@ -19,6 +19,8 @@
 // The reference's counterparts are dilate (src/tools/morphology.rs:20-35),
 // trim_narrow_band's deactivation (src/tools/level_set_track.rs:53-68) and
 // remove_empty_leaves (src/tree/internal.rs:231-247).
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 
 #include "method_state.hpp"
@@ -408,25 +410,83 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
 // ------------------------------------------------------ stencil launches
 
 // The launch shape of a stencil kernel (threads per CTA, persistent CTAs per
-// SM) is chosen by ls_autotune_step; until then the kernels run at 256
-// threads with every SM filled to the occupancy limit.
-template <typename T, int H, int VK, int NT>
+// SM, staging mode) is chosen by ls_autotune_step; until then the kernels run
+// at 256 threads with every SM filled to the occupancy limit and cp.async
+// staging.
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime (the
+// library links only cudart).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    return fn;
+}
+
+// Tensor maps of a value pool (cap leaves of 512 values, x * 64 + y * 8 + z)
+// as a 4-D array (z, y, x, slot) with the box shapes of StageMaps for halo H.
+static int encode_stage_maps(vlr_ctx* ctx, const void* pool, int cap, bool f16, int H, StageMaps* out) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    if (reinterpret_cast<uintptr_t>(pool) % 16u)
+        return set_error(ctx, VLR_ERR_CUDA, "value pool is not 16-byte aligned for tensor copies");
+    const cuuint64_t es = f16 ? 2 : 4;
+    const cuuint64_t dims[4] = {8, 8, 8, (cuuint64_t)cap};
+    const cuuint64_t strides[3] = {8 * es, 64 * es, 512 * es};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    *out = StageMaps{};
+    for (int i = 0; i < (f16 ? 4 : 8); ++i) {
+        const cuuint32_t box[4] = {(i & 4) ? 4u : 8u, (i & 1) ? 8u : (cuuint32_t)H, (i & 2) ? 8u : (cuuint32_t)H, 1u};
+        CUresult r = enc(&out->m[i], f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                         const_cast<void*>(pool), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    }
+    return VLR_OK;
+}
+
+// Tensor maps of the source pool of the advect (which 0) or reinit (1) kernel.
+static int stage_maps(vlr_ctx* ctx, vlr_level_set* ls, int which, const StageMaps** out) {
+    const int H = which == 0 ? ls->halo : 2;
+    if (ls->maps_h[which] != H) {
+        int rc = encode_stage_maps(ctx, ls->vals[which], ls->cap, ls->precision == VLR_PREC_F16, H, &ls->maps[which]);
+        if (rc) return rc;
+        ls->maps_h[which] = H;
+    }
+    *out = &ls->maps[which];
+    return VLR_OK;
+}
+
+template <typename T, int H, int VK, int NT, int ST>
 static int launch_advect_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
-    const size_t smem = advect_smem_bytes(sizeof(T) == 2, H);
-    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, H, VK, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = advect_smem_bytes(sizeof(T) == 2, H, ST);
+    const StageMaps* maps = nullptr;
+    int rc = stage_maps(ctx, ls, 0, &maps);
+    if (rc) return rc;
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, H, VK, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
     VLR_TIMED(ctx, "k_m_advect",
-              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK, NT>, blocks, NT, smem, ctx->stream, A,
+              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK, NT, ST>, blocks, NT, smem, ctx->stream, A,
                                        (const T*)ls->vals[0], (T*)ls->vals[1], (const MGridParams*)ls->d_params,
-                                       (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword)));
+                                       (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword, *maps)));
     return VLR_OK;
 }
 
 template <typename T, int H, int VK>
 static int launch_advect_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
                                StencilShape sh) {
-    return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128>(ctx, ls, A, topo, sh.blocks)
-                        : launch_advect_nt<T, H, VK, 256>(ctx, ls, A, topo, sh.blocks);
+    if (sh.stage)
+        return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128, 1>(ctx, ls, A, topo, sh.blocks)
+                            : launch_advect_nt<T, H, VK, 256, 1>(ctx, ls, A, topo, sh.blocks);
+    return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128, 0>(ctx, ls, A, topo, sh.blocks)
+                        : launch_advect_nt<T, H, VK, 256, 0>(ctx, ls, A, topo, sh.blocks);
 }
 
 template <typename T, int H>
@@ -447,23 +507,29 @@ static int launch_advect(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
     return ls->halo == 2 ? launch_advect_vk<T, 2>(ctx, ls, A, topo, sh) : launch_advect_vk<T, 3>(ctx, ls, A, topo, sh);
 }
 
-template <typename T, int NIT, int NT>
+template <typename T, int NIT, int NT, int ST>
 static int launch_reinit_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
-    const size_t smem = reinit_smem_bytes(sizeof(T) == 2);
-    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, NIT, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = reinit_smem_bytes(sizeof(T) == 2, ST);
+    const StageMaps* maps = nullptr;
+    int rc = stage_maps(ctx, ls, 1, &maps);
+    if (rc) return rc;
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, NIT, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
     VLR_TIMED(ctx, "k_m_reinit",
-              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, NT>, blocks, NT, smem, ctx->stream, A,
+              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, NT, ST>, blocks, NT, smem, ctx->stream, A,
                                        (const T*)ls->vals[1], (T*)ls->vals[0], (const MGridParams*)ls->d_params,
-                                       topo, ls->sp.reinit_mode, ctx->d_errword)));
+                                       topo, ls->sp.reinit_mode, ctx->d_errword, *maps)));
     return VLR_OK;
 }
 
 template <typename T, int NIT>
 static int launch_reinit_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
                                StencilShape sh) {
-    return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128>(ctx, ls, A, topo, sh.blocks)
-                        : launch_reinit_nt<T, NIT, 256>(ctx, ls, A, topo, sh.blocks);
+    if (sh.stage)
+        return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128, 1>(ctx, ls, A, topo, sh.blocks)
+                            : launch_reinit_nt<T, NIT, 256, 1>(ctx, ls, A, topo, sh.blocks);
+    return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128, 0>(ctx, ls, A, topo, sh.blocks)
+                        : launch_reinit_nt<T, NIT, 256, 0>(ctx, ls, A, topo, sh.blocks);
 }
 
 template <typename T>
@@ -478,28 +544,30 @@ static int launch_reinit(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
 }
 
 // Occupancy limit (CTAs per SM) of the stencil kernel of `which` (0 advect,
-// 1 reinit) at NT threads.
-template <typename T, int NT>
+// 1 reinit) at NT threads and staging mode ST.
+template <typename T, int NT, int ST>
 static int stencil_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int which, int* per_sm) {
     *per_sm = 0;
     if (which == 0) {
-        const size_t smem = advect_smem_bytes(sizeof(T) == 2, ls->halo);
+        const size_t smem = advect_smem_bytes(sizeof(T) == 2, ls->halo, ST);
         // every velocity kind instantiates the same staging and tile, so the
-        // constant-velocity kernel stands for the register and smem footprint
+        // mixed-kind kernel stands for the register and smem footprint
         if (ls->halo == 2) {
-            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 2, -1, NT>,
+            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 2, -1, NT, ST>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 2, -1, NT>, NT, smem));
+            VLR_CUDA(ctx,
+                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 2, -1, NT, ST>, NT, smem));
         } else {
-            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 3, -1, NT>,
+            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 3, -1, NT, ST>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 3, -1, NT>, NT, smem));
+            VLR_CUDA(ctx,
+                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 3, -1, NT, ST>, NT, smem));
         }
     } else {
-        const size_t smem = reinit_smem_bytes(sizeof(T) == 2);
-        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const size_t smem = reinit_smem_bytes(sizeof(T) == 2, ST);
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
-        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, NT>, NT, smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, NT, ST>, NT, smem));
     }
     return VLR_OK;
 }
@@ -507,19 +575,22 @@ static int stencil_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int which, int* pe
 template <typename T>
 static int stencil_candidates(vlr_ctx* ctx, vlr_level_set* ls, int which, std::vector<StencilShape>& out) {
     out.clear();
-    for (int nt : {128, 256}) {
-        int occ = 0;
-        int rc = nt == 128 ? stencil_occupancy<T, 128>(ctx, ls, which, &occ)
-                           : stencil_occupancy<T, 256>(ctx, ls, which, &occ);
-        if (rc) return rc;
-        if (occ < 1) continue;
-        int prev = -1;
-        for (int per_sm : {occ, (3 * occ + 3) / 4, (occ + 1) / 2}) {
-            if (per_sm < 1 || per_sm == prev) continue;
-            prev = per_sm;
-            out.push_back(StencilShape{nt, per_sm * ctx->sm_count});
+    for (int st : {0, 1})
+        for (int nt : {128, 256}) {
+            int occ = 0;
+            int rc = st ? (nt == 128 ? stencil_occupancy<T, 128, 1>(ctx, ls, which, &occ)
+                                     : stencil_occupancy<T, 256, 1>(ctx, ls, which, &occ))
+                        : (nt == 128 ? stencil_occupancy<T, 128, 0>(ctx, ls, which, &occ)
+                                     : stencil_occupancy<T, 256, 0>(ctx, ls, which, &occ));
+            if (rc) return rc;
+            if (occ < 1) continue;
+            int prev = -1;
+            for (int per_sm : {occ, (3 * occ + 3) / 4, (occ + 1) / 2}) {
+                if (per_sm < 1 || per_sm == prev) continue;
+                prev = per_sm;
+                out.push_back(StencilShape{nt, per_sm * ctx->sm_count, st});
+            }
         }
-    }
     if (out.empty()) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
     return VLR_OK;
 }
@@ -528,10 +599,10 @@ static int stencil_candidates(vlr_ctx* ctx, vlr_level_set* ls, int which, std::v
 template <typename T>
 static int default_shape(vlr_ctx* ctx, vlr_level_set* ls, int which, StencilShape* sh) {
     int occ = 0;
-    int rc = stencil_occupancy<T, 256>(ctx, ls, which, &occ);
+    int rc = stencil_occupancy<T, 256, 0>(ctx, ls, which, &occ);
     if (rc) return rc;
     if (occ < 1) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
-    *sh = StencilShape{256, occ * ctx->sm_count};
+    *sh = StencilShape{256, occ * ctx->sm_count, 0};
     return VLR_OK;
 }
 

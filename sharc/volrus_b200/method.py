@@ -208,27 +208,31 @@ class LevelSet:
         self.ctx.check(self.ctx.lib.vlr_ls_enqueue(self.ctx.handle, self.handle, n), "vlr_ls_enqueue")
 
     def set_launch_shape(self, advect=None, reinit=None):
-        """Fix the stencil kernels' launch shapes as (threads, CTAs) pairs, or
-        pass nothing to let the next step's autotuner choose them again."""
+        """Fix the stencil kernels' launch shapes as (threads, CTAs[, staging])
+        tuples (staging 0: cp.async row copies, 1: TMA tensor copies; default
+        0), or pass nothing to let the next step's autotuner choose them again."""
         if advect is None:
-            self.ctx.check(self.ctx.lib.vlr_ls_set_launch_shape(self.ctx.handle, self.handle, 0, 0, 0, 0),
+            self.ctx.check(self.ctx.lib.vlr_ls_set_launch_shape(self.ctx.handle, self.handle, 0, 0, 0, 0, 0, 0),
                            "vlr_ls_set_launch_shape")
             return
-        self.ctx.check(self.ctx.lib.vlr_ls_set_launch_shape(self.ctx.handle, self.handle, advect[0], advect[1],
-                                                            reinit[0], reinit[1]), "vlr_ls_set_launch_shape")
+        a = tuple(advect) + (0,) * (3 - len(advect))
+        r = tuple(reinit) + (0,) * (3 - len(reinit))
+        self.ctx.check(self.ctx.lib.vlr_ls_set_launch_shape(self.ctx.handle, self.handle, *a, *r),
+                       "vlr_ls_set_launch_shape")
 
     def launch_shape(self):
-        """{"advect": (threads, CTAs), "reinit": (threads, CTAs), "timed": [(kernel, threads, CTAs, us), ...]}."""
-        shape = (C.c_int * 4)()
+        """{"advect": (threads, CTAs, staging), "reinit": (threads, CTAs, staging),
+        "timed": [(kernel, threads, CTAs, staging, us), ...]}."""
+        shape = (C.c_int * 6)()
         n = C.c_int()
         self.ctx.check(self.ctx.lib.vlr_ls_get_launch_shape(self.ctx.handle, self.handle, shape, C.byref(n), None, 0),
                        "vlr_ls_get_launch_shape")
-        log = np.zeros((max(n.value, 1), 4), np.float32)
+        log = np.zeros((max(n.value, 1), 5), np.float32)
         self.ctx.check(self.ctx.lib.vlr_ls_get_launch_shape(self.ctx.handle, self.handle, shape, C.byref(n),
                                                             ptr(log, C.c_float), len(log)), "vlr_ls_get_launch_shape")
         names = ("k_m_advect", "k_m_reinit")
-        timed = [(names[int(r[0])], int(r[1]), int(r[2]), float(r[3])) for r in log[: n.value]]
-        return {"advect": (shape[0], shape[1]), "reinit": (shape[2], shape[3]), "timed": timed}
+        timed = [(names[int(r[0])], int(r[1]), int(r[2]), int(r[3]), float(r[4])) for r in log[: n.value]]
+        return {"advect": (shape[0], shape[1], shape[2]), "reinit": (shape[3], shape[4], shape[5]), "timed": timed}
 
     def info(self):
         n = C.c_size_t()
