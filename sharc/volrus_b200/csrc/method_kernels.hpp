@@ -33,10 +33,13 @@ struct MTopo {
     int key_bits;
 };
 
-// Tensor maps of a stencil kernel's source value pool for staging mode 1: a
-// 4-D view (z, y, x, slot) of the pool with one box shape per map.  Map i has
-// box extents z = (i & 4 ? 4 : 8), y = (i & 1 ? 8 : H), x = (i & 2 ? 8 : H),
-// slot = 1; f16 pools use maps 0-3, f32 pools 0-7.
+// Tensor maps of a stencil kernel's source value pool for staging mode 1, one
+// box shape per map, with ey = (i & 1 ? 8 : H) and ex = (i & 2 ? 8 : H):
+//   maps 0-3: 3-D view (yz, x, slot) of the pool, where yz = y * 8 + z runs
+//             over the 64 contiguous values of an x-plane; box {ey * 8, ex, 1}
+//             (whole z-rows, so a box row is ey * 8 contiguous values)
+//   maps 4-7: 4-D view (z, y, x, slot); box {4, ey, ex, 1} (the f32 z-halves)
+// f16 pools use maps 0-3, f32 pools 0-7.
 struct StageMaps {
     CUtensorMap m[8];
 };

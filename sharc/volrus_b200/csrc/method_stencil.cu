@@ -20,6 +20,15 @@
 // or two iterations before they are used, so a leaf costs no dependent global
 // round trip.  The float tile is then built from shared memory.
 //
+// A second staging mode (ST = 1) brings the same pieces by TMA: one tensor
+// copy per present neighbour leaf (a box of whole z-rows, or of f32 z-halves)
+// completing on an mbarrier, issued by lane 0 of each warp in turn.  It moves
+// the same bytes and gives bit-identical results; the launch autotuner times
+// both modes.  On B200 the per-copy cost of up to 27 small boxes per leaf
+// (about 216 per SM per leaf round at 8 CTAs) leaves it 25-35% slower than
+// the cp.async rows, which every thread issues in parallel, so cp.async is
+// the mode the autotuner keeps on the measured workloads.
+//
 // Both kernels are latency- and issue-bound (a leaf moves 2-4 KB but runs a few
 // thousand instructions in phases separated by CTA barriers), so a leaf passes
 // as few barriers as its data flow allows (advect 3, reinit 4), results leave
@@ -148,12 +157,17 @@ __device__ __forceinline__ void stage_ready() {
 //   z: the whole row (f16: 8 values = 16 bytes); f32 z-neighbours copy only
 //      the 16-byte half that holds the H <= 4 values the tile uses
 // Each box lands dense (z fastest, then y, then x) at a 128-byte aligned
-// offset of the stage.  The row-offset table (built once per CTA in s_desc)
-// gives, for tile row (x, y) and z-piece k, the element offset p_k such that
-// stage[p_k + z] is voxel z of that row in the leaf below / at / above (k =
-// 0 / 1 / 2).  Up to 27 copies per leaf complete on one mbarrier whose
-// expected byte count is the sum of the issued boxes; the 27 masks still
-// arrive by cp.async.
+// offset of the stage.  A box of whole z-rows is contiguous over (y, z) in the
+// pool, so it is copied through a map whose innermost dimension merges y and
+// z: its rows are ey * 8 values wide (up to 128 bytes for f16) rather than
+// one 16-byte z-row each, which keeps the number of rows the tensor unit
+// walks per leaf low.  The row-offset table (built once per CTA in s_desc,
+// 16-bit entries biased by kRowBias) gives, for tile row (x, y) and z-piece
+// k, the element offset p_k such that stage[p_k + z] is voxel z of that row
+// in the leaf below / at / above (k = 0 / 1 / 2); 16-bit entries keep the
+// CTA within the shared memory that 8 resident CTAs per SM leave it.  Up to
+// 27 copies per leaf complete on one mbarrier whose expected byte count is
+// the sum of the issued boxes; the 27 masks still arrive by cp.async.
 template <typename T, int H>
 struct BoxStage {
     static constexpr int E = 8 + 2 * H;
@@ -175,8 +189,10 @@ struct BoxStage {
     static_assert(H >= 1 && H <= 4, "the f32 z-halves hold up to 4 values");
 };
 
+constexpr int kRowBias = 8;  // f32 k = 0 pieces start up to 4 elements before their box
+
 template <typename T, int H, int NT>
-__device__ __forceinline__ void build_row_offsets(unsigned* s_desc) {
+__device__ __forceinline__ void build_row_offsets(unsigned short* s_off) {
     using B = BoxStage<T, H>;
     constexpr int E = B::E;
     for (int p = threadIdx.x; p < E * E * 3; p += NT) {
@@ -187,19 +203,24 @@ __device__ __forceinline__ void build_row_offsets(unsigned* s_desc) {
         const int d = ax * 9 + ay * 3 + k;
         const int xl = (x & 7) - B::lo(ax), yl = (y & 7) - B::lo(ay);
         const int start = B::off(d) / (int)sizeof(T) + (xl * B::ext(ay) + yl) * B::ez(k);
-        s_desc[p] = (unsigned)(start - B::z0(k));  // may be negative (f32, k = 0): stored as two's complement
+        s_off[p] = (unsigned short)(start - B::z0(k) + kRowBias);
     }
+    static_assert(B::bytes / sizeof(T) + kRowBias < 65536, "row offsets fit 16 bits");
 }
 
-// Copy descriptor of box d: x = shared address, y = z0 | y0 << 8 | x0 << 16 |
-// map << 24, z = bytes.
+// Copy descriptor of box d: x = stage offset (bytes), y = c0 | c1 << 8 |
+// c2 << 16 | map << 24, z = bytes.  Maps 0-3 take coordinates (yz0 = 8 * y0,
+// x0, slot), maps 4-7 (z0, y0, x0, slot); the slot is the neighbour's, added
+// at issue.  Kept as 16 bytes so the issue loop reads it with one load and no
+// unpacking: the loop is on the critical path of its warp.
 template <typename T, int H>
-__device__ __forceinline__ uint4 tma_piece(uint32_t stage, int d) {
+__device__ __forceinline__ uint4 tma_piece(int d) {
     using B = BoxStage<T, H>;
     const int ax = d / 9, ay = (d / 3) % 3, az = d % 3;
-    const unsigned co = (unsigned)B::z0(az) | ((unsigned)B::lo(ay) << 8) | ((unsigned)B::lo(ax) << 16) |
-                        ((unsigned)B::map_of(d) << 24);
-    return make_uint4(stage + (uint32_t)B::off(d), co, (unsigned)B::box_bytes(d), 0u);
+    const int m = B::map_of(d);
+    const unsigned co = (m < 4) ? ((unsigned)(8 * B::lo(ay)) | ((unsigned)B::lo(ax) << 8))
+                                : ((unsigned)B::z0(az) | ((unsigned)B::lo(ay) << 8) | ((unsigned)B::lo(ax) << 16));
+    return make_uint4((unsigned)B::off(d), co | ((unsigned)m << 24), (unsigned)B::box_bytes(d), 0u);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
@@ -227,6 +248,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, unsigned parity) {
     return ok != 0u;
 }
 
+// 3-D tiled tensor copy global -> shared (coordinates yz, x, slot), completing
+// on the mbarrier at `bar`.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+        "%4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
 // 4-D tiled tensor copy global -> shared (coordinates z, y, x, slot), completing
 // on the mbarrier at `bar`.
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -238,23 +270,31 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// All threads (same place as stage_async): thread 0 walks the 27 neighbours
-// and, for each present one, raises the mbarrier's expected bytes by its box
-// and issues its tensor copy, then arrives (the phase cannot complete before
-// that arrival, so every expectation is posted in time); the masks follow by
-// cp.async.  One issuing thread keeps the issue out of the register budget of
-// the other warps, which the stencil arithmetic holds at the 64-register cap.
-__device__ __forceinline__ void stage_tma(const uint4* s_tma, const int* s_nb, const StageMaps& maps, uint32_t bar,
-                                          const uint64_t* __restrict__ masks, uint64_t* s_m) {
-    if (threadIdx.x == 0) {
+// All threads (same place as stage_async): lane 0 of warp w walks the
+// neighbours d = w, w + NW, ... and, for each present one, raises the
+// mbarrier's expected bytes by its box and issues its tensor copy, then
+// arrives; the mbarrier expects one arrival per warp, so the phase cannot
+// complete before every expectation is posted.  The masks follow by cp.async.
+// One issuing lane per warp keeps the issue out of the register budget of the
+// stencil arithmetic (held at the 64-register cap) and splits the serial issue
+// chain NW ways.
+template <int NT>
+__device__ __forceinline__ void stage_tma(const uint4* s_tma, const int* s_nb, const StageMaps& maps,
+                                          uint32_t stage, uint32_t bar, const uint64_t* __restrict__ masks,
+                                          uint64_t* s_m) {
+    if ((threadIdx.x & 31) == 0) {
 #pragma unroll 1
-        for (int d = 0; d < kNbr; ++d) {
+        for (int d = threadIdx.x >> 5; d < kNbr; d += NT / 32) {
             const int sl = s_nb[d];
             if (sl >= 0) {
                 const uint4 pc = s_tma[d];
+                const unsigned m = pc.y >> 24;
                 mbar_expect_tx_only(bar, pc.z);
-                tma_load_4d(pc.x, &maps.m[pc.y >> 24], (int)(pc.y & 255u), (int)((pc.y >> 8) & 255u),
-                            (int)((pc.y >> 16) & 255u), sl, bar);
+                if (m < 4u)
+                    tma_load_3d(stage + pc.x, &maps.m[m], (int)(pc.y & 255u), (int)((pc.y >> 8) & 255u), sl, bar);
+                else
+                    tma_load_4d(stage + pc.x, &maps.m[m], (int)(pc.y & 255u), (int)((pc.y >> 8) & 255u),
+                                (int)((pc.y >> 16) & 255u), sl, bar);
             }
         }
         mbar_arrive(bar);
@@ -289,7 +329,7 @@ __device__ __forceinline__ bool stage_ready_tma(uint32_t bar, unsigned parity) {
 // offsets, per-neighbour copy descriptors and the mbarrier (ST 1).  Callers
 // follow it with a CTA barrier.
 template <typename T, int H, int NT, int ST>
-__device__ __forceinline__ void stage_setup(unsigned* s_desc, uint4* s_tma, uint64_t* s_bar, const T* s_stage,
+__device__ __forceinline__ void stage_setup(unsigned* s_desc, uint4* s_tma, uint64_t* s_bar,
                                             const StageMaps& maps) {
     if constexpr (ST == 0) {
         build_stage_desc<T, H, NT>(s_desc);
@@ -298,9 +338,9 @@ __device__ __forceinline__ void stage_setup(unsigned* s_desc, uint4* s_tma, uint
         if (threadIdx.x < (sizeof(T) == 2 ? 4 : 8))
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.m[threadIdx.x]))
                          : "memory");
-        build_row_offsets<T, H, NT>(s_desc);
-        if (threadIdx.x < kNbr) s_tma[threadIdx.x] = tma_piece<T, H>(smem_addr(s_stage), threadIdx.x);
-        if (threadIdx.x == 0) mbar_init(smem_addr(s_bar), 1u);
+        build_row_offsets<T, H, NT>(reinterpret_cast<unsigned short*>(s_desc));
+        if (threadIdx.x < kNbr) s_tma[threadIdx.x] = tma_piece<T, H>(threadIdx.x);
+        if (threadIdx.x == 0) mbar_init(smem_addr(s_bar), NT / 32);
     }
 }
 
@@ -309,7 +349,7 @@ __device__ __forceinline__ void stage_issue(const unsigned* s_desc, const uint4*
                                             const int* s_nb, const T* __restrict__ vals, const StageMaps& maps,
                                             const uint64_t* __restrict__ masks, T* s_rows, uint64_t* s_m) {
     if constexpr (ST == 0) stage_async<T, H, NT>(s_desc, s_nb, vals, masks, s_rows, s_m);
-    else stage_tma(s_tma, s_nb, maps, smem_addr(s_bar), masks, s_m);
+    else stage_tma<NT>(s_tma, s_nb, maps, smem_addr(s_rows), smem_addr(s_bar), masks, s_m);
 }
 
 // Returns false (on every thread) if the tensor copies did not arrive in time.
@@ -377,10 +417,11 @@ __device__ __forceinline__ void build_row(const T* s_rows, const unsigned* s_des
         p2 = p0 + 16;
         c = s_rows + rc * RP + 8;
     } else {
-        p0 = s_rows + (int)s_desc[3 * r];
-        p1 = s_rows + (int)s_desc[3 * r + 1];
-        p2 = s_rows + (int)s_desc[3 * r + 2];
-        c = s_rows + (int)s_desc[3 * rc + 1];
+        const unsigned short* so = reinterpret_cast<const unsigned short*>(s_desc);
+        p0 = s_rows + ((int)so[3 * r] - kRowBias);
+        p1 = s_rows + ((int)so[3 * r + 1] - kRowBias);
+        p2 = s_rows + ((int)so[3 * r + 2] - kRowBias);
+        c = s_rows + ((int)so[3 * rc + 1] - kRowBias);
     }
     const float nan = __int_as_float(0x7fc00000);
     float mid[8];
@@ -659,7 +700,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     __shared__ unsigned short s_list[kLeafVoxels];
     __shared__ __align__(16) MGridParams s_P;
     __shared__ float2 s_tab[kMaxOctaves][3][8];
-    __shared__ unsigned s_desc[StageDesc<T, H>::NP];
+    __shared__ __align__(16) unsigned s_desc[ST ? (StageDesc<T, H>::NP + 1) / 2 : StageDesc<T, H>::NP];
     __shared__ uint4 s_tma[ST ? kNbr : 1];
     __shared__ uint64_t s_bar;
 
@@ -677,7 +718,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     // prologue: first leaf staged, next leaf's list entry in flight
     int slot = A.list[li];
     int4 o = A.origin[slot];
-    stage_setup<T, H, NT, ST>(s_desc, s_tma, &s_bar, s_raw, maps);
+    stage_setup<T, H, NT, ST>(s_desc, s_tma, &s_bar, maps);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
     stage_issue<T, H, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[0], src, maps, A.mask, s_raw, s_m);
@@ -914,7 +955,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     __shared__ unsigned short s_list[NW][RPW * F];
     __shared__ int s_nbr[2][32];
     __shared__ __align__(16) unsigned s_M[16];
-    __shared__ unsigned s_desc[StageDesc<T, 2>::NP];
+    __shared__ __align__(16) unsigned s_desc[ST ? (StageDesc<T, 2>::NP + 1) / 2 : StageDesc<T, 2>::NP];
     __shared__ uint4 s_tma[ST ? kNbr : 1];
     __shared__ uint64_t s_bar;
     __shared__ float s_dist[NIT == 2 ? F * F * F : 1];  // cut-voxel distances of the 10^3 box (NaN: not cut)
@@ -930,7 +971,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
 
     int slot = A.list[li];
     int4 o = A.origin[slot];
-    stage_setup<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_raw, maps);
+    stage_setup<T, 2, NT, ST>(s_desc, s_tma, &s_bar, maps);
     if (w0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
     stage_issue<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[0], src, maps, A.dmask, s_raw, s_dm);

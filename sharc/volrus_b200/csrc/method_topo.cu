@@ -430,23 +430,28 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // Tensor maps of a value pool (cap leaves of 512 values, x * 64 + y * 8 + z)
-// as a 4-D array (z, y, x, slot) with the box shapes of StageMaps for halo H.
+// with the views and box shapes of StageMaps for halo H.
 static int encode_stage_maps(vlr_ctx* ctx, const void* pool, int cap, bool f16, int H, StageMaps* out) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     if (reinterpret_cast<uintptr_t>(pool) % 16u)
         return set_error(ctx, VLR_ERR_CUDA, "value pool is not 16-byte aligned for tensor copies");
     const cuuint64_t es = f16 ? 2 : 4;
-    const cuuint64_t dims[4] = {8, 8, 8, (cuuint64_t)cap};
-    const cuuint64_t strides[3] = {8 * es, 64 * es, 512 * es};
+    const cuuint64_t dims3[3] = {64, 8, (cuuint64_t)cap};  // (yz, x, slot)
+    const cuuint64_t strides3[2] = {64 * es, 512 * es};
+    const cuuint64_t dims4[4] = {8, 8, 8, (cuuint64_t)cap};  // (z, y, x, slot)
+    const cuuint64_t strides4[3] = {8 * es, 64 * es, 512 * es};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     *out = StageMaps{};
     for (int i = 0; i < (f16 ? 4 : 8); ++i) {
-        const cuuint32_t box[4] = {(i & 4) ? 4u : 8u, (i & 1) ? 8u : (cuuint32_t)H, (i & 2) ? 8u : (cuuint32_t)H, 1u};
-        CUresult r = enc(&out->m[i], f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                         const_cast<void*>(pool), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        const cuuint32_t ey = (i & 1) ? 8u : (cuuint32_t)H, ex = (i & 2) ? 8u : (cuuint32_t)H;
+        const cuuint32_t box3[3] = {ey * 8u, ex, 1u};
+        const cuuint32_t box4[4] = {4u, ey, ex, 1u};
+        const bool four = (i & 4) != 0;
+        CUresult r = enc(&out->m[i], f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         four ? 4 : 3, const_cast<void*>(pool), four ? dims4 : dims3, four ? strides4 : strides3,
+                         four ? box4 : box3, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     }
     return VLR_OK;
