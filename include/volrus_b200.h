@@ -94,6 +94,25 @@ int vlr_advect_particles(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, c
  * (128^3 tiles in ascending origin order, then leaves, then voxels in ZYX
  * order); missing leaves are allocated at the background. */
 int vlr_dilate(vlr_ctx* ctx, vlr_grid* g, unsigned iterations);
+/* Replaces volume_to_mesh(&Grid<f32>, isovalue) -> Mesh
+ * (src/tools/volume_to_mesh.rs:46-201): marching cubes over the cells of every
+ * leaf tile and its 6 face neighbours.  Vertices (x, y, z doubles, world
+ * units) come in the reference's order and with its values: vertex i is the
+ * i-th edge crossing first met in the reference's visit order (tiles in
+ * ascending origin, cells x-major), interpolated from that cell's first edge
+ * endpoint.  Triangles (3 vertex indices) follow per cell in visit order from
+ * this library's own triangulation table (vlr_mc_triangle_table), which
+ * differs from the reference's classic table in the diagonals of some
+ * polygons.  *n_vertices and *n_triangles are always set; up to cap_vertices
+ * vertices and cap_triangles triangles are copied (pass null buffers to
+ * count only).  World-unit f32 grids only. */
+int vlr_volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float isovalue, double* vertices, size_t cap_vertices,
+                       uint32_t* triangles, size_t cap_triangles, size_t* n_vertices, size_t* n_triangles);
+/* The triangulation table used by vlr_volume_to_mesh: 256 cases (bit i set:
+ * corner i below the isovalue) x 16 edge indices, three per triangle, -1
+ * padded.  Host-only; no counterpart in the reference (its table is a
+ * constant, src/tools/volume_to_mesh.rs:226-483). */
+int vlr_mc_triangle_table(int8_t* out);
 
 /* ---- serialised formats ------------------------------------------------
  * .vol byte image (src/io/vol_format.rs:1-160) <-> device grid.  Replaces

@@ -147,6 +147,20 @@ void vo_extend_velocity(void* sdf, void* vx, void* vy, void* vz, float hw) {
 }
 void vo_remove_empty_leaves(void* g) { ((Grid*)g)->remove_empty_leaves(); }
 
+// volume_to_mesh: returns the vertex count and sets *n_tris; copies up to the
+// given capacities (vertices as x, y, z doubles; triangles as 3 indices).
+size_t vo_volume_to_mesh(void* g, float iso, const int8_t* tri, double* verts, size_t cap_v, uint32_t* tris,
+                         size_t cap_t, size_t* n_tris) {
+    std::vector<double> v;
+    std::vector<uint32_t> t;
+    volume_to_mesh(*(Grid*)g, iso, tri, v, t);
+    const size_t nv = v.size() / 3, nt = t.size() / 3;
+    if (verts) std::copy(v.begin(), v.begin() + 3 * std::min(nv, cap_v), verts);
+    if (tris) std::copy(t.begin(), t.begin() + 3 * std::min(nt, cap_t), tris);
+    *n_tris = nt;
+    return nv;
+}
+
 // One step of the reference pipeline, timed on this thread: advect_level_set
 // followed by rebuild_narrow_band (brute-force loop, as the crate runs it)
 // restricted to the first `rebuild_sample` active voxels when non-zero (the

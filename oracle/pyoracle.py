@@ -46,6 +46,8 @@ SIGS = {
     "vo_advect_particles": (None, [P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
     "vo_extend_velocity": (None, [P, P, P, P, C.c_float]),
     "vo_remove_empty_leaves": (None, [P]),
+    "vo_volume_to_mesh": (C.c_size_t, [P, C.c_float, C.POINTER(C.c_int8), dbl_p, C.c_size_t,
+                                       C.POINTER(C.c_uint32), C.c_size_t, size_p]),
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
     "vm_free": (None, [P]),
@@ -190,6 +192,20 @@ class OGrid:
     def extend_velocity(self, vx, vy, vz, half_width):
         """extend_velocity(self as the SDF, vx, vy, vz, half_width), in place on vx, vy, vz."""
         self.lib.vo_extend_velocity(self.h, vx.h, vy.h, vz.h, half_width)
+
+    def volume_to_mesh(self, isovalue=0.0):
+        """(vertices (n, 3) f64, triangles (m, 3) u32) with the triangle table of
+        oracle/mc_table.py."""
+        from oracle import mc_table
+        tab = np.asarray(mc_table.tri_table(), np.int8).reshape(-1)
+        lib = load()
+        nt = C.c_size_t()
+        nv = lib.vo_volume_to_mesh(self.h, isovalue, _p(tab, C.c_int8), None, 0, None, 0, C.byref(nt))
+        v = np.zeros((nv, 3), np.float64)
+        t = np.zeros((nt.value, 3), np.uint32)
+        lib.vo_volume_to_mesh(self.h, isovalue, _p(tab, C.c_int8), _p(v, C.c_double), nv, _p(t, C.c_uint32),
+                              nt.value, C.byref(nt))
+        return v, t
 
     def remove_empty_leaves(self):
         self.lib.vo_remove_empty_leaves(self.h)

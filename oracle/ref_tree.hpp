@@ -450,4 +450,90 @@ inline Grid make_level_set_sphere(double radius, const double center[3], double 
     return g;
 }
 
+
+// volume_to_mesh (src/tools/volume_to_mesh.rs:46-201): cells of the leaf
+// tiles and their 6 face neighbours, tiles in ascending (x, y, z), cells in
+// x-major order within a tile; corners read with Grid::get; an edge vertex is
+// created the first time a cell with that edge flagged is processed (the
+// HashMap edge cache keyed by the sorted corner pair), interpolated from the
+// creating cell's first endpoint toward its second in f32 t, f64 position.
+// `tri` holds the triangle table (16 entries per case, -1 terminated); the
+// edge table is the classification rule (edge flagged iff its corners differ).
+struct CoordPairHash {
+    size_t operator()(const std::pair<Coord, Coord>& p) const {
+        CoordHash h;
+        return h(p.first) * 31u ^ h(p.second);
+    }
+};
+
+inline bool coord_less(const Coord& a, const Coord& b) {
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    return a.z < b.z;
+}
+
+inline void volume_to_mesh(const Grid& g, float iso, const int8_t* tri, std::vector<double>& verts,
+                           std::vector<uint32_t>& tris) {
+    static const int kCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                      {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    static const int kEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                     {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+    verts.clear();
+    tris.clear();
+    std::vector<Coord> cells;
+    g.for_each_leaf([&](const Leaf& l) {
+        const Coord o = l.origin;
+        cells.push_back(o);
+        cells.push_back({o.x - 8, o.y, o.z});
+        cells.push_back({o.x + 8, o.y, o.z});
+        cells.push_back({o.x, o.y - 8, o.z});
+        cells.push_back({o.x, o.y + 8, o.z});
+        cells.push_back({o.x, o.y, o.z - 8});
+        cells.push_back({o.x, o.y, o.z + 8});
+    });
+    std::sort(cells.begin(), cells.end(), coord_less);
+    cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
+    const double vs = g.voxel_size;
+    std::unordered_map<std::pair<Coord, Coord>, uint32_t, CoordPairHash> cache;
+    for (const Coord& o : cells)
+        for (int lx = 0; lx < 8; ++lx)
+            for (int ly = 0; ly < 8; ++ly)
+                for (int lz = 0; lz < 8; ++lz) {
+                    Coord c[8];
+                    float v[8];
+                    int ci = 0;
+                    for (int i = 0; i < 8; ++i) {
+                        c[i] = {o.x + lx + kCorner[i][0], o.y + ly + kCorner[i][1], o.z + lz + kCorner[i][2]};
+                        v[i] = g.get(c[i]);
+                        if (v[i] < iso) ci |= 1 << i;
+                    }
+                    uint32_t ev[12] = {0};
+                    bool any = false;
+                    for (int e = 0; e < 12; ++e) {
+                        const int a = kEdge[e][0], b = kEdge[e][1];
+                        if (((ci >> a) & 1) == ((ci >> b) & 1)) continue;
+                        any = true;
+                        std::pair<Coord, Coord> key =
+                            coord_less(c[a], c[b]) ? std::make_pair(c[a], c[b]) : std::make_pair(c[b], c[a]);
+                        auto it = cache.find(key);
+                        if (it != cache.end()) {
+                            ev[e] = it->second;
+                            continue;
+                        }
+                        const float d = v[b] - v[a];
+                        const double t = (std::fabs(d) > 1e-10f) ? (double)((iso - v[a]) / d) : 0.5;
+                        const double pa[3] = {(double)c[a].x * vs, (double)c[a].y * vs, (double)c[a].z * vs};
+                        const double pb[3] = {(double)c[b].x * vs, (double)c[b].y * vs, (double)c[b].z * vs};
+                        const uint32_t idx = (uint32_t)(verts.size() / 3);
+                        for (int k = 0; k < 3; ++k) verts.push_back(pa[k] + t * (pb[k] - pa[k]));
+                        cache.emplace(key, idx);
+                        ev[e] = idx;
+                    }
+                    if (!any) continue;
+                    const int8_t* row = tri + 16 * ci;
+                    for (int t = 0; t < 15 && row[t] != -1; t += 3)
+                        for (int k = 0; k < 3; ++k) tris.push_back(ev[row[t + k]]);
+                }
+}
+
 }  // namespace vlr_oracle

@@ -14,6 +14,11 @@ int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size
 int trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int make_sphere(vlr_ctx* ctx, double radius, const double c[3], double vs, double hw, vlr_grid* out);
+// Marching-cubes isosurface (mesh.cu): counts always; copies up to the capacities.
+int volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float iso, double* h_verts, size_t cap_v, uint32_t* h_tris,
+                   size_t cap_t, size_t* n_verts, size_t* n_tris);
+// The derived marching-cubes triangle table, 256 x 16 entries (-1 padded).
+int mc_triangle_table(int8_t* out);
 // Add inactive background leaves at `origins` (3 ints each) to a world-unit grid (morphology.cu).
 int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origins);
 

@@ -138,4 +138,39 @@ int sort_reduce(vlr_ctx* ctx, unsigned* keys, float* vals, int n, unsigned key_l
     return VLR_OK;
 }
 
+int radix_sort_pairs(vlr_ctx* ctx, unsigned* keys, unsigned* vals, int n, unsigned key_limit, void* scratch,
+                     unsigned** keys_out, unsigned** vals_out) {
+    cudaStream_t st = ctx->stream;
+    *keys_out = keys;
+    *vals_out = vals;
+    if (n <= 0) return VLR_OK;
+    const int tiles = (n + kRsTile - 1) / kRsTile;
+    char* p = (char*)scratch;
+    unsigned* k2 = (unsigned*)p;
+    p += (size_t)n * 4;
+    unsigned* v2 = (unsigned*)p;
+    p += (size_t)n * 4;
+    int* hist = (int*)p;
+    p += (size_t)256 * tiles * 4;
+    int* offs = (int*)p;
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) <= (unsigned long long)key_limit) ++bits;
+    unsigned *ka = keys, *va = vals, *kb = k2, *vb = v2;
+    for (int shift = 0; shift < bits; shift += 8) {
+        VLR_TIMED(ctx, "k_rs_hist", k_rs_hist<<<tiles, kRsThreads, 0, st>>>(ka, n, shift, tiles, hist));
+        int rc = scan_exclusive(ctx, hist, offs, 256 * tiles, offs + 256 * tiles);
+        if (rc) return rc;
+        // the payload moves as raw 32-bit words
+        VLR_TIMED(ctx, "k_rs_scatter",
+                  k_rs_scatter<<<tiles, kRsThreads, 0, st>>>(ka, reinterpret_cast<const float*>(va), n, shift, tiles,
+                                                             offs, kb, reinterpret_cast<float*>(vb)));
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    *keys_out = ka;
+    *vals_out = va;
+    return VLR_OK;
+}
+
 }  // namespace vlr

@@ -226,6 +226,65 @@ def dilate(grid, iterations: int, ctx: Context | None = None):
         d.close()
 
 
+class Mesh:
+    """``Mesh`` (src/tools/volume_to_mesh.rs:11-40): vertices (n, 3) f64 in
+    world units and triangles (m, 3) u32 vertex indices."""
+
+    def __init__(self, vertices: np.ndarray, triangles: np.ndarray):
+        self.vertices = vertices
+        self.triangles = triangles
+
+    def tri_count(self) -> int:
+        return len(self.triangles)
+
+    def vertex_count(self) -> int:
+        return len(self.vertices)
+
+    def is_watertight(self) -> bool:
+        """Every undirected edge is shared by exactly two triangles."""
+        if len(self.triangles) == 0:
+            return True
+        t = self.triangles.astype(np.int64)
+        e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+        e.sort(axis=1)
+        _, counts = np.unique(e[:, 0] * (1 << 32) + e[:, 1], return_counts=True)
+        return bool(np.all(counts == 2))
+
+
+def volume_to_mesh(grid, isovalue: float = 0.0, ctx: Context | None = None) -> Mesh:
+    """``volume_to_mesh`` (src/tools/volume_to_mesh.rs:46-201) on the GPU:
+    vertices in the reference's order with its values; triangles from this
+    library's triangulation table (``mc_triangle_table``)."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    d, created = _as_device(grid, ctx)
+    try:
+        nv, nt = C.c_size_t(), C.c_size_t()
+        ctx.check(ctx.lib.vlr_volume_to_mesh(ctx.handle, d.handle, C.c_float(isovalue), None, 0, None, 0,
+                                             C.byref(nv), C.byref(nt)), "vlr_volume_to_mesh")
+        v = np.zeros((nv.value, 3), np.float64)
+        t = np.zeros((nt.value, 3), np.uint32)
+        if nv.value or nt.value:
+            ctx.check(ctx.lib.vlr_volume_to_mesh(ctx.handle, d.handle, C.c_float(isovalue),
+                                                 v.ctypes.data_as(C.POINTER(C.c_double)), nv.value,
+                                                 t.ctypes.data_as(C.POINTER(C.c_uint32)), nt.value,
+                                                 C.byref(nv), C.byref(nt)), "vlr_volume_to_mesh")
+        return Mesh(v, t)
+    finally:
+        if created:
+            d.close()
+
+
+def mc_triangle_table() -> np.ndarray:
+    """The triangulation table of ``volume_to_mesh``: (256, 16) int8, three
+    edge indices per triangle, -1 padded.  Host-only (no GPU needed)."""
+    from ._lib import load
+    out = np.zeros((256, 16), np.int8)
+    rc = load().vlr_mc_triangle_table(out.ctypes.data_as(C.POINTER(C.c_int8)))
+    if rc:
+        raise RuntimeError(f"vlr_mc_triangle_table failed: {rc}")
+    return out
+
+
 def make_level_set_sphere(radius: float, center, voxel_size: float, half_width: float, ctx: Context | None = None,
                           device: bool = False):
     """``make_level_set_sphere`` (src/tools/sphere.rs:17-59), generated on the GPU."""

@@ -1,0 +1,196 @@
+"""volume_to_mesh (src/tools/volume_to_mesh.rs:46-201).
+
+CPU: the triangulation table derived by the library (vlr_mc_triangle_table,
+host-only) equals the oracle's independent derivation (oracle/mc_table.py)
+and uses exactly the flagged edges of each case; the oracle restatement
+(oracle/ref_tree.hpp) passes the crate's own tests (volume_to_mesh.rs:510-587)
+and agrees with a small pure-Python restatement of the reference loop.
+
+GPU: vertices bit-exact against the oracle (order and f64 values: the
+reference's visit order, first-touch numbering and interpolation rounding)
+and triangles identical (same table), for spheres, a multi-tile union of
+random spheres straddling negative coordinates, an advected grid, a
+non-zero isovalue, random-valued leaves (ambiguous faces everywhere) and an
+empty grid.
+"""
+import numpy as np
+import pytest
+
+
+def to_oracle(oracle, g):
+    o, m, v = g.to_arrays()
+    return oracle.OGrid.from_arrays(o, m, v, g.background, g.transform.voxel_size, g.transform.origin,
+                                    g.affine.mat, g.affine.voxel_size)
+
+
+def watertight(tris):
+    if len(tris) == 0:
+        return True
+    t = tris.astype(np.int64)
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    e.sort(axis=1)
+    _, counts = np.unique(e[:, 0] * (1 << 32) + e[:, 1], return_counts=True)
+    return bool(np.all(counts == 2))
+
+
+# ------------------------------------------------------------------ CPU
+
+def test_library_table_equals_oracle_derivation():
+    from oracle import mc_table
+    from sharc.volrus_b200 import mc_triangle_table
+    assert np.array_equal(mc_triangle_table(), np.asarray(mc_table.tri_table(), np.int8))
+
+
+def test_table_uses_exactly_the_flagged_edges():
+    from oracle import mc_table
+    et = mc_table.edge_table()
+    for case, row in enumerate(mc_table.tri_table()):
+        used = [v for v in row if v >= 0]
+        assert len(used) % 3 == 0 and len(used) <= 15
+        assert set(used) == {e for e in range(12) if (et[case] >> e) & 1}, case
+        assert row[len(used):] == [-1] * (16 - len(used))
+
+
+def test_oracle_sphere_produces_triangles(oracle):  # volume_to_mesh.rs:510-522
+    v, t = oracle.OGrid.sphere(5.0, (0.0, 0.0, 0.0), 1.0, 3.0).volume_to_mesh(0.0)
+    assert len(t) > 0 and len(v) > 0
+
+
+def test_oracle_sphere_counts_reasonable(oracle):  # volume_to_mesh.rs:524-540
+    _, t = oracle.OGrid.sphere(5.0, (0.0, 0.0, 0.0), 1.0, 3.0).volume_to_mesh(0.0)
+    assert 50 < len(t) < 100_000
+
+
+def test_oracle_sphere_watertight(oracle):  # volume_to_mesh.rs:542-552
+    _, t = oracle.OGrid.sphere(5.0, (0.0, 0.0, 0.0), 1.0, 3.0).volume_to_mesh(0.0)
+    assert watertight(t)
+
+
+def test_oracle_vertices_near_surface(oracle):  # volume_to_mesh.rs:554-579
+    v, _ = oracle.OGrid.sphere(5.0, (0.0, 0.0, 0.0), 0.5, 5.0).volume_to_mesh(0.0)
+    near = np.abs(np.linalg.norm(v, axis=1) - 5.0) < 1.0
+    assert near.mean() > 0.75
+
+
+def test_oracle_empty_grid(oracle):  # volume_to_mesh.rs:581-587
+    v, t = oracle.OGrid.new(3.0, 1.0).volume_to_mesh(0.0)
+    assert len(v) == 0 and len(t) == 0
+
+
+def _python_mesh(og, iso):
+    """Literal restatement of the reference loop (volume_to_mesh.rs:46-201) for small grids."""
+    from oracle import mc_table
+    tri = mc_table.tri_table()
+    o, _, _ = og.arrays()
+    vs = og.meta()[1]
+    cells = set()
+    for x, y, z in o:
+        for d in ((0, 0, 0), (-8, 0, 0), (8, 0, 0), (0, -8, 0), (0, 8, 0), (0, 0, -8), (0, 0, 8)):
+            cells.add((int(x) + d[0], int(y) + d[1], int(z) + d[2]))
+    cache, verts, tris = {}, [], []
+    for ox, oy, oz in sorted(cells):
+        for lx in range(8):
+            for ly in range(8):
+                for lz in range(8):
+                    b = (ox + lx, oy + ly, oz + lz)
+                    cs = [(b[0] + c[0], b[1] + c[1], b[2] + c[2]) for c in mc_table.CORNERS]
+                    val = [np.float32(og.get(c)) for c in cs]
+                    ci = sum(1 << i for i in range(8) if val[i] < np.float32(iso))
+                    ev = [0] * 12
+                    for e, (a, bb) in enumerate(mc_table.EDGE_ENDPOINTS):
+                        if ((ci >> a) & 1) == ((ci >> bb) & 1):
+                            continue
+                        key = tuple(sorted((cs[a], cs[bb])))
+                        if key not in cache:
+                            d = np.float32(val[bb] - val[a])
+                            t = float(np.float32(np.float32(iso) - val[a]) / d) if abs(d) > np.float32(1e-10) else 0.5
+                            pa = [float(c) * vs for c in cs[a]]
+                            pb = [float(c) * vs for c in cs[bb]]
+                            cache[key] = len(verts)
+                            verts.append([pa[k] + t * (pb[k] - pa[k]) for k in range(3)])
+                        ev[e] = cache[key]
+                    r = tri[ci]
+                    for k in range(0, 15, 3):
+                        if r[k] < 0:
+                            break
+                        tris.append([ev[r[k]], ev[r[k + 1]], ev[r[k + 2]]])
+    return np.array(verts, np.float64).reshape(-1, 3), np.array(tris, np.uint32).reshape(-1, 3)
+
+
+def test_oracle_matches_python_restatement(oracle):
+    og = oracle.OGrid.sphere(2.5, (0.3, -0.2, 0.1), 1.0, 2.0)
+    v1, t1 = og.volume_to_mesh(0.25)
+    v2, t2 = _python_mesh(og, 0.25)
+    assert np.array_equal(v1.view(np.uint64), v2.view(np.uint64))
+    assert np.array_equal(t1, t2)
+
+
+# ------------------------------------------------------------------ GPU
+
+def _gpu_vs_oracle(oracle, g, iso):
+    from sharc.volrus_b200 import volume_to_mesh
+    m = volume_to_mesh(g, iso)
+    v2, t2 = to_oracle(oracle, g).volume_to_mesh(iso)
+    assert m.vertices.shape == v2.shape, (m.vertices.shape, v2.shape)
+    assert np.array_equal(m.vertices.view(np.uint64), v2.view(np.uint64)), "vertices differ"
+    assert np.array_equal(m.triangles, t2), "triangles differ"
+    return m
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("args", [(5.0, 1.0, 3.0), (5.0, 0.5, 5.0), (20.0, 1.0, 3.0)], ids=["r5", "r5_vs05", "r20"])
+def test_sphere_mesh_bit_exact(ctx, oracle, args):
+    from sharc.volrus_b200 import make_level_set_sphere
+    r, vs, hw = args
+    g = make_level_set_sphere(r, (0.3, -0.7, 1.1), vs, hw)
+    m = _gpu_vs_oracle(oracle, g, 0.0)
+    assert m.tri_count() > 50 and m.is_watertight()
+
+
+@pytest.mark.gpu
+def test_union_of_spheres_bit_exact(ctx, oracle):
+    from sharc.volrus_b200 import Grid
+    rng = np.random.default_rng(5)
+    og = oracle.OGrid.new(3.0, 1.0)
+    for _ in range(6):
+        s = oracle.OGrid.sphere(float(rng.uniform(4, 12)), tuple(rng.uniform(-30, 30, 3)), 1.0, 3.0)
+        o, msk, v = s.arrays()
+        for (x, y, z), mm, vv in zip(o, msk, v):
+            for off in range(512):
+                if (int(mm[off >> 6]) >> (off & 63)) & 1:
+                    c = (int(x) + (off >> 6), int(y) + ((off >> 3) & 7), int(z) + (off & 7))
+                    if vv[off] < og.get(c) or not og.is_active(c):
+                        og.set(c, float(vv[off]))
+    o, msk, v = og.arrays()
+    g = Grid.from_arrays(o, msk, v, 3.0, None)
+    _gpu_vs_oracle(oracle, g, 0.0)
+    _gpu_vs_oracle(oracle, g, -0.75)
+
+
+@pytest.mark.gpu
+def test_advected_grid_bit_exact(ctx, oracle):
+    from sharc.volrus_b200 import advect_level_set, make_level_set_sphere, make_uniform_velocity
+    g = make_level_set_sphere(9.0, (1.0, 2.0, -3.0), 1.0, 3.0)
+    out = advect_level_set(g, make_uniform_velocity(1.0, (0.7, -0.4, 0.3)), 1.5)
+    _gpu_vs_oracle(oracle, out, 0.0)
+
+
+@pytest.mark.gpu
+def test_random_leaves_bit_exact(ctx, oracle):
+    """Random values: every case of the table, ambiguous faces, ties at the isovalue."""
+    from sharc.volrus_b200 import Grid
+    rng = np.random.default_rng(9)
+    origins = np.array([[0, 0, 0], [8, 0, 0], [0, 8, 0], [-8, -8, 16], [24, 0, -8]], np.int32)
+    masks = rng.integers(0, 2**63, (len(origins), 8), dtype=np.uint64)
+    vals = rng.choice(np.array([-1.0, -0.25, 0.0, 0.5, 1.0], np.float32), (len(origins), 512))
+    vals += rng.normal(0, 0.1, vals.shape).astype(np.float32) * (rng.random(vals.shape) < 0.5)
+    g = Grid.from_arrays(origins, masks, vals.astype(np.float32), 0.75, None)
+    _gpu_vs_oracle(oracle, g, 0.0)
+    _gpu_vs_oracle(oracle, g, 0.5)
+
+
+@pytest.mark.gpu
+def test_empty_grid(ctx):
+    from sharc.volrus_b200 import Grid, volume_to_mesh
+    m = volume_to_mesh(Grid(3.0, 1.0), 0.0)
+    assert m.vertex_count() == 0 and m.tri_count() == 0
