@@ -604,6 +604,85 @@ def bench_large_line(args, ctx, peak, peak_kind):
             "clocks": clk.summary(), "gpu_launches": len(STEP_KERNELS) * min(args.steps, 5)}
 
 
+MESH = dict(radius=96.0, center=(0.5, -0.25, 0.125), voxel_size=1.0, half_width=3.0)
+
+
+def bench_mesh(args, ctx, peak, peak_kind):
+    """volume_to_mesh on a world-unit sphere (r = 96 voxels, half-width 3):
+    one C-ABI call per step with host output buffers (device work, sync and
+    the vertex / triangle downloads inside the timed region), kernel times
+    from the context profiler, and the single-threaded oracle on the same
+    grid as the CPU baseline."""
+    import ctypes as C
+
+    import numpy as np
+
+    from oracle import pyoracle
+    from sharc.volrus_b200 import make_level_set_sphere
+
+    g = make_level_set_sphere(MESH["radius"], MESH["center"], MESH["voxel_size"], MESH["half_width"], ctx=ctx,
+                              device=True)
+    n_leaves = g.leaf_count()
+    nv, nt = C.c_size_t(), C.c_size_t()
+    ctx.check(ctx.lib.vlr_volume_to_mesh(ctx.handle, g.handle, C.c_float(0.0), None, 0, None, 0, C.byref(nv),
+                                         C.byref(nt)), "vlr_volume_to_mesh")
+    verts = np.zeros((nv.value, 3), np.float64)
+    tris = np.zeros((nt.value, 3), np.uint32)
+
+    def call():
+        ctx.check(ctx.lib.vlr_volume_to_mesh(ctx.handle, g.handle, C.c_float(0.0),
+                                             verts.ctypes.data_as(C.POINTER(C.c_double)), nv.value,
+                                             tris.ctypes.data_as(C.POINTER(C.c_uint32)), nt.value, C.byref(nv),
+                                             C.byref(nt)), "vlr_volume_to_mesh")
+
+    for _ in range(max(3, args.warmup)):
+        call()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    call_s = (time.perf_counter() - t0) / args.steps
+    ctx.profile(True)  # kernel times from a separate pass (the events would perturb the timed calls)
+    for _ in range(args.steps):
+        call()
+    names = ("k_mc_classify", "k_mc_emit", "k_rs_hist", "k_rs_scatter")
+    kern = {k: ctx.kernel_time(k) for k in names}
+    ctx.profile(False)
+    kms = {k: v[0] / max(args.steps, 1) for k, v in kern.items()}
+    # tiles visited: every leaf tile and its face neighbours (counted on the host from the leaf list)
+    o, _, _ = g.download().to_arrays()
+    tiles = set()
+    for x, y, z in (o // 8).tolist():
+        for d in ((0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)):
+            tiles.add((x + d[0], y + d[1], z + d[2]))
+    cells = 512 * len(tiles)
+    dev_ms = kms["k_mc_classify"] + kms["k_mc_emit"]
+    # classify + emit bytes: leaf values read twice (each tile reads its own and
+    # its +1 neighbours' layers: ~1.4x a leaf), cell words written and read,
+    # vertices and triangles written
+    algo = 2 * 1.4 * 2048 * len(tiles) + 2 * 4 * cells + 24 * nv.value + 12 * nt.value
+    achieved = algo / (dev_ms * 1e-3) / 1e9
+    host = g.download()
+    ho, hm, hv = host.to_arrays()
+    og = pyoracle.OGrid.from_arrays(ho, hm, hv, host.background, host.transform.voxel_size)
+    t0 = time.perf_counter()
+    ov, ot = og.volume_to_mesh(0.0)
+    cpu_s = time.perf_counter() - t0
+    exact = bool(np.array_equal(ov.view(np.uint64), verts.view(np.uint64)) and np.array_equal(ot, tris))
+    return {
+        "workload": f"world-unit sphere r={MESH['radius']:g} voxels, half-width {MESH['half_width']:g}, isovalue 0",
+        "leaves": n_leaves, "tiles": len(tiles), "cells": cells, "vertices": nv.value, "triangles": nt.value,
+        "value": cells / call_s, "unit": "cells/s (one C-ABI call, host output buffers, downloads included)",
+        "call_ms": call_s * 1e3, "kernels_ms_per_call": kms, "device_ms": dev_ms,
+        "device_cells_per_s": cells / (dev_ms * 1e-3),
+        "roofline": {"bound": "hbm", "kernels": "k_mc_classify + k_mc_emit", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": algo},
+        "d2h_bytes_per_call": int(verts.nbytes + tris.nbytes),
+        "cpu_baseline": {"value": cells / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                         "sample": "the oracle restatement of volume_to_mesh on the same grid, one call"},
+        "matches_oracle": exact,
+    }
+
+
 def bench_adjoint_line(args, ctx):
     """The adjoint configuration on its own (forward + backward per step)."""
     with ClockSampler(args.device) as clk, clk.mark():
@@ -633,6 +712,7 @@ def bench_deformation(args, ctx, peak, peak_kind):
     accuracy = None if args.no_accuracy else {"f16": full_period(args, ctx, F16), "f32": full_period(args, ctx, F32),
                                               "f16_subcell_fix": full_period(args, ctx, F16, reinit_mode=1)}
     adjoint = None if args.no_adjoint else bench_adjoint(args, ctx)
+    mesh = None if args.no_mesh else bench_mesh(args, ctx, peak, peak_kind)
     launches_per_step = len(STEP_KERNELS)  # one CUDA graph per step
     line = {
         "metric": METRIC, "value": r16["value"], "unit": "voxels/s", "ms_per_step": r16["ms_per_step"],
@@ -664,6 +744,8 @@ def bench_deformation(args, ctx, peak, peak_kind):
         line["full_period"] = accuracy
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if mesh is not None:
+        line["volume_to_mesh"] = mesh
     return line
 
 
@@ -777,6 +859,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-grid batched measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the full-period accuracy run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--no-mesh", action="store_true", help="skip the volume_to_mesh measurement")
     ap.add_argument("--launch-shape", default="",
                     help="threads,CTAs[,staging] of advect then reinit, e.g. 128,1184,1,128,888,1 (default: "
                          "autotuned; staging 0 cp.async, 1 TMA)")
@@ -869,7 +952,8 @@ def main():
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("issue_roofline", "fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint"):
+        for k in ("issue_roofline", "fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint",
+                  "volume_to_mesh"):
             if k in res and res[k] is None:
                 continue
             if k in res:
