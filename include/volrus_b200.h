@@ -94,6 +94,13 @@ int vlr_advect_particles(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, c
  * (128^3 tiles in ascending origin order, then leaves, then voxels in ZYX
  * order); missing leaves are allocated at the background. */
 int vlr_dilate(vlr_ctx* ctx, vlr_grid* g, unsigned iterations);
+/* Replaces flood_fill_sign(&mut Grid<f32>) (src/tools/flood_fill.rs:18-107):
+ * in every leaf with an active voxel, each inactive voxel becomes -background
+ * if strictly more of its active 6-neighbours inside the leaf are negative
+ * than not, +background if not, and the leaf's majority sign (negative only
+ * if strictly more active values are negative) if it has none.  Enqueued on
+ * the context stream. */
+int vlr_flood_fill_sign(vlr_ctx* ctx, vlr_grid* g);
 /* Replaces volume_to_mesh(&Grid<f32>, isovalue) -> Mesh
  * (src/tools/volume_to_mesh.rs:46-201): marching cubes over the cells of every
  * leaf tile and its 6 face neighbours.  Vertices (x, y, z doubles, world

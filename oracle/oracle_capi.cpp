@@ -146,6 +146,7 @@ void vo_extend_velocity(void* sdf, void* vx, void* vy, void* vz, float hw) {
     extend_velocity(*(Grid*)sdf, *(Grid*)vx, *(Grid*)vy, *(Grid*)vz, hw);
 }
 void vo_remove_empty_leaves(void* g) { ((Grid*)g)->remove_empty_leaves(); }
+void vo_flood_fill_sign(void* g) { flood_fill_sign(*(Grid*)g); }
 
 // volume_to_mesh: returns the vertex count and sets *n_tris; copies up to the
 // given capacities (vertices as x, y, z doubles; triangles as 3 indices).

@@ -46,6 +46,7 @@ SIGS = {
     "vo_advect_particles": (None, [P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
     "vo_extend_velocity": (None, [P, P, P, P, C.c_float]),
     "vo_remove_empty_leaves": (None, [P]),
+    "vo_flood_fill_sign": (None, [P]),
     "vo_volume_to_mesh": (C.c_size_t, [P, C.c_float, C.POINTER(C.c_int8), dbl_p, C.c_size_t,
                                        C.POINTER(C.c_uint32), C.c_size_t, size_p]),
     "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
@@ -206,6 +207,9 @@ class OGrid:
         lib.vo_volume_to_mesh(self.h, isovalue, _p(tab, C.c_int8), _p(v, C.c_double), nv, _p(t, C.c_uint32),
                               nt.value, C.byref(nt))
         return v, t
+
+    def flood_fill_sign(self):
+        self.lib.vo_flood_fill_sign(self.h)
 
     def remove_empty_leaves(self):
         self.lib.vo_remove_empty_leaves(self.h)

@@ -451,6 +451,42 @@ inline Grid make_level_set_sphere(double radius, const double center[3], double 
 }
 
 
+// flood_fill_sign (src/tools/flood_fill.rs:18-107): per leaf with an active
+// voxel, the leaf's majority sign (negative only if strictly more active
+// values are < 0); each inactive voxel then takes -bg if strictly more of its
+// active 6-neighbours inside the leaf are < 0 than not, +bg if not, and the
+// leaf majority if it has no active neighbour in the leaf.  Reads a snapshot
+// of the leaf, so the result does not depend on the voxel order.
+inline void flood_fill_sign(Grid& g) {
+    const float bg = g.background;
+    g.for_each_leaf_mut([&](Leaf& l) {
+        int neg = 0, pos = 0;
+        for (int off = 0; off < 512; ++off)
+            if (l.is_on(off)) {
+                if (l.values[off] < 0.0f) ++neg;
+                else ++pos;
+            }
+        if (neg == 0 && pos == 0) return;
+        const float global = neg > pos ? -bg : bg;
+        float snap[512];
+        std::memcpy(snap, l.values, sizeof(snap));
+        for (int off = 0; off < 512; ++off) {
+            if (l.is_on(off)) continue;
+            const int lx = off >> 6, ly = (off >> 3) & 7, lz = off & 7;
+            int ln = 0, lp = 0;
+            for (const auto& d : kNbr6) {
+                const int nx = lx + d.x, ny = ly + d.y, nz = lz + d.z;
+                if (nx < 0 || nx > 7 || ny < 0 || ny > 7 || nz < 0 || nz > 7) continue;
+                const int no = (nx << 6) | (ny << 3) | nz;
+                if (!l.is_on(no)) continue;
+                if (snap[no] < 0.0f) ++ln;
+                else ++lp;
+            }
+            l.values[off] = (ln + lp > 0) ? (ln > lp ? -bg : bg) : global;
+        }
+    });
+}
+
 // volume_to_mesh (src/tools/volume_to_mesh.rs:46-201): cells of the leaf
 // tiles and their 6 face neighbours, tiles in ascending (x, y, z), cells in
 // x-major order within a tile; corners read with Grid::get; an edge vertex is

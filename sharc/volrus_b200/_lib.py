@@ -99,6 +99,7 @@ SIGNATURES = {
     "vlr_extend_velocity": (C.c_int, [P, P, P, P, P, C.c_float]),
     "vlr_advect_particles": (C.c_int, [P, P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
     "vlr_dilate": (C.c_int, [P, P, C.c_uint]),
+    "vlr_flood_fill_sign": (C.c_int, [P, P]),
     "vlr_volume_to_mesh": (C.c_int, [P, P, C.c_float, dbl_p, C.c_size_t, C.POINTER(C.c_uint32), C.c_size_t, size_p,
                                      size_p]),
     "vlr_mc_triangle_table": (C.c_int, [C.POINTER(C.c_int8)]),

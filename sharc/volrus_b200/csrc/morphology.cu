@@ -265,6 +265,40 @@ int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origi
 
 }  // namespace vlr
 
+// flood_fill_sign (src/tools/flood_fill.rs:18-107), one CTA per leaf and one
+// thread per voxel: the leaf's active-voxel sign counts by CTA-wide counts,
+// then each inactive voxel's active 6-neighbours inside the leaf, read from a
+// shared-memory snapshot of the leaf, so the result is order independent.
+__global__ void __launch_bounds__(512) k_flood_fill(const uint64_t* __restrict__ mask, float* __restrict__ values,
+                                                   float bg) {
+    __shared__ uint64_t s_m[8];
+    __shared__ float s_v[512];
+    const size_t leaf = blockIdx.x;
+    const int t = threadIdx.x;
+    if (t < 8) s_m[t] = mask[leaf * 8 + t];
+    const float v = values[leaf * 512 + t];
+    s_v[t] = v;
+    __syncthreads();
+    const bool on = (s_m[t >> 6] >> (t & 63)) & 1ull;
+    const int neg = __syncthreads_count(on && v < 0.0f);
+    const int act = __syncthreads_count(on);
+    if (act == 0 || on) return;
+    const float global = neg > act - neg ? -bg : bg;
+    const int lx = t >> 6, ly = (t >> 3) & 7, lz = t & 7;
+    int ln = 0, lp = 0;
+    const int d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const int nx = lx + d[k][0], ny = ly + d[k][1], nz = lz + d[k][2];
+        if (nx < 0 || nx > 7 || ny < 0 || ny > 7 || nz < 0 || nz > 7) continue;
+        const int no = (nx << 6) | (ny << 3) | nz;
+        if (!((s_m[no >> 6] >> (no & 63)) & 1ull)) continue;
+        if (s_v[no] < 0.0f) ++ln;
+        else ++lp;
+    }
+    values[leaf * 512 + t] = (ln + lp > 0) ? (ln > lp ? -bg : bg) : global;
+}
+
 extern "C" {
 
 int vlr_dilate(vlr_ctx* ctx, vlr_grid* g, unsigned iterations) {
@@ -285,6 +319,16 @@ int vlr_dilate(vlr_ctx* ctx, vlr_grid* g, unsigned iterations) {
         VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
     return consume_device_errors(ctx, "vlr_dilate");
+}
+
+int vlr_flood_fill_sign(vlr_ctx* ctx, vlr_grid* g) {
+    if (!ctx || !g) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (g->kind != VLR_KIND_F32_WORLD) return set_error(ctx, VLR_ERR_INVALID, "grid is not a world-unit f32 grid");
+    if (g->n == 0) return VLR_OK;
+    VLR_TIMED(ctx, "k_flood_fill",
+              k_flood_fill<<<g->n, 512, 0, ctx->stream>>>(g->mask, (float*)g->values, g->background));
+    VLR_CUDA(ctx, cudaGetLastError());
+    return VLR_OK;
 }
 
 }  // extern "C"

@@ -226,6 +226,18 @@ def dilate(grid, iterations: int, ctx: Context | None = None):
         d.close()
 
 
+def flood_fill_sign(grid, ctx: Context | None = None):
+    """``flood_fill_sign`` (src/tools/flood_fill.rs:18-107), in place: inactive
+    voxels of each leaf take -background or +background from the signs of
+    their active 6-neighbours in the leaf (the leaf's majority if none)."""
+    ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
+    d, created = _as_device(grid, ctx)
+    ctx.check(ctx.lib.vlr_flood_fill_sign(ctx.handle, d.handle), "vlr_flood_fill_sign")
+    if created:
+        _replace(grid, d.download())
+        d.close()
+
+
 class Mesh:
     """``Mesh`` (src/tools/volume_to_mesh.rs:11-40): vertices (n, 3) f64 in
     world units and triangles (m, 3) u32 vertex indices."""
