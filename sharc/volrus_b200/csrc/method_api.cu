@@ -301,6 +301,81 @@ __global__ void k_gather_sel(const int* list, const int* sel, int k, const uint6
     }
 }
 
+// Output order of a host step without a host round trip: for up to
+// kDevSortLeaves listed leaves of a single grid, one CTA sorts their (x, y, z)
+// keys (bitonic sort in shared memory; keys are leaf coordinates relative to
+// the grid's hash base, bits each, so their order is the lexicographic order
+// of the origins) and writes the sorted list positions and origins.  More
+// leaves: *status = 0 and the host sorts instead.
+constexpr int kDevSortLeaves = 8192;
+constexpr size_t kDevSortSmem = (size_t)kDevSortLeaves * (8 + 2);
+
+__global__ void __launch_bounds__(1024) k_sort_small(const int* __restrict__ list, const int* __restrict__ count,
+                                                    const int4* __restrict__ origin, long long b0, long long b1,
+                                                    long long b2, int bits, int* __restrict__ sel,
+                                                    int32_t* __restrict__ o3, int* __restrict__ status) {
+    extern __shared__ unsigned long long s_key[];
+    unsigned short* s_idx = reinterpret_cast<unsigned short*>(s_key + kDevSortLeaves);
+    const int n = *count;
+    if (n > kDevSortLeaves) {
+        if (threadIdx.x == 0) *status = 0;
+        return;
+    }
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        unsigned long long key = ~0ull;
+        if (i < n) {
+            const int4 o = origin[list[i]];
+            key = ((unsigned long long)((o.x >> 3) - b0) << (2 * bits)) |
+                  ((unsigned long long)((o.y >> 3) - b1) << bits) | (unsigned long long)((o.z >> 3) - b2);
+        }
+        s_key[i] = key;
+        s_idx[i] = (unsigned short)i;
+    }
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < N; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = s_key[i], b = s_key[l];
+                    if (((i & k) == 0) ? (a > b) : (a < b)) {
+                        s_key[i] = b;
+                        s_key[l] = a;
+                        const unsigned short t = s_idx[i];
+                        s_idx[i] = s_idx[l];
+                        s_idx[l] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int p = s_idx[i];
+        sel[i] = p;
+        const int4 o = origin[list[p]];
+        o3[3 * i] = o.x;
+        o3[3 * i + 1] = o.y;
+        o3[3 * i + 2] = o.z;
+    }
+    if (threadIdx.x == 0) *status = 1;
+}
+
+// k_gather_sel with the count and the sort status read on the device.
+template <typename T>
+__global__ void k_gather_sel_dev(const int* list, const int* sel, const int* count, const int* status,
+                                 const uint64_t* mask, const T* vals, uint64_t* m_out, float* v_out) {
+    if (!*status) return;
+    const int k = *count;
+    for (int i = blockIdx.x; i < k; i += gridDim.x) {
+        const int s = list[sel[i]];
+        if (threadIdx.x < 8) m_out[(size_t)i * 8 + threadIdx.x] = mask[(size_t)s * 8 + threadIdx.x];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            v_out[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
+    }
+}
+
 __global__ void k_count_active(const int* list, const int* count_ptr, const uint64_t* mask,
                                unsigned long long* out) {
     int n = *count_ptr;
@@ -704,18 +779,62 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     if (!ctx || !ls || !origins || !masks || !phi || !n_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "host steps replace single-grid states only");
     *n_out = 0;
-    int rc = upload_enqueue(ctx, ls, origins, masks, phi, n_leaves, false);
+    // staging for the device-sorted download (sized first, so the upload
+    // never regrows it while its copies are in flight)
+    const size_t kv = (size_t)kDevSortLeaves;
+    const size_t dl_bytes = kv * (sizeof(float) * kLeafVoxels + 64 + 12 + 4) + 256;
+    void* stg = nullptr;
+    int rc = ls_staging(ctx, ls, std::max(dl_bytes, sizeof(float) * kLeafVoxels * n_leaves + 12 * n_leaves + 16),
+                        &stg);
+    if (rc) return rc;
+    rc = upload_enqueue(ctx, ls, origins, masks, phi, n_leaves, false);
     if (rc) return rc;
     for (int i = 0; i < n_steps; ++i) {
         rc = enqueue_one_step(ctx, ls);
         if (rc) return rc;
     }
-    // leaf count and device errors in one round trip
     int* h = static_cast<int*>(ctx->pinned) + 16;
+    if (3 * ls->key_bits > 63) {  // keys too wide for the device sort: the host sorts
+        VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        rc = consume_device_errors(ctx, "vlr_ls_step_host");
+        if (rc) return rc;
+        return download_n(ctx, ls, (size_t)h[0], -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
+    }
+    float* v = (float*)ls->staging;
+    uint64_t* mm = (uint64_t*)((char*)ls->staging + kv * sizeof(float) * kLeafVoxels);
+    int32_t* o3 = (int32_t*)((char*)mm + kv * 64);
+    int* dsel = (int*)((char*)o3 + kv * 12);
+    int* dstatus = (int*)((char*)dsel + kv * 4);
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDevSortSmem));
+    const vlr::MGridParams& P = ls->h_params[0];
+    k_sort_small<<<1, 1024, kDevSortSmem, ctx->stream>>>(ls->list, ls->scalars, ls->origin, P.base[0], P.base[1],
+                                                          P.base[2], ls->key_bits, dsel, o3, dstatus);
+    const int B = ctx->sm_count * 8;
+    if (ls->precision == VLR_PREC_F16)
+        k_gather_sel_dev<__half><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, ls->scalars, dstatus, ls->mask,
+                                                             (const __half*)ls->vals[0], mm, v);
+    else
+        k_gather_sel_dev<float><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, ls->scalars, dstatus, ls->mask,
+                                                            (const float*)ls->vals[0], mm, v);
+    VLR_CUDA(ctx, cudaGetLastError());
+    // leaf count, sort status and device errors in one round trip
     VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaMemcpyAsync(h + 1, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     rc = consume_device_errors(ctx, "vlr_ls_step_host");
     if (rc) return rc;
-    return download_n(ctx, ls, (size_t)h[0], -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
+    const size_t n = (size_t)h[0];
+    if (!h[1]) return download_n(ctx, ls, n, -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
+    if (n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    if (n) {
+        if (out_origins) VLR_CUDA(ctx, cudaMemcpyAsync(out_origins, o3, 12 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        if (out_masks) VLR_CUDA(ctx, cudaMemcpyAsync(out_masks, mm, 64 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        if (out_phi)
+            VLR_CUDA(ctx, cudaMemcpyAsync(out_phi, v, sizeof(float) * kLeafVoxels * n, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    *n_out = n;
+    return VLR_OK;
 }
 
 int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,

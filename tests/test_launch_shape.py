@@ -79,13 +79,25 @@ def test_invalid_launch_shape_rejected(ctx):
     ls.close()
 
 
+def _vortex_r(precision, radius):
+    from sharc.volrus_b200.method import LevelSet
+    vs = 1 / 512
+    return LevelSet.sphere(radius, (0.5, 0.5, 0.5), vs, {"kind": "vortex", "vs": vs, "period": 3.0}, 0.5 * vs,
+                           precision=precision, integrator=2)
+
+
 @pytest.mark.parametrize("precision", [0, 1], ids=["f32", "f16"])
-def test_host_step_matches_upload_step_download(ctx, precision):
-    """vlr_ls_step_host = vlr_ls_upload + vlr_ls_step + vlr_ls_download."""
-    a = _vortex(precision, None)
+@pytest.mark.parametrize("radius", [None, 0.3], ids=["device_sort", "host_sort_over_8192_leaves"])
+def test_host_step_matches_upload_step_download(ctx, precision, radius):
+    """vlr_ls_step_host = vlr_ls_upload + vlr_ls_step + vlr_ls_download (the
+    host step orders up to 8192 leaves on the device, more on the host)."""
+    make = (lambda: _vortex(precision, None)) if radius is None else (lambda: _vortex_r(precision, radius))
+    a = make()
     a.step(2)
     state = a.arrays()
-    b = _vortex(precision, None)
+    if radius is not None:
+        assert len(state[0]) > 8192
+    b = make()
     b.step(2)
     got = b.step_host(*state, n_steps=3)
     a.upload(*state)
