@@ -661,13 +661,15 @@ def bench_mesh(args, ctx, peak, peak_kind):
     # vertices and triangles written
     algo = 2 * 1.4 * 2048 * len(tiles) + 2 * 4 * cells + 24 * nv.value + 12 * nt.value
     achieved = algo / (dev_ms * 1e-3) / 1e9
-    host = g.download()
-    ho, hm, hv = host.to_arrays()
-    og = pyoracle.OGrid.from_arrays(ho, hm, hv, host.background, host.transform.voxel_size)
-    t0 = time.perf_counter()
-    ov, ot = og.volume_to_mesh(0.0)
-    cpu_s = time.perf_counter() - t0
-    exact = bool(np.array_equal(ov.view(np.uint64), verts.view(np.uint64)) and np.array_equal(ot, tris))
+    cpu_s, exact = None, None
+    if not args.no_cpu_baseline:
+        host = g.download()
+        ho, hm, hv = host.to_arrays()
+        og = pyoracle.OGrid.from_arrays(ho, hm, hv, host.background, host.transform.voxel_size)
+        t0 = time.perf_counter()
+        ov, ot = og.volume_to_mesh(0.0)
+        cpu_s = time.perf_counter() - t0
+        exact = bool(np.array_equal(ov.view(np.uint64), verts.view(np.uint64)) and np.array_equal(ot, tris))
     return {
         "workload": f"world-unit sphere r={MESH['radius']:g} voxels, half-width {MESH['half_width']:g}, isovalue 0",
         "leaves": n_leaves, "tiles": len(tiles), "cells": cells, "vertices": nv.value, "triangles": nt.value,
@@ -677,8 +679,9 @@ def bench_mesh(args, ctx, peak, peak_kind):
         "roofline": {"bound": "hbm", "kernels": "k_mc_classify + k_mc_emit", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": algo},
         "d2h_bytes_per_call": int(verts.nbytes + tris.nbytes),
-        "cpu_baseline": {"value": cells / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
-                         "sample": "the oracle restatement of volume_to_mesh on the same grid, one call"},
+        "cpu_baseline": None if cpu_s is None else {
+            "value": cells / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+            "sample": "the oracle restatement of volume_to_mesh on the same grid, one call"},
         "matches_oracle": exact,
     }
 
@@ -693,6 +696,21 @@ def bench_adjoint_line(args, ctx):
                        "checkpoint_every": 8, "velocity": "128^3 staggered, trilinear upsample"},
             "roofline": None, "e2e": None, "clocks": clk.summary(), "gpu_launches": None,
             "kernels_ms_per_launch": {}, "adjoint": a}
+
+
+def bench_mesh_line(args, ctx, peak, peak_kind):
+    """volume_to_mesh on its own: `value` is the device rate of its two kernels,
+    `e2e` the C-ABI call with host output buffers."""
+    with ClockSampler(args.device) as clk, clk.mark():
+        m = bench_mesh(args, ctx, peak, peak_kind)
+    return {"metric": "cells/s of volume_to_mesh", "value": m["device_cells_per_s"], "unit": "cells/s",
+            "ms_per_step": m["device_ms"], "dtype": "f32 values, f64 vertices",
+            "config": {"workload": "mesh96", "active_voxels": m["cells"], "grid": m["workload"]},
+            "roofline": m["roofline"],
+            "e2e": {"value": m["value"], "unit": "cells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": m["d2h_bytes_per_call"]},
+            "clocks": clk.summary(), "gpu_launches": None, "kernels_ms_per_launch": m["kernels_ms_per_call"],
+            "volume_to_mesh": m}
 
 
 def bench_deformation(args, ctx, peak, peak_kind):
@@ -851,7 +869,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["deformation512", "batched256", "large8192", "adjoint256",
-                                           "reference-sphere128"],
+                                           "reference-sphere128", "mesh96"],
                     default="deformation512")
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--large-spheres", type=int, default=LARGE["spheres"], help="spheres of the large single grid")
@@ -881,6 +899,34 @@ def main():
     else:
         sphere, vel_world, ref_dt = REF_SPHERE, REF_VEL, 1.0
 
+    if args.impl == "reference" and args.workload == "mesh96":
+        if rank != 0:
+            return
+        # the reference's volume_to_mesh restated on the host (its data structure, one thread)
+        from oracle import pyoracle
+        og = pyoracle.OGrid.sphere(MESH["radius"], MESH["center"], MESH["voxel_size"], MESH["half_width"])
+        tiles = set()
+        for x, y, z in (og.arrays()[0] // 8).tolist():
+            for d in ((0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)):
+                tiles.add((x + d[0], y + d[1], z + d[2]))
+        cells = 512 * len(tiles)
+        for _ in range(min(args.warmup, 1)):
+            og.volume_to_mesh(0.0)
+        vals = []
+        for _ in range(min(args.steps, 5)):
+            t0 = time.perf_counter()
+            og.volume_to_mesh(0.0)
+            vals.append(cells / (time.perf_counter() - t0))
+        value = statistics.median(vals)
+        print(json.dumps({
+            "impl": "reference", "metric": "cells/s of volume_to_mesh", "value": value, "unit": "cells/s",
+            "higher_is_better": True, "n_gpus": args.gpus, "steps": len(vals), "warmup": args.warmup,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": args.workload},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": 1, "kind": "port",
+                             "sample": "oracle restatement of volume_to_mesh on the full sphere, one call per step"},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -918,6 +964,8 @@ def main():
         res = bench_adjoint_line(args, ctx)
     elif args.workload == "large8192":
         res = bench_large_line(args, ctx, peak, peak_kind)
+    elif args.workload == "mesh96":
+        res = bench_mesh_line(args, ctx, peak, peak_kind)
     else:
         res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]

@@ -116,6 +116,20 @@ int vlr_ctx_create(int device, vlr_ctx** out) {
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        // a private pool for the library's stream-ordered temporaries, keeping
+        // freed memory for reuse (the device's default pool hands it back to
+        // the driver at every synchronisation, so each call would allocate anew)
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&c->pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e == cudaSuccess) e = cudaMalloc(&c->d_errword, sizeof(unsigned) * 4);
     if (e == cudaSuccess) e = cudaMemset(c->d_errword, 0, sizeof(unsigned) * 4);
     if (e == cudaSuccess) e = cudaMallocHost(&c->pinned, 4096);
@@ -136,6 +150,7 @@ void vlr_ctx_destroy(vlr_ctx* ctx) {
     cudaFree(ctx->d_errword);
     cudaFreeHost(ctx->pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 

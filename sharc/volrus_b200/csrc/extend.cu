@@ -201,7 +201,7 @@ int vlr_extend_velocity(vlr_ctx* ctx, const vlr_grid* sdf, vlr_grid* vx, vlr_gri
     const float band = half_width * vs;
     cudaStream_t st = ctx->stream;
     uint64_t* d_imask = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&d_imask, 128ull * n + 8ull * n, st));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_imask, 128ull * n + 8ull * n, ctx->pool, st));
     uint64_t* d_bmask = d_imask + 8ull * n;
     int* d_bcount = reinterpret_cast<int*>(d_bmask + 8ull * n);
     int* d_boff = d_bcount + n;
@@ -236,7 +236,8 @@ int vlr_extend_velocity(vlr_ctx* ctx, const vlr_grid* sdf, vlr_grid* vx, vlr_gri
     if (nb > INT32_MAX / 2) return set_error(ctx, VLR_ERR_CAPACITY, "too many band voxels");
     VLR_CUDA(ctx, cudaMemcpyAsync(d_boff, boff.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
     int4 *d_dst = nullptr, *d_iface = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&d_dst, sizeof(int4) * (2 * nb + iface.size()) + sizeof(int) * (nb + 1), st));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_dst, sizeof(int4) * (2 * nb + iface.size()) + sizeof(int) * (nb + 1),
+                                          ctx->pool, st));
     int4* d_src = d_dst + nb;
     d_iface = d_src + nb;
     int* d_fb = reinterpret_cast<int*>(d_iface + iface.size());

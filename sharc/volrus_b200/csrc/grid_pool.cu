@@ -310,7 +310,7 @@ int scan_exclusive(vlr_ctx* ctx, const int* d_in, int* d_out, int n, int* d_tota
     int nb = (n + 1023) / 1024;
     int* sums = nullptr;
     int* sums_scan = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&sums, sizeof(int) * (nb + 1) * 2, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&sums, sizeof(int) * (nb + 1) * 2, ctx->pool, ctx->stream));
     sums_scan = sums + nb + 1;
     k_scan_block<<<nb, 1024, 0, ctx->stream>>>(d_in, d_out, n, sums);
     if (nb > 1) {
@@ -344,7 +344,7 @@ __global__ void k_compact_leaves(int n, const int* flags, const int* pos, const 
 int grid_compact(vlr_ctx* ctx, vlr_grid* g, const int* d_flags) {
     if (g->n == 0) return VLR_OK;
     int* pos = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&pos, sizeof(int) * (g->n + 1), ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&pos, sizeof(int) * (g->n + 1), ctx->pool, ctx->stream));
     int* d_total = pos + g->n;
     int rc = scan_exclusive(ctx, d_flags, pos, g->n, d_total);
     if (rc) return rc;

@@ -62,6 +62,9 @@ constexpr int kFaces[6][4] = {{0, 3, 2, 1}, {4, 5, 6, 7}, {0, 1, 5, 4}, {3, 7, 6
 struct McTable {
     int8_t tri[256][16];
     uint8_t ntri[256];
+    // the 3 other cells holding edge e: (dx+1) | (dy+1) << 2 | (dz+1) << 4 | e' << 8,
+    // e' the edge's index in that cell
+    int nb[12][3];
 };
 
 int edge_of(int a, int b) {
@@ -113,6 +116,38 @@ McTable derive_mc_table() {
         }
         t.ntri[cs] = (uint8_t)(n / 3);
     }
+    // an edge along axis a with lower corner L lies in the 4 cells at
+    // delta = (L_u - du) e_u + (L_w - dw) e_w, du, dw in {0, 1}; in the cell
+    // at delta its lower corner is L - delta
+    for (int e = 0; e < 12; ++e) {
+        const int a = kEdgeEnds[e][0], b = kEdgeEnds[e][1];
+        int L[3], axis = 0;
+        for (int k = 0; k < 3; ++k) {
+            L[k] = std::min(kCornerOff[a][k], kCornerOff[b][k]);
+            if (kCornerOff[a][k] != kCornerOff[b][k]) axis = k;
+        }
+        const int u = (axis + 1) % 3, w = (axis + 2) % 3;
+        int q = 0;
+        for (int du = 0; du < 2; ++du)
+            for (int dw = 0; dw < 2; ++dw) {
+                int d[3] = {0, 0, 0};
+                d[u] = L[u] - du;
+                d[w] = L[w] - dw;
+                if (d[u] == 0 && d[w] == 0) continue;
+                int M[3];
+                for (int k = 0; k < 3; ++k) M[k] = L[k] - d[k];
+                int e2 = -1;
+                for (int f = 0; f < 12 && e2 < 0; ++f) {
+                    int N[3], ax2 = 0;
+                    for (int k = 0; k < 3; ++k) {
+                        N[k] = std::min(kCornerOff[kEdgeEnds[f][0]][k], kCornerOff[kEdgeEnds[f][1]][k]);
+                        if (kCornerOff[kEdgeEnds[f][0]][k] != kCornerOff[kEdgeEnds[f][1]][k]) ax2 = k;
+                    }
+                    if (ax2 == axis && N[0] == M[0] && N[1] == M[1] && N[2] == M[2]) e2 = f;
+                }
+                t.nb[e][q++] = (d[0] + 1) | ((d[1] + 1) << 2) | ((d[2] + 1) << 4) | (e2 << 8);
+            }
+    }
     return t;
 }
 
@@ -123,6 +158,7 @@ const McTable& mc_table() {
 
 __constant__ int8_t c_mc_tri[256][16];
 __constant__ uint8_t c_mc_ntri[256];
+__constant__ int c_mc_nb[12][3];
 // corner offsets and edge endpoints for device code (same as kCornerOff, kEdgeEnds)
 __constant__ int c_corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                                    {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
@@ -143,6 +179,7 @@ int ensure_tables(vlr_ctx* ctx) {
         VLR_CUDA(ctx, cudaSetDevice(dev));
         VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_tri, t.tri, sizeof(t.tri)));
         VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_ntri, t.ntri, sizeof(t.ntri)));
+        VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_nb, t.nb, sizeof(t.nb)));
         g_mc_ready[dev] = true;
     }
     return VLR_OK;
@@ -258,24 +295,6 @@ __device__ inline void stage_tile(const GridView& g, const HashView& th, uint64_
     __syncthreads();
 }
 
-// Axis and lower-corner offset of edge e within its cell.
-__device__ inline void edge_geom(int e, int& axis, int* L) {
-    const int a = c_edge[e][0], b = c_edge[e][1];
-    for (int k = 0; k < 3; ++k) {
-        L[k] = min(c_corner[a][k], c_corner[b][k]);
-        if (c_corner[a][k] != c_corner[b][k]) axis = k;
-    }
-}
-
-__device__ inline int edge_at(int axis, const int* L) {
-    for (int e = 0; e < 12; ++e) {
-        int ax = 0, M[3];
-        edge_geom(e, ax, M);
-        if (ax == axis && M[0] == L[0] && M[1] == L[1] && M[2] == L[2]) return e;
-    }
-    return -1;
-}
-
 // Another cell holding the edge: its tile offset (-1..1 per axis) and local
 // cell coordinates; `order` compares it with the current cell in visit order
 // (negative: visited earlier).
@@ -294,6 +313,11 @@ __device__ inline CellRef cell_at(const int* loc, const int* delta) {
     return r;
 }
 
+__device__ inline CellRef loc_self(const int* loc) {
+    const int zero[3] = {0, 0, 0};
+    return cell_at(loc, zero);
+}
+
 __device__ inline int tr_index(const int* toff) { return (toff[0] + 1) * 9 + (toff[1] + 1) * 3 + (toff[2] + 1); }
 
 // lexicographic comparison of (tile offset, local cell) pairs
@@ -305,32 +329,13 @@ __device__ inline bool visited_before(const CellRef& a, const CellRef& b) {
     return false;
 }
 
-// The first processed cell (in visit order) holding edge e of the cell at
-// `loc`, and the edge's index in that cell.
-__device__ inline CellRef edge_creator(int e, const int* loc, const int* s_tr, int& e_out) {
-    int axis = 0, L[3];
-    edge_geom(e, axis, L);
-    const int u = (axis + 1) % 3, w = (axis + 2) % 3;
-    const int zero[3] = {0, 0, 0};
-    CellRef best = cell_at(loc, zero);
-    int bestL[3] = {L[0], L[1], L[2]};
-    for (int du = 0; du < 2; ++du)
-        for (int dw = 0; dw < 2; ++dw) {
-            int delta[3] = {0, 0, 0};
-            delta[u] = L[u] - du;
-            delta[w] = L[w] - dw;
-            if (delta[u] == 0 && delta[w] == 0) continue;
-            const CellRef c = cell_at(loc, delta);
-            if (s_tr[tr_index(c.toff)] < 0) continue;
-            if (visited_before(c, best)) {
-                best = c;
-                bestL[axis] = 0;
-                bestL[u] = du;
-                bestL[w] = dw;
-            }
-        }
-    e_out = edge_at(axis, bestL);
-    return best;
+// The other cell holding edge e of the cell at `loc` listed q-th in c_mc_nb,
+// and the edge's index there.
+__device__ inline CellRef edge_nb(int e, int q, const int* loc, int& e2) {
+    const int code = c_mc_nb[e][q];
+    const int delta[3] = {(code & 3) - 1, ((code >> 2) & 3) - 1, ((code >> 4) & 3) - 1};
+    e2 = code >> 8;
+    return cell_at(loc, delta);
 }
 
 // Block-wide exclusive scan of one int per thread (512 threads).
@@ -389,14 +394,20 @@ __global__ void __launch_bounds__(512) k_mc_classify(GridView g, HashView th, Ti
     const int loc[3] = {c >> 6, (c >> 3) & 7, c & 7};
     const int ci = cell_case(s_v, loc, iso);
     const unsigned fl = edge_flags(ci);
+    // this cell creates a flagged edge iff no other processed cell holding it
+    // is visited earlier
+    const int zero[3] = {0, 0, 0};
+    const CellRef self = cell_at(loc, zero);
     unsigned cm = 0;
     for (int e = 0; e < 12; ++e) {
         if (!((fl >> e) & 1u)) continue;
-        int e2 = 0;
-        const CellRef cr = edge_creator(e, loc, s_tr, e2);
-        if (cr.toff[0] == 0 && cr.toff[1] == 0 && cr.toff[2] == 0 && cr.loc[0] == loc[0] && cr.loc[1] == loc[1] &&
-            cr.loc[2] == loc[2])
-            cm |= 1u << e;
+        bool first = true;
+        for (int q = 0; q < 3 && first; ++q) {
+            int e2;
+            const CellRef c = edge_nb(e, q, loc, e2);
+            if (s_tr[tr_index(c.toff)] >= 0 && visited_before(c, self)) first = false;
+        }
+        if (first) cm |= 1u << e;
     }
     int vt = 0, tt = 0;
     const int vpre = block_scan512(__popc(cm), s_w, &vt);
@@ -449,8 +460,20 @@ __global__ void __launch_bounds__(512) k_mc_emit(GridView g, HashView th, TileBa
                 verts[(size_t)vi * 3 + k] = __dadd_rn(pa, __dmul_rn(t, __dsub_rn(pb, pa)));
             }
         } else {
+            // the creator: the earliest processed other cell holding the edge
             int e2 = -1;
-            const CellRef cr = edge_creator(e, loc, s_tr, e2);
+            CellRef cr = loc_self(loc);
+            bool have = false;
+            for (int q = 0; q < 3; ++q) {
+                int f;
+                const CellRef c = edge_nb(e, q, loc, f);
+                if (s_tr[tr_index(c.toff)] < 0) continue;
+                if (!have || visited_before(c, cr)) {
+                    cr = c;
+                    e2 = f;
+                    have = true;
+                }
+            }
             const int rank = s_tr[tr_index(cr.toff)];
             const uint32_t w2 = words[(size_t)rank * 512 + (cr.loc[0] << 6) + (cr.loc[1] << 3) + cr.loc[2]];
             const unsigned cm2 = (w2 >> 8) & 0xfffu;
@@ -485,7 +508,7 @@ int volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float iso, double* h_verts, 
     const size_t sort_bytes = sort_reduce_scratch_bytes(n7);
     char* buf = nullptr;
     const size_t cand_bytes = (size_t)n7 * (8 + 4 + 4 + 4 + 8 + 4 + 4) + sort_bytes + 256;
-    VLR_CUDA(ctx, cudaMallocAsync((void**)&buf, cand_bytes, st));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&buf, cand_bytes, ctx->pool, st));
     char* p = buf;
     uint64_t* keys = (uint64_t*)p;  p += (size_t)n7 * 8;
     uint64_t* sorted = (uint64_t*)p;  p += (size_t)n7 * 8;
@@ -527,8 +550,8 @@ int volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float iso, double* h_verts, 
     while (hcap < 2 * m) hcap <<= 1;
     char* buf2 = nullptr;
     const size_t b2 = (size_t)m * 8 + (size_t)hcap * 12 + (size_t)m * 512 * 4 + (size_t)m * 16 + 64 + 256;
-    cudaError_t ce = cudaMallocAsync((void**)&buf2, b2, st);
-    if (ce != cudaSuccess) return done(check_cuda(ctx, ce, "cudaMallocAsync(volume_to_mesh cells)"));
+    cudaError_t ce = cudaMallocFromPoolAsync((void**)&buf2, b2, ctx->pool, st);
+    if (ce != cudaSuccess) return done(check_cuda(ctx, ce, "cudaMallocFromPoolAsync(volume_to_mesh cells)"));
     auto done2 = [&](int code) {
         cudaFreeAsync(buf2, st);
         return done(code);
@@ -571,9 +594,10 @@ int volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float iso, double* h_verts, 
     if ((h_verts && cap_v) || (h_tris && cap_t)) {
         double* d_verts = nullptr;
         uint32_t* d_tris = nullptr;
-        ce = cudaMallocAsync((void**)&d_verts, (size_t)std::max<long long>(tot[0], 1) * 24, st);
-        if (ce == cudaSuccess) ce = cudaMallocAsync((void**)&d_tris, (size_t)std::max<long long>(tot[1], 1) * 12, st);
-        if (ce != cudaSuccess) return done2(check_cuda(ctx, ce, "cudaMallocAsync(volume_to_mesh output)"));
+        ce = cudaMallocFromPoolAsync((void**)&d_verts, (size_t)std::max<long long>(tot[0], 1) * 24, ctx->pool, st);
+        if (ce == cudaSuccess)
+            ce = cudaMallocFromPoolAsync((void**)&d_tris, (size_t)std::max<long long>(tot[1], 1) * 12, ctx->pool, st);
+        if (ce != cudaSuccess) return done2(check_cuda(ctx, ce, "cudaMallocFromPoolAsync(volume_to_mesh output)"));
         VLR_TIMED(ctx, "k_mc_emit",
                   k_mc_emit<<<m, 512, 0, st>>>(gv, th, tb, tiles, iso, g->xf.voxel_size, words, vbase, tbase,
                                                d_verts, d_tris));

@@ -237,7 +237,8 @@ int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origi
     if (rc) return rc;
     // new-leaf origins (int4, 16-byte aligned) first, then the destination indices
     int4* d_onew = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&d_onew, sizeof(int4) * m + sizeof(int) * (n + m), ctx->stream));
+    VLR_CUDA(ctx,
+             cudaMallocFromPoolAsync(&d_onew, sizeof(int4) * m + sizeof(int) * (n + m), ctx->pool, ctx->stream));
     int* d_idx = reinterpret_cast<int*>(d_onew + m);
     if (n)
         VLR_CUDA(ctx, cudaMemcpyAsync(d_idx, dst_old.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));

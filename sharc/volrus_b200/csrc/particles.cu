@@ -73,7 +73,7 @@ int vlr_advect_particles(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, c
     if (n == 0) return VLR_OK;
     if (n > (size_t)INT32_MAX / 3) return set_error(ctx, VLR_ERR_CAPACITY, "too many particles");
     double* d = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&d, sizeof(double) * 3 * n, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d, sizeof(double) * 3 * n, ctx->pool, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(d, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
     const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)ctx->sm_count * 16);
     k_advect_particles<<<blocks, 256, 0, ctx->stream>>>(make_view(vx), make_view(vy), make_view(vz), d, (int)n, dt,

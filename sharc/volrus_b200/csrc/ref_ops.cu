@@ -372,7 +372,7 @@ int advect_ref(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, const vlr_gr
     out->n = g->n;
     if (g->n == 0) return grid_index(ctx, out);
     int* nonempty = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&nonempty, sizeof(int) * g->n, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&nonempty, sizeof(int) * g->n, ctx->pool, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(out->origin, g->origin, sizeof(int4) * g->n, cudaMemcpyDeviceToDevice, ctx->stream));
     VLR_TIMED(ctx, "k_advect_ref",
               k_advect_ref<<<g->n, 128, 0, ctx->stream>>>(make_view(g), make_view(vx), make_view(vy), make_view(vz),
@@ -390,8 +390,8 @@ int sample_points(vlr_ctx* ctx, const vlr_grid* g, const double* h_pts, size_t n
     if (n == 0) return VLR_OK;
     double* d_pts = nullptr;
     float* d_out = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&d_pts, sizeof(double) * 3 * n, ctx->stream));
-    VLR_CUDA(ctx, cudaMallocAsync(&d_out, sizeof(float) * n, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_pts, sizeof(double) * 3 * n, ctx->pool, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_out, sizeof(float) * n, ctx->pool, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(d_pts, h_pts, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
     k_sample_points<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(make_view(g), d_pts, (int)n, d_out);
     VLR_CUDA(ctx, cudaGetLastError());
@@ -428,7 +428,7 @@ struct CrossBufs {
 static int alloc_cross(vlr_ctx* ctx, int n, CrossBufs& b) {
     size_t need = sizeof(uint64_t) * 8 * (size_t)n + sizeof(int) * (3 * (size_t)n + 8) + 64;
     char* p = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync((void**)&p, need, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&p, need, ctx->pool, ctx->stream));
     b.xmask = (uint64_t*)p;
     p += sizeof(uint64_t) * 8 * (size_t)n;
     b.total = (unsigned long long*)p;
@@ -455,7 +455,7 @@ int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size
         rc = scan_exclusive(ctx, b.xcount, b.pos, g->n, b.pos + g->n);
         if (rc) return rc;
         int* d_coords = nullptr;
-        VLR_CUDA(ctx, cudaMallocAsync(&d_coords, sizeof(int) * 3 * total, ctx->stream));
+        VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_coords, sizeof(int) * 3 * total, ctx->pool, ctx->stream));
         k_emit_crossings<<<g->n, 512, 0, ctx->stream>>>(make_view(g), b.xmask, b.pos, d_coords);
         VLR_CUDA(ctx, cudaGetLastError());
         std::vector<int32_t> all(3 * total);
@@ -477,7 +477,7 @@ int trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width) {
     float vs = (float)g->xf.voxel_size;
     float thr = half_width * vs;
     int* flags = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&flags, sizeof(int) * g->n, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&flags, sizeof(int) * g->n, ctx->pool, ctx->stream));
     GridView v = make_view(g);
     VLR_TIMED(ctx, "k_trim", k_trim<<<g->n, 256, 0, ctx->stream>>>(v, (float*)g->values, g->mask, thr, flags));
     VLR_CUDA(ctx, cudaGetLastError());
@@ -512,7 +512,7 @@ int rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width) {
         rc = scan_exclusive(ctx, b.xcount, b.pos, g->n, b.pos + g->n);
         if (rc) return rc;
         int* d_coords = nullptr;
-        VLR_CUDA(ctx, cudaMallocAsync(&d_coords, sizeof(int) * 3 * total, ctx->stream));
+        VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_coords, sizeof(int) * 3 * total, ctx->pool, ctx->stream));
         k_emit_crossings<<<g->n, 512, 0, ctx->stream>>>(v, b.xmask, b.pos, d_coords);
         k_rebuild_brute<<<g->n, 256, 0, ctx->stream>>>(v, (float*)g->values, g->mask, d_coords, (int)total, vs, band,
                                                       b.flags);
@@ -570,7 +570,7 @@ int make_sphere(vlr_ctx* ctx, double radius, const double c[3], double vs, doubl
     if (rc) return rc;
     out->n = (int)n_cand;
     int* flags = nullptr;
-    VLR_CUDA(ctx, cudaMallocAsync(&flags, sizeof(int) * n_cand, ctx->stream));
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&flags, sizeof(int) * n_cand, ctx->pool, ctx->stream));
     k_sphere<<<(unsigned)n_cand, 512, 0, ctx->stream>>>((int)lx0, (int)ly0, (int)lz0, (int)nly, (int)nlz, (int)n_cand,
                                                         imin, jmin, kmin, imax, jmax, kmax, radius, c[0], c[1], c[2],
                                                         vs, bg, out->origin, out->mask, (float*)out->values, flags);

@@ -25,6 +25,7 @@ struct vlr_ctx {
     int device = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;       // stream-ordered temporaries; freed memory stays with the pool
     unsigned* d_errword = nullptr;      // device error bits (vlr::kErr*)
     std::string last_error;
     // Scratch reused across calls on this context (grown on demand).
