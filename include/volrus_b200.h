@@ -342,6 +342,19 @@ typedef struct vlr_adjoint vlr_adjoint;
 int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
                    float half_width, const float* vel, int n_stag, double stag_cell, double dt, double period,
                    double t0, int steps, int checkpoint_every, vlr_adjoint** out);
+/* The frozen-band adjoint of a single-grid level set's own step: phi_0 is
+ * the level set's current state (band = its active voxels, values in voxel
+ * units) and each band voxel moves by the level set's backtrace displacement
+ * over one step (its integrator, dt and velocity, computed by the same device
+ * code as its advect kernel), so phi_{k+1}(x) = trilinear(phi_k)(x + d(x)).
+ * The velocity must be time-independent (constant or curl noise; the vortex
+ * is refused with VLR_ERR_UNSUPPORTED); there is no velocity input or
+ * gradient (vlr_adj_set_inputs with vel and grad_vel outputs are refused).
+ * Everything is built on the device.  No counterpart in the reference. */
+int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int checkpoint_every, vlr_adjoint** out);
+/* The per-band-voxel displacement d of a level-set adjoint (float[n_band][3],
+ * voxels). */
+int vlr_adj_displacement(vlr_ctx* ctx, const vlr_adjoint* a, float* out);
 /* Band voxel coordinates (int32[n][3]); coords may be null to query n. */
 int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap, size_t* n);
 /* Replace phi_0 on the band and/or the staggered field (either may be null). */

@@ -26,6 +26,7 @@ struct Problem {
     int n = 0;
     double H = 1.0, dt = 0.0, T = 1.0, t0 = 0.0;
     int K = 0;
+    bool disp = false;  // ub holds fixed displacements, step factor 1 (level-set adjoint)
     std::vector<std::array<double, 3>> ub;
     std::vector<std::vector<Leaf>> states;  // phi_0 .. phi_{K-1} of the last forward run
 };
@@ -77,6 +78,7 @@ void upsample(Problem& P) {
 }
 
 double step_factor(const Problem& P, int k) {
+    if (P.disp) return 1.0;
     const double pi = 3.14159265358979323846;
     return -P.dt * std::cos(pi * (P.t0 + (k + 1) * P.dt) / P.T);
 }
@@ -110,6 +112,34 @@ void* va_create(const int32_t* origins, const uint64_t* masks, const double* phi
     P->t0 = t0;
     P->K = K;
     upsample(*P);
+    return P;
+}
+
+// Displacement form (vlr_adj_create_level_set): phi_{k+1}(x) = trilinear(phi_k)(x + d(x))
+// with d given per band voxel (band order: leaf order, then ZYX).
+void* va_create_disp(const int32_t* origins, const uint64_t* masks, const double* phi, size_t n_leaves, double hw,
+                     const double* disp, int K) {
+    Problem* P = new Problem();
+    P->g.hw = hw;
+    P->g.leaves.resize(n_leaves);
+    for (size_t i = 0; i < n_leaves; ++i) {
+        Leaf& L = P->g.leaves[i];
+        std::memcpy(L.o, origins + 3 * i, 12);
+        std::memcpy(L.m, masks + 8 * i, 64);
+        std::memcpy(L.phi, phi + 512 * i, 512 * sizeof(double));
+        for (int off = 0; off < 512; ++off)
+            if (L.on(off)) {
+                P->bleaf.push_back((int)i);
+                P->boff.push_back(off);
+            }
+    }
+    P->g.reindex();
+    P->n = 0;
+    P->K = K;
+    P->disp = true;
+    P->ub.resize(P->bleaf.size());
+    for (size_t b = 0; b < P->bleaf.size(); ++b)
+        for (int a = 0; a < 3; ++a) P->ub[b][a] = disp[3 * b + a];
     return P;
 }
 
@@ -191,6 +221,7 @@ void va_backward(void* pp, const double* lamK, double* grad_phi0, double* grad_V
         lam.swap(nl);
     }
     std::memcpy(grad_phi0, lam.data(), sizeof(double) * nb);
+    if (P.disp || !grad_V) return;
     std::fill(grad_V, grad_V + P.V.size(), 0.0);
     for (size_t b = 0; b < nb; ++b) {
         const Leaf& L = P.g.leaves[P.bleaf[b]];

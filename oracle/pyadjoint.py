@@ -25,6 +25,22 @@ class AdjointOracle:
         self.nb = self.lib.va_nband(self.h)
         self.V = v.copy()
 
+    @classmethod
+    def from_displacement(cls, origins, masks, phi, half_width, disp, steps):
+        """Displacement form: phi_{k+1}(x) = trilinear(phi_k)(x + d(x)), d per band voxel."""
+        self = cls.__new__(cls)
+        self.lib = load()
+        o = np.ascontiguousarray(origins, np.int32)
+        m = np.ascontiguousarray(masks, np.uint64)
+        p = np.ascontiguousarray(phi, np.float64)
+        d = np.ascontiguousarray(disp, np.float64).reshape(-1)
+        self.n = 0
+        self.h = self.lib.va_create_disp(_p(o, C.c_int32), _p(m, C.c_uint64), _p(p, C.c_double), len(o), half_width,
+                                         _p(d, C.c_double), steps)
+        self.nb = self.lib.va_nband(self.h)
+        self.V = np.zeros(0)
+        return self
+
     def forward(self, phi0_band=None, V=None):
         out = np.zeros(self.nb)
         pb = None if phi0_band is None else np.ascontiguousarray(phi0_band, np.float64)

@@ -56,6 +56,7 @@ SIGS = {
     "va_create": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double, dbl_p, C.c_int, C.c_double, C.c_double,
                       C.c_double, C.c_double, C.c_int]),
     "va_free": (None, [P]),
+    "va_create_disp": (P, [i32_p, u64_p, dbl_p, C.c_size_t, C.c_double, dbl_p, C.c_int]),
     "va_nband": (C.c_int, [P]),
     "va_forward": (None, [P, dbl_p, dbl_p, dbl_p]),
     "va_backward": (None, [P, dbl_p, dbl_p, dbl_p]),

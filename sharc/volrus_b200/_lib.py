@@ -126,6 +126,8 @@ SIGNATURES = {
     "vlr_adj_create": (C.c_int, [P, i32_p, u64_p, flt_p, C.c_size_t, C.c_float, flt_p, C.c_int, C.c_double,
                                  C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, PP]),
     "vlr_adj_band": (C.c_int, [P, P, i32_p, C.c_size_t, size_p]),
+    "vlr_adj_create_level_set": (C.c_int, [P, P, C.c_int, C.c_int, PP]),
+    "vlr_adj_displacement": (C.c_int, [P, P, flt_p]),
     "vlr_adj_set_inputs": (C.c_int, [P, P, flt_p, flt_p]),
     "vlr_adj_forward": (C.c_int, [P, P, flt_p]),
     "vlr_adj_backward": (C.c_int, [P, P, flt_p, flt_p, flt_p]),

@@ -62,6 +62,31 @@ class AdvectionFunction:
         self.ctx.check(self.ctx.lib.vlr_adj_band(self.ctx.handle, h, None, 0, C.byref(nb)), "vlr_adj_band")
         self.n_band = nb.value
 
+    @classmethod
+    def from_level_set(cls, ls, steps: int, checkpoint_every: int):
+        """The frozen-band adjoint of a single-grid level set's own step
+        (``vlr_adj_create_level_set``): phi_0 is its current state and every
+        band voxel moves by its fixed backtrace displacement per step.  There
+        is no velocity input, and ``backward`` returns (dL/dphi_0, None)."""
+        self = cls.__new__(cls)
+        self.ctx = ls.ctx
+        self.n = 0
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.vlr_adj_create_level_set(self.ctx.handle, ls.handle, steps, checkpoint_every,
+                                                             C.byref(h)), "vlr_adj_create_level_set")
+        self.handle = h
+        nb = C.c_size_t()
+        self.ctx.check(self.ctx.lib.vlr_adj_band(self.ctx.handle, h, None, 0, C.byref(nb)), "vlr_adj_band")
+        self.n_band = nb.value
+        return self
+
+    def displacement(self) -> np.ndarray:
+        """(n_band, 3) backtrace displacement of a level-set adjoint, voxels."""
+        d = np.zeros((self.n_band, 3), np.float32)
+        self.ctx.check(self.ctx.lib.vlr_adj_displacement(self.ctx.handle, self.handle, ptr(d, C.c_float)),
+                       "vlr_adj_displacement")
+        return d
+
     def band(self) -> np.ndarray:
         c = np.zeros((self.n_band, 3), np.int32)
         nb = C.c_size_t()
@@ -85,9 +110,10 @@ class AdvectionFunction:
     def backward(self, grad_phik):
         g = np.ascontiguousarray(grad_phik, np.float32)
         g0 = np.zeros(self.n_band, np.float32)
-        gv = np.zeros((3, self.n, self.n, self.n), np.float32)
+        gv = np.zeros((3, self.n, self.n, self.n), np.float32) if self.n else None
         self.ctx.check(self.ctx.lib.vlr_adj_backward(self.ctx.handle, self.handle, ptr(g, C.c_float),
-                                                     ptr(g0, C.c_float), ptr(gv, C.c_float)), "vlr_adj_backward")
+                                                     ptr(g0, C.c_float), None if gv is None else ptr(gv, C.c_float)),
+                       "vlr_adj_backward")
         return g0, gv
 
     def forward_device(self, phik_ptr: int = 0):

@@ -59,6 +59,8 @@ struct vlr_adjoint {
     float* gvel = nullptr;               // dL/dV, 3 x n^3
     float3* G = nullptr;
     int reach = 1;                       // displacement bound per step, voxels (ceil of dt max|V|)
+    int disp = 0;                        // 1: ub holds each band voxel's fixed backtrace displacement
+                                         // (a level set's time-independent velocity), step factor 1
     unsigned* foot_pk = nullptr;         // per pool voxel: packed foot offsets of band voxels, 0 elsewhere
     float4* foot_w = nullptr;            // per pool voxel: (wx, wy, wz, lambda) of band voxels
     unsigned* keys = nullptr;
@@ -379,6 +381,7 @@ int reach_of(const float* vel, size_t nvel, double dt) {
 }
 
 float step_factor(const vlr_adjoint* a, int k) {
+    if (a->disp) return 1.0f;  // the displacement already holds -dt and the integrator
     // s_k = -dt cos(pi t_{k+1} / T)
     const double pi = 3.14159265358979323846;
     double t1 = a->t0 + (double)(k + 1) * a->dt;
@@ -497,9 +500,168 @@ int run_captured(vlr_ctx* ctx, cudaGraphExec_t* exec, F&& enqueue) {
     return VLR_OK;
 }
 
+// Level-set adjoint setup, leaves in list order: origins, phi_0 in f32 voxel
+// units and the band (active voxel) count of each leaf.
+template <typename T>
+__global__ void k_adjls_gather(const int* __restrict__ list, int n, const int4* __restrict__ ls_origin,
+                               const uint64_t* __restrict__ mask, const T* __restrict__ vals, int4* __restrict__ origin,
+                               float* __restrict__ phi, int* __restrict__ cnt) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int s = list[i];
+        if (threadIdx.x == 0) origin[i] = ls_origin[s];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            phi[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
+        if (threadIdx.x < 32) {
+            int c = threadIdx.x < 8 ? __popcll(mask[(size_t)s * 8 + threadIdx.x]) : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (threadIdx.x == 0) cnt[i] = c;
+        }
+    }
+}
+
+// Band indices: leaf i's active voxels take pos[i], pos[i] + 1, ... in ZYX order.
+__global__ void __launch_bounds__(512) k_adjls_band(const int* __restrict__ list, int n,
+                                                   const uint64_t* __restrict__ mask, const int* __restrict__ pos,
+                                                   int* __restrict__ bidx, int* __restrict__ bvox) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int s = list[i];
+        const int t = threadIdx.x, w = t >> 6;
+        const uint64_t word = mask[(size_t)s * 8 + w];
+        int before = __popcll(word & ((1ull << (t & 63)) - 1ull));
+        for (int q = 0; q < w; ++q) before += __popcll(mask[(size_t)s * 8 + q]);
+        const size_t v = (size_t)i * kLeafVoxels + t;
+        if ((word >> (t & 63)) & 1ull) {
+            const int b = pos[i] + before;
+            bidx[v] = b;
+            bvox[b] = (int)v;
+        } else {
+            bidx[v] = -1;
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int checkpoint_every, vlr_adjoint** out) {
+    if (!ctx || !ls || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (steps < 1 || checkpoint_every < 1) return set_error(ctx, VLR_ERR_INVALID, "bad adjoint parameters");
+    if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "level-set adjoint of a single grid only");
+    if (ls->vel_kind != MVEL_CONSTANT && ls->vel_kind != MVEL_CURL)
+        return set_error(ctx, VLR_ERR_UNSUPPORTED,
+                         "level-set adjoint needs a time-independent velocity (constant or curl noise)");
+    if (ls->key_bits > kKeyBits) return set_error(ctx, VLR_ERR_EXTENT, "grid too wide for the adjoint's hash");
+    *out = nullptr;
+    cudaStream_t st = ctx->stream;
+    int n = 0;
+    int rc = read_int(ctx, ls->scalars, &n);
+    if (rc) return rc;
+    if (n <= 0) return set_error(ctx, VLR_ERR_INVALID, "empty level set");
+    if ((long long)n * kLeafVoxels >= (1ll << 31)) return set_error(ctx, VLR_ERR_CAPACITY, "too many leaves");
+    const vlr::MGridParams& P = ls->h_params[0];
+    vlr_adjoint* a = new vlr_adjoint();
+    a->ctx = ctx;
+    a->n_leaves = n;
+    a->hw = P.hw;
+    a->dt = ls->sp.dt;
+    a->t0 = ls->sp.t0;
+    a->period = 1.0;
+    a->steps = steps;
+    a->chk_every = checkpoint_every;
+    a->disp = 1;
+    for (int k = 0; k < 3; ++k) a->base[k] = P.base[k];
+    auto fail = [&](int code) {
+        adj_free(a);
+        delete a;
+        return code;
+    };
+    const size_t pool = (size_t)n * kLeafVoxels;
+    int* cnt = nullptr;  // n + 1 counts, then n + 1 positions
+#define ADJ_MALLOC(p, bytes) \
+    do { cudaError_t e_ = cudaMalloc(&(p), (bytes)); if (e_ != cudaSuccess) return fail(check_cuda(ctx, e_, "cudaMalloc")); } while (0)
+    ADJ_MALLOC(a->origin, sizeof(int4) * n);
+    ADJ_MALLOC(a->phi_init, sizeof(float) * pool);
+    ADJ_MALLOC(a->bidx, sizeof(int) * pool);
+    ADJ_MALLOC(cnt, sizeof(int) * (2 * (size_t)n + 4));
+    int* pos = cnt + n + 2;
+    const int gb = (int)std::min<long long>(n, (long long)ctx->sm_count * 8);
+    if (ls->precision == VLR_PREC_F16)
+        k_adjls_gather<__half><<<gb, 256, 0, st>>>(ls->list, n, ls->origin, ls->mask, (const __half*)ls->vals[0],
+                                                  a->origin, a->phi_init, cnt);
+    else
+        k_adjls_gather<float><<<gb, 256, 0, st>>>(ls->list, n, ls->origin, ls->mask, (const float*)ls->vals[0],
+                                                 a->origin, a->phi_init, cnt);
+    rc = scan_exclusive(ctx, cnt, pos, n, pos + n);
+    if (rc) {
+        cudaFree(cnt);
+        return fail(rc);
+    }
+    int nb = 0;
+    rc = read_int(ctx, pos + n, &nb);
+    if (rc || nb <= 0) {
+        cudaFree(cnt);
+        return fail(rc ? rc : set_error(ctx, VLR_ERR_INVALID, "empty band"));
+    }
+    a->n_band = nb;
+    const int n_chk = steps / checkpoint_every + 1;
+    a->hcap = 64;
+    while ((size_t)a->hcap < 2 * (size_t)n) a->hcap <<= 1;
+    ADJ_MALLOC(a->bvox, sizeof(int) * nb);
+    ADJ_MALLOC(a->nbr, sizeof(int) * kNbr * (size_t)n);
+    ADJ_MALLOC(a->hkey, sizeof(uint64_t) * a->hcap);
+    ADJ_MALLOC(a->hval, sizeof(int) * a->hcap);
+    ADJ_MALLOC(a->phi[0], sizeof(float) * pool);
+    ADJ_MALLOC(a->phi[1], sizeof(float) * pool);
+    ADJ_MALLOC(a->ub, sizeof(float3) * nb);
+    ADJ_MALLOC(a->checkpoints, sizeof(float) * (size_t)nb * n_chk);
+    ADJ_MALLOC(a->segment, sizeof(float) * (size_t)nb * checkpoint_every);
+    ADJ_MALLOC(a->lam[0], sizeof(float) * nb);
+    ADJ_MALLOC(a->lam[1], sizeof(float) * nb);
+    ADJ_MALLOC(a->G, sizeof(float3) * nb);
+    ADJ_MALLOC(a->foot_pk, sizeof(unsigned) * pool);
+    ADJ_MALLOC(a->foot_w, sizeof(float4) * pool);
+#undef ADJ_MALLOC
+    VLR_CUDA(ctx, cudaMemsetAsync(a->foot_pk, 0, sizeof(unsigned) * pool, st));
+    VLR_CUDA(ctx, cudaMemsetAsync(a->hkey, 0xFF, sizeof(uint64_t) * a->hcap, st));  // kEmptyKey
+    k_adjls_band<<<gb, 512, 0, st>>>(ls->list, n, ls->mask, pos, a->bidx, a->bvox);
+    k_adj_hash_insert<<<(n + 255) / 256, 256, 0, st>>>(a->origin, n, a->hkey, a->hval, a->hcap, a->base[0], a->base[1],
+                                                       a->base[2], ctx->d_errword);
+    k_adj_nbr<<<(int)(((size_t)n * kNbr + 255) / 256), 256, 0, st>>>(a->origin, n, a->hkey, a->hval, a->hcap,
+                                                                      a->base[0], a->base[1], a->base[2], a->nbr);
+    unsigned* d_max = reinterpret_cast<unsigned*>(cnt);  // the counts are consumed
+    VLR_CUDA(ctx, cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
+    if (ls->vel_kind == MVEL_CURL)
+        k_m_feet<MVEL_CURL><<<gb, 128, 0, st>>>(a->origin, n, a->bidx, ls->d_params, ls->d_tab, (float)ls->sp.dt,
+                                                ls->sp.integrator, a->ub, d_max, ctx->d_errword);
+    else
+        k_m_feet<MVEL_CONSTANT><<<gb, 128, 0, st>>>(a->origin, n, a->bidx, ls->d_params, ls->d_tab,
+                                                    (float)ls->sp.dt, ls->sp.integrator, a->ub, d_max,
+                                                    ctx->d_errword);
+    VLR_CUDA(ctx, cudaGetLastError());
+    unsigned mbits = 0;
+    VLR_CUDA(ctx, cudaMemcpyAsync(&mbits, d_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(cnt);
+    if (e != cudaSuccess) return fail(check_cuda(ctx, e, "level-set adjoint setup"));
+    rc = consume_device_errors(ctx, "vlr_adj_create_level_set");
+    if (rc) return fail(rc);
+    float mx;
+    std::memcpy(&mx, &mbits, sizeof(mx));
+    a->reach = std::max(1, (int)std::ceil((double)mx * (1.0 + 1e-6)));
+    if (a->reach > 6) return fail(set_error(ctx, VLR_ERR_REACH, "backtrace displacement exceeds 6 voxels per step"));
+    *out = a;
+    return VLR_OK;
+}
+
+int vlr_adj_displacement(vlr_ctx* ctx, const vlr_adjoint* a, float* out) {
+    if (!ctx || !a || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (!a->disp) return set_error(ctx, VLR_ERR_UNSUPPORTED, "not a level-set adjoint");
+    VLR_CUDA(ctx, cudaMemcpyAsync(out, a->ub, sizeof(float3) * a->n_band, cudaMemcpyDeviceToHost, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
 
 int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, const float* phi, size_t n_leaves,
                    float half_width, const float* vel, int n_stag, double stag_cell, double dt, double period,
@@ -616,6 +778,7 @@ int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap
 
 int vlr_adj_set_inputs(vlr_ctx* ctx, vlr_adjoint* a, const float* phi0_band, const float* vel) {
     if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (vel && a->disp) return set_error(ctx, VLR_ERR_UNSUPPORTED, "a level-set adjoint has no velocity field input");
     cudaStream_t st = ctx->stream;
     if (phi0_band) {
         VLR_CUDA(ctx, cudaMemcpyAsync(a->lam[1], phi0_band, sizeof(float) * a->n_band, cudaMemcpyHostToDevice, st));
@@ -663,6 +826,7 @@ int vlr_adj_forward(vlr_ctx* ctx, vlr_adjoint* a, float* phi_k_band) {
 int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_phik_band, float* d_grad_phi0_band,
                             float* d_grad_vel) {
     if (!ctx || !a || !d_grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (d_grad_vel && a->disp) return set_error(ctx, VLR_ERR_UNSUPPORTED, "a level-set adjoint has no velocity gradient");
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
     if (d_grad_phik_band != a->lam[1])
@@ -688,6 +852,7 @@ int vlr_adj_backward_device(vlr_ctx* ctx, vlr_adjoint* a, const float* d_grad_ph
 int vlr_adj_backward(vlr_ctx* ctx, vlr_adjoint* a, const float* grad_phik_band, float* grad_phi0_band,
                      float* grad_vel) {
     if (!ctx || !a || !grad_phik_band) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (grad_vel && a->disp) return set_error(ctx, VLR_ERR_UNSUPPORTED, "a level-set adjoint has no velocity gradient");
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
     VLR_CUDA(ctx, cudaMemcpyAsync(a->lam[1], grad_phik_band, sizeof(float) * nb, cudaMemcpyHostToDevice, st));

@@ -61,6 +61,15 @@ template <typename T, int NIT, int NT, int ST>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, MTopo topo, int mode, unsigned* __restrict__ err,
                            const __grid_constant__ StageMaps maps);
+// Backtrace displacement (voxels) of the voxels of n leaves with bidx >= 0
+// over one step of a time-independent velocity (VK = MVEL_CONSTANT or
+// MVEL_CURL), k_m_advect's arithmetic; *maxabs collects the largest component
+// magnitude (float bits).  128 threads per CTA.
+template <int VK>
+__global__ void k_m_feet(const int4* __restrict__ origin, int n, const int* __restrict__ bidx,
+                         const MGridParams* __restrict__ params, const float2* __restrict__ tab, float dt,
+                         int integrator, float3* __restrict__ disp, unsigned* __restrict__ maxabs,
+                         unsigned* __restrict__ err);
 template <typename T>
 __global__ void k_m_volume(MLeafArrays A, const T* __restrict__ vals, const MGridParams* __restrict__ params,
                            double r0, double r1, double r2, double* __restrict__ partial);

@@ -592,6 +592,37 @@ __device__ __forceinline__ float3 leaf_velocity(const VelConst& V, const float2 
     return u;
 }
 
+// Backtrace displacement (voxels) of local voxel (x, y, z) over one step:
+// Euler (integrator 1), RK2 midpoint (2) or SSP-RK3 (3), velocities from the
+// leaf's staged sin/cos tables at the stage times' cosine factors.
+template <int VK, bool FULL>
+__device__ __forceinline__ float3 backtrace(const VelConst& V, const float2 (*s_tab)[3][8], int x, int y, int z,
+                                            float dt, int integrator, float ct1, float ct2, float ct3) {
+    float fx, fy, fz;
+    const float3 k1 = leaf_velocity<VK, false, FULL>(V, s_tab, x, y, z, 0.f, 0.f, 0.f, ct1);
+    if (integrator == 1) {
+        fx = -dt * k1.x;
+        fy = -dt * k1.y;
+        fz = -dt * k1.z;
+    } else if (integrator == 2) {
+        const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, -0.5f * dt * k1.x, -0.5f * dt * k1.y,
+                                                        -0.5f * dt * k1.z, ct2);
+        fx = -dt * k2.x;
+        fy = -dt * k2.y;
+        fz = -dt * k2.z;
+    } else {
+        const float h = -dt;
+        const float ax = h * k1.x, ay = h * k1.y, az = h * k1.z;
+        const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, ax, ay, az, ct3);
+        const float bx = 0.25f * (ax + h * k2.x), by = 0.25f * (ay + h * k2.y), bz = 0.25f * (az + h * k2.z);
+        const float3 k3 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, bx, by, bz, ct2);
+        fx = (2.0f / 3.0f) * (bx + h * k3.x);
+        fy = (2.0f / 3.0f) * (by + h * k3.y);
+        fz = (2.0f / 3.0f) * (bz + h * k3.z);
+    }
+    return make_float3(fx, fy, fz);
+}
+
 // Backtrace and trilinear sample of the compacted voxels of D; each result is
 // stored straight to the leaf's values in global memory.
 template <typename T, int VK, bool FULL, int H, int NT>
@@ -602,28 +633,8 @@ __device__ __forceinline__ void advect_voxels(const VelConst& V, const float2 (*
     for (int i = threadIdx.x; i < nD; i += NT) {
         const int off = s_list[i];
         const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
-        float fx, fy, fz;
-        const float3 k1 = leaf_velocity<VK, false, FULL>(V, s_tab, x, y, z, 0.f, 0.f, 0.f, ct1);
-        if (integrator == 1) {
-            fx = -dt * k1.x;
-            fy = -dt * k1.y;
-            fz = -dt * k1.z;
-        } else if (integrator == 2) {
-            const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, -0.5f * dt * k1.x, -0.5f * dt * k1.y,
-                                                            -0.5f * dt * k1.z, ct2);
-            fx = -dt * k2.x;
-            fy = -dt * k2.y;
-            fz = -dt * k2.z;
-        } else {
-            const float h = -dt;
-            const float ax = h * k1.x, ay = h * k1.y, az = h * k1.z;
-            const float3 k2 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, ax, ay, az, ct3);
-            const float bx = 0.25f * (ax + h * k2.x), by = 0.25f * (ay + h * k2.y), bz = 0.25f * (az + h * k2.z);
-            const float3 k3 = leaf_velocity<VK, true, FULL>(V, s_tab, x, y, z, bx, by, bz, ct2);
-            fx = (2.0f / 3.0f) * (bx + h * k3.x);
-            fy = (2.0f / 3.0f) * (by + h * k3.y);
-            fz = (2.0f / 3.0f) * (bz + h * k3.z);
-        }
+        const float3 f = backtrace<VK, FULL>(V, s_tab, x, y, z, dt, integrator, ct1, ct2, ct3);
+        const float fx = f.x, fy = f.y, fz = f.z;
         const float px = (float)(x + H) + fx, py = (float)(y + H) + fy, pz = (float)(z + H) + fz;
         const float bxf = floorf(px), byf = floorf(py), bzf = floorf(pz);
         float wx = px - bxf, wy = py - byf, wz = pz - bzf;
@@ -1153,6 +1164,73 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         slot_n = slot_nn;
     }
 }
+
+// --------------------------------------------------------------- feet
+
+// Backtrace displacement of every voxel of n leaves (origins as a level set
+// holds them: x, y, z, grid id) over one step of a time-independent velocity
+// (constant or curl noise), with k_m_advect's arithmetic (same tables, series
+// rotations and integrator): written to disp[bidx[leaf * 512 + voxel]] for
+// voxels with bidx >= 0; the largest component magnitude is folded into
+// *maxabs (float bits of a non-negative value, atomicMax).  Used by the
+// frozen-band adjoint of a level set.
+template <int VK>
+__global__ void __launch_bounds__(128) k_m_feet(const int4* __restrict__ origin, int n, const int* __restrict__ bidx,
+                                               const MGridParams* __restrict__ params, const float2* __restrict__ tab,
+                                               float dt, int integrator, float3* __restrict__ disp,
+                                               unsigned* __restrict__ maxabs, unsigned* __restrict__ err) {
+    constexpr int NTAB = kMaxOctaves * 3 * 8;
+    static_assert(NTAB <= 128, "one table entry per thread");
+    __shared__ __align__(16) MGridParams s_P;
+    __shared__ float2 s_tab[kMaxOctaves][3][8];
+    unsigned bad = 0;
+    float m = 0.f;
+    int cur = -1;
+    for (int li = blockIdx.x; li < n; li += gridDim.x) {
+        const int4 o = origin[li];
+        __syncthreads();  // the previous leaf's table reads are done
+        if (o.w != cur) {
+            load_params(params, o.w, &s_P);
+            __syncthreads();
+            cur = o.w;
+        }
+        const VelConst V = vel_const(s_P);
+        if (threadIdx.x < NTAB) {
+            const int q = threadIdx.x;
+            const int f = q / 24, a = (q / 8) % 3, l = q % 8;
+            if (V.kind != MVEL_CONSTANT && (V.kind == MVEL_CURL ? f < V.octaves : f == 0)) {
+                int oc = (a == 0 ? o.x : (a == 1 ? o.y : o.z)) + l - s_P.tab_lo[a];
+                if (oc < 0 || oc >= s_P.tab_len[a]) {
+                    bad = 1u;
+                    oc = min(max(oc, 0), s_P.tab_len[a] - 1);
+                }
+                (&s_tab[0][0][0])[q] = __ldg(&tab[s_P.tab_off[f][a] + oc]);
+            }
+        }
+        __syncthreads();
+        const bool full = s_P.full_series != 0;
+        for (int off = threadIdx.x; off < kLeafVoxels; off += 128) {
+            const int b = bidx[(size_t)li * kLeafVoxels + off];
+            if (b < 0) continue;
+            const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
+            const float3 f = full ? backtrace<VK, true>(V, s_tab, x, y, z, dt, integrator, 1.f, 1.f, 1.f)
+                                  : backtrace<VK, false>(V, s_tab, x, y, z, dt, integrator, 1.f, 1.f, 1.f);
+            disp[b] = f;
+            const float fm = fmaxf(fabsf(f.x), fmaxf(fabsf(f.y), fabsf(f.z)));
+            if (!(fm == fm)) bad = 1u;
+            else m = fmaxf(m, fm);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxabs, __float_as_uint(m));
+    if (bad) atomicOr(err, kErrReach);
+}
+
+template __global__ void k_m_feet<MVEL_CONSTANT>(const int4*, int, const int*, const MGridParams*, const float2*, float,
+                                                 int, float3*, unsigned*, unsigned*);
+template __global__ void k_m_feet<MVEL_CURL>(const int4*, int, const int*, const MGridParams*, const float2*, float,
+                                             int, float3*, unsigned*, unsigned*);
 
 #define VLR_ADVECT_ARGS(T)                                                                       \
     MLeafArrays, const T*, T*, const MGridParams*, const float2*, MStepParams, MTopo, unsigned*, \
