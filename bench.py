@@ -570,6 +570,53 @@ def large_grid(n_spheres: int, seed: int):
     return sph, vel
 
 
+def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
+    """Frozen-band adjoint of a level set's own step (vlr_adj_create_level_set):
+    K = steps, checkpoints every chk (~sqrt K), L = sum over the band of
+    (phi_K - phi_0(x - shift))^2; forward_device + backward_device timed with
+    CUDA events on the library stream.  Rate = band voxels x K / (forward +
+    backward)."""
+    import torch
+    from sharc.volrus_b200.adjoint import AdvectionFunction
+    free0 = torch.cuda.mem_get_info()[0]
+    t0 = time.perf_counter()
+    fn = AdvectionFunction.from_level_set(ls, steps, chk)
+    create_s = time.perf_counter() - t0
+    nb = fn.n_band
+    dev = torch.device("cuda", args.device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    d_phik, d_lam, d_g0, d_target = (torch.empty(nb, dtype=torch.float32, device=dev) for _ in range(4))
+    held = (free0 - torch.cuda.mem_get_info()[0]) / 2**30
+    with torch.cuda.stream(stream):
+        fn.shifted_phi0_device(shift, d_target.data_ptr())
+    fw, bw = [], []
+    for k in range(1 + 2):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        with torch.cuda.stream(stream):
+            e[0].record(stream)
+            fn.forward_device(d_phik.data_ptr())
+            e[1].record(stream)
+            torch.sub(d_phik, d_target, out=d_lam)
+            d_lam.mul_(2.0)
+            fn.backward_device(d_lam.data_ptr(), d_g0.data_ptr(), 0)
+            e[2].record(stream)
+        ctx.check_device()
+        if k >= 1:
+            fw.append(e[0].elapsed_time(e[1]))
+            bw.append(e[1].elapsed_time(e[2]))
+    loss = float(((d_phik - d_target) ** 2).sum().item())
+    gnorm = float(d_g0.norm().item())
+    fn.close()
+    f, b = statistics.median(fw), statistics.median(bw)
+    return {"workload": f"level-set adjoint, K={steps}, checkpoint every {chk}, L2 loss against phi_0 shifted by "
+                        f"{list(shift)} voxels, FP32 band values",
+            "band_voxels": nb, "forward_ms": f, "backward_ms": b, "create_s": create_s,
+            "device_gib_held": held, "loss": loss, "grad_norm": gnorm,
+            "value": nb * steps / ((f + b) * 1e-3), "unit": "band voxel-steps/s (forward + backward)",
+            "forward_voxels_per_s": nb * steps / (f * 1e-3),
+            "timing": "device buffers, CUDA events on the library stream (forward_device + backward_device)"}
+
+
 def bench_large_line(args, ctx, peak, peak_kind):
     """The large single grid: FP16 line with FP32 beside it."""
     import torch
@@ -590,6 +637,8 @@ def bench_large_line(args, ctx, peak, peak_kind):
                          "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"],
                          "launch_shape": r["launch"], "create_s": build_s,
                          "roofline": roofline_of(r, nb, peak, peak_kind, "large8192")}
+            if prec == F16 and not args.no_adjoint:
+                out["adjoint"] = bench_level_set_adjoint(args, ctx, ls)
             ls.close()
     f = out["f16"]
     return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
@@ -601,7 +650,8 @@ def bench_large_line(args, ctx, peak, peak_kind):
                        "l2": "inputs larger than L2 and flushed between steps"},
             "fp32": out["f32"], "fp16_over_fp32": f["value"] / out["f32"]["value"], "roofline": f["roofline"],
             "kernels_ms_per_launch": f["kernels_ms_per_launch"], "launch_shape": f["launch_shape"], "e2e": None,
-            "clocks": clk.summary(), "gpu_launches": len(STEP_KERNELS) * min(args.steps, 5)}
+            "clocks": clk.summary(), "gpu_launches": len(STEP_KERNELS) * min(args.steps, 5),
+            "adjoint": out.get("adjoint")}
 
 
 MESH = dict(radius=96.0, center=(0.5, -0.25, 0.125), voxel_size=1.0, half_width=3.0)

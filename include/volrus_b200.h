@@ -355,6 +355,10 @@ int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int che
 /* The per-band-voxel displacement d of a level-set adjoint (float[n_band][3],
  * voxels). */
 int vlr_adj_displacement(vlr_ctx* ctx, const vlr_adjoint* a, float* out);
+/* phi_0 translated by (sx, sy, sz) voxels (each within +-8), read on the band:
+ * d_out[b] = phi_0(x_b - s), device buffer of n_band floats, enqueued on the
+ * context stream (the target of an L2 loss against a translated copy). */
+int vlr_adj_shifted_phi0(vlr_ctx* ctx, const vlr_adjoint* a, int sx, int sy, int sz, float* d_out);
 /* Band voxel coordinates (int32[n][3]); coords may be null to query n. */
 int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap, size_t* n);
 /* Replace phi_0 on the band and/or the staggered field (either may be null). */

@@ -80,6 +80,12 @@ class AdvectionFunction:
         self.n_band = nb.value
         return self
 
+    def shifted_phi0_device(self, shift, out_ptr: int):
+        """phi_0 translated by `shift` voxels (each within +-8), read on the band,
+        into a device buffer of n_band floats (enqueued, no wait)."""
+        self.ctx.check(self.ctx.lib.vlr_adj_shifted_phi0(self.ctx.handle, self.handle, int(shift[0]), int(shift[1]),
+                                                         int(shift[2]), out_ptr), "vlr_adj_shifted_phi0")
+
     def displacement(self) -> np.ndarray:
         """(n_band, 3) backtrace displacement of a level-set adjoint, voxels."""
         d = np.zeros((self.n_band, 3), np.float32)

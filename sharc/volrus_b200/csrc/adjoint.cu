@@ -520,6 +520,16 @@ __global__ void k_adjls_gather(const int* __restrict__ list, int n, const int4* 
     }
 }
 
+// out[b] = phi_0 at band voxel b's coordinate minus (sx, sy, sz), |s| <= 8,
+// read with the adjoint's rule for missing leaves.
+__global__ void k_adj_shifted(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
+                              const float* __restrict__ phi, int sx, int sy, int sz, float hw, float* __restrict__ out) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
+        out[b] = adj_read(phi, nbr, slot, (off >> 6) - sx, ((off >> 3) & 7) - sy, (off & 7) - sz, hw);
+    }
+}
+
 // Band indices: leaf i's active voxels take pos[i], pos[i] + 1, ... in ZYX order.
 __global__ void __launch_bounds__(512) k_adjls_band(const int* __restrict__ list, int n,
                                                    const uint64_t* __restrict__ mask, const int* __restrict__ pos,
@@ -652,6 +662,16 @@ int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int che
     a->reach = std::max(1, (int)std::ceil((double)mx * (1.0 + 1e-6)));
     if (a->reach > 6) return fail(set_error(ctx, VLR_ERR_REACH, "backtrace displacement exceeds 6 voxels per step"));
     *out = a;
+    return VLR_OK;
+}
+
+int vlr_adj_shifted_phi0(vlr_ctx* ctx, const vlr_adjoint* a, int sx, int sy, int sz, float* d_out) {
+    if (!ctx || !a || !d_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (sx < -8 || sx > 8 || sy < -8 || sy > 8 || sz < -8 || sz > 8)
+        return set_error(ctx, VLR_ERR_INVALID, "shift beyond 8 voxels");
+    k_adj_shifted<<<blocks_for(ctx, a->n_band), 256, 0, ctx->stream>>>(a->bvox, a->n_band, a->nbr, a->phi_init, sx,
+                                                                        sy, sz, a->hw, d_out);
+    VLR_CUDA(ctx, cudaGetLastError());
     return VLR_OK;
 }
 

@@ -108,6 +108,37 @@ def test_level_set_adjoint_matches_fp64(ctx, precision):
     ls.close()
 
 
+def test_shifted_phi0_target(ctx):
+    """vlr_adj_shifted_phi0 = phi_0(x - s) on the band, missing leaves read as
+    copysign(hw, the clamped position's value in the voxel's own leaf)."""
+    import torch
+    from sharc.volrus_b200.adjoint import AdvectionFunction
+    ls, _ = _level_set(0)
+    o, m, phi = ls.arrays()
+    fn = AdvectionFunction.from_level_set(ls, 2, 1)
+    coords = fn.band()
+    shift = (4, -1, 2)
+    out = torch.empty(fn.n_band, dtype=torch.float32, device="cuda")
+    fn.shifted_phi0_device(shift, out.data_ptr())
+    ls.ctx.synchronize()
+    got = out.cpu().numpy()
+    leaf = {tuple(int(v) for v in oo): i for i, oo in enumerate(o)}
+    for b in np.random.default_rng(7).choice(len(coords), 200, replace=False):
+        x, y, z = (int(c) for c in coords[b])
+        q = (x - shift[0], y - shift[1], z - shift[2])
+        key = tuple(c & ~7 for c in q)
+        if key in leaf:
+            want = phi[leaf[key], ((q[0] & 7) << 6) | ((q[1] & 7) << 3) | (q[2] & 7)]
+        else:
+            own = leaf[tuple(c & ~7 for c in (x, y, z))]
+            lo = [c & ~7 for c in (x, y, z)]
+            cl = [min(max(qq - l, 0), 7) for qq, l in zip(q, lo)]
+            want = np.copysign(np.float32(3.0), phi[own, (cl[0] << 6) | (cl[1] << 3) | cl[2]])
+        assert got[b] == want, (b, got[b], want)
+    fn.close()
+    ls.close()
+
+
 def test_level_set_adjoint_refuses_time_dependent_velocity(ctx):
     from sharc.volrus_b200._lib import VolrusError
     from sharc.volrus_b200.adjoint import AdvectionFunction
