@@ -529,13 +529,24 @@ def bench_adjoint(args, ctx):
         if k >= args.warmup:
             fw.append(e[0].elapsed_time(e[1]))
             bw.append(e[1].elapsed_time(e[2]))
-    # host-resident passes through the C ABI (inputs and outputs in host memory)
-    hw_, t0 = [], time.perf_counter()
-    for k in range(3):
+    # host-resident passes through the C ABI: inputs and outputs in pinned host
+    # buffers allocated once (phi_K out, dL/dphi_K in, dL/dphi_0 and dL/dV out)
+    import ctypes as C
+    from sharc.volrus_b200._lib import ptr
+    h_phik = torch.empty(fn.n_band, dtype=torch.float32).pin_memory().numpy()
+    h_lam = torch.empty(fn.n_band, dtype=torch.float32).pin_memory().numpy()
+    h_g0 = torch.empty(fn.n_band, dtype=torch.float32).pin_memory().numpy()
+    h_gv = torch.empty(3 * n ** 3, dtype=torch.float32).pin_memory().numpy()
+    hw_ = []
+    for k in range(1 + 5):
         t0 = time.perf_counter()
-        phik = fn.forward()
-        fn.backward(2.0 * (phik - target))
-        hw_.append(time.perf_counter() - t0)
+        ctx.check(ctx.lib.vlr_adj_forward(ctx.handle, fn.handle, ptr(h_phik, C.c_float)), "vlr_adj_forward")
+        np.subtract(h_phik, target, out=h_lam)
+        h_lam *= 2.0
+        ctx.check(ctx.lib.vlr_adj_backward(ctx.handle, fn.handle, ptr(h_lam, C.c_float), ptr(h_g0, C.c_float),
+                                           ptr(h_gv, C.c_float)), "vlr_adj_backward")
+        if k >= 1:
+            hw_.append(time.perf_counter() - t0)
     ctx.profile(True)
     phik = fn.forward()
     fn.backward(2.0 * (phik - target))
@@ -550,7 +561,8 @@ def bench_adjoint(args, ctx):
             "value": nb * steps / ((f + b) * 1e-3), "unit": "band voxel-steps/s (forward + backward)",
             "timing": "device buffers, CUDA events on the library stream (forward_device + backward_device)",
             "e2e": {"value": nb * steps / he, "unit": "band voxel-steps/s",
-                    "path": "vlr_adj_forward + vlr_adj_backward with host buffers (dL/dV: 25 MB to the host)",
+                    "path": "vlr_adj_forward + vlr_adj_backward with pinned host buffers (dL/dV: 25 MB to the "
+                            "host)",
                     "h2d_bytes_per_step": nb * 4, "d2h_bytes_per_step": nb * 8 + 3 * n ** 3 * 4},
             "forward_voxels_per_s": nb * steps / (f * 1e-3),
             "kernels_ms_total_per_pass": {k: v[0] for k, v in kern.items()},

@@ -62,6 +62,8 @@ struct vlr_adjoint {
     int disp = 0;                        // 1: ub holds each band voxel's fixed backtrace displacement
                                          // (a level set's time-independent velocity), step factor 1
     unsigned* foot_pk = nullptr;         // per pool voxel: packed foot offsets of band voxels, 0 elsewhere
+    int* lrange = nullptr;               // per leaf: min and max foot offset per axis of its band voxels (6 ints)
+    int* wrange = nullptr;               // per leaf: candidate window per axis for its corners (6 ints)
     float4* foot_w = nullptr;            // per pool voxel: (wx, wy, wz, lambda) of band voxels
     unsigned* keys = nullptr;
     float* pvals = nullptr;
@@ -204,6 +206,62 @@ __global__ void k_adj_pack(const int* __restrict__ bvox, int nb, const float3* _
     }
 }
 
+// Per leaf, the smallest and largest foot offset per axis over its band
+// voxels at this step (empty leaves: min > max).  One warp per leaf.
+__global__ void k_adj_leafrange(const unsigned* __restrict__ foot_pk, int n_leaves, int* __restrict__ lrange) {
+    const int lane = threadIdx.x & 31;
+    for (int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; leaf < n_leaves;
+         leaf += (gridDim.x * blockDim.x) >> 5) {
+        int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+        for (int v = lane; v < kLeafVoxels; v += 32) {
+            const unsigned pk = foot_pk[(size_t)leaf * kLeafVoxels + v];
+            if (!(pk >> 31)) continue;
+            const int f[3] = {(int)((pk >> 14) & 127u) - 64, (int)((pk >> 7) & 127u) - 64, (int)(pk & 127u) - 64};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = min(lo[a], f[a]);
+                hi[a] = max(hi[a], f[a]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = __reduce_min_sync(0xffffffffu, lo[a]);
+            hi[a] = __reduce_max_sync(0xffffffffu, hi[a]);
+        }
+        if (lane < 3) {
+            lrange[leaf * 6 + lane] = lo[lane];
+            lrange[leaf * 6 + 3 + lane] = hi[lane];
+        }
+    }
+}
+
+// Per leaf, the window of candidate offsets dx (per axis) for its corners b:
+// a band voxel x = b + dx has b in its foot cell only if dx = -f(x) - {0, 1},
+// f(x) its foot offset; x lies in the 27-leaf neighbourhood (|f| <= R < 8),
+// so dx runs over [-max f - 1, -min f] taken over the neighbourhood's band
+// voxels, within [-1 - R, R].  Empty neighbourhoods get an empty window.
+__global__ void k_adj_window(const int* __restrict__ nbr, const int* __restrict__ lrange, int n_leaves, int R,
+                             int* __restrict__ wrange) {
+    for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n_leaves; leaf += gridDim.x * blockDim.x) {
+        int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+        for (int d = 0; d < kNbr; ++d) {
+            const int s = nbr[(size_t)leaf * kNbr + d];
+            if (s < 0) continue;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = min(lo[a], lrange[s * 6 + a]);
+                hi[a] = max(hi[a], lrange[s * 6 + 3 + a]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const bool empty = lo[a] > hi[a];
+            wrange[leaf * 6 + a] = empty ? 1 : max(-hi[a] - 1, -1 - R);
+            wrange[leaf * 6 + 3 + a] = empty ? 0 : min(-lo[a], R);
+        }
+    }
+}
+
 // Adjoint of step k as a gather, one band voxel b per thread:
 //   G(b)      += lambda(b) s grad trilinear(phi_k)(p(b))      (b's own foot)
 //   lambda'(b) = sum over band voxels x of lambda(x) w_b(p(x))  (b as a corner)
@@ -212,13 +270,16 @@ __global__ void k_adj_pack(const int* __restrict__ bvox, int nb, const float3* _
 // visited in a fixed order (x, then y, then z ascending), each x's foot taken
 // from the same foot_of() as the forward step (through k_adj_pack), so the
 // transpose is exact and the sum order is fixed: deterministic, with no sort
-// and no float atomics.  RT > 0 fixes R at compile time (unrolled window).
+// and no float atomics.  RT = 1: the whole window [-2, 1]^3, unrolled.  RT =
+// 0: the visit is narrowed to the leaf's window from k_adj_window (offsets
+// outside it cannot hold b as a corner), which keeps the order of the
+// contributing terms, hence the sums, unchanged; smooth fields leave 2-3
+// offsets per axis, against 2R + 2 in the whole window.
 template <int RT>
 __global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
                              const float* __restrict__ phi_k, const unsigned* __restrict__ foot_pk,
-                             const float4* __restrict__ foot_w, float s, float hw, int R_run,
+                             const float4* __restrict__ foot_w, float s, float hw, const int* __restrict__ wrange,
                              float* __restrict__ lam_out, float3* __restrict__ G) {
-    const int R = RT > 0 ? RT : R_run;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
         const int cx = off >> 6, cy = (off >> 3) & 7, cz = off & 7;
@@ -246,16 +307,26 @@ __global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __
             G[b] = g;
         }
         const int* nrow = nbr + slot * kNbr;
+        int x0 = -2, y0 = -2, z0 = -2, x1 = 1, y1 = 1, z1 = 1;
+        if (RT == 0) {
+            const int* w6 = wrange + slot * 6;
+            x0 = __ldg(&w6[0]);
+            y0 = __ldg(&w6[1]);
+            z0 = __ldg(&w6[2]);
+            x1 = __ldg(&w6[3]);
+            y1 = __ldg(&w6[4]);
+            z1 = __ldg(&w6[5]);
+        }
         float acc = 0.f;
 #pragma unroll
-        for (int dx = -1 - R; dx <= R; ++dx) {
+        for (int dx = x0; dx <= x1; ++dx) {
             const int x = cx + dx;
 #pragma unroll
-            for (int dy = -1 - R; dy <= R; ++dy) {
+            for (int dy = y0; dy <= y1; ++dy) {
                 const int y = cy + dy;
                 const int nb2 = nbx(x) * 9 + nbx(y) * 3;
 #pragma unroll
-                for (int dz = -1 - R; dz <= R; ++dz) {
+                for (int dz = z0; dz <= z1; ++dz) {
                     const int z = cz + dz;
                     const int ns = __ldg(&nrow[nb2 + nbx(z)]);
                     if (ns < 0) continue;
@@ -368,7 +439,7 @@ void adj_free(vlr_adjoint* a) {
     adj_drop_graphs(a);
     void* ptrs[] = {a->origin, a->nbr, a->hkey, a->hval, a->phi[0], a->phi[1], a->phi_init, a->bidx, a->bvox,
                     a->ub, a->vel, a->checkpoints, a->segment, a->lam[0], a->lam[1], a->G, a->keys, a->pvals,
-                    a->scratch, a->gvel, a->foot_pk, a->foot_w};
+                    a->scratch, a->gvel, a->foot_pk, a->foot_w, a->lrange, a->wrange};
     for (void* p : ptrs) cudaFree(p);
 }
 
@@ -456,18 +527,23 @@ int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
                       k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk, a->foot_pk,
                                                                       a->foot_w));
             const int gb = blocks_for(ctx, nb);
-            if (a->reach == 1)
+            const int nl = a->n_leaves;
+            // the narrowed window pays when the whole window is large (reach >= 2)
+            // or the band is, where its two small per-leaf passes are cheap
+            if (a->reach == 1 && nb < (1u << 20)) {
                 VLR_TIMED(ctx, "k_adj_lambda",
                           k_adj_lambda<1><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, 1, lam_out, a->G));
-            else if (a->reach == 2)
-                VLR_TIMED(ctx, "k_adj_lambda",
-                          k_adj_lambda<2><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, 2, lam_out, a->G));
-            else
+                                                              a->foot_w, sk, a->hw, nullptr, lam_out, a->G));
+            } else {
+                VLR_TIMED(ctx, "k_adj_leafrange",
+                          k_adj_leafrange<<<blocks_for(ctx, 32ll * nl), 256, 0, st>>>(a->foot_pk, nl, a->lrange));
+                VLR_TIMED(ctx, "k_adj_window",
+                          k_adj_window<<<blocks_for(ctx, nl), 256, 0, st>>>(a->nbr, a->lrange, nl, a->reach,
+                                                                            a->wrange));
                 VLR_TIMED(ctx, "k_adj_lambda",
                           k_adj_lambda<0><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, a->reach, lam_out, a->G));
+                                                              a->foot_w, sk, a->hw, a->wrange, lam_out, a->G));
+            }
             lam = lam_out;
         }
         (void)cur;
@@ -632,6 +708,8 @@ int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int che
     ADJ_MALLOC(a->G, sizeof(float3) * nb);
     ADJ_MALLOC(a->foot_pk, sizeof(unsigned) * pool);
     ADJ_MALLOC(a->foot_w, sizeof(float4) * pool);
+    ADJ_MALLOC(a->lrange, sizeof(int) * 6 * (size_t)n);
+    ADJ_MALLOC(a->wrange, sizeof(int) * 6 * (size_t)n);
 #undef ADJ_MALLOC
     VLR_CUDA(ctx, cudaMemsetAsync(a->foot_pk, 0, sizeof(unsigned) * pool, st));
     VLR_CUDA(ctx, cudaMemsetAsync(a->hkey, 0xFF, sizeof(uint64_t) * a->hcap, st));  // kEmptyKey
@@ -747,6 +825,8 @@ int vlr_adj_create(vlr_ctx* ctx, const int32_t* origins, const uint64_t* masks, 
     ADJ_MALLOC(a->gvel, sizeof(float) * nvel);
     ADJ_MALLOC(a->foot_pk, sizeof(unsigned) * 512 * n_leaves);
     ADJ_MALLOC(a->foot_w, sizeof(float4) * 512 * n_leaves);
+    ADJ_MALLOC(a->lrange, sizeof(int) * 6 * n_leaves);
+    ADJ_MALLOC(a->wrange, sizeof(int) * 6 * n_leaves);
     VLR_CUDA(ctx, cudaMemsetAsync(a->foot_pk, 0, sizeof(unsigned) * 512 * n_leaves, ctx->stream));
     ADJ_MALLOC(a->G, sizeof(float3) * nb);
     ADJ_MALLOC(a->keys, sizeof(unsigned) * a->n_pairs_cap);

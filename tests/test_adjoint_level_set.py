@@ -14,9 +14,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _level_set(precision):
+def _level_set(precision, amplitude=1.0):
     from sharc.volrus_b200.method import LevelSet, random_sphere_grids
-    gr = random_sphere_grids(1, seed=21, extent_log2=(6.0, 6.5), spheres=(3, 5), radius=(6.0, 12.0))
+    gr = random_sphere_grids(1, seed=21, extent_log2=(6.0, 6.5), spheres=(3, 5), radius=(6.0, 12.0),
+                             amplitude=amplitude)
     sph, vel, _ = gr[0]
     ls = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=precision, integrator=3)
     return ls, vel
@@ -37,13 +38,13 @@ def _oracle_band(o, m):
     return np.array(out, np.int32).reshape(-1, 3)
 
 
-@pytest.mark.parametrize("precision", [0, 1], ids=["f32", "f16"])
-def test_level_set_adjoint_matches_fp64(ctx, precision):
+@pytest.mark.parametrize("precision,amplitude", [(0, 1.0), (1, 1.0), (0, 1.8)], ids=["f32", "f16", "f32_fast"])
+def test_level_set_adjoint_matches_fp64(ctx, precision, amplitude):
     from oracle import pyoracle
     from oracle.pyadjoint import AdjointOracle
     from sharc.volrus_b200.adjoint import AdvectionFunction
 
-    ls, vel = _level_set(precision)
+    ls, vel = _level_set(precision, amplitude)
     ls.step(2)  # an evolved state: the adjoint starts from whatever the level set holds
     o, m, phi = ls.arrays()
     K, C = 6, 2
