@@ -140,18 +140,15 @@ __device__ __forceinline__ Foot foot_of(float3 u, float s) {
     return f;
 }
 
-// One forward step over all band voxels (non-band voxels are copied).
-__global__ void k_adj_forward(const int4* __restrict__ origin, const int* __restrict__ nbr,
-                              const int* __restrict__ bidx, const float3* __restrict__ ub,
-                              const float* __restrict__ src, float* __restrict__ dst, int n_leaves, float s, float hw,
-                              unsigned* err) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_leaves * kLeafVoxels; t += gridDim.x * blockDim.x) {
+// One forward step over the band voxels, one thread each.  Non-band voxels
+// never change, and both state buffers hold phi_0 there (the callers copy it
+// into both), so they are not touched.
+__global__ void k_adj_forward(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
+                              const float3* __restrict__ ub, const float* __restrict__ src, float* __restrict__ dst,
+                              float s, float hw, unsigned* err) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int t = bvox[b];
         const int slot = t >> 9, off = t & 511;
-        const int b = bidx[t];
-        if (b < 0) {
-            dst[t] = src[t];
-            continue;
-        }
         Foot f = foot_of(ub[b], s);
         int x = (off >> 6) + f.fx, y = ((off >> 3) & 7) + f.fy, z = (off & 7) + f.fz;
         if (x < -8 || y < -8 || z < -8 || x > 14 || y > 14 || z > 14) {
@@ -461,9 +458,8 @@ float step_factor(const vlr_adjoint* a, int k) {
 
 int enqueue_forward_step(vlr_ctx* ctx, vlr_adjoint* a, int k, const float* src, float* dst) {
     VLR_TIMED(ctx, "k_adj_forward",
-              k_adj_forward<<<blocks_for(ctx, (long long)a->n_leaves * 512), 256, 0, ctx->stream>>>(
-                  a->origin, a->nbr, a->bidx, a->ub, src, dst, a->n_leaves, step_factor(a, k), a->hw,
-                  ctx->d_errword));
+              k_adj_forward<<<blocks_for(ctx, a->n_band), 256, 0, ctx->stream>>>(
+                  a->bvox, a->n_band, a->nbr, a->ub, src, dst, step_factor(a, k), a->hw, ctx->d_errword));
     VLR_CUDA(ctx, cudaGetLastError());
     return VLR_OK;
 }
@@ -473,7 +469,10 @@ int enqueue_forward_step(vlr_ctx* ctx, vlr_adjoint* a, int k, const float* src, 
 int adj_forward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
     cudaStream_t st = ctx->stream;
     const size_t nb = (size_t)a->n_band;
+    // both state buffers start as phi_0 (the steps rewrite band voxels only)
     VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[0], a->phi_init, sizeof(float) * 512 * a->n_leaves, cudaMemcpyDeviceToDevice,
+                                  st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(a->phi[1], a->phi_init, sizeof(float) * 512 * a->n_leaves, cudaMemcpyDeviceToDevice,
                                   st));
     int cur = 0;
     for (int k = 0; k < a->steps; ++k) {
