@@ -679,7 +679,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
                                                            unsigned* __restrict__ err,
                                                            const __grid_constant__ StageMaps maps) {
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
-    constexpr int VPT = kLeafVoxels / NT;  // voxels per thread in whole-leaf passes
     dep_wait();
     dep_launch();
     // clear this step's re-tracking state (keep flags, proposal table, leaf hash)
@@ -868,19 +867,20 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
 
 // -------------------------------------------------------------- reinit
 
+// Godunov upwind |grad phi| for the sign of s.  Per axis the upwind one-sided
+// differences are u = max(sg (p - phi_-), 0) and w = max(sg (p - phi_+), 0),
+// sg = +-1 the sign of s (exact), and the axis term is max(u, w)^2, which
+// equals max(u^2, w^2) bit for bit (u, w >= 0 and rounding is monotone): the
+// same value as the sign-split form max(max(a-, 0)^2, min(a+, 0)^2) for s >=
+// 0 and its mirror for s < 0, without the sign branch.
 __device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym, float yp, float zm, float zp, float s) {
-    float am0 = p - xm, am1 = p - ym, am2 = p - zm;
-    float ap0 = xp - p, ap1 = yp - p, ap2 = zp - p;
-    float u0, u1, u2, w0, w1, w2;
-    if (s >= 0.f) {
-        u0 = fmaxf(am0, 0.f); u1 = fmaxf(am1, 0.f); u2 = fmaxf(am2, 0.f);
-        w0 = fminf(ap0, 0.f); w1 = fminf(ap1, 0.f); w2 = fminf(ap2, 0.f);
-    } else {
-        u0 = fminf(am0, 0.f); u1 = fminf(am1, 0.f); u2 = fminf(am2, 0.f);
-        w0 = fmaxf(ap0, 0.f); w1 = fmaxf(ap1, 0.f); w2 = fmaxf(ap2, 0.f);
-    }
-    float g2 = fmaxf(u0 * u0, w0 * w0) + fmaxf(u1 * u1, w1 * w1);
-    g2 += fmaxf(u2 * u2, w2 * w2);
+    const float sg = (s >= 0.f) ? 1.f : -1.f;
+    const float mx = fmaxf(fmaxf(sg * (p - xm), 0.f), fmaxf(sg * (p - xp), 0.f));
+    const float my = fmaxf(fmaxf(sg * (p - ym), 0.f), fmaxf(sg * (p - yp), 0.f));
+    const float mz = fmaxf(fmaxf(sg * (p - zm), 0.f), fmaxf(sg * (p - zp), 0.f));
+    // squares rounded before the sums, as in the sign-split form (no contraction)
+    float g2 = __fmul_rn(mx, mx) + __fmul_rn(my, my);
+    g2 += __fmul_rn(mz, mz);
     return sqrtf(g2);
 }
 
