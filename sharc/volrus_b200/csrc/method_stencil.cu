@@ -1028,10 +1028,15 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         if (slot_n >= 0)
             stage_issue<T, 2, NT, ST>(s_desc, s_tma, &s_bar, s_nbr[cur ^ 1], src, maps, A.dmask, s_raw, s_dm);
         if (NIT == 2) {
-            // iteration 1 on the voxels of D in the 10^3 box, compacted per warp:
-            // lane l of warp w owns D row r = l * NW + w
+            // iteration 1 on the voxels of D in the 10^3 box that iteration 2
+            // reads (the leaf and the 6 face slabs of its ring; the ring's
+            // edges and corners are never read), compacted per warp: lane l of
+            // warp w owns D row r = l * NW + w
             const int r = lane * NW + warp;
-            unsigned row = (r < F * F) ? s_D[r] : 0u;
+            const int rx = r / F, ry = r - rx * F;
+            const int edges = (rx == 0 || rx == F - 1) + (ry == 0 || ry == F - 1);
+            const unsigned keep = edges == 0 ? 0x3FFu : (edges == 1 ? 0x1FEu : 0u);
+            unsigned row = (r < F * F) ? (s_D[r] & keep) : 0u;
             const int c = __popc(row);
             int incl = c;
 #pragma unroll
