@@ -114,20 +114,20 @@ int consume_device_errors(vlr_ctx* ctx, const char* what) {
 }
 
 void grid_free_arrays(vlr_grid* g) {
-    cudaFree(g->origin);
-    cudaFree(g->mask);
-    cudaFree(g->values);
-    cudaFree(g->nbr);
-    cudaFree(g->hkey);
-    cudaFree(g->hval);
+    if (g->block) {
+        // stream-ordered: later work on the context stream may reuse the memory
+        if (g->ctx && g->ctx->stream) cudaFreeAsync(g->block, g->ctx->stream);
+        else cudaFree(g->block);
+    }
+    g->block = nullptr;
     g->origin = nullptr;
     g->mask = nullptr;
     g->values = nullptr;
     g->nbr = nullptr;
     g->hkey = nullptr;
     g->hval = nullptr;
-    g->cap = 0;
     g->hcap = 0;
+    g->cap = 0;
 }
 
 static int next_pow2(long long v) {
@@ -136,17 +136,34 @@ static int next_pow2(long long v) {
     return p;
 }
 
+// The grid's arrays in one allocation from the context's pool (256-byte
+// aligned pieces): a step that makes a new grid costs no synchronising
+// cudaMalloc.
 int grid_alloc(vlr_ctx* ctx, vlr_grid* g, int cap) {
     grid_free_arrays(g);
+    if (!g->ctx) g->ctx = ctx;
     int c = std::max(cap, 1);
     size_t vb = value_bytes(g->kind);
-    VLR_CUDA(ctx, cudaMalloc(&g->origin, sizeof(int4) * c));
-    VLR_CUDA(ctx, cudaMalloc(&g->mask, sizeof(uint64_t) * 8 * c));
-    VLR_CUDA(ctx, cudaMalloc(&g->values, vb * kLeafVoxels * c));
-    VLR_CUDA(ctx, cudaMalloc(&g->nbr, sizeof(int) * kNbr * c));
     g->hcap = next_pow2(2ll * c);
-    VLR_CUDA(ctx, cudaMalloc(&g->hkey, sizeof(uint64_t) * g->hcap));
-    VLR_CUDA(ctx, cudaMalloc(&g->hval, sizeof(int) * g->hcap));
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t s_origin = up(sizeof(int4) * c), s_mask = up(sizeof(uint64_t) * 8 * c),
+                 s_values = up(vb * kLeafVoxels * c), s_nbr = up(sizeof(int) * kNbr * (size_t)c),
+                 s_hkey = up(sizeof(uint64_t) * g->hcap), s_hval = up(sizeof(int) * g->hcap);
+    char* p = nullptr;
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&p, s_origin + s_mask + s_values + s_nbr + s_hkey + s_hval, ctx->pool,
+                                          ctx->stream));
+    g->block = p;
+    g->origin = (int4*)p;
+    p += s_origin;
+    g->mask = (uint64_t*)p;
+    p += s_mask;
+    g->values = p;
+    p += s_values;
+    g->nbr = (int*)p;
+    p += s_nbr;
+    g->hkey = (uint64_t*)p;
+    p += s_hkey;
+    g->hval = (int*)p;
     g->cap = c;
     return VLR_OK;
 }
@@ -371,6 +388,7 @@ int grid_compact(vlr_ctx* ctx, vlr_grid* g, const int* d_flags) {
     VLR_CUDA(ctx, cudaGetLastError());
     VLR_CUDA(ctx, cudaFreeAsync(pos, ctx->stream));
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::swap(g->block, tmp.block);
     std::swap(g->origin, tmp.origin);
     std::swap(g->mask, tmp.mask);
     std::swap(g->values, tmp.values);

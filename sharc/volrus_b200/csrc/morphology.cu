@@ -250,6 +250,7 @@ int grid_add_leaves(vlr_ctx* ctx, vlr_grid* g, const std::vector<int32_t>& origi
     VLR_CUDA(ctx, cudaGetLastError());
     VLR_CUDA(ctx, cudaFreeAsync(d_onew, ctx->stream));
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::swap(g->block, tmp.block);
     std::swap(g->origin, tmp.origin);
     std::swap(g->mask, tmp.mask);
     std::swap(g->values, tmp.values);

@@ -50,6 +50,7 @@ struct vlr_grid {
     float background = 0.0f;
     vlr_transform xf{};
     long long base[3] = {0, 0, 0};
+    void* block = nullptr;  // one stream-ordered allocation (ctx->pool) holding the arrays below
     int4* origin = nullptr;
     uint64_t* mask = nullptr;
     void* values = nullptr;
