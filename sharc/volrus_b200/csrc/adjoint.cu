@@ -343,6 +343,77 @@ __global__ void k_adj_lambda(const int* __restrict__ bvox, int nb, const int* __
     }
 }
 
+// k_adj_lambda<1> for small bands, four lanes per band voxel: lane q of the
+// quad visits offset dx = q - 2 of the whole window [-2, 1]^3 (dy, dz
+// ascending) and the quad sums its four partial sums in the fixed order
+// ((q0 + q1) + q2) + q3; lane 0 adds b's own gradient term.  Deterministic;
+// the rounding differs from the one-thread order only in how the partial sums
+// associate.  Fills the GPU where one thread per band voxel leaves most warp
+// slots empty.
+__global__ void k_adj_lambda_quad(const int* __restrict__ bvox, int nb, const int* __restrict__ nbr,
+                                  const float* __restrict__ phi_k, const unsigned* __restrict__ foot_pk,
+                                  const float4* __restrict__ foot_w, float s, float hw, float* __restrict__ lam_out,
+                                  float3* __restrict__ G) {
+    const int q = threadIdx.x & 3;
+    for (long long gq = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 2; gq < nb;
+         gq += ((long long)gridDim.x * blockDim.x) >> 2) {
+        const int b = (int)gq;
+        const int sv = bvox[b], slot = sv >> 9, off = sv & 511;
+        const int cx = off >> 6, cy = (off >> 3) & 7, cz = off & 7;
+        if (q == 0) {
+            const unsigned pk = foot_pk[sv];
+            const float4 w4 = foot_w[sv];
+            const float l = w4.w;
+            const int x = cx + (int)((pk >> 14) & 127u) - 64, y = cy + (int)((pk >> 7) & 127u) - 64,
+                      z = cz + (int)(pk & 127u) - 64;
+            const float wx[2] = {1 - w4.x, w4.x}, wy[2] = {1 - w4.y, w4.y}, wz[2] = {1 - w4.z, w4.z};
+            float c[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) c[k] = adj_read(phi_k, nbr, slot, x + (k >> 2), y + ((k >> 1) & 1), z + (k & 1), hw);
+            float gx = wy[0] * wz[0] * (c[4] - c[0]) + wy[1] * wz[0] * (c[6] - c[2]) + wy[0] * wz[1] * (c[5] - c[1]) +
+                       wy[1] * wz[1] * (c[7] - c[3]);
+            float gy = wx[0] * wz[0] * (c[2] - c[0]) + wx[1] * wz[0] * (c[6] - c[4]) + wx[0] * wz[1] * (c[3] - c[1]) +
+                       wx[1] * wz[1] * (c[7] - c[5]);
+            float gz = wx[0] * wy[0] * (c[1] - c[0]) + wx[1] * wy[0] * (c[5] - c[4]) + wx[0] * wy[1] * (c[3] - c[2]) +
+                       wx[1] * wy[1] * (c[7] - c[6]);
+            float3 g = G[b];
+            g.x += l * s * gx;
+            g.y += l * s * gy;
+            g.z += l * s * gz;
+            G[b] = g;
+        }
+        const int* nrow = nbr + slot * kNbr;
+        float acc = 0.f;
+        const int dx = q - 2;
+        const int x = cx + dx;
+#pragma unroll
+        for (int dy = -2; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            const int nb2 = nbx(x) * 9 + nbx(y) * 3;
+#pragma unroll
+            for (int dz = -2; dz <= 1; ++dz) {
+                const int z = cz + dz;
+                const int ns = __ldg(&nrow[nb2 + nbx(z)]);
+                if (ns < 0) continue;
+                const size_t e = (size_t)ns * kLeafVoxels + voxel_off(x, y, z);
+                const unsigned pk = __ldg(&foot_pk[e]);
+                const int i = 64 - dx - (int)((pk >> 14) & 127u), j = 64 - dy - (int)((pk >> 7) & 127u),
+                          k = 64 - dz - (int)(pk & 127u);
+                if (!(pk >> 31) || (unsigned)i > 1u || (unsigned)j > 1u || (unsigned)k > 1u) continue;
+                const float4 w4 = __ldg(&foot_w[e]);
+                const float wx = i ? w4.x : 1 - w4.x, wy = j ? w4.y : 1 - w4.y, wz = k ? w4.z : 1 - w4.z;
+                acc += w4.w * wx * wy * wz;
+            }
+        }
+        // the quad's lanes are consecutive; sum in lane order
+        const unsigned qmask = 0xFu << (threadIdx.x & 28);
+        const float a1 = __shfl_sync(qmask, acc, (threadIdx.x & 31 & ~3) + 1);
+        const float a2 = __shfl_sync(qmask, acc, (threadIdx.x & 31 & ~3) + 2);
+        const float a3 = __shfl_sync(qmask, acc, (threadIdx.x & 31 & ~3) + 3);
+        if (q == 0) lam_out[b] = ((acc + a1) + a2) + a3;
+    }
+}
+
 // Transpose of the upsample: 3 x 8 (node, G_a * weight) pairs per band voxel.
 __global__ void k_adj_emit_vel(const int* __restrict__ bvox, const int4* __restrict__ origin, int nb,
                                const float3* __restrict__ G, int n, float H, unsigned* __restrict__ keys,
@@ -530,9 +601,10 @@ int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
             // the narrowed window pays when the whole window is large (reach >= 2)
             // or the band is, where its two small per-leaf passes are cheap
             if (a->reach == 1 && nb < (1u << 20)) {
+                // small band: a quad of lanes per band voxel fills the GPU
                 VLR_TIMED(ctx, "k_adj_lambda",
-                          k_adj_lambda<1><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
-                                                              a->foot_w, sk, a->hw, nullptr, lam_out, a->G));
+                          k_adj_lambda_quad<<<blocks_for(ctx, 4ll * nb), 256, 0, st>>>(
+                              a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk, a->foot_w, sk, a->hw, lam_out, a->G));
             } else {
                 VLR_TIMED(ctx, "k_adj_leafrange",
                           k_adj_leafrange<<<blocks_for(ctx, 32ll * nl), 256, 0, st>>>(a->foot_pk, nl, a->lrange));
