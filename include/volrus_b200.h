@@ -309,6 +309,11 @@ int vlr_ls_info(vlr_ctx* ctx, const vlr_level_set* ls, size_t* n_leaves, uint64_
  * and allocations: the host-resident form of a step is upload, step, download. */
 int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
                   size_t n_leaves);
+/* Set the step counter of a level set (its time is t0 + step * dt, computed in
+ * f32 by the kernels).  A run continued in a new level set (one with a larger
+ * capacity, say) and created with the same t0 resumes at the same time, bit for
+ * bit, once its counter is set to the old one's.  step >= 0. */
+int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step);
 /* The host-resident form of n_steps steps in one call: replace the state with
  * host leaves (as vlr_ls_upload), step, and write the result (as
  * vlr_ls_download) into caller buffers of cap_leaves leaves; *n_out = leaves

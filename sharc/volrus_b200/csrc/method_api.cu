@@ -844,6 +844,18 @@ int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const
     return upload_impl(ctx, ls, origins, masks, phi, n_leaves, false);
 }
 
+int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (step < 0) return set_error(ctx, VLR_ERR_INVALID, "step must be >= 0");
+    if (!ls->scalars) return set_error(ctx, VLR_ERR_INVALID, "level set has no state");
+    // the look-back scan tags its status words with step + 1: clear them so no
+    // word of an earlier step can carry the tag of a step to come
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (ls->cap + 1 + scan_scratch_ints(ls->cap)), ctx->stream));
+    VLR_CUDA(ctx, cudaMemcpyAsync(ls->scalars + 1, &step, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
+
 int vlr_ls_volume(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* volume) {
     if (!ctx || !ls || !volume) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     double r[3] = {0, 0, 0};

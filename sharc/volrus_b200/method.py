@@ -284,6 +284,10 @@ class LevelSet:
         self.ctx.check(self.ctx.lib.vlr_ls_upload(self.ctx.handle, self.handle, ptr(o, C.c_int32), ptr(m, C.c_uint64),
                                                   ptr(p, C.c_float), len(o)), "vlr_ls_upload")
 
+    def set_step(self, step: int):
+        """Set the step counter (time = t0 + step * dt): resume a run in a new level set."""
+        self.ctx.check(self.ctx.lib.vlr_ls_set_step(self.ctx.handle, self.handle, int(step)), "vlr_ls_set_step")
+
     def volume(self, ref=(0.0, 0.0, 0.0)) -> float:
         """Enclosed volume in voxel units^3 (FP64 reduction)."""
         r = np.asarray(ref, np.float64)

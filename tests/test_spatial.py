@@ -1,0 +1,275 @@
+"""Spatial decomposition of one level set over ranks (sharc/volrus_b200/spatial.py).
+
+CPU: Morton keys against a bit-by-bit interleave, balanced key ranges, the
+ghost sends against a brute-force neighbourhood search, the record packing,
+and the whole decomposition with the FP64 method oracle as the per-rank
+stepper: 2-4 emulated ranks with rebalancing, and two gloo processes over
+torch.distributed, each bit-identical to the undivided oracle run (curl noise
+with RK3, and the time-dependent vortex).
+
+GPU: the same decomposition with the library's step on each emulated rank
+(one device, ranks stepped in turn, exchanges in process) is bit-identical to
+the undivided run on the device, in FP32 and FP16, including level sets
+re-created mid-run with their step counter carried over.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from sharc.volrus_b200 import spatial
+from sharc.volrus_b200.spatial import GHOST_DEPTH, Leaves, Partition
+
+
+def _slow_key(c):
+    x, y, z = (int(v) + (1 << 20) for v in c)
+    k = 0
+    for b in range(21):
+        k |= ((x >> b) & 1) << (3 * b + 2)
+        k |= ((y >> b) & 1) << (3 * b + 1)
+        k |= ((z >> b) & 1) << (3 * b)
+    return k
+
+
+def test_morton_keys_interleave_bits():
+    rng = np.random.default_rng(1)
+    c = np.concatenate([rng.integers(-(1 << 20), 1 << 20, (200, 3)), [[0, 0, 0], [-1, -1, -1], [(1 << 20) - 1] * 3,
+                                                                     [-(1 << 20)] * 3]])
+    got = spatial.morton_keys_of_leaf_coords(c)
+    assert [int(k) for k in got] == [_slow_key(v) for v in c]
+    assert np.array_equal(spatial.morton_keys(c * 8 + 3), got)
+    with pytest.raises(ValueError):
+        spatial.morton_keys_of_leaf_coords(np.array([[1 << 20, 0, 0]]))
+
+
+def _random_leaves(n, seed, span=12, dtype=np.float32):
+    rng = np.random.default_rng(seed)
+    c = np.unique(rng.integers(-span, span, (n, 3)), axis=0)
+    o = (c * 8).astype(np.int32)
+    m = rng.integers(0, 2 ** 63, (len(o), 8), dtype=np.uint64)
+    p = rng.standard_normal((len(o), 512)).astype(dtype)
+    return Leaves(o, m, p)
+
+
+def test_partition_is_balanced_and_deterministic():
+    lv = _random_leaves(3000, 2)
+    k = lv.keys()
+    cost = spatial.leaf_cost(lv.masks)
+    for world in (1, 2, 3, 5, 8):
+        p1 = Partition.balanced(k, cost, world)
+        p2 = Partition.balanced(k[::-1].copy(), cost[::-1].copy(), world)
+        assert np.array_equal(p1.splitters, p2.splitters)
+        own = p1.owner(k)
+        assert own.min() >= 0 and own.max() < world
+        loads = np.bincount(own, weights=cost, minlength=world)
+        assert loads.max() - loads.min() <= 2 * cost.max() + 1e-9, (world, loads)
+        # ranges are contiguous in key order
+        assert np.all(np.diff(own[np.argsort(k)]) >= 0)
+
+
+def test_ghost_sends_cover_the_two_leaf_neighbourhood():
+    lv = _random_leaves(1500, 3, span=8)
+    world = 3
+    part, shares = spatial.split(lv, world)
+    shards = [spatial.Shard(r, part, shares[r], None) for r in range(world)]
+    sends = [s.ghost_sends() for s in shards]
+    for r in range(world):
+        recv = Leaves.concat([sends[q][r] for q in range(world) if r in sends[q]])
+        got = {tuple(v) for v in recv.origins.tolist()}
+        mine = shares[r].origins.astype(np.int64) >> 3
+        need = set()
+        for q in range(world):
+            if q == r:
+                continue
+            oc = shares[q].origins.astype(np.int64) >> 3
+            d = np.abs(oc[:, None, :] - mine[None, :, :]).max(axis=2) if len(mine) else np.zeros((len(oc), 0))
+            near = (d <= GHOST_DEPTH).any(axis=1) if d.shape[1] else np.zeros(len(oc), bool)
+            need |= {tuple(v) for v in shares[q].origins[near].tolist()}
+        assert need <= got
+        # nothing is sent that lies farther than GHOST_DEPTH from every coordinate rank r owns
+        for o in recv.origins:
+            nb = (np.asarray(o, np.int64) >> 3) + spatial._offsets(GHOST_DEPTH)
+            assert (part.owner(spatial.morton_keys_of_leaf_coords(nb)) == r).any()
+        assert not got & {tuple(v) for v in shares[r].origins.tolist()}
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_records_pack_and_unpack(dtype):
+    lv = _random_leaves(50, 4, dtype=dtype)
+    back = Leaves.unpack(lv.pack(), dtype)
+    assert np.array_equal(back.origins, lv.origins) and np.array_equal(back.masks, lv.masks)
+    assert np.array_equal(back.phi.view(np.uint8), lv.phi.view(np.uint8))
+    assert len(Leaves.unpack(Leaves.empty(dtype).pack(), dtype)) == 0
+    with pytest.raises(ValueError):
+        Leaves.unpack(np.zeros(7, np.uint8), dtype)
+
+
+# ------------------------------------------------------------------ oracle-stepped decomposition
+
+class OracleStepper:
+    """One FP64 method-oracle step of a rank's local leaves (test checker)."""
+
+    def __init__(self, vel, integrator, reinit_iters, dt, hw, t0=0.0):
+        self.vel, self.integrator, self.reinit_iters, self.dt, self.hw, self.t0 = vel, integrator, reinit_iters, dt, \
+            hw, t0
+        self.steps = 0
+
+    def __call__(self, lv):
+        from oracle import pyoracle
+        t = self.t0 + self.steps * self.dt
+        self.steps += 1
+        if len(lv) == 0:
+            return Leaves.empty(np.float64)
+        g = pyoracle.MOGrid.from_arrays(lv.origins, lv.masks, lv.phi, self.hw)
+        assert g.step(self.vel, self.integrator, self.reinit_iters, t, self.dt, nthreads=4)
+        o, m, p = g.arrays()
+        return Leaves(o, m, p)
+
+
+def _curl_case():
+    from oracle import pyoracle
+    from sharc.volrus_b200.method import curl_noise
+    rng = np.random.default_rng(11)
+    sph = np.column_stack([rng.uniform(0, 96, (14, 3)), rng.uniform(4, 12, 14)])
+    g = pyoracle.MOGrid.spheres(sph, 3.0)
+    o, m, p = g.arrays()
+    return Leaves(o, m, p), curl_noise(5, 96.0, 1.0), 3, 1.0, 3.0
+
+
+def _vortex_case():
+    from oracle import pyoracle
+    vs = 1.0 / 128
+    g = pyoracle.MOGrid.sphere(0.15, (0.35, 0.35, 0.35), vs, 3.0)
+    o, m, p = g.arrays()
+    return Leaves(o, m, p), {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs, 3.0
+
+
+def _undivided(lv, stepper, steps):
+    for _ in range(steps):
+        lv = stepper(lv)
+    return lv.sorted_xyz()
+
+
+def _assert_same(a, b):
+    assert np.array_equal(a.origins, b.origins), (len(a), len(b))
+    assert np.array_equal(a.masks, b.masks)
+    assert np.array_equal(a.phi.view(np.uint8), b.phi.view(np.uint8))
+
+
+@pytest.mark.parametrize("world,rebalance", [(2, 0), (3, 2), (4, 1)])
+def test_emulated_ranks_match_undivided_oracle_curl(oracle, world, rebalance):
+    lv, vel, integ, dt, hw = _curl_case()
+    steps = 4
+    ref = _undivided(lv, OracleStepper(vel, integ, 2, dt, hw), steps)
+    got, shards = spatial.emulate(lv, world, lambda r: OracleStepper(vel, integ, 2, dt, hw), steps, rebalance)
+    _assert_same(got, ref)
+    assert sum(len(s.owned) for s in shards) == len(ref)
+    assert all(len(s.owned) for s in shards)
+
+
+def test_emulated_ranks_match_undivided_oracle_vortex(oracle):
+    lv, vel, integ, dt, hw = _vortex_case()
+    steps = 3
+    ref = _undivided(lv, OracleStepper(vel, integ, 2, dt, hw), steps)
+    got, _ = spatial.emulate(lv, 3, lambda r: OracleStepper(vel, integ, 2, dt, hw), steps, 2)
+    _assert_same(got, ref)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, steps, q):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        lv, vel, integ, dt, hw = _curl_case()
+        sls = spatial.SpatialLevelSet(lv, OracleStepper(vel, integ, 2, dt, hw), check_duplicates=True)
+        sls.step(2)
+        sls.rebalance()
+        sls.step(steps - 2)
+        whole = sls.gather()
+        q.put((rank, whole.pack(), len(sls.arrays()), sls.active_voxels()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_match_undivided_oracle(oracle):
+    world, steps = 2, 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, steps, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    lv, vel, integ, dt, hw = _curl_case()
+    ref = _undivided(lv, OracleStepper(vel, integ, 2, dt, hw), steps)
+    for rank, packed, n_owned, active in out:
+        _assert_same(Leaves.unpack(packed, np.float64), ref)
+        assert active == ref.active_voxels()
+    assert out[0][2] + out[1][2] == len(ref) and min(out[0][2], out[1][2]) > 0
+
+
+# ------------------------------------------------------------------ device
+
+class _AlwaysRecreate(spatial.DeviceStepper):
+    def _fits(self, lv):
+        return False
+
+
+def _device_case(kind):
+    from sharc.volrus_b200.method import LevelSet, random_sphere_grids
+    if kind == "curl":
+        gr = random_sphere_grids(1, seed=17, extent_log2=(7.0, 7.2), spheres=(24, 28), radius=(5.0, 14.0))
+        sph, vel, _ = gr[0]
+        ls = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=0, integrator=3)
+        o, m, p = ls.arrays()
+        ls.close()
+        return Leaves(o, m, p), vel, 3, 1.0
+    vs = 1.0 / 256
+    ls = LevelSet.sphere(0.15, (0.35, 0.35, 0.35), vs, {"kind": "vortex", "vs": vs, "period": 3.0}, 0.5 * vs)
+    o, m, p = ls.arrays()
+    ls.close()
+    return Leaves(o, m, p), {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,precision,world,recreate", [("curl", 0, 2, False), ("curl", 1, 3, False),
+                                                           ("curl", 1, 2, True), ("vortex", 1, 3, True)],
+                         ids=["curl_f32_2", "curl_f16_3", "curl_f16_2_recreate", "vortex_f16_3_recreate"])
+def test_device_ranks_match_undivided_device_run(ctx, kind, precision, world, recreate):
+    from sharc.volrus_b200.method import LevelSet
+    lv, vel, integ, dt = _device_case(kind)
+    steps = 6
+    ls = LevelSet.from_leaves(lv.origins, lv.masks, lv.phi, vel, dt, 3.0, precision, integ, 2, 0.0)
+    if precision == 1:  # start both runs from the same FP16-rounded state
+        o, m, p = ls.arrays()
+        lv = Leaves(o, m, p)
+    ls.step(steps)
+    o, m, p = ls.arrays()
+    ref = Leaves(o, m, p)
+    ls.close()
+    cls = _AlwaysRecreate if recreate else spatial.DeviceStepper
+    steppers = []
+
+    def make(r):
+        s = cls(vel, dt, 3.0, precision, integ, 2, 0.0)
+        steppers.append(s)
+        return s
+
+    got, shards = spatial.emulate(lv, world, make, steps, rebalance_every=3)
+    for s in steppers:
+        s.close()
+    _assert_same(got, ref)
+    assert all(len(s.owned) for s in shards)
