@@ -314,6 +314,17 @@ int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const
  * capacity, say) and created with the same t0 resumes at the same time, bit for
  * bit, once its counter is set to the old one's.  step >= 0. */
 int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step);
+/* Device-resident forms of vlr_ls_upload and vlr_ls_download, for callers
+ * that keep leaves in device memory on the context's device (the exchange of a
+ * grid divided over GPUs).  Records as in vlr_ls_upload: origins i32[3] on the
+ * 8-voxel lattice, masks u64[8], values f32[512] in voxel units.  The upload
+ * replaces the state and keeps the time; the download writes the allocated
+ * leaves in the level set's list order (unsorted) and sets *n_out, failing
+ * with VLR_ERR_CAPACITY above cap_leaves.  Both return after their work. */
+int vlr_ls_upload_device(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* d_origins, const uint64_t* d_masks,
+                         const float* d_phi, size_t n_leaves);
+int vlr_ls_download_device(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* d_origins, uint64_t* d_masks,
+                           float* d_phi, size_t cap_leaves, size_t* n_out);
 /* The host-resident form of n_steps steps in one call: replace the state with
  * host leaves (as vlr_ls_upload), step, and write the result (as
  * vlr_ls_download) into caller buffers of cap_leaves leaves; *n_out = leaves

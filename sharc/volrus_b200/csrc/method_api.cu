@@ -488,6 +488,36 @@ int upload_enqueue(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, cons
     return ls_enqueue_index(ctx, ls);
 }
 
+// Device-resident leaves: origins i32[3] -> the pool's int4 origins (origins
+// not on the 8-voxel lattice flag kErrInput), f32 values -> the pool's type.
+__global__ void k_upload_dev_origins(const int32_t* o3, int n, int4* origin, unsigned* err) {
+    unsigned bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int x = o3[3 * i], y = o3[3 * i + 1], z = o3[3 * i + 2];
+        bad |= (unsigned)((x | y | z) & 7);
+        origin[i] = make_int4(x, y, z, 0);
+    }
+    if (bad) atomicOr(err, kErrInput);
+}
+
+// The listed leaves in list order into device buffers (origins i32[3], masks,
+// f32 values), one CTA per leaf.
+template <typename T>
+__global__ void k_export_dev(const int* list, const int* count, const int4* origin, const uint64_t* mask,
+                             const T* vals, int32_t* o3, uint64_t* m_out, float* v_out) {
+    const int n = *count;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int s = list[i];
+        if (threadIdx.x < 3) {
+            const int4 o = origin[s];
+            o3[3 * i + threadIdx.x] = threadIdx.x == 0 ? o.x : (threadIdx.x == 1 ? o.y : o.z);
+        }
+        if (threadIdx.x < 8) m_out[(size_t)i * 8 + threadIdx.x] = mask[(size_t)s * 8 + threadIdx.x];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            v_out[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
+    }
+}
+
 int upload_impl(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
                 size_t n, bool reset_step) {
     int rc = upload_enqueue(ctx, ls, origins, masks, phi, n, reset_step);
@@ -842,6 +872,54 @@ int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const
     if (!ctx || !ls || !origins || !masks || !phi) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "upload replaces single-grid states only");
     return upload_impl(ctx, ls, origins, masks, phi, n_leaves, false);
+}
+
+int vlr_ls_upload_device(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* d_origins, const uint64_t* d_masks,
+                         const float* d_phi, size_t n_leaves) {
+    if (!ctx || !ls || (n_leaves && (!d_origins || !d_masks || !d_phi)))
+        return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "upload replaces single-grid states only");
+    if (n_leaves > (size_t)ls->cap) return set_error(ctx, VLR_ERR_CAPACITY, "more leaves than the level set's capacity");
+    const int n = (int)n_leaves;
+    if (n) {
+        k_upload_dev_origins<<<ls->grid_blocks, 256, 0, ctx->stream>>>(d_origins, n, ls->origin, ctx->d_errword);
+        VLR_CUDA(ctx, cudaMemcpyAsync(ls->mask, d_masks, 64 * n_leaves, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (ls->precision == VLR_PREC_F16)
+            k_from_f32<__half><<<ls->grid_blocks, 256, 0, ctx->stream>>>(d_phi, (__half*)ls->vals[0],
+                                                                          kLeafVoxels * n_leaves);
+        else
+            VLR_CUDA(ctx, cudaMemcpyAsync(ls->vals[0], d_phi, sizeof(float) * kLeafVoxels * n_leaves,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
+        VLR_CUDA(ctx, cudaGetLastError());
+    }
+    // origins are checked before the index is built from them
+    int rc = consume_device_errors(ctx, "vlr_ls_upload_device");
+    if (rc) return rc;
+    return ls_init_lists(ctx, ls, n, false);
+}
+
+int vlr_ls_download_device(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* d_origins, uint64_t* d_masks,
+                           float* d_phi, size_t cap_leaves, size_t* n_out) {
+    if (!ctx || !ls || !n_out || !d_origins || !d_masks || !d_phi)
+        return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *n_out = 0;
+    size_t n = 0;
+    int rc = vlr_ls_info(ctx, ls, &n, nullptr, nullptr);
+    if (rc) return rc;
+    if (n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+    if (n) {
+        const int B = (int)std::min<size_t>(n, (size_t)ctx->sm_count * 8);
+        if (ls->precision == VLR_PREC_F16)
+            k_export_dev<__half><<<B, 256, 0, ctx->stream>>>(ls->list, ls->scalars, ls->origin, ls->mask,
+                                                             (const __half*)ls->vals[0], d_origins, d_masks, d_phi);
+        else
+            k_export_dev<float><<<B, 256, 0, ctx->stream>>>(ls->list, ls->scalars, ls->origin, ls->mask,
+                                                            (const float*)ls->vals[0], d_origins, d_masks, d_phi);
+        VLR_CUDA(ctx, cudaGetLastError());
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    *n_out = n;
+    return VLR_OK;
 }
 
 int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step) {

@@ -28,6 +28,7 @@ enum : unsigned {
     kErrReach = 1u << 2,       // a backtrace left the staged neighbourhood
     kErrExtent = 1u << 3,      // a leaf coordinate left the hashable range
     kErrTimeout = 1u << 4,     // a bounded device wait gave up
+    kErrInput = 1u << 5,       // device-resident input failed a check (leaf origin not a multiple of 8)
 };
 
 __host__ __device__ inline uint64_t mix64(uint64_t k) {

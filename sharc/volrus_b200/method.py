@@ -284,6 +284,22 @@ class LevelSet:
         self.ctx.check(self.ctx.lib.vlr_ls_upload(self.ctx.handle, self.handle, ptr(o, C.c_int32), ptr(m, C.c_uint64),
                                                   ptr(p, C.c_float), len(o)), "vlr_ls_upload")
 
+    def upload_device(self, d_origins: int, d_masks: int, d_phi: int, n: int):
+        """Replace the state with n leaves in device memory (pointers: i32[3] origins,
+        u64[8] masks, f32[512] values), keeping time and allocations."""
+        self.ctx.check(self.ctx.lib.vlr_ls_upload_device(self.ctx.handle, self.handle, C.c_void_p(d_origins),
+                                                         C.c_void_p(d_masks), C.c_void_p(d_phi), int(n)),
+                       "vlr_ls_upload_device")
+
+    def download_device(self, d_origins: int, d_masks: int, d_phi: int, cap: int) -> int:
+        """The allocated leaves, in list order, into device buffers of ``cap``
+        records; returns their count."""
+        k = C.c_size_t()
+        self.ctx.check(self.ctx.lib.vlr_ls_download_device(self.ctx.handle, self.handle, C.c_void_p(d_origins),
+                                                           C.c_void_p(d_masks), C.c_void_p(d_phi), int(cap),
+                                                           C.byref(k)), "vlr_ls_download_device")
+        return k.value
+
     def set_step(self, step: int):
         """Set the step counter (time = t0 + step * dt): resume a run in a new level set."""
         self.ctx.check(self.ctx.lib.vlr_ls_set_step(self.ctx.handle, self.handle, int(step)), "vlr_ls_set_step")

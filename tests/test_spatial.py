@@ -1,7 +1,7 @@
 """Spatial decomposition of one level set over ranks (sharc/volrus_b200/spatial.py).
 
 CPU: Morton keys against a bit-by-bit interleave, balanced key ranges, the
-ghost sends against a brute-force neighbourhood search, the record packing,
+ghost sends against a brute-force neighbourhood search, the active counts,
 and the whole decomposition with the FP64 method oracle as the per-rank
 stepper: 2-4 emulated ranks with rebalancing, and two gloo processes over
 torch.distributed, each bit-identical to the undivided oracle run (curl noise
@@ -9,14 +9,16 @@ with RK3, and the time-dependent vortex).
 
 GPU: the same decomposition with the library's step on each emulated rank
 (one device, ranks stepped in turn, exchanges in process) is bit-identical to
-the undivided run on the device, in FP32 and FP16, including level sets
-re-created mid-run with their step counter carried over.
+the undivided run on the device, in FP32 and FP16, with the leaves moved
+into and out of each rank's level set by the device-resident C ABI, and with
+level sets re-created mid-run with their step counter carried over.
 """
 import os
 import socket
 
 import numpy as np
 import pytest
+import torch
 import torch.multiprocessing as mp
 
 from sharc.volrus_b200 import spatial
@@ -37,11 +39,13 @@ def test_morton_keys_interleave_bits():
     rng = np.random.default_rng(1)
     c = np.concatenate([rng.integers(-(1 << 20), 1 << 20, (200, 3)), [[0, 0, 0], [-1, -1, -1], [(1 << 20) - 1] * 3,
                                                                      [-(1 << 20)] * 3]])
-    got = spatial.morton_keys_of_leaf_coords(c)
-    assert [int(k) for k in got] == [_slow_key(v) for v in c]
-    assert np.array_equal(spatial.morton_keys(c * 8 + 3), got)
+    got = spatial.morton_keys_of_leaf_coords(torch.from_numpy(c))
+    assert got.tolist() == [_slow_key(v) for v in c]
+    assert min(got.tolist()) >= 0
+    lv = Leaves.from_numpy(c * 8, np.zeros((len(c), 8), np.uint64), np.zeros((len(c), 512), np.float32))
+    assert torch.equal(lv.keys(), got)
     with pytest.raises(ValueError):
-        spatial.morton_keys_of_leaf_coords(np.array([[1 << 20, 0, 0]]))
+        spatial.morton_keys_of_leaf_coords(torch.tensor([[1 << 20, 0, 0]]))
 
 
 def _random_leaves(n, seed, span=12, dtype=np.float32):
@@ -50,23 +54,34 @@ def _random_leaves(n, seed, span=12, dtype=np.float32):
     o = (c * 8).astype(np.int32)
     m = rng.integers(0, 2 ** 63, (len(o), 8), dtype=np.uint64)
     p = rng.standard_normal((len(o), 512)).astype(dtype)
-    return Leaves(o, m, p)
+    return Leaves.from_numpy(o, m, p)
+
+
+def test_active_counts_and_host_round_trip():
+    lv = _random_leaves(40, 5)
+    o, m, p = lv.numpy()
+    want = np.unpackbits(m.view(np.uint8).reshape(-1, 64), axis=1).sum(axis=1)
+    assert lv.active_per_leaf().tolist() == want.tolist()
+    assert lv.active_voxels() == int(want.sum())
+    back = Leaves.from_numpy(o, m, p)
+    assert torch.equal(back.masks, lv.masks) and torch.equal(back.phi, lv.phi) and torch.equal(back.origins,
+                                                                                              lv.origins)
 
 
 def test_partition_is_balanced_and_deterministic():
     lv = _random_leaves(3000, 2)
     k = lv.keys()
-    cost = spatial.leaf_cost(lv.masks)
+    cost = spatial.leaf_cost(lv)
     for world in (1, 2, 3, 5, 8):
         p1 = Partition.balanced(k, cost, world)
-        p2 = Partition.balanced(k[::-1].copy(), cost[::-1].copy(), world)
-        assert np.array_equal(p1.splitters, p2.splitters)
+        p2 = Partition.balanced(k.flip(0), cost.flip(0), world)
+        assert torch.equal(p1.splitters, p2.splitters)
         own = p1.owner(k)
-        assert own.min() >= 0 and own.max() < world
-        loads = np.bincount(own, weights=cost, minlength=world)
-        assert loads.max() - loads.min() <= 2 * cost.max() + 1e-9, (world, loads)
+        assert int(own.min()) >= 0 and int(own.max()) < world
+        loads = torch.bincount(own, weights=cost, minlength=world)
+        assert float(loads.max() - loads.min()) <= 2 * float(cost.max()) + 1e-9, (world, loads)
         # ranges are contiguous in key order
-        assert np.all(np.diff(own[np.argsort(k)]) >= 0)
+        assert bool((torch.diff(own[torch.argsort(k)]) >= 0).all())
 
 
 def test_ghost_sends_cover_the_two_leaf_neighbourhood():
@@ -76,34 +91,23 @@ def test_ghost_sends_cover_the_two_leaf_neighbourhood():
     shards = [spatial.Shard(r, part, shares[r], None) for r in range(world)]
     sends = [s.ghost_sends() for s in shards]
     for r in range(world):
-        recv = Leaves.concat([sends[q][r] for q in range(world) if r in sends[q]])
+        recv = Leaves.concat([sends[q][r] for q in range(world) if r in sends[q]], lv)
         got = {tuple(v) for v in recv.origins.tolist()}
-        mine = shares[r].origins.astype(np.int64) >> 3
+        mine = shares[r].coords().numpy()
         need = set()
         for q in range(world):
             if q == r:
                 continue
-            oc = shares[q].origins.astype(np.int64) >> 3
-            d = np.abs(oc[:, None, :] - mine[None, :, :]).max(axis=2) if len(mine) else np.zeros((len(oc), 0))
-            near = (d <= GHOST_DEPTH).any(axis=1) if d.shape[1] else np.zeros(len(oc), bool)
-            need |= {tuple(v) for v in shares[q].origins[near].tolist()}
+            oc = shares[q].coords().numpy()
+            d = np.abs(oc[:, None, :] - mine[None, :, :]).max(axis=2)
+            near = (d <= GHOST_DEPTH).any(axis=1)
+            need |= {tuple(v) for v in shares[q].origins.numpy()[near].tolist()}
         assert need <= got
         # nothing is sent that lies farther than GHOST_DEPTH from every coordinate rank r owns
-        for o in recv.origins:
-            nb = (np.asarray(o, np.int64) >> 3) + spatial._offsets(GHOST_DEPTH)
-            assert (part.owner(spatial.morton_keys_of_leaf_coords(nb)) == r).any()
+        for c in recv.coords():
+            nb = c + spatial._offsets(GHOST_DEPTH)
+            assert bool((part.owner(spatial.morton_keys_of_leaf_coords(nb)) == r).any())
         assert not got & {tuple(v) for v in shares[r].origins.tolist()}
-
-
-@pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_records_pack_and_unpack(dtype):
-    lv = _random_leaves(50, 4, dtype=dtype)
-    back = Leaves.unpack(lv.pack(), dtype)
-    assert np.array_equal(back.origins, lv.origins) and np.array_equal(back.masks, lv.masks)
-    assert np.array_equal(back.phi.view(np.uint8), lv.phi.view(np.uint8))
-    assert len(Leaves.unpack(Leaves.empty(dtype).pack(), dtype)) == 0
-    with pytest.raises(ValueError):
-        Leaves.unpack(np.zeros(7, np.uint8), dtype)
 
 
 # ------------------------------------------------------------------ oracle-stepped decomposition
@@ -121,11 +125,11 @@ class OracleStepper:
         t = self.t0 + self.steps * self.dt
         self.steps += 1
         if len(lv) == 0:
-            return Leaves.empty(np.float64)
-        g = pyoracle.MOGrid.from_arrays(lv.origins, lv.masks, lv.phi, self.hw)
+            return Leaves.empty(torch.float64)
+        o, m, p = lv.numpy()
+        g = pyoracle.MOGrid.from_arrays(o, m, p, self.hw)
         assert g.step(self.vel, self.integrator, self.reinit_iters, t, self.dt, nthreads=4)
-        o, m, p = g.arrays()
-        return Leaves(o, m, p)
+        return Leaves.from_numpy(*g.arrays())
 
 
 def _curl_case():
@@ -134,16 +138,14 @@ def _curl_case():
     rng = np.random.default_rng(11)
     sph = np.column_stack([rng.uniform(0, 96, (14, 3)), rng.uniform(4, 12, 14)])
     g = pyoracle.MOGrid.spheres(sph, 3.0)
-    o, m, p = g.arrays()
-    return Leaves(o, m, p), curl_noise(5, 96.0, 1.0), 3, 1.0, 3.0
+    return Leaves.from_numpy(*g.arrays()), curl_noise(5, 96.0, 1.0), 3, 1.0, 3.0
 
 
 def _vortex_case():
     from oracle import pyoracle
     vs = 1.0 / 128
     g = pyoracle.MOGrid.sphere(0.15, (0.35, 0.35, 0.35), vs, 3.0)
-    o, m, p = g.arrays()
-    return Leaves(o, m, p), {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs, 3.0
+    return Leaves.from_numpy(*g.arrays()), {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs, 3.0
 
 
 def _undivided(lv, stepper, steps):
@@ -153,9 +155,10 @@ def _undivided(lv, stepper, steps):
 
 
 def _assert_same(a, b):
-    assert np.array_equal(a.origins, b.origins), (len(a), len(b))
-    assert np.array_equal(a.masks, b.masks)
-    assert np.array_equal(a.phi.view(np.uint8), b.phi.view(np.uint8))
+    (ao, am, ap), (bo, bm, bp) = a.numpy(), b.numpy()
+    assert np.array_equal(ao, bo), (len(ao), len(bo))
+    assert np.array_equal(am, bm)
+    assert np.array_equal(ap.view(np.uint8), bp.view(np.uint8))
 
 
 @pytest.mark.parametrize("world,rebalance", [(2, 0), (3, 2), (4, 1)])
@@ -196,7 +199,7 @@ def _rank_main(rank, world, port, steps, q):
         sls.rebalance()
         sls.step(steps - 2)
         whole = sls.gather()
-        q.put((rank, whole.pack(), len(sls.arrays()), sls.active_voxels()))
+        q.put((rank, whole.numpy(), len(sls.arrays()), sls.active_voxels()))
     finally:
         dist.destroy_process_group()
 
@@ -215,8 +218,8 @@ def test_two_gloo_ranks_match_undivided_oracle(oracle):
         assert p.exitcode == 0
     lv, vel, integ, dt, hw = _curl_case()
     ref = _undivided(lv, OracleStepper(vel, integ, 2, dt, hw), steps)
-    for rank, packed, n_owned, active in out:
-        _assert_same(Leaves.unpack(packed, np.float64), ref)
+    for rank, arrays, n_owned, active in out:
+        _assert_same(Leaves.from_numpy(*arrays), ref)
         assert active == ref.active_voxels()
     assert out[0][2] + out[1][2] == len(ref) and min(out[0][2], out[1][2]) > 0
 
@@ -234,14 +237,14 @@ def _device_case(kind):
         gr = random_sphere_grids(1, seed=17, extent_log2=(7.0, 7.2), spheres=(24, 28), radius=(5.0, 14.0))
         sph, vel, _ = gr[0]
         ls = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=0, integrator=3)
-        o, m, p = ls.arrays()
+        arrays = ls.arrays()
         ls.close()
-        return Leaves(o, m, p), vel, 3, 1.0
+        return arrays, vel, 3, 1.0
     vs = 1.0 / 256
     ls = LevelSet.sphere(0.15, (0.35, 0.35, 0.35), vs, {"kind": "vortex", "vs": vs, "period": 3.0}, 0.5 * vs)
-    o, m, p = ls.arrays()
+    arrays = ls.arrays()
     ls.close()
-    return Leaves(o, m, p), {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs
+    return arrays, {"kind": "vortex", "vs": vs, "period": 3.0}, 2, 0.5 * vs
 
 
 @pytest.mark.gpu
@@ -250,15 +253,12 @@ def _device_case(kind):
                          ids=["curl_f32_2", "curl_f16_3", "curl_f16_2_recreate", "vortex_f16_3_recreate"])
 def test_device_ranks_match_undivided_device_run(ctx, kind, precision, world, recreate):
     from sharc.volrus_b200.method import LevelSet
-    lv, vel, integ, dt = _device_case(kind)
+    (o, m, p), vel, integ, dt = _device_case(kind)
     steps = 6
-    ls = LevelSet.from_leaves(lv.origins, lv.masks, lv.phi, vel, dt, 3.0, precision, integ, 2, 0.0)
-    if precision == 1:  # start both runs from the same FP16-rounded state
-        o, m, p = ls.arrays()
-        lv = Leaves(o, m, p)
+    ls = LevelSet.from_leaves(o, m, p, vel, dt, 3.0, precision, integ, 2, 0.0)
+    o, m, p = ls.arrays()  # the start state as stored (FP16-rounded for FP16 leaves)
     ls.step(steps)
-    o, m, p = ls.arrays()
-    ref = Leaves(o, m, p)
+    ref = Leaves.from_numpy(*ls.arrays())
     ls.close()
     cls = _AlwaysRecreate if recreate else spatial.DeviceStepper
     steppers = []
@@ -268,8 +268,39 @@ def test_device_ranks_match_undivided_device_run(ctx, kind, precision, world, re
         steppers.append(s)
         return s
 
-    got, shards = spatial.emulate(lv, world, make, steps, rebalance_every=3)
+    got, shards = spatial.emulate(Leaves.from_numpy(o, m, p, "cuda"), world, make, steps, rebalance_every=3)
     for s in steppers:
         s.close()
     _assert_same(got, ref)
     assert all(len(s.owned) for s in shards)
+    assert got.device.type == "cuda"
+
+
+@pytest.mark.gpu
+def test_device_upload_download_round_trip_and_errors(ctx):
+    """vlr_ls_upload_device / vlr_ls_download_device: the same leaves back (list
+    order, so compared sorted), an origin off the 8-voxel lattice refused with
+    the context still usable, and a download into too few records refused."""
+    from sharc.volrus_b200._lib import VolrusError
+    from sharc.volrus_b200.method import LevelSet
+    (o, m, p), vel, integ, dt = _device_case("curl")
+    ls = LevelSet.from_leaves(o[:10], m[:10], p[:10], vel, dt, 3.0, 0, integ, 2, 0.0, capacity=2 * len(o))
+    lv = Leaves.from_numpy(o, m, p, "cuda")
+    ls.upload_device(lv.origins.data_ptr(), lv.masks.data_ptr(), lv.phi.data_ptr(), len(lv))
+    out = Leaves(torch.empty((len(lv), 3), dtype=torch.int32, device="cuda"),
+                 torch.empty((len(lv), 8), dtype=torch.int64, device="cuda"),
+                 torch.empty((len(lv), 512), dtype=torch.float32, device="cuda"))
+    n = ls.download_device(out.origins.data_ptr(), out.masks.data_ptr(), out.phi.data_ptr(), len(lv))
+    assert n == len(lv)
+    _assert_same(out.sorted_xyz(), lv.sorted_xyz())
+    with pytest.raises(VolrusError):
+        ls.download_device(out.origins.data_ptr(), out.masks.data_ptr(), out.phi.data_ptr(), len(lv) - 1)
+    bad = lv.origins.clone()
+    bad[3, 1] += 4
+    with pytest.raises(VolrusError):
+        ls.upload_device(bad.data_ptr(), lv.masks.data_ptr(), lv.phi.data_ptr(), len(lv))
+    # the next valid upload restores a usable state
+    ls.upload_device(lv.origins.data_ptr(), lv.masks.data_ptr(), lv.phi.data_ptr(), len(lv))
+    ls.step(1)
+    assert ls.leaf_count() > 0
+    ls.close()
