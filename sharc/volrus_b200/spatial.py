@@ -51,6 +51,7 @@ import numpy as np
 import torch
 
 GHOST_DEPTH = 2  # leaves; derivation in the module docstring
+_CHUNK = 1 << 24  # neighbour coordinates evaluated per batch (bounds the temporaries)
 _BIAS = 1 << 20  # leaf coordinates (origin >> 3) are biased to 21-bit non-negative fields
 _POP8 = torch.tensor([bin(i).count("1") for i in range(256)], dtype=torch.int64)
 
@@ -130,12 +131,14 @@ def _spread(v: torch.Tensor) -> torch.Tensor:
     return x
 
 
-def morton_keys_of_leaf_coords(c: torch.Tensor) -> torch.Tensor:
+def morton_keys_of_leaf_coords(c: torch.Tensor, check: bool = True) -> torch.Tensor:
     """63-bit Z-order keys (i64, non-negative) of leaf coordinates (origin >> 3),
     x in the highest bit of each triple.  Coordinates are biased by 2^20
-    (|origin| < 2^23 voxels)."""
+    (|origin| < 2^23 voxels).  A key grows with each coordinate when the other
+    two are fixed (it is 4 spread(x) + 2 spread(y) + spread(z)), so over a box
+    the smallest and largest keys are those of its low and high corners."""
     c = c.to(torch.int64).reshape(-1, 3) + _BIAS
-    if c.numel() and (int(c.min()) < 0 or int(c.max()) >= (1 << 21)):
+    if check and c.numel() and (int(c.min()) < 0 or int(c.max()) >= (1 << 21)):
         raise ValueError("leaf coordinate outside the 21-bit key range (|origin| >= 2^23 voxels)")
     return (_spread(c[:, 0]) << 2) | (_spread(c[:, 1]) << 1) | _spread(c[:, 2])
 
@@ -188,13 +191,6 @@ def _offsets(d: int, device="cpu") -> torch.Tensor:
     return torch.stack(torch.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
 
 
-def _near_keys(coords: torch.Tensor, d: int) -> torch.Tensor:
-    """Sorted unique keys of every leaf coordinate within Chebyshev distance d of ``coords``."""
-    if len(coords) == 0:
-        return torch.zeros(0, dtype=torch.int64, device=coords.device)
-    return torch.unique(torch.cat([morton_keys_of_leaf_coords(coords + o) for o in _offsets(d, coords.device)]))
-
-
 def _member(keys: torch.Tensor, sorted_set: torch.Tensor) -> torch.Tensor:
     if len(sorted_set) == 0:
         return torch.zeros(len(keys), dtype=torch.bool, device=keys.device)
@@ -213,6 +209,7 @@ class Shard:
         self.check_duplicates = check_duplicates
         self.like = Leaves.empty(owned.phi.dtype, owned.device)
         self.owned = self.like
+        self.owned_keys = torch.zeros(0, dtype=torch.int64, device=owned.device)
         self.absorb([owned])
 
     # phase 1: ghost leaves for the other ranks
@@ -223,14 +220,27 @@ class Shard:
         if self.part.world > 63:
             raise NotImplementedError("more than 63 ranks")
         c = self.owned.coords()
-        bits = torch.zeros(len(c), dtype=torch.int64, device=c.device)
-        for o in _offsets(GHOST_DEPTH, c.device):
-            bits |= torch.bitwise_left_shift(torch.ones_like(bits), self.part.owner(morton_keys_of_leaf_coords(c + o)))
+        d = GHOST_DEPTH
+        # the owners over a leaf's box lie between those of its corner keys (keys
+        # grow along each axis, owners along the keys): leaves whose whole box
+        # is this rank's send nothing
+        lo = self.part.owner(morton_keys_of_leaf_coords(c - d))
+        hi = self.part.owner(morton_keys_of_leaf_coords(c + d))
+        cand = torch.nonzero((lo != self.rank) | (hi != self.rank)).reshape(-1)
         out = {}
-        for q in range(self.part.world):
-            if q == self.rank:
-                continue
-            sel = torch.nonzero((bits >> q) & 1).reshape(-1)
+        if len(cand) == 0:
+            return out
+        offs = _offsets(d, c.device)
+        hits = {q: [] for q in range(self.part.world) if q != self.rank}
+        step = max(1, _CHUNK // len(offs))
+        for i in range(0, len(cand), step):
+            ci = cand[i:i + step]
+            box = (c[ci][:, None, :] + offs[None]).reshape(-1, 3)
+            own = self.part.owner(morton_keys_of_leaf_coords(box, False)).reshape(len(ci), len(offs))
+            for q in hits:
+                hits[q].append(ci[(own == q).any(dim=1)])
+        for q, parts in hits.items():
+            sel = torch.cat(parts)
             if len(sel):
                 out[q] = self.owned.take(sel)
         return out
@@ -241,9 +251,24 @@ class Shard:
 
     # phase 3: exact outputs to the owners of their keys
     def route(self, out: Leaves) -> dict[int, Leaves]:
-        exact = _near_keys(self.owned.coords(), 1)
+        """Outputs within one leaf of an owned input leaf, by the owner of their key:
+        an output that is itself an owned input leaf, or one with an owned
+        input leaf among its 26 neighbours."""
         k = out.keys()
-        sel = torch.nonzero(_member(k, exact)).reshape(-1)
+        exact = _member(k, self.owned_keys)
+        rest = torch.nonzero(~exact).reshape(-1)
+        if len(rest):
+            cr = out.coords()[rest]
+            morton_keys_of_leaf_coords(torch.cat([cr - 1, cr + 1]))  # range check of the whole 3^3 box
+            offs = _offsets(1, k.device)
+            step = max(1, _CHUNK // len(offs))
+            near = []
+            for i in range(0, len(cr), step):
+                box = (cr[i:i + step][:, None, :] + offs[None]).reshape(-1, 3)
+                near.append(_member(morton_keys_of_leaf_coords(box, False), self.owned_keys).reshape(-1, len(offs))
+                            .any(dim=1))
+            exact[rest] = torch.cat(near)
+        sel = torch.nonzero(exact).reshape(-1)
         own = self.part.owner(k[sel])
         return {int(q): out.take(sel[own == q]) for q in torch.unique(own).tolist()}
 
@@ -252,6 +277,7 @@ class Shard:
         allp = Leaves.concat(parts, self.like)
         if len(allp) == 0:
             self.owned = self.like
+            self.owned_keys = torch.zeros(0, dtype=torch.int64, device=self.like.device)
             return
         ks, order = torch.sort(allp.keys(), stable=True)
         first = torch.ones(len(ks), dtype=torch.bool, device=ks.device)
@@ -264,6 +290,7 @@ class Shard:
             if not same:
                 raise AssertionError("a leaf arrived from two ranks with different contents")
         self.owned = allp.take(order[first])
+        self.owned_keys = ks[first]
 
     def migrate(self, part: Partition) -> dict[int, Leaves]:
         """Owned leaves grouped by their owner under a new partition."""
@@ -417,7 +444,7 @@ class DeviceStepper:
             lo, hi = o.min(axis=0) - self.margin, o.max(axis=0) + 7 + self.margin
             vel["domain"] = (tuple(int(v) for v in lo), tuple(int(v) for v in hi))
             self.box = (lo, hi)
-        self.cap = 4 * len(lv) + 4096
+        self.cap = 3 * len(lv) + 4096
         self.ls = LevelSet.from_leaves(o, m, p.astype(np.float32), vel, self.dt, self.hw, self.precision,
                                        self.integrator, self.reinit_iters, self.t0, self.cap, self.reinit_mode,
                                        ctx=self.ctx)
