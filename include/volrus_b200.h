@@ -328,8 +328,11 @@ int vlr_ls_download_device(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* d_ori
 /* The host-resident form of n_steps steps in one call: replace the state with
  * host leaves (as vlr_ls_upload), step, and write the result (as
  * vlr_ls_download) into caller buffers of cap_leaves leaves; *n_out = leaves
- * written.  Waits once for the leaf count and device errors and once for the
- * copies.  No counterpart in the reference (its step is serial Rust). */
+ * written.  The copies of the first min(n_leaves, cap_leaves) records start
+ * before the leaf count is known, so records past *n_out (up to that bound)
+ * may be overwritten; the call then waits once for the count, the device
+ * errors and those copies, and copies any records beyond them.  No
+ * counterpart in the reference (its step is serial Rust). */
 int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
                      size_t n_leaves, int n_steps, int32_t* out_origins, uint64_t* out_masks, float* out_phi,
                      size_t cap_leaves, size_t* n_out);

@@ -847,6 +847,25 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
         k_gather_sel_dev<float><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, ls->scalars, dstatus, ls->mask,
                                                             (const float*)ls->vals[0], mm, v);
     VLR_CUDA(ctx, cudaGetLastError());
+    // copies of the records [lo, hi) of the sorted output into the caller's buffers
+    auto copy_out = [&](size_t lo, size_t hi) -> int {
+        if (hi <= lo) return VLR_OK;
+        const size_t k = hi - lo;
+        if (out_origins)
+            VLR_CUDA(ctx, cudaMemcpyAsync(out_origins + 3 * lo, o3 + 3 * lo, 12 * k, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        if (out_masks)
+            VLR_CUDA(ctx, cudaMemcpyAsync(out_masks + 8 * lo, mm + 8 * lo, 64 * k, cudaMemcpyDeviceToHost, ctx->stream));
+        if (out_phi)
+            VLR_CUDA(ctx, cudaMemcpyAsync(out_phi + kLeafVoxels * lo, v + kLeafVoxels * lo,
+                                          sizeof(float) * kLeafVoxels * k, cudaMemcpyDeviceToHost, ctx->stream));
+        return VLR_OK;
+    };
+    // the output holds about as many leaves as the input: copy that many
+    // before the count is known, so the copies overlap the count's round trip
+    const size_t guess = std::min(std::min(n_leaves, cap_leaves), kv);
+    rc = copy_out(0, guess);
+    if (rc) return rc;
     // leaf count, sort status and device errors in one round trip
     VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(h + 1, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -855,12 +874,9 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     const size_t n = (size_t)h[0];
     if (!h[1]) return download_n(ctx, ls, n, -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
     if (n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
-    if (n) {
-        if (out_origins) VLR_CUDA(ctx, cudaMemcpyAsync(out_origins, o3, 12 * n, cudaMemcpyDeviceToHost, ctx->stream));
-        if (out_masks) VLR_CUDA(ctx, cudaMemcpyAsync(out_masks, mm, 64 * n, cudaMemcpyDeviceToHost, ctx->stream));
-        if (out_phi)
-            VLR_CUDA(ctx, cudaMemcpyAsync(out_phi, v, sizeof(float) * kLeafVoxels * n, cudaMemcpyDeviceToHost,
-                                          ctx->stream));
+    if (n > guess) {
+        rc = copy_out(guess, n);
+        if (rc) return rc;
         VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
     *n_out = n;
