@@ -314,6 +314,13 @@ int vlr_ls_upload(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const
  * capacity, say) and created with the same t0 resumes at the same time, bit for
  * bit, once its counter is set to the old one's.  step >= 0. */
 int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step);
+/* The terms of vlr_ls_volume before their sum: one FP64 partial per
+ * allocated leaf, in the level set's list order (the order of
+ * vlr_ls_download_device, and after an upload the upload's order), into the
+ * device buffer d_partials of cap entries; *n_out = leaves.  A grid divided
+ * over GPUs sums the partials of the leaves each rank owns. */
+int vlr_ls_volume_partials(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* d_partials, size_t cap,
+                           size_t* n_out);
 /* Device-resident forms of vlr_ls_upload and vlr_ls_download, for callers
  * that keep leaves in device memory on the context's device (the exchange of a
  * grid divided over GPUs).  Records as in vlr_ls_upload: origins i32[3] on the

@@ -938,6 +938,29 @@ int vlr_ls_download_device(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* d_ori
     return VLR_OK;
 }
 
+int vlr_ls_volume_partials(vlr_ctx* ctx, vlr_level_set* ls, const double ref[3], double* d_partials,
+                           size_t cap, size_t* n_out) {
+    if (!ctx || !ls || !d_partials || !n_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *n_out = 0;
+    size_t n = 0;
+    int rc = vlr_ls_info(ctx, ls, &n, nullptr, nullptr);
+    if (rc) return rc;
+    if (n > cap) return set_error(ctx, VLR_ERR_CAPACITY, "partials buffer too small");
+    double r[3] = {0, 0, 0};
+    if (ref) std::memcpy(r, ref, sizeof(r));
+    MLeafArrays A = ls->arrays();
+    if (ls->precision == VLR_PREC_F16)
+        k_m_volume<__half><<<ls->grid_blocks, 256, 0, ctx->stream>>>(A, (const __half*)ls->vals[0], ls->d_params,
+                                                                     r[0], r[1], r[2], d_partials);
+    else
+        k_m_volume<float><<<ls->grid_blocks, 256, 0, ctx->stream>>>(A, (const float*)ls->vals[0], ls->d_params, r[0],
+                                                                    r[1], r[2], d_partials);
+    VLR_CUDA(ctx, cudaGetLastError());
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *n_out = n;
+    return VLR_OK;
+}
+
 int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step) {
     if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     if (step < 0) return set_error(ctx, VLR_ERR_INVALID, "step must be >= 0");

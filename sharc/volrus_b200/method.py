@@ -300,6 +300,16 @@ class LevelSet:
                                                            C.byref(k)), "vlr_ls_download_device")
         return k.value
 
+    def volume_partials(self, d_partials: int, cap: int, ref=(0.0, 0.0, 0.0)) -> int:
+        """One FP64 volume term per allocated leaf, in list order, into a device
+        buffer of ``cap`` doubles; returns the leaf count."""
+        r = np.asarray(ref, np.float64)
+        k = C.c_size_t()
+        self.ctx.check(self.ctx.lib.vlr_ls_volume_partials(self.ctx.handle, self.handle, ptr(r, C.c_double),
+                                                           C.c_void_p(d_partials), int(cap), C.byref(k)),
+                       "vlr_ls_volume_partials")
+        return k.value
+
     def set_step(self, step: int):
         """Set the step counter (time = t0 + step * dt): resume a run in a new level set."""
         self.ctx.check(self.ctx.lib.vlr_ls_set_step(self.ctx.handle, self.handle, int(step)), "vlr_ls_set_step")

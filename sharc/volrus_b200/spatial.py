@@ -470,10 +470,34 @@ class DeviceStepper:
                                     self.out.phi.data_ptr(), self.cap)
         return self.out.take(slice(0, n))
 
+    def volume(self, lv: Leaves, n_first: int, ref=(0.0, 0.0, 0.0)) -> float:
+        """FP64 enclosed volume over the first ``n_first`` leaves of ``lv`` (the
+        owned ones; the ghosts after them supply the gradients): the sum of
+        their per-leaf terms (``vlr_ls_volume_partials``) in leaf order."""
+        if n_first == 0:
+            return 0.0
+        if not self._fits(lv):
+            self._create(lv)  # the level set lists leaves in the order given
+        else:
+            lv = Leaves(lv.origins.contiguous(), lv.masks.contiguous(), lv.phi.to(torch.float32).contiguous())
+            torch.cuda.current_stream(lv.device).synchronize()
+            self.ls.upload_device(lv.origins.data_ptr(), lv.masks.data_ptr(), lv.phi.data_ptr(), len(lv))
+        buf = torch.empty(self.cap, dtype=torch.float64, device=lv.device)
+        self.ls.volume_partials(buf.data_ptr(), self.cap, ref)
+        return float(buf[:n_first].sum())
+
     def close(self):
         if self.ls is not None:
             self.ls.close()
             self.ls = None
+
+
+def volume_shards(shards: Sequence[Shard], exchange, ref=(0.0, 0.0, 0.0)) -> list[float]:
+    """Each shard's FP64 volume over its owned leaves, with the ghost ring
+    exchanged first so the gradients at the range edges are the undivided
+    grid's.  The stepper must provide ``volume(leaves, n_owned, ref)``."""
+    ghosts = exchange([s.ghost_sends() for s in shards])
+    return [s.stepper.volume(Leaves.concat([s.owned, *g], s.like), len(s.owned), ref) for s, g in zip(shards, ghosts)]
 
 
 def split(leaves: Leaves, world: int) -> tuple[Partition, list[Leaves]]:
@@ -527,6 +551,11 @@ class SpatialLevelSet:
         s = self.shard
         (parts,) = self.ex([{q: s.owned for q in range(self.ex.world)}])
         return Leaves.concat(parts, s.like).sorted_xyz()
+
+    def volume(self, ref=(0.0, 0.0, 0.0)) -> float:
+        """FP64 enclosed volume of the whole grid: the ranks' sums added in rank order."""
+        (v,) = volume_shards([self.shard], self.ex, ref)
+        return float(sum(float(t[0]) for t in self.ex.all_gather_1d(torch.tensor([v], dtype=torch.float64))))
 
     def active_voxels(self) -> int:
         return int(sum(int(t[0]) for t in self.ex.all_gather_1d(

@@ -269,11 +269,17 @@ def test_device_ranks_match_undivided_device_run(ctx, kind, precision, world, re
         return s
 
     got, shards = spatial.emulate(Leaves.from_numpy(o, m, p, "cuda"), world, make, steps, rebalance_every=3)
-    for s in steppers:
-        s.close()
     _assert_same(got, ref)
     assert all(len(s.owned) for s in shards)
     assert got.device.type == "cuda"
+    # FP64 volume: the ranks' owned-leaf sums against the undivided level set's
+    ls = LevelSet.from_leaves(*ref.numpy(), vel, dt, 3.0, precision, integ, 2, 0.0)
+    v_ref = ls.volume((1.0, 2.0, 3.0))
+    ls.close()
+    v = sum(spatial.volume_shards(shards, spatial.LocalExchange(), (1.0, 2.0, 3.0)))
+    assert abs(v - v_ref) <= 1e-12 * abs(v_ref), (v, v_ref)
+    for s in steppers:
+        s.close()
 
 
 @pytest.mark.gpu
