@@ -529,7 +529,10 @@ class SpatialLevelSet:
     Every rank passes the same global leaves (on its own device; each keeps
     only its share) and a stepper for its device (``DeviceStepper``);
     ``step`` runs decomposed steps, ``arrays`` returns the owned leaves,
-    ``gather`` the whole grid on every rank."""
+    ``gather`` the whole grid on every rank.  With NCCL, each process sets its
+    device (``torch.cuda.set_device``) before the process group is used; the
+    first transfer of a group is an all_gather that every rank joins, so the
+    point-to-point batches that follow may leave a rank out."""
 
     def __init__(self, leaves: Leaves, stepper: Callable[[Leaves], Leaves], group=None,
                  check_duplicates: bool = False):
