@@ -17,6 +17,8 @@ from __future__ import annotations
 import enum
 from dataclasses import dataclass, field
 
+import math
+
 import numpy as np
 
 from . import _lib
@@ -43,6 +45,10 @@ class VoxelTransform:
     def with_origin(voxel_size: float, origin) -> "VoxelTransform":
         return VoxelTransform(float(voxel_size), tuple(float(o) for o in origin))
 
+    @staticmethod
+    def identity() -> "VoxelTransform":
+        return VoxelTransform(1.0, (0.0, 0.0, 0.0))
+
     def index_to_world(self, c):
         return tuple(c[i] * self.voxel_size + self.origin[i] for i in range(3))
 
@@ -50,30 +56,123 @@ class VoxelTransform:
         inv = 1.0 / self.voxel_size
         return tuple((w[i] - self.origin[i]) * inv for i in range(3))
 
+    def world_to_index(self, w):
+        """Nearest index, halves away from zero (src/grid.rs:103-110)."""
+        return tuple(_round_i32(f) for f in self.world_to_index_f64(w))
+
+
+def _round_i32(f: float) -> int:
+    """Rust's ``f.round() as i32``: halves away from zero, then a saturating
+    cast (NaN -> 0)."""
+    if f != f:
+        return 0
+    r = math.floor(f + 0.5) if f >= 0.0 else -math.floor(-f + 0.5)
+    return int(min(max(r, -2 ** 31), 2 ** 31 - 1))
+
+
+def invert_4x4(m) -> np.ndarray:
+    """Inverse of a 4x4 matrix by the Laplace expansion in 2x2 minors of rows
+    (0, 1) and (2, 3): the adjugate's entries are sums of three products of an
+    entry and a minor, scaled by 1/det (the method of src/grid.rs:301-345, so
+    the bits match the crate's)."""
+    m = [[float(v) for v in r] for r in np.asarray(m, np.float64).reshape(4, 4)]
+    s = [m[0][0] * m[1][1] - m[1][0] * m[0][1], m[0][0] * m[1][2] - m[1][0] * m[0][2],
+         m[0][0] * m[1][3] - m[1][0] * m[0][3], m[0][1] * m[1][2] - m[1][1] * m[0][2],
+         m[0][1] * m[1][3] - m[1][1] * m[0][3], m[0][2] * m[1][3] - m[1][2] * m[0][3]]
+    c = [m[2][0] * m[3][1] - m[3][0] * m[2][1], m[2][0] * m[3][2] - m[3][0] * m[2][2],
+         m[2][0] * m[3][3] - m[3][0] * m[2][3], m[2][1] * m[3][2] - m[3][1] * m[2][2],
+         m[2][1] * m[3][3] - m[3][1] * m[2][3], m[2][2] * m[3][3] - m[3][2] * m[2][3]]
+    det = s[0] * c[5] - s[1] * c[4] + s[2] * c[3] + s[3] * c[2] - s[4] * c[1] + s[5] * c[0]
+    if not abs(det) > 1e-30:
+        raise ValueError("singular matrix")
+    k = 1.0 / det
+    a = [[(m[1][1] * c[5] - m[1][2] * c[4] + m[1][3] * c[3]), (-m[0][1] * c[5] + m[0][2] * c[4] - m[0][3] * c[3]),
+          (m[3][1] * s[5] - m[3][2] * s[4] + m[3][3] * s[3]), (-m[2][1] * s[5] + m[2][2] * s[4] - m[2][3] * s[3])],
+         [(-m[1][0] * c[5] + m[1][2] * c[2] - m[1][3] * c[1]), (m[0][0] * c[5] - m[0][2] * c[2] + m[0][3] * c[1]),
+          (-m[3][0] * s[5] + m[3][2] * s[2] - m[3][3] * s[1]), (m[2][0] * s[5] - m[2][2] * s[2] + m[2][3] * s[1])],
+         [(m[1][0] * c[4] - m[1][1] * c[2] + m[1][3] * c[0]), (-m[0][0] * c[4] + m[0][1] * c[2] - m[0][3] * c[0]),
+          (m[3][0] * s[4] - m[3][1] * s[2] + m[3][3] * s[0]), (-m[2][0] * s[4] + m[2][1] * s[2] - m[2][3] * s[0])],
+         [(-m[1][0] * c[3] + m[1][1] * c[1] - m[1][2] * c[0]), (m[0][0] * c[3] - m[0][1] * c[1] + m[0][2] * c[0]),
+          (-m[3][0] * s[3] + m[3][1] * s[1] - m[3][2] * s[0]), (m[2][0] * s[3] - m[2][1] * s[1] + m[2][2] * s[0])]]
+    return np.array([[v * k for v in r] for r in a], np.float64)
+
 
 @dataclass
 class AffineMap:
     """Forward rows of the 4x4 ``AffineMap`` (src/grid.rs:131-296)."""
     mat: np.ndarray = field(default_factory=lambda: np.eye(3, 4, dtype=np.float64))
     voxel_size: float = 1.0
+    # rows of the inverse as the crate stores them at construction (None:
+    # computed from ``mat`` by invert_4x4, as for a general map)
+    inv: np.ndarray | None = None
 
     @staticmethod
     def from_uniform_scale(s: float) -> "AffineMap":
         m = np.zeros((3, 4), np.float64)
         m[0, 0] = m[1, 1] = m[2, 2] = s
-        return AffineMap(m, float(s))
+        i = np.zeros((3, 4), np.float64)
+        i[0, 0] = i[1, 1] = i[2, 2] = 1.0 / float(s)
+        return AffineMap(m, float(s), i)
 
     @staticmethod
     def from_voxel_transform(vt: VoxelTransform) -> "AffineMap":
         m = np.zeros((3, 4), np.float64)
         m[0, 0] = m[1, 1] = m[2, 2] = vt.voxel_size
         m[:, 3] = vt.origin
-        return AffineMap(m, float(vt.voxel_size))
+        inv_s = 1.0 / float(vt.voxel_size)
+        i = np.zeros((3, 4), np.float64)
+        i[0, 0] = i[1, 1] = i[2, 2] = inv_s
+        i[:, 3] = [-float(t) * inv_s for t in vt.origin]
+        return AffineMap(m, float(vt.voxel_size), i)
+
+    @staticmethod
+    def identity() -> "AffineMap":
+        return AffineMap(np.eye(3, 4, dtype=np.float64), 1.0, np.eye(3, 4, dtype=np.float64))
+
+    @staticmethod
+    def from_scale_rotate_translate(scale, rotation, translate) -> "AffineMap":
+        """Forward = T R S (src/grid.rs:205-234); voxel size = length of the
+        linear part's first column."""
+        m = np.zeros((3, 4), np.float64)
+        for r in range(3):
+            for c in range(3):
+                m[r, c] = float(rotation[r][c]) * float(scale[c])
+            m[r, 3] = float(translate[r])
+        vs = math.sqrt(m[0, 0] * m[0, 0] + m[1, 0] * m[1, 0] + m[2, 0] * m[2, 0])
+        a = AffineMap(m, vs)
+        a.inv = a.inverse()[:3].copy()
+        return a
+
+    def forward(self) -> np.ndarray:
+        """The 4x4 index-to-world matrix."""
+        f = np.zeros((4, 4), np.float64)
+        f[:3] = self.mat
+        f[3, 3] = 1.0
+        return f
+
+    def inverse(self) -> np.ndarray:
+        """The 4x4 world-to-index matrix, as the crate holds it."""
+        if self.inv is None:
+            return invert_4x4(self.forward())
+        i = np.zeros((4, 4), np.float64)
+        i[:3] = self.inv
+        i[3, 3] = 1.0
+        return i
 
     def index_to_world(self, c):
         x, y, z = (float(v) for v in c)
         m = self.mat
         return tuple(m[r, 0] * x + m[r, 1] * y + m[r, 2] * z + m[r, 3] for r in range(3))
+
+    def world_to_index_f64(self, w):
+        """Continuous index of a world position through the inverse (src/grid.rs:268-277)."""
+        x, y, z = (float(v) for v in w)
+        i = self.inverse()
+        return tuple(i[r, 0] * x + i[r, 1] * y + i[r, 2] * z + i[r, 3] for r in range(3))
+
+    def world_to_index(self, w):
+        """Nearest index, halves away from zero (src/grid.rs:261-264)."""
+        return tuple(_round_i32(f) for f in self.world_to_index_f64(w))
 
 
 def _leaf_origin(c):
@@ -106,6 +205,14 @@ class Grid:
         g = cls(float(np.float32(half_width * voxel_size)), voxel_size)
         g.name = "sdf"
         g.grid_class = GridClass.LEVEL_SET
+        return g
+
+    @classmethod
+    def with_affine(cls, background: float, map: AffineMap) -> "Grid":
+        """``Grid::with_affine`` (src/grid.rs:378-388): the uniform transform
+        takes the map's voxel size and no translation."""
+        g = cls(background, map.voxel_size)
+        g.affine = map
         return g
 
     @classmethod
@@ -169,6 +276,14 @@ class Grid:
             return False
         off = _offset(c)
         return bool((int(self._m[row, off >> 6]) >> (off & 63)) & 1)
+
+    def get_world(self, pos) -> float:
+        """Value at the voxel nearest a world position, through the affine map (src/grid.rs:494-497)."""
+        return self.get(self.affine.world_to_index(pos))
+
+    def set_world(self, pos, value: float):
+        """Set the voxel nearest a world position (src/grid.rs:500-503)."""
+        self.set(self.affine.world_to_index(pos), value)
 
     def set(self, c, value: float):
         row = self._leaf_row(c, True)

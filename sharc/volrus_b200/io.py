@@ -19,7 +19,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import Context
-from .grid import Grid, GridClass
+from .grid import AffineMap, Grid, GridClass
 from .tools import DeviceGrid
 
 
@@ -74,6 +74,8 @@ class NanoGrid:
         ctx = g.ctx
         k = int(g.grid_class if grid_class is None else grid_class)
         inv = None
+        if affine_inv is None and isinstance(getattr(grid, "affine", None), AffineMap):
+            affine_inv = grid.affine.inverse()[:3]  # the inverse the crate's map holds
         if affine_inv is not None:
             inv_a = np.ascontiguousarray(np.asarray(affine_inv, np.float64).reshape(-1)[:12])
             inv = inv_a.ctypes.data_as(C.POINTER(C.c_double))

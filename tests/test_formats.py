@@ -264,3 +264,26 @@ def test_device_vol_round_trip_deformation_sphere(ctx, oracle, tmp_path):
     assert p.stat().st_size == pf.VOL_HEADER + d.leaf_count() * pf.VOL_LEAF
     back = load_vol(str(p), ctx)
     _same(back.download(), d.download())
+
+
+@pytest.mark.gpu
+def test_device_nano_from_host_grid_with_rotated_affine(ctx):
+    """A host grid built with ``Grid::with_affine`` over a rotated, scaled,
+    translated map writes the inverse the crate's map holds (its 4x4
+    cofactor inverse, src/grid.rs:205-234, 301-345) into the NanoGrid header,
+    byte for byte as the oracle writer given that inverse."""
+    from sharc.volrus_b200.grid import AffineMap, invert_4x4
+    from sharc.volrus_b200.io import NanoGrid
+    rot = [[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]]
+    am = AffineMap.from_scale_rotate_translate((0.5, 0.5, 0.5), rot, (100.0, -50.0, 25.0))
+    g = Grid.with_affine(0.0, am)
+    for c in ((1, 2, 3), (-9, 0, 17), (40, -33, 5)):
+        g.set(c, float(sum(c)))
+    got = NanoGrid.from_grid(g).as_bytes()
+    inv = invert_4x4(am.forward())[:3]
+    assert np.array_equal(pf.nano_header(got)["affine_inv"][:3], inv)
+    assert got == pf.nano_from_grid(g, affine_inv=inv)
+    # a uniform map's inverse is 1 / voxel size exactly, as the crate stores it
+    u = Grid.with_affine(0.0, AffineMap.from_uniform_scale(0.3))
+    u.set((0, 0, 0), 1.0)
+    assert pf.nano_header(NanoGrid.from_grid(u).as_bytes())["affine_inv"][0][0] == 1.0 / 0.3
