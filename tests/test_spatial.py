@@ -180,6 +180,20 @@ def test_emulated_ranks_match_undivided_oracle_vortex(oracle):
     _assert_same(got, ref)
 
 
+def test_emulated_ranks_some_owning_nothing(oracle):
+    """More ranks than leaves: empty ranks step nothing, send and receive
+    nothing, and may own leaves after a step or a rebalance."""
+    from oracle import pyoracle
+    g = pyoracle.MOGrid.spheres(np.array([[20.0, 20.0, 20.0, 4.0]]), 3.0)
+    lv = Leaves.from_numpy(*g.arrays())
+    vel = {"kind": "constant", "c": (0.7, 0.3, -0.2)}
+    ref = _undivided(lv, OracleStepper(vel, 1, 2, 1.0, 3.0), 3)
+    for world in (9, 40):
+        got, shards = spatial.emulate(lv, world, lambda r: OracleStepper(vel, 1, 2, 1.0, 3.0), 3, 1)
+        _assert_same(got, ref)
+        assert world <= len(lv) or any(len(s.owned) == 0 for s in shards)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
