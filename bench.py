@@ -775,6 +775,101 @@ def bench_mesh_line(args, ctx, peak, peak_kind):
             "volume_to_mesh": m}
 
 
+TOOLS = dict(radius=160.0, center=(0.5, -0.25, 0.125), voxel_size=1.0, half_width=3.0, particles=1 << 20)
+
+
+def bench_tools_line(args, ctx, peak, peak_kind):
+    """The crate's other tools on one sphere (radius 160 voxels, half-width 3),
+    each call timed on the device (CUDA events on the library stream, L2
+    flushed before it, a fresh copy of the input for the in-place tools):
+    find_zero_crossings, trim and rebuild_narrow_band, dilate (1 iteration),
+    flood_fill_sign, extend_velocity (half-width 3), volume_to_mesh, the .vol
+    and NanoGrid writers and readers, and the RK4 particle update (2^20
+    particles in the band).  Rates are the input's active voxels (particles
+    for the update) per second of device time; `value` is the median over
+    the grid tools."""
+    import numpy as np
+    import torch
+
+    from sharc.volrus_b200 import (DeviceGrid, VelocityField, dilate, extend_velocity, find_zero_crossings,
+                                   flood_fill_sign, make_level_set_sphere, make_uniform_velocity, rebuild_narrow_band,
+                                   trim_narrow_band, volume_to_mesh)
+    from sharc.volrus_b200.io import NanoGrid, read_vol, write_vol
+    from sharc.volrus_b200.tools import advect_particles
+
+    dev = torch.device("cuda", args.device)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sph = {k: TOOLS[k] for k in ("radius", "center", "voxel_size", "half_width")}
+    host = make_level_set_sphere(**sph, ctx=ctx)
+    n_active, n_leaves = host.active_voxel_count(), host.leaf_count()
+    vel = make_uniform_velocity(1.0, (0.5, -0.25, 1.0))
+    dvel = VelocityField(*[DeviceGrid.upload(c, ctx) for c in (vel.vx, vel.vy, vel.vz)])
+    vol_bytes = write_vol(host)
+    nano = NanoGrid.from_grid(host).as_bytes()
+    rng = np.random.default_rng(5)
+    o, m, _ = host.to_arrays()
+    pts = (o[rng.integers(0, len(o), TOOLS["particles"])] + rng.uniform(0, 8, (TOOLS["particles"], 3))).astype(
+        np.float64)
+
+    def timed(fn, fresh=None, reps=None):
+        reps = reps or max(3, min(args.steps, 10))
+        ts = []
+        for r in range(reps + 1):
+            arg = fresh() if fresh else None
+            ctx.synchronize()
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            out = fn(arg)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            ctx.synchronize()
+            if r:  # the first call warms up
+                ts.append(e0.elapsed_time(e1))
+            for x in (arg, out):
+                if isinstance(x, DeviceGrid):
+                    x.close()
+        return statistics.median(ts)
+
+    fresh = lambda: DeviceGrid.upload(host, ctx)
+    res = {}
+    with ClockSampler(args.device) as clk, clk.mark():
+        res["find_zero_crossings"] = timed(lambda g: find_zero_crossings(g, ctx=ctx), fresh)
+        res["trim_narrow_band"] = timed(lambda g: trim_narrow_band(g, 2.0, ctx=ctx), fresh)
+        res["rebuild_narrow_band"] = timed(lambda g: rebuild_narrow_band(g, 3.0, ctx=ctx), fresh)
+        res["dilate"] = timed(lambda g: dilate(g, 1, ctx=ctx), fresh)
+        res["flood_fill_sign"] = timed(lambda g: flood_fill_sign(g, ctx=ctx), fresh)
+        ext = lambda: [DeviceGrid.upload(host, ctx) for _ in range(4)]
+
+        def run_ext(gs):
+            extend_velocity(*gs, 3.0, ctx=ctx)
+            for g in gs:
+                g.close()
+        res["extend_velocity"] = timed(run_ext, ext)
+        res["volume_to_mesh"] = timed(lambda g: volume_to_mesh(g, 0.0, ctx=ctx), fresh)
+        res["write_vol"] = timed(lambda g: write_vol(g), fresh)
+        res["read_vol"] = timed(lambda _: read_vol(vol_bytes, ctx))
+        res["nano_from_grid"] = timed(lambda g: NanoGrid.from_grid(g), fresh)
+        res["nano_to_grid"] = timed(lambda _: NanoGrid.from_bytes(nano).to_grid(ctx))
+        t_part = timed(lambda _: advect_particles(pts, dvel, 1.0, ctx=ctx))
+    grid_rates = {k: n_active / (v * 1e-3) for k, v in res.items()}
+    value = statistics.median(grid_rates.values())
+    return {"metric": "active voxels/s per tool call (median over the grid tools)", "value": value,
+            "unit": "voxels/s", "ms_per_step": statistics.median(res.values()), "dtype": "f32",
+            "config": {"workload": "tools160", "leaves": n_leaves, "active_voxels": n_active,
+                       "sphere": sph, "particles": TOOLS["particles"],
+                       "l2": "flushed before every call (256 MiB write outside the call's events)",
+                       "timing": "CUDA events on the library stream around the public call; host copies "
+                                 "of the crate-facing calls (crossing list, .vol and NanoGrid bytes, particle "
+                                 "positions) are inside the events"},
+            "roofline": None, "e2e": None, "clocks": clk.summary(), "gpu_launches": None, "kernels_ms_per_launch": {},
+            "tools_ms_per_call": res, "tools_voxels_per_s": grid_rates,
+            "advect_particles": {"ms_per_call": t_part, "particles_per_s": TOOLS["particles"] / (t_part * 1e-3),
+                                 "integrator": "RK4 through three uniform velocity grids"}}
+
+
 def bench_deformation(args, ctx, peak, peak_kind):
     import torch
     from sharc.volrus_b200.method import F16, F32
@@ -931,7 +1026,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["deformation512", "batched256", "large8192", "adjoint256",
-                                           "reference-sphere128", "mesh96"],
+                                           "reference-sphere128", "mesh96", "tools160"],
                     default="deformation512")
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--large-spheres", type=int, default=LARGE["spheres"], help="spheres of the large single grid")
@@ -1028,6 +1123,8 @@ def main():
         res = bench_large_line(args, ctx, peak, peak_kind)
     elif args.workload == "mesh96":
         res = bench_mesh_line(args, ctx, peak, peak_kind)
+    elif args.workload == "tools160":
+        res = bench_tools_line(args, ctx, peak, peak_kind)
     else:
         res = bench_ref_sphere(args, ctx, peak, peak_kind)
     value = res["value"]
@@ -1063,7 +1160,7 @@ def main():
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
         for k in ("issue_roofline", "fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint",
-                  "volume_to_mesh"):
+                  "volume_to_mesh", "tools_ms_per_call", "tools_voxels_per_s", "advect_particles"):
             if k in res and res[k] is None:
                 continue
             if k in res:

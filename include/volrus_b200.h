@@ -163,8 +163,9 @@ int vlr_sample_trilinear(vlr_ctx* ctx, const vlr_grid* g, const double* world_xy
 int vlr_advect_level_set(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, const vlr_grid* vy,
                          const vlr_grid* vz, double dt, vlr_grid** out);
 
-/* find_zero_crossings (src/tools/level_set_track.rs:14-47): writes up to cap
- * coordinates (int32[3] each, sorted (x, y, z)) and the total count. */
+/* find_zero_crossings (src/tools/level_set_track.rs:14-47): writes the first
+ * cap coordinates (int32[3] each) of the crossing list sorted (x, y, z), and
+ * the total count.  A cap of the grid's active voxel count holds them all. */
 int vlr_find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* coords, size_t cap, size_t* count);
 
 /* trim_narrow_band (src/tools/level_set_track.rs:53-68), in place. */

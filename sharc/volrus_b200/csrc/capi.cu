@@ -278,9 +278,10 @@ int vlr_advect_level_set(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, co
 int vlr_find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* coords, size_t cap, size_t* count) {
     if (!ctx || !g || !count) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     if (g->kind != VLR_KIND_F32_WORLD) return set_error(ctx, VLR_ERR_INVALID, "grid is not a world-unit f32 grid");
-    int rc = find_zero_crossings(ctx, g, coords, cap, count);
+    bool sorted = false;
+    int rc = find_zero_crossings(ctx, g, coords, cap, count, &sorted);
     if (rc) return rc;
-    if (coords && cap) {
+    if (coords && cap && !sorted) {  // keys over 63 bits: sort on the host
         size_t m = std::min(cap, *count);
         std::vector<size_t> order(m);
         std::iota(order.begin(), order.end(), 0);

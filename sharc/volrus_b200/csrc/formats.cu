@@ -331,16 +331,36 @@ int vlr_grid_to_nano(vlr_ctx* ctx, const vlr_grid* g, int grid_class, const doub
     if (rc) return rc;
     // active bounding box, (0, 0, 0) for a grid without active voxels
     int32_t lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+    // per leaf from its mask words (offset x * 64 + y * 8 + z): word x is the
+    // x-plane, the bytes of the words' OR are the y-rows, the OR of those
+    // bytes the z-columns
     for (size_t i = 0; i < n; ++i) {
         const unsigned char* r = b + kNanoHeader + i * kNanoLeaf;
-        for (int off = 0; off < 512; ++off) {
-            if (!((rd<uint64_t>(r + 16 + 8 * (off >> 6)) >> (off & 63)) & 1u)) continue;
-            const int32_t c[3] = {rd<int32_t>(r) + (off >> 6), rd<int32_t>(r + 4) + ((off >> 3) & 7),
-                                  rd<int32_t>(r + 8) + (off & 7)};
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = std::min(lo[a], c[a]);
-                hi[a] = std::max(hi[a], c[a]);
-            }
+        uint64_t any = 0;
+        int x0 = 8, x1 = -1;
+        for (int x = 0; x < 8; ++x) {
+            const uint64_t w = rd<uint64_t>(r + 16 + 8 * x);
+            if (!w) continue;
+            any |= w;
+            x0 = std::min(x0, x);
+            x1 = x;
+        }
+        if (!any) continue;
+        int y0 = 8, y1 = -1;
+        unsigned zb = 0;
+        for (int y = 0; y < 8; ++y) {
+            const unsigned row = (unsigned)(any >> (8 * y)) & 0xFFu;
+            if (!row) continue;
+            zb |= row;
+            y0 = std::min(y0, y);
+            y1 = y;
+        }
+        const int z0 = __builtin_ctz(zb), z1 = 31 - __builtin_clz(zb);
+        const int32_t o[3] = {rd<int32_t>(r), rd<int32_t>(r + 4), rd<int32_t>(r + 8)};
+        const int l3[3] = {x0, y0, z0}, h3[3] = {x1, y1, z1};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], o[a] + l3[a]);
+            hi[a] = std::max(hi[a], o[a] + h3[a]);
         }
     }
     if (lo[0] == INT32_MAX)

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "ref_ops.hpp"
+#include "sort_reduce.hpp"
 
 namespace vlr {
 
@@ -441,7 +442,101 @@ static int alloc_cross(vlr_ctx* ctx, int n, CrossBufs& b) {
     return VLR_OK;
 }
 
-int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size_t cap, size_t* count) {
+// Crossing-list sort on the device: the bounding box of the coordinates, then
+// (x, y, z)-major keys of their offsets to it, sorted by two stable 32-bit
+// radix passes (low word, then high word) that carry the list index.
+__global__ void k_cross_box(const int* __restrict__ c, int n, int* __restrict__ box) {
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = min(lo[a], c[3 * i + a]);
+            hi[a] = max(hi[a], c[3 * i + a]);
+        }
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = __reduce_min_sync(0xffffffffu, lo[a]);
+        hi[a] = __reduce_max_sync(0xffffffffu, hi[a]);
+    }
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&box[a], lo[a]);
+            atomicMax(&box[3 + a], hi[a]);
+        }
+}
+
+__global__ void k_cross_keys(const int* __restrict__ c, int n, int bx, int by, int bz, int bits,
+                             uint64_t* __restrict__ keys, unsigned* __restrict__ lo, unsigned* __restrict__ idx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t k = ((uint64_t)(unsigned)(c[3 * i] - bx) << (2 * bits)) |
+                           ((uint64_t)(unsigned)(c[3 * i + 1] - by) << bits) | (uint64_t)(unsigned)(c[3 * i + 2] - bz);
+        keys[i] = k;
+        lo[i] = (unsigned)k;
+        idx[i] = (unsigned)i;
+    }
+}
+
+__global__ void k_cross_hi(const uint64_t* __restrict__ keys, const unsigned* __restrict__ idx, int n,
+                           unsigned* __restrict__ hi) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        hi[i] = (unsigned)(keys[idx[i]] >> 32);
+}
+
+__global__ void k_cross_gather(const int* __restrict__ c, const unsigned* __restrict__ idx, int n,
+                               int* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x)
+        out[i] = c[3 * idx[i / 3] + i % 3];
+}
+
+// Sorts the n crossing coordinates d_c into d_out by (x, y, z) on the device;
+// *sorted = false (nothing written) when the box needs keys over 63 bits.
+static int sort_crossings_device(vlr_ctx* ctx, const int* d_c, int n, int* d_out, bool* sorted) {
+    *sorted = false;
+    cudaStream_t st = ctx->stream;
+    const size_t sort_bytes = sort_reduce_scratch_bytes(n);
+    char* buf = nullptr;
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&buf, (size_t)n * 20 + sort_bytes + 256, ctx->pool, st));
+    auto done = [&](int code) {
+        cudaFreeAsync(buf, st);
+        return code;
+    };
+    char* p = buf;
+    uint64_t* keys = (uint64_t*)p;  p += (size_t)n * 8;
+    unsigned* lo = (unsigned*)p;  p += (size_t)n * 4;
+    unsigned* idx = (unsigned*)p;  p += (size_t)n * 4;
+    unsigned* hi = (unsigned*)p;  p += (size_t)n * 4;
+    int* box = (int*)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    void* scratch = (void*)(((uintptr_t)(box + 8) + 15) & ~(uintptr_t)15);
+    const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    int* hb = static_cast<int*>(ctx->pinned) + 32;
+    std::memcpy(hb, init, sizeof(init));
+    VLR_CUDA(ctx, cudaMemcpyAsync(box, hb, sizeof(init), cudaMemcpyHostToDevice, st));
+    const int blocks = ctx->sm_count * 8;
+    k_cross_box<<<blocks, 256, 0, st>>>(d_c, n, box);
+    VLR_CUDA(ctx, cudaMemcpyAsync(hb, box, sizeof(init), cudaMemcpyDeviceToHost, st));
+    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+    int bits = 0;
+    for (int a = 0; a < 3; ++a) {
+        const long long ext = (long long)hb[3 + a] - hb[a];
+        while (bits < 40 && (1ll << bits) <= ext) ++bits;
+    }
+    if (3 * bits > 63) return done(VLR_OK);
+    k_cross_keys<<<blocks, 256, 0, st>>>(d_c, n, hb[0], hb[1], hb[2], bits, keys, lo, idx);
+    unsigned *k1, *v1, *k2, *v2;
+    int rc = radix_sort_pairs(ctx, lo, idx, n, 0xffffffffu, scratch, &k1, &v1);
+    if (rc) return done(rc);
+    k_cross_hi<<<blocks, 256, 0, st>>>(keys, v1, n, hi);
+    if (v1 != idx) VLR_CUDA(ctx, cudaMemcpyAsync(idx, v1, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+    rc = radix_sort_pairs(ctx, hi, idx, n, 0x7fffffffu, scratch, &k2, &v2);
+    if (rc) return done(rc);
+    (void)k1;
+    (void)k2;
+    k_cross_gather<<<blocks, 256, 0, st>>>(d_c, v2, n, d_out);
+    VLR_CUDA(ctx, cudaGetLastError());
+    *sorted = true;
+    return done(VLR_OK);
+}
+
+int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size_t cap, size_t* count,
+                        bool* sorted) {
     *count = 0;
     if (g->n == 0) return VLR_OK;
     CrossBufs b;
@@ -455,18 +550,23 @@ int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size
         rc = scan_exclusive(ctx, b.xcount, b.pos, g->n, b.pos + g->n);
         if (rc) return rc;
         int* d_coords = nullptr;
-        VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_coords, sizeof(int) * 3 * total, ctx->pool, ctx->stream));
+        VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_coords, sizeof(int) * 6 * total, ctx->pool, ctx->stream));
         k_emit_crossings<<<g->n, 512, 0, ctx->stream>>>(make_view(g), b.xmask, b.pos, d_coords);
         VLR_CUDA(ctx, cudaGetLastError());
-        std::vector<int32_t> all(3 * total);
-        VLR_CUDA(ctx, cudaMemcpyAsync(all.data(), d_coords, sizeof(int) * 3 * total, cudaMemcpyDeviceToHost,
-                                      ctx->stream));
+        // emitted leaf by leaf (leaves in (x, y, z) order, voxels ZYX), which
+        // is not the global (x, y, z) order: sorted on the device when the
+        // keys fit 63 bits, else by the caller on the host
+        bool dev_sorted = false;
+        if (sorted) {
+            rc = sort_crossings_device(ctx, d_coords, (int)total, d_coords + 3 * total, &dev_sorted);
+            if (rc) return rc;
+        }
+        const int* src = dev_sorted ? d_coords + 3 * total : d_coords;
+        size_t m = std::min<size_t>(cap, total);
+        VLR_CUDA(ctx, cudaMemcpyAsync(h_coords, src, sizeof(int) * 3 * m, cudaMemcpyDeviceToHost, ctx->stream));
         VLR_CUDA(ctx, cudaFreeAsync(d_coords, ctx->stream));
         VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        // Leaves are kept in (x, y, z) order and bits in ZYX order, so the
-        // emitted list is already sorted (x, y, z).
-        size_t m = std::min<size_t>(cap, total);
-        std::memcpy(h_coords, all.data(), sizeof(int32_t) * 3 * m);
+        if (sorted) *sorted = dev_sorted;
     }
     VLR_CUDA(ctx, cudaFreeAsync(b.xmask, ctx->stream));
     return VLR_OK;

@@ -10,7 +10,10 @@ GridView make_view(const vlr_grid* g);
 int advect_ref(vlr_ctx* ctx, const vlr_grid* g, const vlr_grid* vx, const vlr_grid* vy, const vlr_grid* vz, double dt,
                vlr_grid* out);
 int sample_points(vlr_ctx* ctx, const vlr_grid* g, const double* h_pts, size_t n, float* h_out);
-int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size_t cap, size_t* count);
+// The crossings in (x, y, z) order when *sorted comes back true (sorted on the
+// device); in emission order (leaf by leaf) when it is false or null.
+int find_zero_crossings(vlr_ctx* ctx, const vlr_grid* g, int32_t* h_coords, size_t cap, size_t* count,
+                        bool* sorted = nullptr);
 int trim_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int rebuild_narrow_band(vlr_ctx* ctx, vlr_grid* g, float half_width);
 int make_sphere(vlr_ctx* ctx, double radius, const double c[3], double vs, double hw, vlr_grid* out);

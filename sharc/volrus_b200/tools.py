@@ -143,12 +143,12 @@ def find_zero_crossings(grid, ctx: Context | None = None) -> np.ndarray:
     ctx = ctx or (grid.ctx if isinstance(grid, DeviceGrid) else Context.default())
     g, _ = _as_device(grid, ctx)
     cnt = C.c_size_t()
-    ctx.check(ctx.lib.vlr_find_zero_crossings(ctx.handle, g.handle, None, 0, C.byref(cnt)), "vlr_find_zero_crossings")
-    out = np.zeros((cnt.value, 3), np.int32)
-    if cnt.value:
-        ctx.check(ctx.lib.vlr_find_zero_crossings(ctx.handle, g.handle, ptr(out, C.c_int32), cnt.value,
-                                                  C.byref(cnt)), "vlr_find_zero_crossings")
-    return out
+    # a crossing is an active voxel: one call with room for all of them
+    cap = g.active_voxel_count()
+    out = np.empty((max(cap, 1), 3), np.int32)
+    ctx.check(ctx.lib.vlr_find_zero_crossings(ctx.handle, g.handle, ptr(out, C.c_int32), cap, C.byref(cnt)),
+              "vlr_find_zero_crossings")
+    return out[: cnt.value].copy()
 
 
 def trim_narrow_band(grid, half_width: float, ctx: Context | None = None):
