@@ -212,20 +212,20 @@ STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_
 # profiles/stencils_deformation512_full.md (2,853 leaves) and
 # profiles/stencils_batched256_subset48_full.md (151,238 leaves).
 TRAFFIC_PER_LEAF: dict = {
-    ("deformation512", "k_m_advect", 2): 3531264 / 2850,
-    ("deformation512", "k_m_reinit", 2): 3519744 / 2850,
-    ("batched256", "k_m_advect", 2): (192670464 + 161785856) / 151238,
-    ("batched256", "k_m_reinit", 2): (194985984 + 136462080) / 151238,
+    ("deformation512", "k_m_advect", 2): 3531264 / 2853,
+    ("deformation512", "k_m_reinit", 2): 3518464 / 2853,
+    ("batched256", "k_m_advect", 2): (191877632 + 158914816) / 151238,
+    ("batched256", "k_m_reinit", 2): (194146816 + 136635904) / 151238,
 }
 
 
 # Warp instructions per leaf of one launch (smsp__inst_executed.sum / leaves)
 # from the same ncu captures, FP16, 128-thread CTAs.
 INST_PER_LEAF: dict = {
-    ("deformation512", "k_m_advect"): 12154621 / 2850,
-    ("deformation512", "k_m_reinit"): 17443240 / 2850,
-    ("batched256", "k_m_advect"): 1063617820 / 151238,
-    ("batched256", "k_m_reinit"): 864912635 / 151238,
+    ("deformation512", "k_m_advect"): 12236456 / 2853,
+    ("deformation512", "k_m_reinit"): 16721413 / 2853,
+    ("batched256", "k_m_advect"): 1064426333 / 151238,
+    ("batched256", "k_m_reinit"): 821863623 / 151238,
 }
 SM_COUNT = 148
 ISSUE_PER_SM_PER_CYCLE = 4  # one warp instruction per scheduler per cycle

@@ -302,64 +302,50 @@ __global__ void k_gather_sel(const int* list, const int* sel, int k, const uint6
 }
 
 // Output order of a host step without a host round trip: for up to
-// kDevSortLeaves listed leaves of a single grid, one CTA sorts their (x, y, z)
-// keys (bitonic sort in shared memory; keys are leaf coordinates relative to
-// the grid's hash base, bits each, so their order is the lexicographic order
-// of the origins) and writes the sorted list positions and origins.  More
-// leaves: *status = 0 and the host sorts instead.
+// kDevSortLeaves listed leaves of a single grid, their (x, y, z) keys (leaf
+// coordinates relative to the grid's hash base, bits each, so key order is
+// the lexicographic order of the origins) are ranked on the device: a leaf's
+// rank is the number of smaller keys (the keys are distinct: origins are
+// unique), counted by kRankLanes lanes per leaf across the whole GPU, and the
+// leaf's list position and origin are written at its rank.  More leaves:
+// *status = 0 and the host sorts instead.
 constexpr int kDevSortLeaves = 8192;
-constexpr size_t kDevSortSmem = (size_t)kDevSortLeaves * (8 + 2);
+constexpr int kRankLanes = 4;
 
-__global__ void __launch_bounds__(1024) k_sort_small(const int* __restrict__ list, const int* __restrict__ count,
-                                                    const int4* __restrict__ origin, long long b0, long long b1,
-                                                    long long b2, int bits, int* __restrict__ sel,
-                                                    int32_t* __restrict__ o3, int* __restrict__ status) {
-    extern __shared__ unsigned long long s_key[];
-    unsigned short* s_idx = reinterpret_cast<unsigned short*>(s_key + kDevSortLeaves);
+__global__ void k_rank_keys(const int* __restrict__ list, const int* __restrict__ count,
+                            const int4* __restrict__ origin, long long b0, long long b1, long long b2, int bits,
+                            unsigned long long* __restrict__ keys, int* __restrict__ status) {
     const int n = *count;
-    if (n > kDevSortLeaves) {
-        if (threadIdx.x == 0) *status = 0;
-        return;
-    }
-    int N = 1;
-    while (N < n) N <<= 1;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        unsigned long long key = ~0ull;
-        if (i < n) {
-            const int4 o = origin[list[i]];
-            key = ((unsigned long long)((o.x >> 3) - b0) << (2 * bits)) |
+    if (blockIdx.x == 0 && threadIdx.x == 0) *status = (n <= kDevSortLeaves) ? 1 : 0;
+    if (n > kDevSortLeaves) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 o = origin[list[i]];
+        keys[i] = ((unsigned long long)((o.x >> 3) - b0) << (2 * bits)) |
                   ((unsigned long long)((o.y >> 3) - b1) << bits) | (unsigned long long)((o.z >> 3) - b2);
-        }
-        s_key[i] = key;
-        s_idx[i] = (unsigned short)i;
     }
-    __syncthreads();
-    for (int k = 2; k <= N; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < N; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = s_key[i], b = s_key[l];
-                    if (((i & k) == 0) ? (a > b) : (a < b)) {
-                        s_key[i] = b;
-                        s_key[l] = a;
-                        const unsigned short t = s_idx[i];
-                        s_idx[i] = s_idx[l];
-                        s_idx[l] = t;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int p = s_idx[i];
-        sel[i] = p;
-        const int4 o = origin[list[p]];
-        o3[3 * i] = o.x;
-        o3[3 * i + 1] = o.y;
-        o3[3 * i + 2] = o.z;
+}
+
+__global__ void __launch_bounds__(256) k_rank_scatter(const int* __restrict__ list, const int* __restrict__ count,
+                                                      const int4* __restrict__ origin,
+                                                      const unsigned long long* __restrict__ keys,
+                                                      int* __restrict__ sel, int32_t* __restrict__ o3) {
+    const int n = *count;
+    if (n > kDevSortLeaves) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((t & ~31) / kRankLanes >= n) return;  // whole warps past the last leaf
+    const int i = t / kRankLanes, s = t % kRankLanes;
+    const unsigned long long ki = i < n ? keys[i] : 0ull;
+    int less = 0;
+    for (int j = s; j < n; j += kRankLanes) less += (__ldg(&keys[j]) < ki) ? 1 : 0;
+#pragma unroll
+    for (int d = 1; d < kRankLanes; d <<= 1) less += __shfl_xor_sync(0xffffffffu, less, d);
+    if (s == 0 && i < n) {
+        sel[less] = i;
+        const int4 o = origin[list[i]];
+        o3[3 * less] = o.x;
+        o3[3 * less + 1] = o.y;
+        o3[3 * less + 2] = o.z;
     }
-    if (threadIdx.x == 0) *status = 1;
 }
 
 // k_gather_sel with the count and the sort status read on the device.
@@ -812,7 +798,7 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     // staging for the device-sorted download (sized first, so the upload
     // never regrows it while its copies are in flight)
     const size_t kv = (size_t)kDevSortLeaves;
-    const size_t dl_bytes = kv * (sizeof(float) * kLeafVoxels + 64 + 12 + 4) + 256;
+    const size_t dl_bytes = kv * (sizeof(float) * kLeafVoxels + 64 + 12 + 4 + 8) + 256;
     void* stg = nullptr;
     int rc = ls_staging(ctx, ls, std::max(dl_bytes, sizeof(float) * kLeafVoxels * n_leaves + 12 * n_leaves + 16),
                         &stg);
@@ -835,10 +821,12 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     int32_t* o3 = (int32_t*)((char*)mm + kv * 64);
     int* dsel = (int*)((char*)o3 + kv * 12);
     int* dstatus = (int*)((char*)dsel + kv * 4);
-    VLR_CUDA(ctx, cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDevSortSmem));
+    unsigned long long* dkeys = reinterpret_cast<unsigned long long*>(((uintptr_t)(dstatus + 4) + 15) & ~(uintptr_t)15);
     const vlr::MGridParams& P = ls->h_params[0];
-    k_sort_small<<<1, 1024, kDevSortSmem, ctx->stream>>>(ls->list, ls->scalars, ls->origin, P.base[0], P.base[1],
-                                                          P.base[2], ls->key_bits, dsel, o3, dstatus);
+    k_rank_keys<<<ctx->sm_count, 256, 0, ctx->stream>>>(ls->list, ls->scalars, ls->origin, P.base[0], P.base[1],
+                                                        P.base[2], ls->key_bits, dkeys, dstatus);
+    k_rank_scatter<<<kDevSortLeaves * kRankLanes / 256, 256, 0, ctx->stream>>>(ls->list, ls->scalars, ls->origin,
+                                                                               dkeys, dsel, o3);
     const int B = ctx->sm_count * 8;
     if (ls->precision == VLR_PREC_F16)
         k_gather_sel_dev<__half><<<B, 256, 0, ctx->stream>>>(ls->list, dsel, ls->scalars, dstatus, ls->mask,
