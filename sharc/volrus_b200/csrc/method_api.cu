@@ -310,7 +310,7 @@ __global__ void k_gather_sel(const int* list, const int* sel, int k, const uint6
 // leaf's list position and origin are written at its rank.  More leaves:
 // *status = 0 and the host sorts instead.
 constexpr int kDevSortLeaves = 8192;
-constexpr int kRankLanes = 4;
+constexpr int kRankLanes = 16;
 
 __global__ void k_rank_keys(const int* __restrict__ list, const int* __restrict__ count,
                             const int4* __restrict__ origin, long long b0, long long b1, long long b2, int bits,
@@ -336,6 +336,7 @@ __global__ void __launch_bounds__(256) k_rank_scatter(const int* __restrict__ li
     const int i = t / kRankLanes, s = t % kRankLanes;
     const unsigned long long ki = i < n ? keys[i] : 0ull;
     int less = 0;
+#pragma unroll 4
     for (int j = s; j < n; j += kRankLanes) less += (__ldg(&keys[j]) < ki) ? 1 : 0;
 #pragma unroll
     for (int d = 1; d < kRankLanes; d <<= 1) less += __shfl_xor_sync(0xffffffffu, less, d);
