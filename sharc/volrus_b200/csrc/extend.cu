@@ -29,6 +29,15 @@ using namespace vlr;
 namespace {
 
 constexpr int kMaxLocal = 4096;  // interface voxels held per 27-leaf neighbourhood
+constexpr int kBuckets = 24;     // 1-voxel distance shells around the leaf centre (a candidate is < 20 away)
+
+// Shell of a candidate (local coordinates packed as in s_cand): the floor of
+// its distance from the leaf centre (3.5, 3.5, 3.5).
+__device__ __forceinline__ int ev_bucket(unsigned e) {
+    const int cx = 2 * ((int)(e & 31u) - 8) - 7, cy = 2 * ((int)((e >> 5) & 31u) - 8) - 7,
+              cz = 2 * ((int)(e >> 10) - 8) - 7;
+    return min((int)(0.5f * sqrtf((float)(cx * cx + cy * cy + cz * cz))), kBuckets - 1);
+}
 
 __device__ __forceinline__ bool ev_key_less(int ax, int ay, int az, int bx, int by, int bz) {
     const int sh[3] = {7, 3, 0};
@@ -87,6 +96,8 @@ __global__ void __launch_bounds__(256) k_ev_search(const int4* __restrict__ orig
                                                    int4* __restrict__ dst, int4* __restrict__ src,
                                                    int* __restrict__ fb_list, int* __restrict__ fb_count) {
     __shared__ unsigned s_cand[kMaxLocal];  // (x+8) | (y+8) << 5 | (z+8) << 10, local to the leaf
+    __shared__ unsigned s_sorted[kMaxLocal];  // the same, grouped by shell
+    __shared__ int s_start[kBuckets + 1], s_cur[kBuckets];
     __shared__ int s_n;
     __shared__ uint64_t s_b[8];
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
@@ -115,6 +126,30 @@ __global__ void __launch_bounds__(256) k_ev_search(const int4* __restrict__ orig
         __syncthreads();
         const int nc = min(s_n, kMaxLocal);
         const bool overflow = s_n > kMaxLocal;
+        // group the candidates by shell: a voxel at distance r from the centre
+        // is at least b - r from every candidate of shell b, so once that
+        // bound exceeds its best distance the later shells cannot win (the
+        // winner is the minimum by (distance, key), whatever the visit order)
+        if (threadIdx.x < kBuckets) s_cur[threadIdx.x] = 0;
+        __syncthreads();
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) atomicAdd(&s_cur[ev_bucket(s_cand[c])], 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int b = 0; b < kBuckets; ++b) {
+                const int h = s_cur[b];
+                s_start[b] = acc;
+                s_cur[b] = acc;
+                acc += h;
+            }
+            s_start[kBuckets] = acc;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+            const unsigned e = s_cand[c];
+            s_sorted[atomicAdd(&s_cur[ev_bucket(e)], 1)] = e;
+        }
+        __syncthreads();
         const int4 o = origin[i];
         for (int off = threadIdx.x; off < kLeafVoxels; off += blockDim.x) {
             const int q = off >> 6, bit = off & 63;
@@ -123,15 +158,23 @@ __global__ void __launch_bounds__(256) k_ev_search(const int4* __restrict__ orig
             for (int qq = 0; qq < q; ++qq) rank += __popcll(s_b[qq]);
             const int x = q, y = bit >> 3, z = bit & 7;
             int best = INT_MAX, bx = 0, by = 0, bz = 0;
-            for (int c = 0; c < nc; ++c) {
-                const unsigned e = s_cand[c];
-                const int cx = (int)(e & 31u) - 8, cy = (int)((e >> 5) & 31u) - 8, cz = (int)(e >> 10) - 8;
-                const int d2 = (cx - x) * (cx - x) + (cy - y) * (cy - y) + (cz - z) * (cz - z);
-                if (d2 < best || (d2 == best && ev_key_less(o.x + cx, o.y + cy, o.z + cz, o.x + bx, o.y + by, o.z + bz))) {
-                    best = d2;
-                    bx = cx;
-                    by = cy;
-                    bz = cz;
+            const float rv = 0.5f * sqrtf((float)((2 * x - 7) * (2 * x - 7) + (2 * y - 7) * (2 * y - 7) +
+                                                  (2 * z - 7) * (2 * z - 7)));
+            for (int b = 0; b < kBuckets; ++b) {
+                // 0.01 voxel of slack covers the rounding of the shell index
+                const float lb = (float)b - 0.01f - rv;
+                if (lb > 0.f && lb * lb > (float)best) break;
+                for (int c = s_start[b]; c < s_start[b + 1]; ++c) {
+                    const unsigned e = s_sorted[c];
+                    const int cx = (int)(e & 31u) - 8, cy = (int)((e >> 5) & 31u) - 8, cz = (int)(e >> 10) - 8;
+                    const int d2 = (cx - x) * (cx - x) + (cy - y) * (cy - y) + (cz - z) * (cz - z);
+                    if (d2 < best ||
+                        (d2 == best && ev_key_less(o.x + cx, o.y + cy, o.z + cz, o.x + bx, o.y + by, o.z + bz))) {
+                        best = d2;
+                        bx = cx;
+                        by = cy;
+                        bz = cz;
+                    }
                 }
             }
             const int p = boff[i] + rank;
@@ -215,44 +258,50 @@ int vlr_extend_velocity(vlr_ctx* ctx, const vlr_grid* sdf, vlr_grid* vx, vlr_gri
     VLR_CUDA(ctx, cudaMemcpyAsync(bc.data(), d_bcount, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     VLR_CUDA(ctx, cudaMemcpyAsync(org.data(), sdf->origin, sizeof(int4) * n, cudaMemcpyDeviceToHost, st));
     VLR_CUDA(ctx, cudaStreamSynchronize(st));
-    // the interface list (for searches that leave the 27-leaf neighbourhood)
-    std::vector<int4> iface;
-    for (int i = 0; i < n; ++i)
-        for (int q = 0; q < 8; ++q)
-            for (uint64_t w = im[8ull * i + q]; w; w &= w - 1) {
-                const int bit = __builtin_ctzll(w);
-                iface.push_back(make_int4(org[i].x + q, org[i].y + (bit >> 3), org[i].z + (bit & 7), 0));
-            }
+    bool any_iface = false;
+    for (size_t k = 0; k < im.size() && !any_iface; ++k) any_iface = im[k] != 0;
     std::vector<int> boff(n);
     long long nb = 0;
     for (int i = 0; i < n; ++i) {
         boff[i] = (int)nb;
         nb += bc[i];
     }
-    if (iface.empty() || nb == 0) {  // no interface: nothing changes (level_set_track.rs:138-140)
+    if (!any_iface || nb == 0) {  // no interface: nothing changes (level_set_track.rs:138-140)
         VLR_CUDA(ctx, cudaFreeAsync(d_imask, st));
         return VLR_OK;
     }
     if (nb > INT32_MAX / 2) return set_error(ctx, VLR_ERR_CAPACITY, "too many band voxels");
     VLR_CUDA(ctx, cudaMemcpyAsync(d_boff, boff.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
-    int4 *d_dst = nullptr, *d_iface = nullptr;
-    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_dst, sizeof(int4) * (2 * nb + iface.size()) + sizeof(int) * (nb + 1),
-                                          ctx->pool, st));
+    int4* d_dst = nullptr;
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_dst, sizeof(int4) * 2 * nb + sizeof(int) * (nb + 1), ctx->pool, st));
     int4* d_src = d_dst + nb;
-    d_iface = d_src + nb;
-    int* d_fb = reinterpret_cast<int*>(d_iface + iface.size());
+    int* d_fb = reinterpret_cast<int*>(d_src + nb);
     int* d_fbn = d_fb + nb;
     VLR_CUDA(ctx, cudaMemsetAsync(d_fbn, 0, sizeof(int), st));
-    VLR_CUDA(ctx, cudaMemcpyAsync(d_iface, iface.data(), sizeof(int4) * iface.size(), cudaMemcpyHostToDevice, st));
     k_ev_search<<<B, 256, 0, st>>>(sdf->origin, sdf->nbr, n, d_imask, d_bmask, d_boff, d_dst, d_src, d_fb, d_fbn);
     VLR_CUDA(ctx, cudaGetLastError());
     int n_fb = 0;
     VLR_CUDA(ctx, cudaMemcpyAsync(&n_fb, d_fbn, sizeof(int), cudaMemcpyDeviceToHost, st));
     VLR_CUDA(ctx, cudaStreamSynchronize(st));
     if (n_fb > 0) {
+        // the whole interface list, only for the voxels whose search left the
+        // 27-leaf neighbourhood (or whose neighbourhood overflowed)
+        std::vector<int4> iface;
+        for (int i = 0; i < n; ++i)
+            for (int q = 0; q < 8; ++q)
+                for (uint64_t w = im[8ull * i + q]; w; w &= w - 1) {
+                    const int bit = __builtin_ctzll(w);
+                    iface.push_back(make_int4(org[i].x + q, org[i].y + (bit >> 3), org[i].z + (bit & 7), 0));
+                }
+        int4* d_iface = nullptr;
+        VLR_CUDA(ctx, cudaMallocFromPoolAsync(&d_iface, sizeof(int4) * iface.size(), ctx->pool, st));
+        VLR_CUDA(ctx, cudaMemcpyAsync(d_iface, iface.data(), sizeof(int4) * iface.size(), cudaMemcpyHostToDevice, st));
         k_ev_brute<<<std::max(1, std::min((n_fb + 127) / 128, ctx->sm_count * 8)), 128, 0, st>>>(
             d_iface, (int)iface.size(), d_fb, n_fb, d_dst, d_src);
         VLR_CUDA(ctx, cudaGetLastError());
+        VLR_CUDA(ctx, cudaFreeAsync(d_iface, st));
+        // the host list must outlive its copy
+        VLR_CUDA(ctx, cudaStreamSynchronize(st));
     }
     // leaves of the band voxels, added to each velocity grid where missing
     std::vector<int32_t> band_leaves;
