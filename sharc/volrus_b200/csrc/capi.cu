@@ -149,6 +149,9 @@ void vlr_ctx_destroy(vlr_ctx* ctx) {
     cudaFree(ctx->scratch);
     cudaFree(ctx->d_errword);
     cudaFreeHost(ctx->pinned);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
+    for (auto& e : ctx->stage_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;

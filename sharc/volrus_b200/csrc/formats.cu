@@ -169,9 +169,7 @@ int grid_to_records(vlr_ctx* ctx, const vlr_grid* g, unsigned char* out, size_t 
     k_pack_records<<<warp_blocks(ctx, (long long)n), 256, 0, ctx->stream>>>(
         g->origin, g->mask, (const float*)g->values, (int)n, d_rec, stride, o_off, m_off, v_off, pad_off);
     VLR_CUDA(ctx, cudaGetLastError());
-    VLR_CUDA(ctx, cudaMemcpyAsync(out, d_rec, n * stride, cudaMemcpyDeviceToHost, ctx->stream));
-    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return VLR_OK;
+    return d2h_copy(ctx, out, d_rec, n * stride);
 }
 
 vlr_transform uniform_transform(double vs) {

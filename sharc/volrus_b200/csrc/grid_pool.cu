@@ -96,6 +96,41 @@ int timer_collect(vlr_ctx* ctx) {
     return VLR_OK;
 }
 
+int d2h_copy(vlr_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    constexpr size_t kChunk = 4u << 20;
+    cudaStream_t st = ctx->stream;
+    if (!bytes) return VLR_OK;
+    cudaPointerAttributes at{};
+    const bool pinned_dst = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a pageable pointer may leave an error behind on older drivers
+    if (pinned_dst || bytes < 2 * kChunk) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        VLR_CUDA(ctx, cudaStreamSynchronize(st));
+        return VLR_OK;
+    }
+    if (!ctx->stage) {
+        VLR_CUDA(ctx, cudaMallocHost(&ctx->stage, 2 * kChunk));
+        for (int b = 0; b < 2; ++b) VLR_CUDA(ctx, cudaEventCreateWithFlags(&ctx->stage_ev[b], cudaEventDisableTiming));
+    }
+    char* stage = static_cast<char*>(ctx->stage);
+    char* out = static_cast<char*>(dst);
+    const char* in = static_cast<const char*>(src);
+    const size_t n = (bytes + kChunk - 1) / kChunk;
+    for (size_t k = 0; k <= n; ++k) {
+        if (k < n) {  // half k & 1 was emptied by the host copy of chunk k - 2
+            const size_t len = std::min(kChunk, bytes - k * kChunk);
+            VLR_CUDA(ctx, cudaMemcpyAsync(stage + (k & 1) * kChunk, in + k * kChunk, len, cudaMemcpyDeviceToHost, st));
+            VLR_CUDA(ctx, cudaEventRecord(ctx->stage_ev[k & 1], st));
+        }
+        if (k > 0) {
+            const size_t j = k - 1, len = std::min(kChunk, bytes - j * kChunk);
+            VLR_CUDA(ctx, cudaEventSynchronize(ctx->stage_ev[j & 1]));
+            std::memcpy(out + j * kChunk, stage + (j & 1) * kChunk, len);
+        }
+    }
+    return VLR_OK;
+}
+
 int consume_device_errors(vlr_ctx* ctx, const char* what) {
     unsigned* h = (unsigned*)ctx->pinned;
     VLR_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_errword, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));

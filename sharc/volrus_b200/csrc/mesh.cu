@@ -602,12 +602,18 @@ int volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float iso, double* h_verts, 
                   k_mc_emit<<<m, 512, 0, st>>>(gv, th, tb, tiles, iso, g->xf.voxel_size, words, vbase, tbase,
                                                d_verts, d_tris));
         const size_t cv = std::min<size_t>(cap_v, (size_t)tot[0]), ct = std::min<size_t>(cap_t, (size_t)tot[1]);
-        if (h_verts && cv) ce = cudaMemcpyAsync(h_verts, d_verts, cv * 24, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess && h_tris && ct) ce = cudaMemcpyAsync(h_tris, d_tris, ct * 12, cudaMemcpyDeviceToHost, st);
+        ce = cudaGetLastError();
+        if (ce != cudaSuccess) {
+            cudaFreeAsync(d_verts, st);
+            cudaFreeAsync(d_tris, st);
+            return done2(check_cuda(ctx, ce, "volume_to_mesh output"));
+        }
+        int rc2 = VLR_OK;
+        if (h_verts && cv) rc2 = d2h_copy(ctx, h_verts, d_verts, cv * 24);
+        if (!rc2 && h_tris && ct) rc2 = d2h_copy(ctx, h_tris, d_tris, ct * 12);
         cudaFreeAsync(d_verts, st);
         cudaFreeAsync(d_tris, st);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-        if (ce != cudaSuccess) return done2(check_cuda(ctx, ce, "volume_to_mesh output"));
+        if (rc2) return done2(rc2);
         rc = consume_device_errors(ctx, "volume_to_mesh");
         if (rc) return done2(rc);
     }

@@ -32,6 +32,8 @@ struct vlr_ctx {
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     void* pinned = nullptr;             // small pinned host buffer for scalar read-backs
+    void* stage = nullptr;              // pinned double buffer for large copies into pageable memory
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     vlr_kernel_timer timer;
 };
 
@@ -92,6 +94,11 @@ int ctx_scratch(vlr_ctx* ctx, size_t bytes, void** out);
 int scan_exclusive(vlr_ctx* ctx, const int* d_in, int* d_out, int n, int* d_total);
 // Read the device error word, clear it, and map it to a status.
 int consume_device_errors(vlr_ctx* ctx, const char* what);
+// Device-to-host copy of `bytes` on the context stream, returning after it.
+// Large copies into pageable memory go through a pinned double buffer (the
+// DMA of one chunk overlaps the host copy of the previous one), twice the
+// driver's own pageable rate here; small or pinned destinations take one copy.
+int d2h_copy(vlr_ctx* ctx, void* dst, const void* src, size_t bytes);
 int read_int(vlr_ctx* ctx, const int* d_ptr, int* out);
 
 // Kernel timing: bracket a launch with timer_begin/timer_end (no-ops unless
