@@ -34,7 +34,9 @@ enum {
     VLR_ERR_REACH = 5,     /* a backtrace left the staged neighbourhood (time step too large) */
     VLR_ERR_NOMEM = 6,     /* device allocation failed */
     VLR_ERR_FORMAT = 7,    /* malformed flat-grid buffer */
-    VLR_ERR_TIMEOUT = 8,   /* a bounded device-side wait gave up */
+    VLR_ERR_TIMEOUT = 8,   /* a bounded device-side wait gave up; the operation's outputs (a level set's
+                              state included) are undefined: synchronise the context and upload or
+                              re-create the level set before stepping it again */
     VLR_ERR_UNSUPPORTED = 9
 };
 

@@ -144,7 +144,7 @@ int vlr_ctx_create(int device, vlr_ctx** out) {
 
 void vlr_ctx_destroy(vlr_ctx* ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->device);
+    vlr::DeviceGuard guard(ctx->device);  // the caller's current device is restored on return
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->scratch);
     cudaFree(ctx->d_errword);

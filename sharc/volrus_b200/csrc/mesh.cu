@@ -176,7 +176,8 @@ int ensure_tables(vlr_ctx* ctx) {
     std::lock_guard<std::mutex> lock(g_mc_mu);
     if (!g_mc_ready[dev]) {
         const McTable& t = mc_table();
-        VLR_CUDA(ctx, cudaSetDevice(dev));
+        DeviceGuard guard(dev);
+        VLR_CUDA(ctx, guard.status);
         VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_tri, t.tri, sizeof(t.tri)));
         VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_ntri, t.ntri, sizeof(t.ntri)));
         VLR_CUDA(ctx, cudaMemcpyToSymbol(c_mc_nb, t.nb, sizeof(t.nb)));

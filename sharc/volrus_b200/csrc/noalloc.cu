@@ -15,14 +15,20 @@
 //     rejected with VLR_ERR_CAPACITY.  The array is 4.5 MiB and every GPU
 //     that loads the library holds it until the process exits.
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) and caches it; make that first call before any
-//     stream capture begins.
+//     (cudaGetSymbolAddress, with that device made current and the caller's
+//     current device restored afterwards) and caches it together with the
+//     device's CUDA context; make that first call before any stream capture
+//     begins.  If the context changes later (a cudaDeviceReset by the host
+//     application or another library), the next call looks the address up
+//     again instead of writing through a stale pointer.
 //   * every call on a device shares the one array, which keeps the previous
 //     call's contents: the counter that must start at zero is cleared on each
 //     call.  Calls whose kernels overlap on the GPU (two contexts or streams
 //     on the same device) race on the array and must be serialised by the
 //     caller.
 #include <mutex>
+
+#include <cuda.h>
 
 #include "vlr_host.hpp"
 
@@ -39,22 +45,53 @@ constexpr size_t kScratchBytes = kTotalSlot + kXmaskBytes + 2 * kCountBytes;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_mu;
-void* g_scratch_addr[128] = {};  // device address of g_noalloc_scratch, per device ordinal
+struct ScratchSlot {
+    void* addr = nullptr;    // device address of g_noalloc_scratch
+    CUcontext cu = nullptr;  // the device's context when the address was resolved
+};
+ScratchSlot g_scratch[128];  // per device ordinal
 
-// Looks up (once per device, with that device current) the device address of
-// the scratch array; host code may not use the symbol itself as a pointer.
+using PFN_ctx_get_current = CUresult (*)(CUcontext*);
+
+// cuCtxGetCurrent from the driver (through the runtime, so the library links
+// only cudart); null if the driver does not offer it.
+PFN_ctx_get_current ctx_get_current() {
+    static PFN_ctx_get_current fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_ctx_get_current>(f);
+    }();
+    return fn;
+}
+
+// Device address of the scratch array on the context's device.  Host code
+// may not use the symbol itself as a pointer, so the address is looked up
+// with cudaGetSymbolAddress with that device current, then cached with the
+// device's CUDA context; a changed context (device reset) is looked up anew.
+// The calling thread's current device is restored before returning.
 int scratch_address(vlr_ctx* ctx, unsigned char** out) {
     int dev = ctx->device;
     if (dev < 0 || dev >= 128) return set_error(ctx, VLR_ERR_INVALID, "device ordinal out of range");
+    PFN_ctx_get_current get_cur = ctx_get_current();
+    if (!get_cur) return set_error(ctx, VLR_ERR_CUDA, "cuCtxGetCurrent is not available from the driver");
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        VLR_CUDA(ctx, cudaSetDevice(dev));
+    DeviceGuard guard(dev);
+    VLR_CUDA(ctx, guard.status);
+    CUcontext cu = nullptr;
+    if (get_cur(&cu) != CUDA_SUCCESS || !cu)
+        return set_error(ctx, VLR_ERR_CUDA, "no CUDA context is current on the library's device");
+    ScratchSlot& s = g_scratch[dev];
+    if (!s.addr || s.cu != cu) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return check_cuda(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_scratch_addr[dev] = p;
+        s.addr = p;
+        s.cu = cu;
     }
-    *out = (unsigned char*)g_scratch_addr[dev];
+    *out = (unsigned char*)s.addr;
     return VLR_OK;
 }
 

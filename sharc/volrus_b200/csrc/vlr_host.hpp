@@ -68,6 +68,41 @@ struct vlr_grid {
 
 namespace vlr {
 
+// Makes `device` current for a scope and restores the calling thread's
+// previous current device on exit (also on early returns), so a one-time
+// per-device set-up does not change which device the caller works on.
+struct DeviceGuard {
+    int prev = -1;
+    int dev = -1;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceGuard(int device) : dev(device) {
+        status = cudaGetDevice(&prev);
+        if (status == cudaSuccess && prev != dev) status = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
+// Device temporaries of one host function: each pointer registered with
+// track() is freed (cudaFree, which waits for the work using it) when the
+// holder goes out of scope, on every return path, so an early error return
+// leaks nothing.
+struct DeviceTemps {
+    std::vector<void*> ptrs;
+    template <typename P>
+    P* track(P* p) {
+        ptrs.push_back((void*)p);
+        return p;
+    }
+    ~DeviceTemps() {
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+    }
+};
+
 // Error helpers: record a message on the context and return a status.
 int set_error(vlr_ctx* ctx, int code, const std::string& msg);
 int check_cuda(vlr_ctx* ctx, cudaError_t e, const char* what);

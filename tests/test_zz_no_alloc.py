@@ -5,9 +5,12 @@ device memory when they need the crossings (inside a stream capture, in a
 real-time loop, or when another allocator owns the device memory).  It keeps
 its scratch in one fixed device array shared by all calls, so this test calls
 it twice in a row on different grids through the C ABI and checks each
-result against ``vlr_find_zero_crossings`` (exact: both are integer
-coordinates), which also shows that the second call does not see the first
-call's leftovers.  The file name makes pytest collect it last.
+result against ``vlr_find_zero_crossings`` and against the CPU oracle's
+restatement of the crate's ``find_zero_crossings`` on the same leaves (exact:
+all are integer coordinates), which also shows that the second call does not
+see the first call's leftovers.  It also checks that a call leaves the
+calling thread's current device unchanged.  The file name makes pytest
+collect it last.
 """
 import ctypes as C
 
@@ -42,11 +45,19 @@ def test_noalloc_matches_regular_entry_point_twice_in_a_row():
     big = make_level_set_sphere(32.0, (64.0, 64.0, 64.0), 1.0, 3.0, ctx=ctx, device=True)
     small = advect_level_set(make_level_set_sphere(9.0, (-3.0, 5.0, 1.5), 0.5, 3.0, ctx=ctx, device=True),
                              make_uniform_velocity(0.5, (0.3, -0.2, 0.7)), 1.0)
+    import torch
+    from oracle import pyoracle
     for g in (big, small):
         ref = find_zero_crossings(g)
+        host = g.download()
+        o, m, v = host.to_arrays()
+        og = pyoracle.OGrid.from_arrays(o, m, v, host.background, host.transform.voxel_size)
+        dev_before = torch.cuda.current_device()
         got, n = crossings_noalloc(ctx, g, len(ref) + 16)
+        assert torch.cuda.current_device() == dev_before
         assert n == len(ref) > 0
         assert np.array_equal(sorted_rows(got), ref)
+        assert np.array_equal(sorted_rows(got), sorted_rows(og.zero_crossings()))
 
 
 def test_noalloc_reports_total_beyond_cap_and_rejects_large_grids():
