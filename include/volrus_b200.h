@@ -110,17 +110,16 @@ int vlr_flood_fill_sign(vlr_ctx* ctx, vlr_grid* g);
  * i-th edge crossing first met in the reference's visit order (tiles in
  * ascending origin, cells x-major), interpolated from that cell's first edge
  * endpoint.  Triangles (3 vertex indices) follow per cell in visit order from
- * this library's own triangulation table (vlr_mc_triangle_table), which
- * differs from the reference's classic table in the diagonals of some
- * polygons.  *n_vertices and *n_triangles are always set; up to cap_vertices
- * vertices and cap_triangles triangles are copied (pass null buffers to
- * count only).  World-unit f32 grids only. */
+ * the crate's own triangle table (src/tools/volume_to_mesh.rs:246-503, returned
+ * by vlr_mc_triangle_table), so both lists equal the crate's.  *n_vertices
+ * and *n_triangles are always set; up to cap_vertices vertices and
+ * cap_triangles triangles are copied (pass null buffers to count only).  World-unit f32 grids only. */
 int vlr_volume_to_mesh(vlr_ctx* ctx, const vlr_grid* g, float isovalue, double* vertices, size_t cap_vertices,
                        uint32_t* triangles, size_t cap_triangles, size_t* n_vertices, size_t* n_triangles);
 /* The triangulation table used by vlr_volume_to_mesh: 256 cases (bit i set:
  * corner i below the isovalue) x 16 edge indices, three per triangle, -1
- * padded.  Host-only; no counterpart in the reference (its table is a
- * constant, src/tools/volume_to_mesh.rs:226-483). */
+ * padded: the crate's TRI_TABLE (src/tools/volume_to_mesh.rs:246-503).
+ * Host-only; the reference keeps it as a private constant. */
 int vlr_mc_triangle_table(int8_t* out);
 
 /* ---- serialised formats ------------------------------------------------

@@ -32,17 +32,11 @@
 // count in visit order.
 //
 // Triangle table.  Vertices depend only on the edge table, which is the
-// classification rule.  The reference's triangle table (the classic
-// 256-case table) is not reproduced here; this file derives its own (same
-// corner and edge numbering): on each face, walked counter-clockwise from
-// outside, a crossing where the walk leaves the inside (below the isovalue)
-// is joined to the crossing where it last entered it, so ambiguous faces cut
-// each inside corner off on its own; the joins chain into cycles, taken in
-// order of their lowest edge, each fanned from that edge with normals toward
-// increasing values.  Neighbouring cells join a shared face identically, so
-// the surface closes across cells.  At most 5 triangles per case, like the
-// classic table; the triangles differ from the reference's in the diagonal
-// chosen inside some polygons.
+// classification rule.  Triangles come from the crate's own 256-case table
+// (src/tools/volume_to_mesh.rs:246-503, the classic Lorensen & Cline / Bourke
+// table), carried in mc_tri_table.inc with the same corner and edge
+// numbering, so each cell emits the same triangles in the same order as the
+// crate; a cell's triangles are the table row's triples up to its -1.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -56,8 +50,10 @@ namespace {
 constexpr int kCornerOff[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
 constexpr int kEdgeEnds[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-// faces as corner cycles, counter-clockwise about the outward normal
-constexpr int kFaces[6][4] = {{0, 3, 2, 1}, {4, 5, 6, 7}, {0, 1, 5, 4}, {3, 7, 6, 2}, {0, 4, 7, 3}, {1, 2, 6, 5}};
+// the crate's triangle table (src/tools/volume_to_mesh.rs:246-503), 16 entries per case, -1 terminated
+constexpr int8_t kTriTable[256][16] = {
+#include "mc_tri_table.inc"
+};
 
 struct McTable {
     int8_t tri[256][16];
@@ -67,53 +63,12 @@ struct McTable {
     int nb[12][3];
 };
 
-int edge_of(int a, int b) {
-    for (int e = 0; e < 12; ++e)
-        if ((kEdgeEnds[e][0] == a && kEdgeEnds[e][1] == b) || (kEdgeEnds[e][0] == b && kEdgeEnds[e][1] == a))
-            return e;
-    return -1;
-}
-
-McTable derive_mc_table() {
+McTable build_mc_table() {
     McTable t;
-    std::memset(t.tri, -1, sizeof(t.tri));
     for (int cs = 0; cs < 256; ++cs) {
-        int succ[12];
-        for (int& s : succ) s = -1;
-        for (const auto& f : kFaces) {
-            int leave_k[2], leave_e[2], enter_k[2], enter_e[2], nl = 0, ne = 0;
-            for (int k = 0; k < 4; ++k) {
-                const int a = f[k], b = f[(k + 1) & 3];
-                const int ia = (cs >> a) & 1, ib = (cs >> b) & 1;
-                if (ia && !ib) { leave_k[nl] = k; leave_e[nl++] = edge_of(a, b); }
-                if (ib && !ia) { enter_k[ne] = k; enter_e[ne++] = edge_of(a, b); }
-            }
-            for (int i = 0; i < nl; ++i) {
-                // the entering crossing that last precedes this leaving one on the walk
-                int best = -1;
-                for (int j = 0; j < ne; ++j)
-                    if (enter_k[j] < leave_k[i] && (best < 0 || enter_k[j] > enter_k[best])) best = j;
-                if (best < 0)
-                    for (int j = 0; j < ne; ++j)
-                        if (best < 0 || enter_k[j] > enter_k[best]) best = j;
-                succ[leave_e[i]] = enter_e[best];
-            }
-        }
         int n = 0;
-        bool seen[12] = {false};
-        for (int e = 0; e < 12; ++e) {
-            if (succ[e] < 0 || seen[e]) continue;
-            int cyc[12], len = 0;
-            for (int x = e; !seen[x]; x = succ[x]) {
-                seen[x] = true;
-                cyc[len++] = x;
-            }
-            for (int i = 1; i + 1 < len; ++i) {
-                t.tri[cs][n++] = (int8_t)cyc[0];
-                t.tri[cs][n++] = (int8_t)cyc[i + 1];
-                t.tri[cs][n++] = (int8_t)cyc[i];
-            }
-        }
+        while (n < 15 && kTriTable[cs][n] >= 0) n += 3;
+        std::memcpy(t.tri[cs], kTriTable[cs], 16);
         t.ntri[cs] = (uint8_t)(n / 3);
     }
     // an edge along axis a with lower corner L lies in the 4 cells at
@@ -152,7 +107,7 @@ McTable derive_mc_table() {
 }
 
 const McTable& mc_table() {
-    static const McTable t = derive_mc_table();
+    static const McTable t = build_mc_table();
     return t;
 }
 
@@ -168,7 +123,7 @@ __constant__ int c_edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}
 std::mutex g_mc_mu;
 bool g_mc_ready[128] = {};
 
-// Copies the derived table into this device's constant memory (once per
+// Copies the triangle table into this device's constant memory (once per
 // device, with that device current).
 int ensure_tables(vlr_ctx* ctx) {
     const int dev = ctx->device;

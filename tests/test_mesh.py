@@ -1,14 +1,16 @@
 """volume_to_mesh (src/tools/volume_to_mesh.rs:46-201).
 
-CPU: the triangulation table derived by the library (vlr_mc_triangle_table,
-host-only) equals the oracle's independent derivation (oracle/mc_table.py)
-and uses exactly the flagged edges of each case; the oracle restatement
+CPU: the library's triangle table (vlr_mc_triangle_table, host-only) equals
+the crate's TRI_TABLE (src/tools/volume_to_mesh.rs:246-503) entry for entry,
+through the golden fixture tests/golden/mc_tri_table.json written from the
+crate's source by tests/golden/make_mc_tri_table.py, and every row uses
+exactly the flagged edges of its case; the oracle restatement
 (oracle/ref_tree.hpp) passes the crate's own tests (volume_to_mesh.rs:510-587)
 and agrees with a small pure-Python restatement of the reference loop.
 
 GPU: vertices bit-exact against the oracle (order and f64 values: the
 reference's visit order, first-touch numbering and interpolation rounding)
-and triangles identical (same table), for spheres, a multi-tile union of
+and triangles identical (the crate's table), for spheres, a multi-tile union of
 random spheres straddling negative coordinates, an advected grid, a
 non-zero isovalue, random-valued leaves (ambiguous faces everywhere) and an
 empty grid.
@@ -35,10 +37,16 @@ def watertight(tris):
 
 # ------------------------------------------------------------------ CPU
 
-def test_library_table_equals_oracle_derivation():
+def test_library_table_equals_crate_table():
+    import json
+    from pathlib import Path
     from oracle import mc_table
     from sharc.volrus_b200 import mc_triangle_table
-    assert np.array_equal(mc_triangle_table(), np.asarray(mc_table.tri_table(), np.int8))
+    golden = json.loads((Path(__file__).parent / "golden" / "mc_tri_table.json").read_text())["rows"]
+    assert np.array_equal(mc_triangle_table(), np.asarray(golden, np.int8))
+    assert np.array_equal(np.asarray(mc_table.tri_table(), np.int8), np.asarray(golden, np.int8))
+    # spot checks of well-known rows of the classic table
+    assert golden[1][:4] == [0, 8, 3, -1] and golden[3][:7] == [1, 8, 3, 9, 8, 1, -1]
 
 
 def test_table_uses_exactly_the_flagged_edges():
