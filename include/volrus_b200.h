@@ -87,9 +87,36 @@ int vlr_extend_velocity(vlr_ctx* ctx, const vlr_grid* sdf, vlr_grid* vx, vlr_gri
 /* Replaces the position update of advect_particles (RK4, rk4 = 1) and
  * advect_particles_euler (rk4 = 0) (src/tools/advection.rs:58-110): positions
  * (f64, 3 per particle, world units) move in place through VelocityField
- * {vx, vy, vz}; re-binning into the point grid's leaves stays with the caller. */
+ * {vx, vy, vz}; the position update alone (vlr_advect_points below is the
+ * whole crate call, re-binning included). */
 int vlr_advect_particles(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, const vlr_grid* vz, double* positions,
                          size_t n, double dt, int rk4);
+/* A particle of the crate's PointDataGrid (Particle, src/points/point_grid.rs:
+ * 9-17): world position, velocity attribute, id. */
+typedef struct vlr_particle {
+    double position[3];
+    double velocity[3];
+    uint64_t id;
+} vlr_particle;
+/* Replaces advect_particles(&mut PointDataGrid, &VelocityField, dt) (RK4,
+ * rk4 = 1) and advect_particles_euler (rk4 = 0) (src/tools/advection.rs:58-110)
+ * including their closing PointDataGrid::rebin (src/points/point_grid.rs:
+ * 258-266).  `particles` holds the point grid's particles in binned order
+ * (leaves in ascending (x, y, z) origin order, each leaf's particles in its
+ * stored order) and is rewritten in place: positions moved, then the
+ * particles re-binned into the leaf of AffineMap::world_to_index(position)
+ * aligned to 8, leaves again in ascending origin order and each leaf's
+ * particles in their drain order (the crate drains leaves in HashMap order;
+ * ascending order makes the result deterministic).  world_to_index holds rows
+ * 0..2 of the point grid's inverse 4x4 map (AffineMap::inverse).  The
+ * re-binned leaves go to leaf_origins (cap_leaves x 3) and leaf_start
+ * (cap_leaves + 1 entries: first particle of each leaf, then n); *n_leaves
+ * is always set, and VLR_ERR_CAPACITY (particles left unchanged) reports
+ * more leaves than cap_leaves (cap_leaves = n always suffices).  At most
+ * 2^28 particles per call. */
+int vlr_advect_points(vlr_ctx* ctx, const vlr_grid* vx, const vlr_grid* vy, const vlr_grid* vz,
+                      const double world_to_index[12], vlr_particle* particles, size_t n, double dt, int rk4,
+                      int32_t* leaf_origins, uint32_t* leaf_start, size_t cap_leaves, size_t* n_leaves);
 /* Replaces dilate(&mut Grid<f32>, iterations) (src/tools/morphology.rs:20-35):
  * every inactive voxel with an active 6-neighbour becomes active with the
  * value of the neighbour that comes first in the tree's iteration order

@@ -6,7 +6,9 @@
 #include "ref_tree.hpp"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
+#include <cmath>
 
 using namespace vlr_oracle;
 
@@ -117,6 +119,53 @@ void vo_advect_particles(void* vx, void* vy, void* vz, double* pos, size_t n, do
         for (int a = 0; a < 3; ++a) k4[a] = dt * v[a];
         for (int a = 0; a < 3; ++a) p[a] = p[a] + (k1[a] + 2.0 * k2[a] + 2.0 * k3[a] + k4[a]) / 6.0;
     }
+}
+
+// PointDataGrid::rebin (src/points/point_grid.rs:258-266) after a position
+// update: each particle goes to the leaf of AffineMap::world_to_index(pos)
+// (src/grid.rs:259-277: rows of the inverse map applied left to right in f64,
+// f64::round half away from zero, saturating `as i32`) aligned to 8
+// (Coord::aligned(3), src/math/coord.rs:63-70).  The crate drains its leaves
+// in HashMap order; with leaves drained in ascending (x, y, z) order and
+// particles given in that binned order, the re-inserted grid is a stable
+// sort of the particles by their new leaf.  Writes the permutation (new
+// position -> input index) and returns the leaf count; leaf origins (3 ints)
+// and the first particle of each leaf (n_leaves + 1 entries) go to `origins`
+// and `start` when non-null.
+static int32_t rust_round_to_i32(double f) {
+    const double r = std::round(f);  // half away from zero, like f64::round
+    if (r != r) return 0;
+    if (r >= 2147483647.0) return 2147483647;
+    if (r <= -2147483648.0) return (-2147483647 - 1);
+    return (int32_t)r;
+}
+
+size_t vo_rebin_points(const double* pos, size_t n, const double* inv, uint32_t* perm, int32_t* origins,
+                       uint32_t* start) {
+    std::vector<std::array<int32_t, 3>> leaf(n);
+    for (size_t i = 0; i < n; ++i) {
+        const double* p = pos + 3 * i;
+        for (int a = 0; a < 3; ++a) {
+            const double* r = inv + 4 * a;
+            const double f = r[0] * p[0] + r[1] * p[1] + r[2] * p[2] + r[3];
+            leaf[i][a] = rust_round_to_i32(f) & ~7;
+        }
+    }
+    std::vector<uint32_t> idx(n);
+    for (size_t i = 0; i < n; ++i) idx[i] = (uint32_t)i;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return leaf[a] < leaf[b]; });
+    size_t nl = 0;
+    for (size_t j = 0; j < n; ++j) {
+        if (perm) perm[j] = idx[j];
+        if (j == 0 || leaf[idx[j]] != leaf[idx[j - 1]]) {
+            if (origins)
+                for (int a = 0; a < 3; ++a) origins[3 * nl + a] = leaf[idx[j]][a];
+            if (start) start[nl] = (uint32_t)j;
+            ++nl;
+        }
+    }
+    if (start) start[nl] = (uint32_t)n;
+    return nl;
 }
 
 void* vo_advect_level_set(void* g, void* vx, void* vy, void* vz, double dt) {

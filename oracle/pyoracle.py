@@ -44,6 +44,8 @@ SIGS = {
     "vo_rebuild_narrow_band": (None, [P, C.c_float, C.c_int]),
     "vo_dilate": (None, [P, C.c_uint]),
     "vo_advect_particles": (None, [P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
+    "vo_rebin_points": (C.c_size_t, [dbl_p, C.c_size_t, dbl_p, C.POINTER(C.c_uint32), i32_p,
+                                     C.POINTER(C.c_uint32)]),
     "vo_extend_velocity": (None, [P, P, P, P, C.c_float]),
     "vo_remove_empty_leaves": (None, [P]),
     "vo_flood_fill_sign": (None, [P]),
@@ -230,6 +232,22 @@ def advect_particles(vx, vy, vz, positions, dt, rk4=True):
     p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3).copy()
     load().vo_advect_particles(vx.h, vy.h, vz.h, _p(p, C.c_double), len(p), dt, 1 if rk4 else 0)
     return p
+
+
+def rebin_points(positions, world_to_index_rows):
+    """PointDataGrid::rebin (src/points/point_grid.rs:258-266) of particles
+    given in binned order, leaves drained in ascending origin order: returns
+    (perm, leaf_origins (k, 3), leaf_start (k + 1)) with perm[j] the input index
+    of the j-th particle of the re-binned grid."""
+    p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+    inv = np.ascontiguousarray(world_to_index_rows, np.float64).reshape(12)
+    n = len(p)
+    perm = np.zeros(max(n, 1), np.uint32)
+    org = np.zeros((max(n, 1), 3), np.int32)
+    start = np.zeros(n + 1, np.uint32)
+    k = load().vo_rebin_points(_p(p, C.c_double), n, _p(inv, C.c_double), _p(perm, C.c_uint32),
+                               _p(org, C.c_int32), _p(start, C.c_uint32))
+    return perm[:n], org[:k], start[:k + 1]
 
 
 def uniform_velocity(voxel_size, vel, bbox_min=None, bbox_max=None):

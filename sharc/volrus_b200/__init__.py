@@ -10,6 +10,7 @@ CPU fallback.
 """
 from ._lib import Context, VolrusError
 from .grid import AffineMap, Grid, GridClass, VoxelTransform
+from .points import PARTICLE, PointDataGrid, particle
 from .tools import (DeviceGrid, Mesh, VelocityField, advect_level_set, advect_particles, advect_particles_euler,
                     dilate, extend_velocity, find_zero_crossings, flood_fill_sign, make_level_set_sphere,
                     make_uniform_velocity, mc_triangle_table, rebuild_narrow_band, sample_trilinear,
@@ -19,5 +20,5 @@ __all__ = [
     "AffineMap", "Context", "DeviceGrid", "Grid", "GridClass", "VelocityField", "VolrusError", "VoxelTransform",
     "advect_level_set", "advect_particles", "advect_particles_euler", "dilate", "extend_velocity", "find_zero_crossings", "make_level_set_sphere", "make_uniform_velocity",
     "rebuild_narrow_band", "sample_trilinear", "trim_narrow_band", "Mesh", "volume_to_mesh", "mc_triangle_table",
-    "flood_fill_sign",
+    "flood_fill_sign", "PointDataGrid", "PARTICLE", "particle",
 ]

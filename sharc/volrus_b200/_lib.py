@@ -98,6 +98,8 @@ SIGNATURES = {
     "vlr_grid_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
     "vlr_extend_velocity": (C.c_int, [P, P, P, P, P, C.c_float]),
     "vlr_advect_particles": (C.c_int, [P, P, P, P, dbl_p, C.c_size_t, C.c_double, C.c_int]),
+    "vlr_advect_points": (C.c_int, [P, P, P, P, dbl_p, C.c_void_p, C.c_size_t, C.c_double, C.c_int, i32_p,
+                                    C.POINTER(C.c_uint32), C.c_size_t, size_p]),
     "vlr_dilate": (C.c_int, [P, P, C.c_uint]),
     "vlr_flood_fill_sign": (C.c_int, [P, P]),
     "vlr_volume_to_mesh": (C.c_int, [P, P, C.c_float, dbl_p, C.c_size_t, C.POINTER(C.c_uint32), C.c_size_t, size_p,

@@ -202,16 +202,53 @@ def _particles(positions, velocity: VelocityField, dt: float, rk4: bool, ctx):
     return p
 
 
-def advect_particles(positions, velocity: VelocityField, dt: float, ctx: Context | None = None) -> np.ndarray:
-    """Position update of ``advect_particles`` (src/tools/advection.rs:58-95):
-    RK4 through the velocity field; (n, 3) world positions in, new ones out.
-    Re-binning into a point grid's leaves is the caller's (``PointDataGrid::rebin``)."""
-    return _particles(positions, velocity, dt, True, ctx)
+def _advect_points(points, velocity: VelocityField, dt: float, rk4: bool, ctx):
+    """advect_particles on a PointDataGrid, in place: RK4 / Euler position
+    update and the closing PointDataGrid::rebin, in one C-ABI call."""
+    from .points import PARTICLE
+    ctx = ctx or Context.default()
+    parts = np.ascontiguousarray(points.particles, PARTICLE).copy()
+    n = len(parts)
+    inv = points.inverse_rows()
+    origins = np.zeros((max(n, 1), 3), np.int32)
+    start = np.zeros(n + 1, np.uint32)
+    nl = C.c_size_t()
+    made = [_as_device(g, ctx) for g in (velocity.vx, velocity.vy, velocity.vz)]
+    try:
+        ctx.check(ctx.lib.vlr_advect_points(ctx.handle, made[0][0].handle, made[1][0].handle, made[2][0].handle,
+                                            ptr(inv, C.c_double), parts.ctypes.data_as(C.c_void_p), n, float(dt),
+                                            1 if rk4 else 0, ptr(origins, C.c_int32), ptr(start, C.c_uint32),
+                                            max(n, 1), C.byref(nl)), "vlr_advect_points")
+    finally:
+        for d, created in made:
+            if created:
+                d.close()
+    k = nl.value
+    points.particles = parts
+    points.leaf_origins = origins[:k].copy()
+    points.leaf_start = start[:k + 1].copy()
+    return points
 
 
-def advect_particles_euler(positions, velocity: VelocityField, dt: float, ctx: Context | None = None) -> np.ndarray:
-    """Position update of ``advect_particles_euler`` (src/tools/advection.rs:97-110)."""
-    return _particles(positions, velocity, dt, False, ctx)
+def advect_particles(points, velocity: VelocityField, dt: float, ctx: Context | None = None):
+    """``advect_particles`` (src/tools/advection.rs:58-95): RK4 through the
+    velocity field.  Given a :class:`PointDataGrid` it is the crate call,
+    position update then ``PointDataGrid::rebin``, in place (the grid is also
+    returned); given an (n, 3) array of world positions it returns the new
+    positions (the update alone)."""
+    from .points import PointDataGrid
+    if isinstance(points, PointDataGrid):
+        return _advect_points(points, velocity, dt, True, ctx)
+    return _particles(points, velocity, dt, True, ctx)
+
+
+def advect_particles_euler(points, velocity: VelocityField, dt: float, ctx: Context | None = None):
+    """``advect_particles_euler`` (src/tools/advection.rs:97-110), like
+    :func:`advect_particles` with a forward Euler update."""
+    from .points import PointDataGrid
+    if isinstance(points, PointDataGrid):
+        return _advect_points(points, velocity, dt, False, ctx)
+    return _particles(points, velocity, dt, False, ctx)
 
 
 def dilate(grid, iterations: int, ctx: Context | None = None):
