@@ -29,7 +29,8 @@ enum {
     VLR_OK = 0,
     VLR_ERR_INVALID = 1,   /* bad argument (null pointer, duplicate leaf, unaligned origin, ...) */
     VLR_ERR_CUDA = 2,      /* CUDA runtime error */
-    VLR_ERR_CAPACITY = 3,  /* leaf pool or hash capacity exceeded */
+    VLR_ERR_CAPACITY = 3,  /* leaf pool or hash capacity exceeded (a level-set step that reports it is
+                              abandoned and leaves the state undefined, as for VLR_ERR_TIMEOUT) */
     VLR_ERR_EXTENT = 4,    /* grid spans more than 2^24 voxels along an axis */
     VLR_ERR_REACH = 5,     /* a backtrace left the staged neighbourhood (time step too large) */
     VLR_ERR_NOMEM = 6,     /* device allocation failed */
@@ -67,6 +68,19 @@ int vlr_ctx_stream(vlr_ctx* ctx, void** stream);
  * No counterpart in the reference. */
 int vlr_ctx_profile(vlr_ctx* ctx, int enable);
 int vlr_ctx_profile_read(vlr_ctx* ctx, const char* kernel, double* total_ms, long long* launches);
+/* Bound of every device-side wait of the context's kernels (the look-back
+ * scan of a level-set step, the TMA staging barrier), in polls; 0 restores
+ * each wait's default (about half a second).  A wait that reaches its bound
+ * sets VLR_ERR_TIMEOUT for the operation and the rest of that step is
+ * abandoned.  Takes effect for work enqueued afterwards.  No counterpart in
+ * the reference (its code is serial). */
+int vlr_ctx_set_wait_limit(vlr_ctx* ctx, uint32_t polls);
+/* Test hook for the timeout path: while `on` is non-zero, the first chunk of
+ * every level-set step's look-back scan withholds its prefix, so the waits
+ * of the later chunks run out (VLR_ERR_TIMEOUT once the bound is reached)
+ * instead of completing.  Off by default; it makes no GPU fault or hang, only
+ * a bounded wait that gives up.  No counterpart in the reference. */
+int vlr_ctx_test_stall(vlr_ctx* ctx, int on);
 
 /* ---- grids (reference semantics: f32 values in world units) ------------ */
 

@@ -93,6 +93,8 @@ SIGNATURES = {
     "vlr_ctx_stream": (C.c_int, [P, PP]),
     "vlr_ctx_profile": (C.c_int, [P, C.c_int]),
     "vlr_ctx_profile_read": (C.c_int, [P, C.c_char_p, dbl_p, C.POINTER(C.c_longlong)]),
+    "vlr_ctx_set_wait_limit": (C.c_int, [P, C.c_uint32]),
+    "vlr_ctx_test_stall": (C.c_int, [P, C.c_int]),
     "vlr_grid_create": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t, PP]),
     "vlr_grid_info": (C.c_int, [P, P, size_p, C.POINTER(C.c_uint64), flt_p, C.POINTER(vlr_transform)]),
     "vlr_grid_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),

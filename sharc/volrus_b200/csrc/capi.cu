@@ -159,6 +159,26 @@ void vlr_ctx_destroy(vlr_ctx* ctx) {
 
 const char* vlr_last_error(const vlr_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
+// Words 2 and 3 of the device error word hold the test-stall flag and the
+// wait bound; kernels read them when they start.
+int vlr_ctx_set_wait_limit(vlr_ctx* ctx, uint32_t polls) {
+    if (!ctx) return VLR_ERR_INVALID;
+    unsigned* h = (unsigned*)ctx->pinned + 48;  // a slot no other read-back uses
+    *h = polls;
+    VLR_CUDA(ctx, cudaMemcpyAsync(ctx->d_errword + 3, h, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
+
+int vlr_ctx_test_stall(vlr_ctx* ctx, int on) {
+    if (!ctx) return VLR_ERR_INVALID;
+    unsigned* h = (unsigned*)ctx->pinned + 49;
+    *h = on ? 1u : 0u;
+    VLR_CUDA(ctx, cudaMemcpyAsync(ctx->d_errword + 2, h, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
+
 int vlr_ctx_synchronize(vlr_ctx* ctx) {
     if (!ctx) return VLR_ERR_INVALID;
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -128,6 +128,27 @@ __device__ __forceinline__ float3 velocity(const MGridParams& P, const float2* _
 __device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Error word layout (vlr_ctx::d_errword): [0] error bits of the current
+// operation (kErr*), [1] spare, [2] test hook: non-zero makes the look-back
+// scan's first chunk withhold its prefix, [3] bound of the device-side waits
+// in polls (0: each wait's own default).
+//
+// A step whose bounded wait gave up, or whose leaf pool or hash overflowed,
+// is abandoned: every later kernel of the step, and of any step enqueued
+// after it, returns at once while that bit is set, so nothing works on a
+// half-built topology (the host reports VLR_ERR_TIMEOUT or VLR_ERR_CAPACITY
+// and requires a new state before the next step).
+__device__ __forceinline__ bool step_aborted(const unsigned* err) {
+    return (*reinterpret_cast<const volatile unsigned*>(err) & (kErrTimeout | kErrCapacity | kErrHashFull)) != 0u;
+}
+__device__ __forceinline__ long long wait_limit(const unsigned* err, long long dflt) {
+    const unsigned v = reinterpret_cast<const volatile unsigned*>(err)[3];
+    return v ? (long long)v : dflt;
+}
+__device__ __forceinline__ bool test_stall(const unsigned* err) {
+    return reinterpret_cast<const volatile unsigned*>(err)[2] != 0u;
+}
+
 // Hash lookup of a leaf coordinate within a grid (key packs the grid id).
 __device__ __forceinline__ uint64_t mkey(long long lx, long long ly, long long lz, int gid, const long long* base,
                                          int bits) {

@@ -52,6 +52,17 @@ int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     ls->maps_h[0] = ls->maps_h[1] = 0;  // tensor maps are encoded for the pools allocated here
     size_t vb = (ls->precision == VLR_PREC_F16) ? 2 : 4;
     ls->hcap = next_pow2i(2ll * cap);
+    {
+        // refuse up front what cannot fit, rather than filling the device first
+        const size_t c = (size_t)cap, h = (size_t)ls->hcap;
+        const size_t need = c * (16 + 64 + 64 + 2 * vb * kLeafVoxels + 4 * kNbr + 4 * 9 + 8) +
+                            4 * scan_scratch_ints(cap) + h * 24 + 256;
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need > free_b)
+            return set_error(ctx, VLR_ERR_NOMEM,
+                             "level set of " + std::to_string(cap) + " slots needs " + std::to_string(need >> 20) +
+                                 " MiB, more than the device's free " + std::to_string(free_b >> 20) + " MiB");
+    }
     VLR_CUDA(ctx, cudaMalloc(&ls->origin, sizeof(int4) * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->mask, 64ull * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->dmask, 64ull * cap));
@@ -67,6 +78,7 @@ int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     VLR_CUDA(ctx, cudaMalloc(&ls->pos, sizeof(int) * (cap + 1 + scan_scratch_ints(cap))));
     VLR_CUDA(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (cap + 1 + scan_scratch_ints(cap)), ctx->stream));
     VLR_CUDA(ctx, cudaMalloc(&ls->newinfo, sizeof(int) * cap));
+    VLR_CUDA(ctx, cudaMemsetAsync(ls->newinfo, 0xff, sizeof(int) * cap, ctx->stream));  // -1: no new leaf
     VLR_CUDA(ctx, cudaMalloc(&ls->free_stack, sizeof(int) * cap));
     VLR_CUDA(ctx, cudaMalloc(&ls->scalars, sizeof(int) * 8));
     VLR_CUDA(ctx, cudaMalloc(&ls->hkey, sizeof(uint64_t) * ls->hcap));
@@ -248,7 +260,9 @@ int ls_init_lists(vlr_ctx* ctx, vlr_level_set* ls, int n, bool reset_step) {
     int rc = ls_enqueue_index(ctx, ls);
     if (rc) return rc;
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return consume_device_errors(ctx, "method grid index");
+    rc = consume_device_errors(ctx, "method grid index");
+    if (rc == VLR_OK) ls->state_lost = false;  // a complete new state
+    return rc;
 }
 
 // Staging buffer of at least `bytes` owned by the level set.
@@ -400,11 +414,17 @@ int create_sphere_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m
     void* v_tmp = nullptr;
     int* touched = nullptr;
     int* pos = nullptr;
+    DeviceTemps temps;  // freed on every return
     VLR_CUDA(ctx, cudaMalloc(&o_tmp, sizeof(int4) * n_cand));
+    temps.track(o_tmp);
     VLR_CUDA(ctx, cudaMalloc(&m_tmp, 64ull * n_cand));
+    temps.track(m_tmp);
     VLR_CUDA(ctx, cudaMalloc(&v_tmp, vb * kLeafVoxels * n_cand));
+    temps.track(v_tmp);
     VLR_CUDA(ctx, cudaMalloc(&touched, sizeof(int) * (n_cand + 1)));
+    temps.track(touched);
     VLR_CUDA(ctx, cudaMalloc(&pos, sizeof(int) * (n_cand + 1)));
+    temps.track(pos);
     int blocks = std::min<long long>(n_cand, (long long)ctx->sm_count * 16);
     if (ls->precision == VLR_PREC_F16)
         k_m_sphere<__half><<<blocks, 256, 0, ctx->stream>>>(lo[0] >> 3, lo[1] >> 3, lo[2] >> 3, (int)nl[1], (int)nl[2],
@@ -432,11 +452,6 @@ int create_sphere_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m
                                                        ls->origin, ls->mask, (float*)ls->vals[0]);
     VLR_CUDA(ctx, cudaGetLastError());
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    cudaFree(o_tmp);
-    cudaFree(m_tmp);
-    cudaFree(v_tmp);
-    cudaFree(touched);
-    cudaFree(pos);
     return ls_init_lists(ctx, ls, n, true);
 }
 
@@ -562,6 +577,10 @@ void drop_graph(vlr_level_set* ls) {
 // the kernel timers paused), then graph replays (direct launches while the
 // per-kernel timers are on).
 int enqueue_one_step(vlr_ctx* ctx, vlr_level_set* ls) {
+    if (ls->state_lost)
+        return set_error(ctx, VLR_ERR_INVALID,
+                         "the level set's state is undefined after a step failed with VLR_ERR_TIMEOUT or "
+                         "VLR_ERR_CAPACITY: upload a state first");
     if (ls->autotune && !ls->tuned) {
         const bool timing = ctx->timer.enabled;
         ctx->timer.enabled = false;
@@ -705,7 +724,9 @@ int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps) {
         if (rc) return rc;
     }
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return consume_device_errors(ctx, "vlr_ls_step");
+    const int rc = consume_device_errors(ctx, "vlr_ls_step");
+    if (rc == VLR_ERR_TIMEOUT || rc == VLR_ERR_CAPACITY) ls->state_lost = true;
+    return rc;
 }
 
 int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int advect_staging,

@@ -214,15 +214,25 @@ int create_spheres_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* 
     double4* d_sph = nullptr;
     uint64_t* m_tmp = nullptr;
     void* v_tmp = nullptr;
+    DeviceTemps temps;  // freed on every return
     VLR_CUDA(ctx, cudaMalloc(&d_cand, sizeof(int4) * n_cand));
+    temps.track(d_cand);
     VLR_CUDA(ctx, cudaMalloc(&d_off, sizeof(int) * (n_cand + 1)));
+    temps.track(d_off);
     VLR_CUDA(ctx, cudaMalloc(&d_sidx, sizeof(int) * std::max<size_t>(sidx.size(), 1)));
+    temps.track(d_sidx);
     VLR_CUDA(ctx, cudaMalloc(&d_sph, sizeof(double4) * spheres.size()));
+    temps.track(d_sph);
     VLR_CUDA(ctx, cudaMalloc(&o_tmp, sizeof(int4) * n_cand));
+    temps.track(o_tmp);
     VLR_CUDA(ctx, cudaMalloc(&m_tmp, 64ull * n_cand));
+    temps.track(m_tmp);
     VLR_CUDA(ctx, cudaMalloc(&v_tmp, vb * kLeafVoxels * n_cand));
+    temps.track(v_tmp);
     VLR_CUDA(ctx, cudaMalloc(&touched, sizeof(int) * (n_cand + 1)));
+    temps.track(touched);
     VLR_CUDA(ctx, cudaMalloc(&pos, sizeof(int) * (n_cand + 1)));
+    temps.track(pos);
     VLR_CUDA(ctx, cudaMemcpyAsync(d_cand, cand.data(), sizeof(int4) * n_cand, cudaMemcpyHostToDevice, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(int) * (n_cand + 1), cudaMemcpyHostToDevice, ctx->stream));
     if (!sidx.empty())
@@ -256,9 +266,6 @@ int create_spheres_impl(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* 
                                                          ls->origin, ls->mask, (float*)ls->vals[0]);
     VLR_CUDA(ctx, cudaGetLastError());
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    for (void* p : {(void*)d_cand, (void*)d_off, (void*)d_sidx, (void*)d_sph, (void*)o_tmp, (void*)m_tmp, v_tmp,
-                    (void*)touched, (void*)pos})
-        cudaFree(p);
     return ls_init_lists(ctx, ls, n, true);
 }
 

@@ -71,6 +71,7 @@ struct vlr_level_set {
     StencilShape adv_shape;  // launch shapes of the stencil kernels
     StencilShape re_shape;
     bool tuned = false;      // shapes chosen (by the autotuner or the caller)
+    bool state_lost = false; // a step failed with VLR_ERR_TIMEOUT or VLR_ERR_CAPACITY: the state is undefined
     bool autotune = true;    // choose the shapes on the first step
     std::vector<TuneEntry> tune_log[2];  // candidates timed by the autotuner (advect, reinit)
     // tensor maps of the stencil kernels' source pools for TMA staging:

@@ -314,10 +314,10 @@ __device__ __forceinline__ void stage_tma(const uint4* s_tma, const int* s_nb, c
 // it-th leaf a CTA processes completes phase it of the mbarrier, so the
 // parity waited for is it & 1.
 constexpr int kStageSpin = 1 << 20;
-__device__ __forceinline__ bool stage_ready_tma(uint32_t bar, unsigned parity) {
+__device__ __forceinline__ bool stage_ready_tma(uint32_t bar, unsigned parity, long long limit) {
     cp_async_wait_all();
     bool ok = false;
-    for (int i = 0; i < kStageSpin; ++i)
+    for (long long i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) {
             ok = true;
             break;
@@ -354,12 +354,12 @@ __device__ __forceinline__ void stage_issue(const unsigned* s_desc, const uint4*
 
 // Returns false (on every thread) if the tensor copies did not arrive in time.
 template <int ST>
-__device__ __forceinline__ bool stage_wait(uint64_t* s_bar, unsigned parity) {
+__device__ __forceinline__ bool stage_wait(uint64_t* s_bar, unsigned parity, long long limit) {
     if constexpr (ST == 0) {
         stage_ready();
         return true;
     } else {
-        return stage_ready_tma(smem_addr(s_bar), parity);
+        return stage_ready_tma(smem_addr(s_bar), parity, limit);
     }
 }
 
@@ -681,6 +681,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     dep_wait();
     dep_launch();
+    if (step_aborted(err)) return;
     // clear this step's re-tracking state (keep flags, proposal table, leaf hash)
     for (int i = blockIdx.x * NT + threadIdx.x; i < max(topo.cap, topo.hcap); i += gridDim.x * NT) {
         if (i < topo.cap) topo.keep[i] = 0;
@@ -718,6 +719,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
     const int G = gridDim.x;
     int li = blockIdx.x;
     if (li >= count) return;
+    const long long stage_limit = wait_limit(err, kStageSpin);
     const int step = *A.step;
     const float t1 = sp.t0 + (float)(step + 1) * sp.dt;
     const float dt = sp.dt;
@@ -777,7 +779,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_advect(MLeafArrays A, const
             }
         }
         // barrier 1: this leaf's rows and masks are in shared memory
-        if (!stage_wait<ST>(&s_bar, (unsigned)cur)) {
+        if (!stage_wait<ST>(&s_bar, (unsigned)cur, stage_limit)) {
             if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
             return;
         }
@@ -949,6 +951,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     static_assert(NT == 128 || NT == 256, "128 or 256 threads per CTA");
     dep_wait();
     dep_launch();
+    if (step_aborted(err)) return;
     constexpr int E = 12;  // phi1 tile: leaf + 2-voxel ring
     constexpr int F = 10;  // phi2 tile and D rows: leaf + 1-voxel ring
     constexpr int NW = NT / 32;
@@ -975,6 +978,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
     const int G = gridDim.x;
     int li = blockIdx.x;
     if (li >= count) return;
+    const long long stage_limit = wait_limit(err, kStageSpin);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const bool fix = (mode == 1);
@@ -995,7 +999,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_m_reinit(MLeafArrays A, const
         if (slot_n >= 0) o_n = A.origin[slot_n];
         const int nb_n = (w0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
         const int slot_nn = (li + 2 * G < count) ? A.list[li + 2 * G] : -1;
-        if (!stage_wait<ST>(&s_bar, (unsigned)cur)) {  // barrier 1
+        if (!stage_wait<ST>(&s_bar, (unsigned)cur, stage_limit)) {  // barrier 1
             if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
             return;
         }

@@ -30,7 +30,7 @@ namespace vlr {
 // scalars: [0] count  [1] step  [2] free top  [3] spare
 //          [4] new count  [5] recycled count  [6] new free top  [7] chunk ticket
 constexpr int kChunk = 256;
-constexpr long long kSpinLimit = 1ll << 22;
+constexpr long long kSpinLimit = 1ll << 22;  // default bound of the look-back wait (about half a second)
 
 __device__ __forceinline__ void dir_of(int d, int& dx, int& dy, int& dz) {
     dx = d / 9 - 1;
@@ -58,9 +58,12 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
                                                        int cap, unsigned* err) {
     dep_wait();
     dep_launch();
+    if (step_aborted(err)) return;
     __shared__ int s_ticket;
     __shared__ int s_warp[kChunk / 32];
     __shared__ int s_prefix;
+    const long long spin_limit = wait_limit(err, kSpinLimit);
+    const bool hold_first = test_stall(err);
     const int count = scalars[0];
     const unsigned tag = (unsigned)scalars[1] + 1u;
     const int nchunks = (count + kChunk - 1) / kChunk;
@@ -116,7 +119,8 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
             const unsigned wtag = tag & 0x3fffffffu;
             unsigned prefix = 0;
             if (chunk == 0) {
-                if (lane == 0) atomicExch(&status[0], pack_status(tag, 2, total));
+                // (test hook: withheld, so that every later chunk's wait runs out)
+                if (lane == 0 && !hold_first) atomicExch(&status[0], pack_status(tag, 2, total));
             } else {
                 if (lane == 0) atomicExch(&status[chunk], pack_status(tag, 1, total));
                 int q = chunk - 1;
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
                     const int first_p = pmask ? __ffs(pmask) - 1 : 32;
                     const unsigned upto = first_p >= 31 ? 0xffffffffu : ((2u << first_p) - 1u);
                     if (invalid & upto) {
-                        if (++spins > kSpinLimit) {  // bounded wait: report and continue
+                        if (++spins > spin_limit) {  // bounded wait: report and continue
                             if (lane == 0) atomicOr(err, kErrTimeout);
                             break;
                         }
@@ -207,6 +211,7 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
                                                    const int* recycled, int* scalars, int cap, unsigned* err) {
     dep_wait();
     dep_launch();
+    if (step_aborted(err)) return;
     const int n = min(scalars[4], cap);
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -257,9 +262,11 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
 }
 
 __global__ void k_t_nbr(const int* list, int* scalars, const int4* origin, const uint64_t* hkey, const int* hval,
-                        int hcap, const MGridParams* __restrict__ params, int bits, int* nbr, int cap) {
+                        int hcap, const MGridParams* __restrict__ params, int bits, int* nbr, int cap,
+                        const unsigned* err) {
     dep_wait();
     dep_launch();
+    if (step_aborted(err)) return;
     const int count = min(scalars[4], cap);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)count * kNbr;
          t += (long long)gridDim.x * blockDim.x) {
@@ -402,7 +409,8 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
     VLR_TIMED(ctx, "k_t_nbr",
               VLR_CUDA(ctx, pdl_launch(k_t_nbr, B, 256, 0, st, (const int*)ls->list, ls->scalars,
                                        (const int4*)ls->origin, (const uint64_t*)ls->hkey, (const int*)ls->hval,
-                                       ls->hcap, (const MGridParams*)ls->d_params, ls->key_bits, ls->nbr, ls->cap)));
+                                       ls->hcap, (const MGridParams*)ls->d_params, ls->key_bits, ls->nbr, ls->cap,
+                                       (const unsigned*)ctx->d_errword)));
     VLR_CUDA(ctx, cudaGetLastError());
     return VLR_OK;
 }
