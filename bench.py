@@ -1036,8 +1036,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-mesh", action="store_true", help="skip the volume_to_mesh measurement")
     ap.add_argument("--launch-shape", default="",
-                    help="threads,CTAs[,staging] of advect then reinit, e.g. 128,1184,1,128,888,1 (default: "
-                         "autotuned; staging 0 cp.async, 1 TMA)")
+                    help="threads,CTAs[,staging] of advect then reinit, e.g. 128,1184,0,128,888,0 (default: "
+                         "autotuned; 128 threads and staging 0 are the only kernels built)")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)

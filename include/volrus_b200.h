@@ -331,12 +331,12 @@ int vlr_ls_step(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
  * reports device-side errors. */
 int vlr_ls_enqueue(vlr_ctx* ctx, vlr_level_set* ls, int n_steps);
 /* Launch shapes of the advect and reinitialisation kernels: threads per CTA
- * (128 or 256), persistent CTAs (> 0) and the staging of the halo tiles (0:
- * 16-byte cp.async row copies by every thread; 1: one TMA tensor copy per
- * present neighbour leaf, completing on an mbarrier).  Fixing them turns the
- * first-step autotuning off; advect_threads = 0 turns it back on for the next
- * step.  Results never depend on the shape.  No counterpart in the reference
- * (its step is serial Rust). */
+ * (128 only), persistent CTAs (> 0) and the staging of the halo tiles (0 only:
+ * cp.async row copies by every thread, double-buffered; other values are
+ * rejected with VLR_ERR_INVALID).  Fixing them turns the first-step autotuning
+ * off; advect_threads = 0 turns it back on for the next step.  Results never
+ * depend on the shape.  No counterpart in the reference (its step is serial
+ * Rust). */
 int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads, int advect_ctas, int advect_staging,
                             int reinit_threads, int reinit_ctas, int reinit_staging);
 /* shape[0..5] = advect threads, CTAs, staging, reinit threads, CTAs, staging

@@ -35,17 +35,10 @@ struct MGridParams {
     int tab_off[kMaxOctaves][3];  // first float2 of family f, axis a
     int tab_lo[3];         // index coordinate of table entry 0 (per axis)
     int tab_len[3];
-    int full_series;       // 1: rotation angles may reach 1 rad (full Taylor series); 0: below 0.05 rad
+    int series;            // rotation series order: 0 angles below 0.004 rad, 1 below 0.05 rad, 2 below 1 rad
     int doubling;          // curl: dphi[o] = 2^o dphi[0] exactly (rotations by double-angle formulas)
     long long base[3];     // hash key base (leaf coordinates)
 };
-
-// sin and cos of |d| < 0.05 (Taylor to d^5 / d^4, error < 3e-10).
-__device__ __forceinline__ void tiny_sincos(float d, float& s, float& c) {
-    float d2 = d * d;
-    s = d * (1.0f - d2 * (1.0f / 6.0f) * (1.0f - d2 * (1.0f / 20.0f)));
-    c = 1.0f - d2 * 0.5f * (1.0f - d2 * (1.0f / 12.0f));
-}
 
 // Step-wide parameters (shared by all grids of a batch).
 struct MStepParams {
@@ -62,62 +55,6 @@ __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 template <typename T> __device__ __forceinline__ T from_f(float v);
 template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
-
-// sin and cos of a small angle |d| < 1 (Taylor to d^9 / d^10, error < 3e-9).
-__device__ __forceinline__ void small_sincos(float d, float& s, float& c) {
-    float d2 = d * d;
-    s = d * (1.0f - d2 * (1.0f / 6.0f) * (1.0f - d2 * (1.0f / 20.0f) * (1.0f - d2 * (1.0f / 42.0f) * (1.0f - d2 * (1.0f / 72.0f)))));
-    c = 1.0f - d2 * 0.5f * (1.0f - d2 * (1.0f / 12.0f) * (1.0f - d2 * (1.0f / 30.0f) * (1.0f - d2 * (1.0f / 56.0f) * (1.0f - d2 * (1.0f / 90.0f)))));
-}
-
-// (sin, cos) of the table angle at integer coordinate i (axis a, family f),
-// rotated by dphi * off.  Sets *bad if i lies outside the table.
-template <bool kOffset>
-__device__ __forceinline__ float2 table_sc(const MGridParams& P, const float2* __restrict__ tab, int f, int a, int i,
-                                           float off, unsigned& bad) {
-    int k = i - P.tab_lo[a];
-    if (k < 0 || k >= P.tab_len[a]) {
-        bad = 1u;
-        k = min(max(k, 0), P.tab_len[a] - 1);
-    }
-    float2 t = __ldg(&tab[P.tab_off[f][a] + k]);
-    if (!kOffset) return t;
-    float sd, cd;
-    small_sincos(P.dphi[f] * off, sd, cd);
-    return make_float2(t.x * cd + t.y * sd, t.y * cd - t.x * sd);
-}
-
-// Velocity in voxels per unit time at position (ix + ox, iy + oy, iz + oz).
-// `ct` is the vortex time factor cos(pi t / T).
-template <bool kOffset>
-__device__ __forceinline__ float3 velocity(const MGridParams& P, const float2* __restrict__ tab, int ix, int iy, int iz,
-                                           float ox, float oy, float oz, float ct, unsigned& bad) {
-    if (P.vel_kind == MVEL_CONSTANT) return make_float3(P.c[0], P.c[1], P.c[2]);
-    if (P.vel_kind == MVEL_VORTEX) {
-        float2 X = table_sc<kOffset>(P, tab, 0, 0, ix, ox, bad);
-        float2 Y = table_sc<kOffset>(P, tab, 0, 1, iy, oy, bad);
-        float2 Z = table_sc<kOffset>(P, tab, 0, 2, iz, oz, bad);
-        float k = P.vel_scale * ct;
-        // u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z), v = -sin(2 pi x) sin^2(pi y) sin(2 pi z),
-        // w = -sin(2 pi x) sin(2 pi y) sin^2(pi z), times cos(pi t / T), world units / voxel size
-        float sycy = Y.x * Y.y, szcz = Z.x * Z.y, sxcx = X.x * X.y;
-        return make_float3(8.0f * k * X.x * X.x * sycy * szcz, -4.0f * k * sxcx * Y.x * Y.x * szcz,
-                           -4.0f * k * sxcx * sycy * Z.x * Z.x);
-    }
-    float3 u = make_float3(0.f, 0.f, 0.f);
-    for (int o = 0; o < P.octaves; ++o) {
-        float2 X = table_sc<kOffset>(P, tab, o, 0, ix, ox, bad);
-        float2 Y = table_sc<kOffset>(P, tab, o, 1, iy, oy, bad);
-        float2 Z = table_sc<kOffset>(P, tab, o, 2, iz, oz, bad);
-        float a = P.ak[o];
-        float gx = a * X.y * Y.x * Z.x, gy = a * X.x * Y.y * Z.x, gz = a * X.x * Y.x * Z.y;
-        const float* e = P.e[o];
-        u.x += gy * e[2] - gz * e[1];
-        u.y += gz * e[0] - gx * e[2];
-        u.z += gx * e[1] - gy * e[0];
-    }
-    return u;
-}
 
 // Programmatic dependent launch: the kernels of a step are launched with
 // programmatic stream serialization, so a kernel's CTAs may be scheduled while

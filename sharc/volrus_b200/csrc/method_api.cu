@@ -44,12 +44,10 @@ void ls_free(vlr_level_set* ls) {
     ls->d_params = nullptr;
     ls->d_tab = nullptr;
     ls->d_partial = ls->d_sum = nullptr;
-    ls->maps_h[0] = ls->maps_h[1] = 0;
 }
 
 int ls_alloc(vlr_ctx* ctx, vlr_level_set* ls, int cap) {
     ls->cap = cap;
-    ls->maps_h[0] = ls->maps_h[1] = 0;  // tensor maps are encoded for the pools allocated here
     size_t vb = (ls->precision == VLR_PREC_F16) ? 2 : 4;
     ls->hcap = next_pow2i(2ll * cap);
     {
@@ -212,11 +210,12 @@ int ls_setup_grids(vlr_ctx* ctx, vlr_level_set* ls, const vlr_method_desc* m, co
         P.doubling = (P.vel_kind == MVEL_CURL && P.octaves >= 2) ? 1 : 0;
         for (int o = 1; o < P.octaves && P.doubling; ++o)
             if (P.dphi[o] != 2.0f * P.dphi[o - 1]) P.doubling = 0;
-        // rotation angles stay below dphi * disp; the short series is exact to f32 below 0.05 rad
+        // rotation angles stay below dphi * disp; the shortest series exact to
+        // well below f32 resolution at that angle is used
         double max_angle = 0.0, gdisp = speed_bound(vels[g]) * m->dt;
         for (int f = 0; f < (P.doubling ? 1 : kMaxOctaves); ++f)
             max_angle = std::max(max_angle, std::fabs((double)P.dphi[f]) * gdisp);
-        P.full_series = max_angle > 0.05 ? 1 : 0;
+        P.series = max_angle < 0.004 ? 0 : (max_angle < 0.05 ? 1 : 2);
     }
     VLR_CUDA(ctx, cudaMalloc(&ls->d_params, sizeof(MGridParams) * n));
     VLR_CUDA(ctx, cudaMemcpy(ls->d_params, ls->h_params.data(), sizeof(MGridParams) * n, cudaMemcpyHostToDevice));
@@ -738,12 +737,9 @@ int vlr_ls_set_launch_shape(vlr_ctx* ctx, vlr_level_set* ls, int advect_threads,
         ls->tuned = false;
         return VLR_OK;
     }
-    auto ok_nt = [](int t) { return t == 128 || t == 256; };
-    auto ok_st = [](int s) { return s == 0 || s == 1; };
-    if (!ok_nt(advect_threads) || !ok_nt(reinit_threads) || advect_ctas < 1 || reinit_ctas < 1 ||
-        !ok_st(advect_staging) || !ok_st(reinit_staging))
-        return set_error(ctx, VLR_ERR_INVALID,
-                         "launch shape: threads must be 128 or 256, CTAs > 0 and staging 0 or 1");
+    if (advect_threads != kAdvectThreads || advect_staging != 0 || reinit_threads != kReinitThreads ||
+        reinit_staging != 0 || advect_ctas < 1 || reinit_ctas < 1)
+        return set_error(ctx, VLR_ERR_INVALID, "launch shape: 128 threads, staging 0 and CTAs > 0 for both kernels");
     ls->adv_shape = StencilShape{advect_threads, advect_ctas, advect_staging};
     ls->re_shape = StencilShape{reinit_threads, reinit_ctas, reinit_staging};
     ls->autotune = false;

@@ -1,6 +1,5 @@
 // Declarations shared by the method kernels and their host orchestration.
 #pragma once
-#include <cuda.h>  // CUtensorMap (a plain 128-byte struct; no driver library is linked)
 
 #include "method.cuh"
 
@@ -33,34 +32,23 @@ struct MTopo {
     int key_bits;
 };
 
-// Tensor maps of a stencil kernel's source value pool for staging mode 1, one
-// box shape per map, with ey = (i & 1 ? 8 : H) and ex = (i & 2 ? 8 : H):
-//   maps 0-3: 3-D view (yz, x, slot) of the pool, where yz = y * 8 + z runs
-//             over the 64 contiguous values of an x-plane; box {ey * 8, ex, 1}
-//             (whole z-rows, so a box row is ey * 8 contiguous values)
-//   maps 4-7: 4-D view (z, y, x, slot); box {4, ey, ex, 1} (the f32 z-halves)
-// f16 pools use maps 0-3, f32 pools 0-7.
-struct StageMaps {
-    CUtensorMap m[8];
-};
-
-// Staging of the stencil kernels' halo tiles (ST): 0 = asynchronous 16-byte
-// copies by every thread (cp.async), 1 = one tensor copy per present
-// neighbour leaf (cp.async.bulk.tensor, TMA) completing on an mbarrier.
-// VK: velocity kind of every grid (MVEL_*), or -1 when a batch mixes kinds.
-// NT: threads per CTA (128 or 256); the result depends neither on NT, on ST
-// nor on the grid size.
-template <typename T, int H, int VK, int NT, int ST>
+constexpr int kAdvectThreads = 128;
+constexpr int kReinitThreads = 128;
+// The advect kernel (method_advect.cu): 128 threads per CTA, persistent over
+// the leaf list.  VK: velocity kind of every grid (MVEL_*), or -1 when a batch
+// mixes kinds.  The result depends neither on the grid size nor on VK.
+template <typename T, int H, int VK>
 __global__ void k_m_advect(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
                            const MGridParams* __restrict__ params, const float2* __restrict__ tab, MStepParams sp,
-                           MTopo topo, unsigned* __restrict__ err, const __grid_constant__ StageMaps maps);
-// Dynamic shared memory of the stencil kernels (bytes).
-size_t advect_smem_bytes(int precision_f16, int halo, int stage);
-size_t reinit_smem_bytes(int precision_f16, int stage);
-template <typename T, int NIT, int NT, int ST>
+                           MTopo topo, unsigned* __restrict__ err);
+// The reinitialisation kernel (method_reinit.cu): NIT iterations (0..2),
+// FIX = 1 with the subcell fix at cut voxels; 128 threads per CTA.
+template <typename T, int NIT, int FIX>
 __global__ void k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
-                           const MGridParams* __restrict__ params, MTopo topo, int mode, unsigned* __restrict__ err,
-                           const __grid_constant__ StageMaps maps);
+                           const MGridParams* __restrict__ params, MTopo topo, unsigned* __restrict__ err);
+// Dynamic shared memory of the stencil kernels (bytes).
+size_t advect_smem_bytes(int precision_f16, int halo);
+size_t reinit_smem_bytes(int precision_f16, int nit, int fix);
 // Backtrace displacement (voxels) of the voxels of n leaves with bidx >= 0
 // over one step of a time-independent velocity (VK = MVEL_CONSTANT or
 // MVEL_CURL), k_m_advect's arithmetic; *maxabs collects the largest component

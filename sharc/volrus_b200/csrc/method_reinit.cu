@@ -1,0 +1,475 @@
+// The reinitialisation kernel of the METHOD step: NIT (0..2) Jacobi
+// iterations of Godunov-upwind reinitialisation fused in one pass (the first
+// iteration runs on the 10^3 box around the leaf so that the second needs no
+// exchange), trim to |phi| < hw, the new activity mask, and the re-tracking
+// bookkeeping: keep flags and proposals of missing neighbour leaves the band
+// spills into.
+//
+// One CTA of 128 threads works on one 8^3 leaf at a time and strides over the
+// ordered leaf list (persistent).  Per leaf:
+//
+//   stage      the advected field around the leaf, 2-voxel halo, row-packed
+//              as in the advect kernel (tile row (x, y) holds z in [-4, 12)),
+//              and the 27 neighbours' dilated masks arrive by cp.async one
+//              leaf ahead into the other of two buffers.  The pieces of
+//              absent leaves are set to NaN when the copies are issued, so
+//              the stage is complete at its barrier; a 6-neighbour stencil
+//              reads NaN as copysign(hw, its centre value).
+//   phase 1    every warp owns rows of the 10^3 box (row r = lane * 4 + warp):
+//              it copies them from the stage into the phi2 tile, builds their
+//              dilated-mask bits, and runs iteration 1 on its rows' voxels of
+//              D (compacted per warp, no CTA barrier); the faces of the box
+//              are included, its edges and corners are not (iteration 2
+//              never reads them).  Meanwhile every voxel's outside-D result
+//              copysign(hw, value) is written to global memory, coalesced.
+//   phase 2    iteration 2 on the leaf's voxels of D (compacted per warp over
+//              the dilated mask's x-planes), trim, stores over the outside-D
+//              results, activity bits into a shared mask.
+//   phase 3    mask out, spill toward absent neighbours, keep flags and
+//              proposals (hash of the missing leaf, atomicMin of the
+//              proposer's direction).
+//
+// Three CTA barriers per leaf.  Every leaf is computed by one CTA with the
+// same arithmetic whatever the grid size; side effects on shared per-step
+// state are idempotent (flags set to 1, atomicMin), so relaunching the kernel
+// on the same inputs leaves the step's result unchanged.
+#include "method_kernels.hpp"
+
+namespace vlr {
+namespace {
+
+constexpr int kNT = kReinitThreads;
+constexpr int kNW = kNT / 32;
+constexpr int kH = 2;                            // halo of the stage
+constexpr int kE = 8 + 2 * kH;                   // 12: stage rows per axis
+constexpr int kF = 10;                           // phi2 box and D rows: leaf + 1-voxel ring
+constexpr int kNP = 3 * kE * kE;                 // pieces per stage
+constexpr int kRPW = (kF * kF + kNW - 1) / kNW;  // box rows per warp
+
+__device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Staged row layout (as in the advect kernel): RP values, z = 0 at Z0.
+template <typename T>
+struct Row {
+    static constexpr int RP = sizeof(T) == 2 ? 24 : 16;
+    static constexpr int Z0 = sizeof(T) == 2 ? 8 : 4;
+};
+
+// Copy descriptor of piece p = 3 r + k: neighbour d (bits 0-4), first value
+// in the leaf (5-13), first value in the stage (14-26), k (27-28).
+template <typename T>
+__device__ __forceinline__ unsigned piece_desc(int p) {
+    constexpr int RP = Row<T>::RP, Z0 = Row<T>::Z0;
+    const int r = p / 3, k = p - 3 * r;
+    const int x = r / kE - kH, y = r % kE - kH;
+    const unsigned d = (unsigned)(nb_axis(x) * 9 + nb_axis(y) * 3 + k);
+    const unsigned g = (unsigned)(((x & 7) << 6) | ((y & 7) << 3) | (k == 0 ? 4 : 0));
+    const unsigned s = (unsigned)(r * RP + (k == 0 ? Z0 - 4 : (k == 1 ? Z0 : Z0 + 8)));
+    return d | (g << 5) | (s << 14) | ((unsigned)k << 27);
+}
+
+// One leaf's stage: copies of the present pieces, NaN in the pieces of
+// absent leaves, and the 27 dilated masks (zero for absent leaves).
+template <typename T>
+__device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s_nb, const T* __restrict__ vals,
+                                            const uint64_t* __restrict__ masks, T* stage, uint64_t* s_m) {
+    for (int p = threadIdx.x; p < kNP; p += kNT) {
+        const unsigned dsc = s_desc[p];
+        const int sl = s_nb[dsc & 31u];
+        T* dst = stage + ((dsc >> 14) & 8191u);
+        const unsigned k = dsc >> 27;
+        if (sl < 0) {
+            if constexpr (sizeof(T) == 2) {
+                const uint64_t nan4 = 0x7e007e007e007e00ull;
+                uint64_t* o = reinterpret_cast<uint64_t*>(dst);
+                o[0] = nan4;
+                if (k == 1) o[1] = nan4;
+            } else {
+                const unsigned nan = 0x7fc00000u;
+                uint4* o = reinterpret_cast<uint4*>(dst);
+                o[0] = make_uint4(nan, nan, nan, nan);
+                if (k == 1) o[1] = make_uint4(nan, nan, nan, nan);
+            }
+            continue;
+        }
+        const T* src = vals + (size_t)sl * kLeafVoxels + ((dsc >> 5) & 511u);
+        if constexpr (sizeof(T) == 2) {
+            if (k == 1) cp_async16(dst, src);
+            else cp_async8(dst, src);
+        } else {
+            cp_async16(dst, src);
+            if (k == 1) cp_async16(dst + 4, src + 4);
+        }
+    }
+    if (threadIdx.x < kNbr * 4) {
+        const int d = threadIdx.x >> 2, q = threadIdx.x & 3;
+        const int sl = s_nb[d];
+        if (sl >= 0) cp_async16(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
+        else *reinterpret_cast<uint4*>(s_m + d * 8 + 2 * q) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    cp_async_commit();
+}
+
+// Stage value at local voxel (x, y, z), x, y, z in [-2, 10).
+template <typename T>
+__device__ __forceinline__ const T* at(const T* stage, int x, int y, int z) {
+    return stage + ((x + kH) * kE + (y + kH)) * Row<T>::RP + Row<T>::Z0 + z;
+}
+
+// Godunov upwind |grad phi| for the sign of s.  Per axis the upwind one-sided
+// differences are u = max(sg (p - phi_-), 0) and w = max(sg (p - phi_+), 0),
+// sg = +-1 the sign of s (exact), and the axis term is max(u, w)^2, which
+// equals max(u^2, w^2) bit for bit (u, w >= 0 and rounding is monotone): the
+// same value as the sign-split form max(max(a-, 0)^2, min(a+, 0)^2) for s >=
+// 0 and its mirror for s < 0, without the sign branch.
+__device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym, float yp, float zm, float zp, float s) {
+    const float sg = (s >= 0.f) ? 1.f : -1.f;
+    const float mx = fmaxf(fmaxf(sg * (p - xm), 0.f), fmaxf(sg * (p - xp), 0.f));
+    const float my = fmaxf(fmaxf(sg * (p - ym), 0.f), fmaxf(sg * (p - yp), 0.f));
+    const float mz = fmaxf(fmaxf(sg * (p - zm), 0.f), fmaxf(sg * (p - zp), 0.f));
+    // squares rounded before the sums, as in the sign-split form (no contraction)
+    float g2 = __fmul_rn(mx, mx) + __fmul_rn(my, my);
+    g2 += __fmul_rn(mz, mz);
+    return sqrtf(g2);
+}
+
+// NaN marks a voxel of an unallocated leaf; a 6-neighbour stencil reads it as
+// copysign(hw, phi(centre)).
+__device__ __forceinline__ float nbv(float v, float centre, float hw) { return (v != v) ? copysignf(hw, centre) : v; }
+
+struct Nb6 {
+    float xm, xp, ym, yp, zm, zp;
+};
+
+// The 6 neighbours of the value at c (axis strides SX, SY, 1), NaNs resolved
+// against the centre value p.
+template <typename T, int SX, int SY>
+__device__ __forceinline__ Nb6 load_nb6(const T* c, float p, float hw) {
+    return Nb6{nbv(to_f(c[-SX]), p, hw), nbv(to_f(c[SX]), p, hw), nbv(to_f(c[-SY]), p, hw),
+               nbv(to_f(c[SY]), p, hw),  nbv(to_f(c[-1]), p, hw), nbv(to_f(c[1]), p, hw)};
+}
+
+__device__ __forceinline__ float godunov_update(float p, const Nb6& n, float s) {
+    const float G = godunov_g(p, n.xm, n.xp, n.ym, n.yp, n.zm, n.zp, s);
+    return p - 0.5f * s * (G - 1.0f);
+}
+
+// Subcell fix of the reinitialisation (Russo & Smereka, J. Comput. Phys. 163,
+// 2000): if the 6-neighbourhood of phi0 (the field before reinitialisation)
+// changes sign at this voxel, the distance to the interface estimated as
+// phi0 / |grad phi0| (per axis the largest of the central and the two
+// one-sided differences, at least 1e-6); NaN otherwise.  Cut voxels relax
+// toward it, phi <- phi - 1/2 (sign(phi0) |phi| - d), instead of taking the
+// Godunov update, so reinitialisation does not move the interface.
+__device__ __forceinline__ float cut_distance(float p, const Nb6& n) {
+    const bool cut = (p * n.xm < 0.f) | (p * n.xp < 0.f) | (p * n.ym < 0.f) | (p * n.yp < 0.f) |
+                     (p * n.zm < 0.f) | (p * n.zp < 0.f);
+    if (!cut) return __int_as_float(0x7fc00000);
+    const float mx = fmaxf(fmaxf(fabsf(n.xp - n.xm) * 0.5f, fabsf(n.xp - p)), fmaxf(fabsf(p - n.xm), 1e-6f));
+    const float my = fmaxf(fmaxf(fabsf(n.yp - n.ym) * 0.5f, fabsf(n.yp - p)), fmaxf(fabsf(p - n.ym), 1e-6f));
+    const float mz = fmaxf(fmaxf(fabsf(n.zp - n.zm) * 0.5f, fabsf(n.zp - p)), fmaxf(fabsf(p - n.zm), 1e-6f));
+    return p / sqrtf(mx * mx + my * my + mz * mz);
+}
+
+__device__ __forceinline__ float cut_relax(float phi, float phi0, float d) {
+    return phi - 0.5f * (copysignf(fabsf(phi), phi0) - d);
+}
+
+// 10-bit row of the dilated mask along z in [-1, 9) at (x, y) in [-1, 9)^2,
+// from the 27 neighbour masks (bit i = z + 1).
+__device__ __forceinline__ unsigned d_row(const uint64_t* s_m, int x, int y) {
+    const int base = nb_axis(x) * 9 + nb_axis(y) * 3;
+    const int bi = ((x & 7) << 3) | (y & 7);
+    const unsigned char* m = (const unsigned char*)s_m;
+    return ((unsigned)m[base * 64 + bi] >> 7) | ((unsigned)m[(base + 1) * 64 + bi] << 1) |
+           (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
+}
+
+// copysign(hw, value) of every voxel of the leaf, row by row into the output
+// (coalesced); the voxels of D are overwritten in phase 2.
+template <typename T>
+__device__ __forceinline__ void write_outside(const T* stage, T* __restrict__ out, float hw, int t) {
+    if (t >= 64) return;
+    const int x = t >> 3, y = t & 7;
+    const T* crow = at(stage, x, y, 0);
+    if constexpr (sizeof(T) == 2) {
+        const uint64_t h = __half_as_ushort(__float2half_rn(hw)) & 0x7fffu;
+        const uint64_t hw4 = h | (h << 16) | (h << 32) | (h << 48);
+        const uint64_t* c = reinterpret_cast<const uint64_t*>(crow);
+        const uint64_t a = hw4 | (c[0] & 0x8000800080008000ull), b = hw4 | (c[1] & 0x8000800080008000ull);
+        *reinterpret_cast<uint4*>(out + t * 8) =
+            make_uint4((unsigned)a, (unsigned)(a >> 32), (unsigned)b, (unsigned)(b >> 32));
+    } else {
+        const unsigned hb = __float_as_uint(hw) & 0x7fffffffu;
+        const uint4* c = reinterpret_cast<const uint4*>(crow);
+        uint4* o = reinterpret_cast<uint4*>(out + t * 8);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint4 v = c[h];
+            o[h] = make_uint4(hb | (v.x & 0x80000000u), hb | (v.y & 0x80000000u), hb | (v.z & 0x80000000u),
+                              hb | (v.w & 0x80000000u));
+        }
+    }
+}
+
+}  // namespace
+
+template <typename T, int NIT, int FIX>
+struct ReinitLayout {
+    static constexpr size_t stage = (size_t)kE * kE * Row<T>::RP * sizeof(T);
+    static constexpr size_t masks = (size_t)kNbr * 64;
+    static constexpr size_t p2 = NIT == 2 ? (size_t)kF * kF * kF * 4 : 0;               // phi2 on the 10^3 box
+    static constexpr size_t dist = (NIT == 2 && FIX) ? (size_t)kF * kF * kF * 4 : 0;    // cut distances
+    static constexpr size_t bytes = 2 * stage + 2 * masks + p2 + dist;
+    static_assert(stage % 16 == 0, "16-byte aligned buffers");
+};
+
+template <typename T, int NIT, int FIX>
+__global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __restrict__ src, T* __restrict__ dst,
+                                                     const MGridParams* __restrict__ params, MTopo topo,
+                                                     unsigned* __restrict__ err) {
+    dep_wait();
+    dep_launch();
+    if (step_aborted(err)) return;
+    using Lay = ReinitLayout<T, NIT, FIX>;
+    constexpr int RP = Row<T>::RP;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* const mk0 = smem_dyn + 2 * Lay::stage;
+    float* s_p2 = reinterpret_cast<float*>(mk0 + 2 * Lay::masks);
+    float* s_dist = reinterpret_cast<float*>(mk0 + 2 * Lay::masks + Lay::p2);
+    auto stage_of = [&](int b) { return reinterpret_cast<T*>(smem_dyn + b * Lay::stage); };
+    auto masks_of = [&](int b) { return reinterpret_cast<uint64_t*>(mk0 + b * Lay::masks); };
+    __shared__ unsigned s_desc[kNP];
+    __shared__ unsigned short s_list1[kNW][kRPW * kF];
+    __shared__ unsigned short s_list2[kNW][128];
+    __shared__ int s_nbr[2][32];
+    __shared__ __align__(16) unsigned s_M[16];
+
+    const int count = *A.count;
+    const int Gs = gridDim.x;
+    int li = blockIdx.x;
+    if (li >= count) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    for (int p = threadIdx.x; p < kNP; p += kNT) s_desc[p] = piece_desc<T>(p);
+    int slot = A.list[li];
+    int4 o = A.origin[slot];
+    if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
+    __syncthreads();
+    issue_stage<T>(s_desc, s_nbr[0], src, A.dmask, stage_of(0), masks_of(0));
+    int slot_n = (li + Gs < count) ? A.list[li + Gs] : -1;
+    float hw = params[o.w].hw;
+
+    for (unsigned it = 0;; ++it) {
+        const int b = it & 1;
+        int4 o_n = make_int4(0, 0, 0, -1);
+        if (slot_n >= 0) o_n = A.origin[slot_n];
+        const int nb_n = (warp == 0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
+        const int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
+        if (warp == 0) s_nbr[b ^ 1][lane] = nb_n;
+        cp_async_wait_all();
+        __syncthreads();  // barrier A: this leaf's stage is complete; the previous leaf is done
+        const T* stage = stage_of(b);
+        const uint64_t* s_m = masks_of(b);
+        const int* nbr = s_nbr[b];
+        T* out = dst + (size_t)slot * kLeafVoxels;
+        if (slot_n >= 0) issue_stage<T>(s_desc, s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1));
+        write_outside<T>(stage, out, hw, threadIdx.x);
+        if (threadIdx.x < 16) s_M[threadIdx.x] = 0u;
+        if (NIT == 2) {
+            // iteration 1 on this warp's rows of the 10^3 box: r = lane * kNW + warp
+            const int r = lane * kNW + warp;
+            const int rx = r / kF, ry = r - rx * kF;
+            unsigned row = 0;
+            if (r < kF * kF) {
+                // phi2 starts as phi1 on the row; iteration 1 overwrites the voxels of D
+                const T* c = at(stage, rx - 1, ry - 1, -1);
+                float* d2 = s_p2 + r * kF;
+#pragma unroll
+                for (int i = 0; i < kF; ++i) d2[i] = to_f(c[i]);
+                const int edges = (rx == 0 || rx == kF - 1) + (ry == 0 || ry == kF - 1);
+                const unsigned keep = edges == 0 ? 0x3FFu : (edges == 1 ? 0x1FEu : 0u);
+                row = d_row(s_m, rx - 1, ry - 1) & keep;
+            }
+            const int c = __popc(row);
+            int incl = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
+            }
+            const int nW = __shfl_sync(0xffffffffu, incl, 31);
+            int pos = incl - c;
+            unsigned short* wl = s_list1[warp];
+            while (row) {
+                const int z = __ffs(row) - 1;
+                row &= row - 1u;
+                wl[pos++] = (unsigned short)(r * kF + z);
+            }
+            __syncwarp();
+            for (int i = lane; i < nW; i += 32) {
+                const int t = wl[i];
+                const int rr = t / kF, zr = t - rr * kF;
+                const int xr = rr / kF, yr = rr - xr * kF;
+                const T* c1 = at(stage, xr - 1, yr - 1, zr - 1);
+                const float p = to_f(c1[0]);
+                const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p, hw);
+                const float d = FIX ? cut_distance(p, n) : __int_as_float(0x7fc00000);
+                if (FIX) s_dist[t] = d;
+                s_p2[t] = (d == d) ? cut_relax(p, p, d) : godunov_update(p, n, p * rsqrtf(p * p + 1.0f));
+            }
+        }
+        __syncthreads();  // barrier C: phi2 complete on the box, outside-D results stored
+        {
+            // iteration 2 (or 1) on the leaf's voxels of D: warp w takes x-planes
+            // w and w + 4; lane l the 4 bits 4 (l & 15) .. of plane w + 4 (l >> 4)
+            const uint64_t* dm = s_m + 13 * 8;
+            const int q = warp + kNW * (lane >> 4);
+            const unsigned bits = (unsigned)(dm[q] >> (4 * (lane & 15))) & 0xFu;
+            const int c = __popc(bits);
+            int incl = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
+            }
+            const int nW = __shfl_sync(0xffffffffu, incl, 31);
+            int pos = incl - c;
+            unsigned short* wl = s_list2[warp];
+            unsigned bb = bits;
+            while (bb) {
+                const int z = __ffs(bb) - 1;
+                bb &= bb - 1u;
+                wl[pos++] = (unsigned short)(q * 64 + 4 * (lane & 15) + z);
+            }
+            __syncwarp();
+            for (int i = lane; i < nW; i += 32) {
+                const int off = wl[i];
+                const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
+                const T* c1 = at(stage, x, y, z);
+                const float p1 = to_f(c1[0]);
+                float v;
+                if (NIT == 0) {
+                    v = p1;
+                } else if (NIT == 1) {
+                    const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p1, hw);
+                    const float d = FIX ? cut_distance(p1, n) : __int_as_float(0x7fc00000);
+                    v = (d == d) ? cut_relax(p1, p1, d) : godunov_update(p1, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                } else {
+                    const int t10 = ((x + 1) * kF + (y + 1)) * kF + (z + 1);
+                    const float* c2 = s_p2 + t10;
+                    const float p2 = c2[0];
+                    const float d = FIX ? s_dist[t10] : __int_as_float(0x7fc00000);
+                    if (d == d) {
+                        v = cut_relax(p2, p1, d);
+                    } else {
+                        const Nb6 n{nbv(c2[-kF * kF], p2, hw), nbv(c2[kF * kF], p2, hw), nbv(c2[-kF], p2, hw),
+                                    nbv(c2[kF], p2, hw),       nbv(c2[-1], p2, hw),      nbv(c2[1], p2, hw)};
+                        v = godunov_update(p2, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                    }
+                }
+                const bool on = fabsf(v) < hw;
+                if (!on) v = copysignf(hw, v);
+                out[off] = from_f<T>(v);
+                if (on) atomicOr(&s_M[off >> 5], 1u << (off & 31));
+            }
+        }
+        __syncthreads();  // barrier D: the new mask words are in shared memory
+        if (threadIdx.x < 16) reinterpret_cast<unsigned*>(A.mask + (size_t)slot * 8)[threadIdx.x] = s_M[threadIdx.x];
+        if (warp == 1) {
+            // spill mask from 64-bit (x*8+y) plane masks of z = 0, z = 7 and any z
+            const unsigned char* B = (const unsigned char*)s_M;
+            const unsigned b0 = B[lane], b1 = B[lane + 32];
+            const uint64_t z0 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 1u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 1u) << 32);
+            const uint64_t z7 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 0x80u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 0x80u) << 32);
+            const uint64_t za = (uint64_t)__ballot_sync(0xffffffffu, b0 != 0u) |
+                                ((uint64_t)__ballot_sync(0xffffffffu, b1 != 0u) << 32);
+            bool spl = false;
+            if (lane < kNbr && lane != 13) {
+                const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+                const uint64_t plane = dz < 0 ? z0 : (dz > 0 ? z7 : za);
+                const uint64_t xs = dx < 0 ? 0xFFull : (dx > 0 ? (0xFFull << 56) : ~0ull);
+                const uint64_t ys = dy < 0 ? 0x0101010101010101ull : (dy > 0 ? 0x8080808080808080ull : ~0ull);
+                spl = (plane & xs & ys) != 0ull;
+            }
+            // spill toward absent neighbours only: those are the proposals the
+            // allocation scan resolves (present ones are kept right here)
+            const unsigned sbits = __ballot_sync(0xffffffffu, spl && nbr[lane] < 0);
+            if (lane == 0) {
+                A.spill[slot] = sbits;
+                A.nonempty[slot] = (za != 0ull) ? 1 : 0;
+                if (za != 0ull) topo.keep[slot] = 1;
+            }
+            // re-tracking proposals: an existing neighbour touched by the spill
+            // survives; a missing one is proposed, keeping the proposer whose
+            // direction seen from the new leaf comes first (atomicMin).
+            if (spl) {
+                const int n = nbr[lane];
+                if (n >= 0) {
+                    topo.keep[n] = 1;
+                } else {
+                    const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+                    const MGridParams& P = params[o.w];
+                    const uint64_t key = mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy,
+                                              (long long)(o.z >> 3) + dz, o.w, P.base, topo.key_bits);
+                    bool done = false;
+                    if (key != kEmptyKey) {
+                        uint32_t m = (uint32_t)topo.hcap - 1u, pp = (uint32_t)mix64(key) & m;
+                        for (int probe = 0; probe < topo.hcap; ++probe) {
+                            const unsigned long long prev = atomicCAS((unsigned long long*)&topo.pkey[pp],
+                                                                      (unsigned long long)kEmptyKey,
+                                                                      (unsigned long long)key);
+                            if (prev == kEmptyKey || prev == key) {
+                                atomicMin(&topo.pval[pp], kNbr - 1 - lane);
+                                done = true;
+                                break;
+                            }
+                            pp = (pp + 1u) & m;
+                        }
+                    }
+                    if (!done) atomicOr(err, key == kEmptyKey ? kErrExtent : kErrHashFull);
+                }
+            }
+        }
+        if (slot_n < 0) break;
+        li += Gs;
+        slot = slot_n;
+        if (o_n.w != o.w) hw = params[o_n.w].hw;
+        o = o_n;
+        slot_n = slot_nn;
+    }
+}
+
+#define VLR_REINIT_ARGS(T) MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*
+#define VLR_INST_REINIT(T)                                            \
+    template __global__ void k_m_reinit<T, 0, 0>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 1, 0>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 2, 0>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 0, 1>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 1, 1>(VLR_REINIT_ARGS(T)); \
+    template __global__ void k_m_reinit<T, 2, 1>(VLR_REINIT_ARGS(T));
+VLR_INST_REINIT(float)
+VLR_INST_REINIT(__half)
+
+size_t reinit_smem_bytes(int precision_f16, int nit, int fix) {
+#define VLR_RS(T)                                                                                 \
+    (nit == 0 ? (fix ? ReinitLayout<T, 0, 1>::bytes : ReinitLayout<T, 0, 0>::bytes)              \
+              : nit == 1 ? (fix ? ReinitLayout<T, 1, 1>::bytes : ReinitLayout<T, 1, 0>::bytes)   \
+                         : (fix ? ReinitLayout<T, 2, 1>::bytes : ReinitLayout<T, 2, 0>::bytes))
+    return precision_f16 ? VLR_RS(__half) : VLR_RS(float);
+#undef VLR_RS
+}
+
+}  // namespace vlr

@@ -10,9 +10,9 @@
 // Launch shape of a stencil kernel: threads per CTA, persistent CTAs and the
 // staging of its halo tiles.
 struct StencilShape {
-    int nt = 0;       // 128 or 256 (0: not chosen)
+    int nt = 0;       // threads per CTA (128; 0: not chosen)
     int blocks = 0;   // grid size (CTAs per SM x SMs)
-    int stage = 0;    // 0: cp.async row copies, 1: TMA tensor copies per neighbour leaf
+    int stage = 0;    // staging of the halo tile: 0, row pieces by cp.async (the only mode)
 };
 
 // One timed candidate of the launch autotuner.
@@ -74,10 +74,6 @@ struct vlr_level_set {
     bool state_lost = false; // a step failed with VLR_ERR_TIMEOUT or VLR_ERR_CAPACITY: the state is undefined
     bool autotune = true;    // choose the shapes on the first step
     std::vector<TuneEntry> tune_log[2];  // candidates timed by the autotuner (advect, reinit)
-    // tensor maps of the stencil kernels' source pools for TMA staging:
-    // [0] advect (vals[0], halo maps_h[0]), [1] reinit (vals[1], halo 2)
-    vlr::StageMaps maps[2];
-    int maps_h[2] = {0, 0};  // halo the maps were encoded for (0: not yet)
     int scan_levels = 0;
 
     vlr::MLeafArrays arrays() const {

@@ -19,8 +19,6 @@
 // The reference's counterparts are dilate (src/tools/morphology.rs:20-35),
 // trim_narrow_band's deactivation (src/tools/level_set_track.rs:53-68) and
 // remove_empty_leaves (src/tree/internal.rs:231-247).
-#include <cudaTypedefs.h>
-
 #include <algorithm>
 
 #include "method_state.hpp"
@@ -422,94 +420,24 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
 // at 256 threads with every SM filled to the occupancy limit and cp.async
 // staging.
 
-// cuTensorMapEncodeTiled from the driver, found through the runtime (the
-// library links only cudart).
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
-                cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            f = nullptr;
-        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    }();
-    return fn;
-}
-
-// Tensor maps of a value pool (cap leaves of 512 values, x * 64 + y * 8 + z)
-// with the views and box shapes of StageMaps for halo H.
-static int encode_stage_maps(vlr_ctx* ctx, const void* pool, int cap, bool f16, int H, StageMaps* out) {
-    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-    if (!enc) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    if (reinterpret_cast<uintptr_t>(pool) % 16u)
-        return set_error(ctx, VLR_ERR_CUDA, "value pool is not 16-byte aligned for tensor copies");
-    const cuuint64_t es = f16 ? 2 : 4;
-    const cuuint64_t dims3[3] = {64, 8, (cuuint64_t)cap};  // (yz, x, slot)
-    const cuuint64_t strides3[2] = {64 * es, 512 * es};
-    const cuuint64_t dims4[4] = {8, 8, 8, (cuuint64_t)cap};  // (z, y, x, slot)
-    const cuuint64_t strides4[3] = {8 * es, 64 * es, 512 * es};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    *out = StageMaps{};
-    for (int i = 0; i < (f16 ? 4 : 8); ++i) {
-        const cuuint32_t ey = (i & 1) ? 8u : (cuuint32_t)H, ex = (i & 2) ? 8u : (cuuint32_t)H;
-        const cuuint32_t box3[3] = {ey * 8u, ex, 1u};
-        const cuuint32_t box4[4] = {4u, ey, ex, 1u};
-        const bool four = (i & 4) != 0;
-        CUresult r = enc(&out->m[i], f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                         four ? 4 : 3, const_cast<void*>(pool), four ? dims4 : dims3, four ? strides4 : strides3,
-                         four ? box4 : box3, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return set_error(ctx, VLR_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    }
-    return VLR_OK;
-}
-
-// Tensor maps of the source pool of the advect (which 0) or reinit (1) kernel.
-static int stage_maps(vlr_ctx* ctx, vlr_level_set* ls, int which, const StageMaps** out) {
-    const int H = which == 0 ? ls->halo : 2;
-    if (ls->maps_h[which] != H) {
-        int rc = encode_stage_maps(ctx, ls->vals[which], ls->cap, ls->precision == VLR_PREC_F16, H, &ls->maps[which]);
-        if (rc) return rc;
-        ls->maps_h[which] = H;
-    }
-    *out = &ls->maps[which];
-    return VLR_OK;
-}
-
-template <typename T, int H, int VK, int NT, int ST>
-static int launch_advect_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
-    const size_t smem = advect_smem_bytes(sizeof(T) == 2, H, ST);
-    const StageMaps* maps = nullptr;
-    int rc = stage_maps(ctx, ls, 0, &maps);
-    if (rc) return rc;
-    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, H, VK, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    VLR_TIMED(ctx, "k_m_advect",
-              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK, NT, ST>, blocks, NT, smem, ctx->stream, A,
-                                       (const T*)ls->vals[0], (T*)ls->vals[1], (const MGridParams*)ls->d_params,
-                                       (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword, *maps)));
-    return VLR_OK;
-}
-
 template <typename T, int H, int VK>
-static int launch_advect_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
-                               StencilShape sh) {
-    if (sh.stage)
-        return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128, 1>(ctx, ls, A, topo, sh.blocks)
-                            : launch_advect_nt<T, H, VK, 256, 1>(ctx, ls, A, topo, sh.blocks);
-    return sh.nt == 128 ? launch_advect_nt<T, H, VK, 128, 0>(ctx, ls, A, topo, sh.blocks)
-                        : launch_advect_nt<T, H, VK, 256, 0>(ctx, ls, A, topo, sh.blocks);
+static int launch_advect_vk(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
+    const size_t smem = advect_smem_bytes(sizeof(T) == 2, H);
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, H, VK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    VLR_TIMED(ctx, "k_m_advect",
+              VLR_CUDA(ctx, pdl_launch(k_m_advect<T, H, VK>, blocks, kAdvectThreads, smem, ctx->stream, A,
+                                       (const T*)ls->vals[0], (T*)ls->vals[1], (const MGridParams*)ls->d_params,
+                                       (const float2*)ls->d_tab, ls->sp, topo, ctx->d_errword)));
+    return VLR_OK;
 }
 
 template <typename T, int H>
-static int launch_advect_vk(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
-                            StencilShape sh) {
+static int launch_advect_h(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
     switch (ls->vel_kind) {
-        case MVEL_CONSTANT: return launch_advect_shape<T, H, MVEL_CONSTANT>(ctx, ls, A, topo, sh);
-        case MVEL_VORTEX: return launch_advect_shape<T, H, MVEL_VORTEX>(ctx, ls, A, topo, sh);
-        case MVEL_CURL: return launch_advect_shape<T, H, MVEL_CURL>(ctx, ls, A, topo, sh);
-        default: return launch_advect_shape<T, H, -1>(ctx, ls, A, topo, sh);
+        case MVEL_CONSTANT: return launch_advect_vk<T, H, MVEL_CONSTANT>(ctx, ls, A, topo, blocks);
+        case MVEL_VORTEX: return launch_advect_vk<T, H, MVEL_VORTEX>(ctx, ls, A, topo, blocks);
+        case MVEL_CURL: return launch_advect_vk<T, H, MVEL_CURL>(ctx, ls, A, topo, blocks);
+        default: return launch_advect_vk<T, H, -1>(ctx, ls, A, topo, blocks);
     }
 }
 
@@ -517,32 +445,26 @@ template <typename T>
 static int launch_advect(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
     MLeafArrays A = ls->arrays();
     MTopo topo = topo_of(ls);
-    return ls->halo == 2 ? launch_advect_vk<T, 2>(ctx, ls, A, topo, sh) : launch_advect_vk<T, 3>(ctx, ls, A, topo, sh);
+    return ls->halo == 2 ? launch_advect_h<T, 2>(ctx, ls, A, topo, sh.blocks)
+                         : launch_advect_h<T, 3>(ctx, ls, A, topo, sh.blocks);
 }
 
-template <typename T, int NIT, int NT, int ST>
-static int launch_reinit_nt(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
-    const size_t smem = reinit_smem_bytes(sizeof(T) == 2, ST);
-    const StageMaps* maps = nullptr;
-    int rc = stage_maps(ctx, ls, 1, &maps);
-    if (rc) return rc;
-    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, NIT, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <typename T, int NIT, int FIX>
+static int launch_reinit_fix(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
+    const size_t smem = reinit_smem_bytes(sizeof(T) == 2, NIT, FIX);
+    VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, NIT, FIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
     VLR_TIMED(ctx, "k_m_reinit",
-              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, NT, ST>, blocks, NT, smem, ctx->stream, A,
+              VLR_CUDA(ctx, pdl_launch(k_m_reinit<T, NIT, FIX>, blocks, kReinitThreads, smem, ctx->stream, A,
                                        (const T*)ls->vals[1], (T*)ls->vals[0], (const MGridParams*)ls->d_params,
-                                       topo, ls->sp.reinit_mode, ctx->d_errword, *maps)));
+                                       topo, ctx->d_errword)));
     return VLR_OK;
 }
 
 template <typename T, int NIT>
-static int launch_reinit_shape(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo,
-                               StencilShape sh) {
-    if (sh.stage)
-        return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128, 1>(ctx, ls, A, topo, sh.blocks)
-                            : launch_reinit_nt<T, NIT, 256, 1>(ctx, ls, A, topo, sh.blocks);
-    return sh.nt == 128 ? launch_reinit_nt<T, NIT, 128, 0>(ctx, ls, A, topo, sh.blocks)
-                        : launch_reinit_nt<T, NIT, 256, 0>(ctx, ls, A, topo, sh.blocks);
+static int launch_reinit_nit(vlr_ctx* ctx, vlr_level_set* ls, const MLeafArrays& A, const MTopo& topo, int blocks) {
+    return ls->sp.reinit_mode == 1 ? launch_reinit_fix<T, NIT, 1>(ctx, ls, A, topo, blocks)
+                                   : launch_reinit_fix<T, NIT, 0>(ctx, ls, A, topo, blocks);
 }
 
 template <typename T>
@@ -550,72 +472,80 @@ static int launch_reinit(vlr_ctx* ctx, vlr_level_set* ls, StencilShape sh) {
     MLeafArrays A = ls->arrays();
     MTopo topo = topo_of(ls);
     switch (ls->reinit_iters) {
-        case 0: return launch_reinit_shape<T, 0>(ctx, ls, A, topo, sh);
-        case 1: return launch_reinit_shape<T, 1>(ctx, ls, A, topo, sh);
-        default: return launch_reinit_shape<T, 2>(ctx, ls, A, topo, sh);
+        case 0: return launch_reinit_nit<T, 0>(ctx, ls, A, topo, sh.blocks);
+        case 1: return launch_reinit_nit<T, 1>(ctx, ls, A, topo, sh.blocks);
+        default: return launch_reinit_nit<T, 2>(ctx, ls, A, topo, sh.blocks);
     }
 }
 
-// Occupancy limit (CTAs per SM) of the stencil kernel of `which` (0 advect,
-// 1 reinit) at NT threads and staging mode ST.
-template <typename T, int NT, int ST>
-static int stencil_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int which, int* per_sm) {
+// Occupancy limit (CTAs per SM) of the advect kernel; every velocity kind
+// instantiates the same staging, so the mixed-kind kernel stands for the
+// register and shared-memory footprint.
+template <typename T>
+static int advect_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int* per_sm) {
     *per_sm = 0;
-    if (which == 0) {
-        const size_t smem = advect_smem_bytes(sizeof(T) == 2, ls->halo, ST);
-        // every velocity kind instantiates the same staging and tile, so the
-        // mixed-kind kernel stands for the register and smem footprint
-        if (ls->halo == 2) {
-            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 2, -1, NT, ST>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            VLR_CUDA(ctx,
-                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 2, -1, NT, ST>, NT, smem));
-        } else {
-            VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 3, -1, NT, ST>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            VLR_CUDA(ctx,
-                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 3, -1, NT, ST>, NT, smem));
-        }
-    } else {
-        const size_t smem = reinit_smem_bytes(sizeof(T) == 2, ST);
-        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = advect_smem_bytes(sizeof(T) == 2, ls->halo);
+    if (ls->halo == 2) {
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 2, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
-        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, NT, ST>, NT, smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 2, -1>, kAdvectThreads,
+                                                                    smem));
+    } else {
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_advect<T, 3, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_advect<T, 3, -1>, kAdvectThreads,
+                                                                    smem));
     }
     return VLR_OK;
 }
 
+// Occupancy limit (CTAs per SM) of the reinit kernel (its 2-iteration
+// instance at the level set's reinitialisation mode stands for all).
+template <typename T>
+static int reinit_occupancy(vlr_ctx* ctx, vlr_level_set* ls, int* per_sm) {
+    *per_sm = 0;
+    const int fix = ls->sp.reinit_mode == 1;
+    const size_t smem = reinit_smem_bytes(sizeof(T) == 2, 2, fix);
+    if (fix) {
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, 1>, kReinitThreads,
+                                                                    smem));
+    } else {
+        VLR_CUDA(ctx, cudaFuncSetAttribute(k_m_reinit<T, 2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        VLR_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_m_reinit<T, 2, 0>, kReinitThreads,
+                                                                    smem));
+    }
+    return VLR_OK;
+}
+
+// Candidate launch shapes of a stencil kernel (128 threads per CTA): the
+// occupancy limit, 3/4 and 1/2 of it, in persistent CTAs over all SMs.
 template <typename T>
 static int stencil_candidates(vlr_ctx* ctx, vlr_level_set* ls, int which, std::vector<StencilShape>& out) {
     out.clear();
-    for (int st : {0, 1})
-        for (int nt : {128, 256}) {
-            int occ = 0;
-            int rc = st ? (nt == 128 ? stencil_occupancy<T, 128, 1>(ctx, ls, which, &occ)
-                                     : stencil_occupancy<T, 256, 1>(ctx, ls, which, &occ))
-                        : (nt == 128 ? stencil_occupancy<T, 128, 0>(ctx, ls, which, &occ)
-                                     : stencil_occupancy<T, 256, 0>(ctx, ls, which, &occ));
-            if (rc) return rc;
-            if (occ < 1) continue;
-            int prev = -1;
-            for (int per_sm : {occ, (3 * occ + 3) / 4, (occ + 1) / 2}) {
-                if (per_sm < 1 || per_sm == prev) continue;
-                prev = per_sm;
-                out.push_back(StencilShape{nt, per_sm * ctx->sm_count, st});
-            }
-        }
+    int occ = 0;
+    int rc = which == 0 ? advect_occupancy<T>(ctx, ls, &occ) : reinit_occupancy<T>(ctx, ls, &occ);
+    if (rc) return rc;
+    int prev = -1;
+    for (int per_sm : {occ, (3 * occ + 3) / 4, (occ + 1) / 2}) {
+        if (per_sm < 1 || per_sm == prev) continue;
+        prev = per_sm;
+        out.push_back(StencilShape{which == 0 ? kAdvectThreads : kReinitThreads, per_sm * ctx->sm_count, 0});
+    }
     if (out.empty()) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
     return VLR_OK;
 }
 
-// The shape used when none has been chosen: 256 threads, occupancy-limited.
+// The shape used when none has been chosen: occupancy-limited.
 template <typename T>
 static int default_shape(vlr_ctx* ctx, vlr_level_set* ls, int which, StencilShape* sh) {
     int occ = 0;
-    int rc = stencil_occupancy<T, 256, 0>(ctx, ls, which, &occ);
+    int rc = which == 0 ? advect_occupancy<T>(ctx, ls, &occ) : reinit_occupancy<T>(ctx, ls, &occ);
     if (rc) return rc;
     if (occ < 1) return set_error(ctx, VLR_ERR_CUDA, "stencil kernel does not fit on an SM");
-    *sh = StencilShape{256, occ * ctx->sm_count, 0};
+    *sh = StencilShape{which == 0 ? kAdvectThreads : kReinitThreads, occ * ctx->sm_count, 0};
     return VLR_OK;
 }
 

@@ -209,8 +209,9 @@ class LevelSet:
 
     def set_launch_shape(self, advect=None, reinit=None):
         """Fix the stencil kernels' launch shapes as (threads, CTAs[, staging])
-        tuples (staging 0: cp.async row copies, 1: TMA tensor copies; default
-        0), or pass nothing to let the next step's autotuner choose them again."""
+        tuples (threads 128 and staging 0, cp.async row copies, are the only
+        kernels built), or pass nothing to let the next step's autotuner choose
+        the CTA counts again."""
         if advect is None:
             self.ctx.check(self.ctx.lib.vlr_ls_set_launch_shape(self.ctx.handle, self.handle, 0, 0, 0, 0, 0, 0),
                            "vlr_ls_set_launch_shape")

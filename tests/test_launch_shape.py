@@ -1,24 +1,21 @@
 """Launch shapes of the stencil kernels do not change results.
 
-The advect and reinitialisation kernels run at 128 or 256 threads per CTA
-over any number of persistent CTAs, chosen on a level set's first step by the
-launch autotuner (every candidate is launched on the same inputs and timed).
-Each leaf is computed by one CTA with the same arithmetic whatever the shape
-and whichever staging brought its halo tile into shared memory (16-byte
-cp.async row copies, or one TMA tensor copy per neighbour leaf), so every
-shape, and the autotuned step itself, must give bit-identical leaves, masks
-and values.
+The advect and reinitialisation kernels run at 128 threads per CTA over any
+number of persistent CTAs, chosen on a level set's first step by the launch
+autotuner (every candidate CTA count is launched on the same inputs and
+timed).  Each leaf is computed by one CTA with the same arithmetic whatever
+the CTA count, so every shape, and the autotuned step itself, must give
+bit-identical leaves, masks and values.
 """
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-# (threads, CTAs, staging): staging 0 = cp.async row copies, 1 = TMA tensor copies
-SHAPES = [((128, 148 * 8, 0), (128, 148 * 8, 0)), ((256, 148 * 4, 0), (256, 148 * 2, 0)),
-          ((128, 37, 0), (256, 19, 0)), ((256, 1, 0), (128, 1, 0)),
-          ((128, 148 * 7, 1), (128, 148 * 6, 1)), ((256, 148 * 2, 1), (256, 148 * 3, 1)),
-          ((128, 5, 1), (256, 1, 1)), ((256, 148 * 3, 0), (128, 148 * 5, 1))]
+# (threads, CTAs, staging): 128 threads and staging 0 (cp.async row copies) are the only kernels built
+SHAPES = [((128, 148 * 8, 0), (128, 148 * 8, 0)), ((128, 148 * 4, 0), (128, 148 * 2, 0)),
+          ((128, 37, 0), (128, 19, 0)), ((128, 1, 0), (128, 1, 0)),
+          ((128, 5, 0), (128, 148 * 6, 0)), ((128, 148 * 6, 0), (128, 2, 0))]
 
 
 def _same(a, b):
@@ -53,11 +50,11 @@ def test_results_independent_of_launch_shape(ctx, make, precision):
     ref = make(precision, None)  # autotuned on its first step
     ref.step(steps)
     tuned = ref.launch_shape()
-    assert tuned["advect"][0] in (128, 256) and tuned["reinit"][0] in (128, 256)
-    assert tuned["advect"][2] in (0, 1) and tuned["reinit"][2] in (0, 1)
-    assert len(tuned["timed"]) >= 8 and all(us > 0 for *_, us in tuned["timed"])
+    assert tuned["advect"][0] == 128 and tuned["reinit"][0] == 128
+    assert tuned["advect"][2] == 0 and tuned["reinit"][2] == 0
+    assert all(us > 0 for *_, us in tuned["timed"])
     for k in ("k_m_advect", "k_m_reinit"):
-        assert {st for name, _, _, st, _ in tuned["timed"] if name == k} == {0, 1}, "both stagings are timed"
+        assert len({c for name, _, c, _, _ in tuned["timed"] if name == k}) >= 2, "several CTA counts are timed"
     want = ref.arrays()
     ref.close()
     for shape in SHAPES:
@@ -73,6 +70,7 @@ def test_invalid_launch_shape_rejected(ctx):
     from sharc.volrus_b200._lib import VolrusError
     ls = _vortex(0, None)
     for bad in [((64, 100), (128, 100)), ((128, 0), (128, 100)), ((128, 100), (512, 100)),
+                ((256, 100), (128, 100)), ((128, 100), (256, 100)), ((128, 100, 1), (128, 100, 0)),
                 ((128, 100, 2), (128, 100, 0)), ((128, 100, 0), (128, 100, -1))]:
         with pytest.raises(VolrusError):
             ls.set_launch_shape(*bad)
