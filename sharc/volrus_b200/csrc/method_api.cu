@@ -486,7 +486,9 @@ int upload_enqueue(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, cons
     k_init_lists<<<ls->grid_blocks, 256, 0, ctx->stream>>>(ls->list, ls->free_stack, ls->scalars, (int)n, ls->cap,
                                                            reset_step ? 1 : 0);
     VLR_CUDA(ctx, cudaGetLastError());
-    return ls_enqueue_index(ctx, ls);
+    rc = ls_enqueue_index(ctx, ls);
+    if (rc == VLR_OK) ls->state_lost = false;  // a complete new state is on its way
+    return rc;
 }
 
 // Device-resident leaves: origins i32[3] -> the pool's int4 origins (origins
@@ -831,6 +833,7 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     if (3 * ls->key_bits > 63) {  // keys too wide for the device sort: the host sorts
         VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         rc = consume_device_errors(ctx, "vlr_ls_step_host");
+        if (rc == VLR_ERR_TIMEOUT || rc == VLR_ERR_CAPACITY) ls->state_lost = true;
         if (rc) return rc;
         return download_n(ctx, ls, (size_t)h[0], -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
     }
@@ -876,6 +879,7 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     VLR_CUDA(ctx, cudaMemcpyAsync(h, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(h + 1, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     rc = consume_device_errors(ctx, "vlr_ls_step_host");
+    if (rc == VLR_ERR_TIMEOUT || rc == VLR_ERR_CAPACITY) ls->state_lost = true;
     if (rc) return rc;
     const size_t n = (size_t)h[0];
     if (!h[1]) return download_n(ctx, ls, n, -1, nullptr, out_origins, out_masks, out_phi, cap_leaves, n_out);
