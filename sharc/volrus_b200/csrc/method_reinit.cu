@@ -281,7 +281,10 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         __syncthreads();  // barrier A: this leaf's stage is complete; the previous leaf is done
         const T* stage = stage_of(b);
         const uint64_t* s_m = masks_of(b);
-        const int* nbr = s_nbr[b];
+        // this leaf's neighbour slot for the lane's direction, read into a
+        // register here: the next iteration's neighbour row lands in this
+        // buffer before its barrier A, while warp 1 may still be proposing
+        const int my_nb = lane < kNbr ? s_nbr[b][lane] : -1;
         T* out = dst + (size_t)slot * kLeafVoxels;
         if (slot_n >= 0) issue_stage<T>(s_desc, s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1));
         write_outside<T>(stage, out, hw, threadIdx.x);
@@ -406,7 +409,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
             }
             // spill toward absent neighbours only: those are the proposals the
             // allocation scan resolves (present ones are kept right here)
-            const unsigned sbits = __ballot_sync(0xffffffffu, spl && nbr[lane] < 0);
+            const unsigned sbits = __ballot_sync(0xffffffffu, spl && my_nb < 0);
             if (lane == 0) {
                 A.spill[slot] = sbits;
                 A.nonempty[slot] = (za != 0ull) ? 1 : 0;
@@ -416,7 +419,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
             // survives; a missing one is proposed, keeping the proposer whose
             // direction seen from the new leaf comes first (atomicMin).
             if (spl) {
-                const int n = nbr[lane];
+                const int n = my_nb;
                 if (n >= 0) {
                     topo.keep[n] = 1;
                 } else {
