@@ -3,24 +3,33 @@
 
 Prints ONE JSON line on rank 0.  Metric: active voxels per second per step.
 
-Default workload ``deformation512`` (the deformation test): unit cube at
-512^3 voxels, sphere of radius 0.15 at (0.35, 0.35, 0.35), half-width 3,
-vortex velocity with period T = 3 sampled analytically, RK2 midpoint
-backtrace at CFL 0.5 (dt = 0.5 * vs / 2), two Godunov reinitialisation
-iterations and band re-tracking per step.  ``value`` is the FP16-leaf step;
-the plain FP32 step is reported beside it under ``fp32``.
+Default workload ``large8192``: one grid, the union of 8,000 seeded random
+spheres with radii U(6, 40) voxels and centres uniform in an 8192^3 index
+extent, half-width 3 (2.5 M leaves, 384 M active voxels), divergence-free
+curl-noise velocity (3 octaves, 1 voxel/step), SSP-RK3 backtrace, two Godunov
+reinitialisation iterations and band re-tracking per step.  ``value`` is the
+FP16-leaf step (f32 arithmetic); the plain FP32 step is under ``fp32``.
+Beside it: ``e2e`` (the host-resident step through vlr_ls_step_host, pinned
+buffers, copies inside the wall-clock timed region), ``ref_step`` (the
+crate's own advect_level_set + rebuild_narrow_band on the GPU over the same
+grid), ``data_path`` (constant velocity, Euler, no reinitialisation
+iteration), ``batched256`` and ``deformation512`` sections, the full-period
+accuracy runs, the level-set adjoint and volume_to_mesh.  ``cpu_baseline`` is
+the FP64 method oracle on a box of the grid on all host threads.
 
-Other workload: ``reference-sphere128`` (sphere r=32 in 128^3, v=(1,0.5,0.25),
-dt=1, hw=3; step = advect_level_set + rebuild_narrow_band, bit-exact with the
-reference's CPU code).
+Other workloads: ``deformation512`` (unit cube at 512^3, sphere r = 0.15,
+vortex T = 3, RK2 at CFL 0.5), ``batched256`` (256 uneven grids in one pool),
+``adjoint256``, ``reference-sphere128`` (sphere r = 32 in 128^3,
+v = (1, 0.5, 0.25), dt = 1, hw = 3; the crate's step, bit-exact), ``mesh96``
+and ``tools160``.
 
-Timing: W warm-up steps, then K timed steps, each bracketed by CUDA events on
-the library's stream; a 256 MiB write flushes the L2 between steps, outside
-the events.  ``e2e`` times the host-resident form of the step through the C
-ABI (upload from pinned host memory, one step, download) with a wall clock.
-``--impl reference`` times the reference algorithm on the host CPU (the C++
-restatement of the crate's advect_level_set + rebuild_narrow_band with its
-data structure, one thread as the crate runs it) on the same sphere.
+Timing: W warm-up steps, then exactly K timed steps, each bracketed by CUDA
+events on the library's stream; a 256 MiB write flushes the L2 between
+steps, outside the events.  ``--impl reference`` times the crate's own step
+(a C++ restatement of advect_level_set + rebuild_narrow_band with its data
+structure, one thread as the crate runs it) on the host CPU, for large8192 on
+a box of the same grid with the whole-grid rate extrapolated (see
+RefLargeSample).
 """
 from __future__ import annotations
 
@@ -201,6 +210,98 @@ def cpu_reference_algorithm(sphere: dict, velocity_world, dt: float, sample_voxe
                                f"voxels, extrapolated), 1 thread")
 
 
+LARGE_ORACLE_BOX = 1536   # FP64 method oracle sample: spheres near this box at the grid's centre
+LARGE_REF_BOX = 1024      # the crate's step sample: spheres near this box at the grid's centre
+
+
+def _large_box_spheres(args, box):
+    import numpy as np
+    from sharc.volrus_b200.method import large_sphere_grid, spheres_near_box
+    sph, vel = large_sphere_grid(args.large_spheres, LARGE["seed"])
+    lo = np.full(3, LARGE["extent"] / 2 - box / 2)
+    return sph, spheres_near_box(sph, lo, lo + box, 3.0), vel
+
+
+def cpu_method_oracle_large(args, threads: int | None = None):
+    """FP64 method oracle (the same RK3 + 2x Godunov + re-track step) on the
+    spheres of the large grid whose band reaches a 1536^3 box at its centre,
+    one step on all host threads; the rate per active voxel is that of the
+    whole grid, whose spheres are alike."""
+    import numpy as np
+    from oracle import pyoracle
+    threads = threads or os.cpu_count() or 1
+    _, sub, vel = _large_box_spheres(args, LARGE_ORACLE_BOX)
+    g = pyoracle.MOGrid.spheres(sub, 3.0)
+    n_act = int(np.unpackbits(g.arrays()[1].view(np.uint8)).sum())
+    t0 = time.perf_counter()
+    g.step(vel, 3, 2, 0.0, 1.0, threads)
+    t = time.perf_counter() - t0
+    return (n_act / t, threads,
+            f"FP64 method oracle, one SSP-RK3 + 2x Godunov + re-track step of the {len(sub)} spheres of the large "
+            f"grid near a {LARGE_ORACLE_BOX}^3 box at its centre ({n_act} active voxels) on {threads} host threads; "
+            f"rate per active voxel")
+
+
+class RefLargeSample:
+    """The crate's step (advect_level_set + rebuild_narrow_band, restated in C++
+    with its data structure, one thread as the crate runs it) on the spheres of
+    the large grid near a 1024^3 box at its centre, with the curl-noise
+    velocity sampled at every voxel of the band into three grids (the crate's
+    VelocityField).
+
+    The crate's rebuild_narrow_band (src/tools/level_set_track.rs:80-114)
+    loops, for every active voxel, over every zero crossing of the grid, so a
+    step of the whole grid costs advect + crossing search per voxel plus
+    (active voxels x crossings of the whole grid) distance evaluations.  Each
+    sample times advect and the crossing search over the box's grid and the
+    distance loop over `sample_voxels` voxels; the whole-grid rate is
+    1 / (t_advect/voxel + t_cross/voxel + t_pair x M), with M the box's
+    crossings scaled by the ratio of the whole grid's sphere area to the
+    box's."""
+
+    def __init__(self, args, sample_voxels: int = 200):
+        import numpy as np
+        from oracle import pyoracle
+        self.lib = pyoracle.load()
+        self.pyoracle = pyoracle
+        sph, sub, vel = _large_box_spheres(args, LARGE_REF_BOX)
+        o, m, p = pyoracle.MOGrid.spheres(sub, 3.0).arrays()
+        self.arrays = (o, m, p.astype(np.float32))
+        off = np.arange(512)
+        q = o[:, None, :].astype(np.float64) + np.stack([off >> 6, (off >> 3) & 7, off & 7], axis=1)[None]
+        u = curl_velocity(vel, q[..., 0], q[..., 1], q[..., 2], np)
+        self.vel = [pyoracle.OGrid.from_arrays(o, m, c.astype(np.float32), 0.0, 1.0) for c in u]
+        self.n_active = int(np.unpackbits(m.view(np.uint8)).sum())
+        self.area_ratio = float((sph[:, 3] ** 2).sum() / (sub[:, 3] ** 2).sum())
+        self.n_spheres = len(sub)
+        self.sample_voxels = sample_voxels
+
+    def step(self):
+        import ctypes as C
+        g = self.pyoracle.OGrid.from_arrays(*self.arrays, 3.0, 1.0)
+        h = C.c_void_p(g.h)
+        ta, tr, tc = C.c_double(), C.c_double(), C.c_double()
+        nr, nc = C.c_size_t(), C.c_size_t()
+        self.lib.vo_time_ref_step(C.byref(h), self.vel[0].h, self.vel[1].h, self.vel[2].h, 1.0, C.c_float(3.0),
+                                  self.sample_voxels, C.byref(ta), C.byref(tr), C.byref(nr), C.byref(tc),
+                                  C.byref(nc))
+        g.h = h.value
+        t_pair = max(tr.value - tc.value, 0.0) / max(nr.value * nc.value, 1)
+        per_voxel = (ta.value + tc.value) / self.n_active + t_pair * nc.value * self.area_ratio
+        box_per_voxel = (ta.value + tc.value) / self.n_active + t_pair * nc.value
+        return {"value": 1.0 / per_voxel, "box_value": 1.0 / box_per_voxel,
+                "advect_only_value": self.n_active / ta.value, "t_advect_s": ta.value, "t_cross_s": tc.value,
+                "t_pair_ns": t_pair * 1e9, "box_crossings": nc.value,
+                "grid_crossings_est": nc.value * self.area_ratio}
+
+    def describe(self):
+        return (f"the crate's step (C++ restatement of advect_level_set + rebuild_narrow_band with its tree, 1 thread) "
+                f"on the {self.n_spheres} spheres near a {LARGE_REF_BOX}^3 box at the grid's centre "
+                f"({self.n_active} active voxels, curl noise sampled into three grids); the distance loop on "
+                f"{self.sample_voxels} voxels; whole-grid rate from the per-voxel times and the box's crossings "
+                f"x {self.area_ratio:.1f} (sphere area of the grid / of the box's spheres)")
+
+
 # ---------------------------------------------------------------- GPU legs
 
 STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_t_nbr")
@@ -300,7 +401,7 @@ def time_steps(args, ctx, ls, flush, stream, clock=None, steps=None, warmup=None
             "kernels": {k: v[0] / max(v[1], 1) for k, v in kern.items()}, "ls": ls, "launch": ls.launch_shape()}
 
 
-def run_method(args, ctx, precision, flush, stream, clock=None):
+def run_method(args, ctx, precision, flush, stream, clock=None, steps=None):
     from sharc.volrus_b200.method import LevelSet
 
     vs = DEFORM["voxel_size"]
@@ -308,7 +409,7 @@ def run_method(args, ctx, precision, flush, stream, clock=None):
     dt = 0.5 * vs / 2.0
     ls = LevelSet.sphere(DEFORM["radius"], DEFORM["center"], vs, vel, dt, half_width=DEFORM["half_width"],
                          precision=precision, integrator=2, reinit_iters=2, ctx=ctx)
-    return time_steps(args, ctx, ls, flush, stream, clock)
+    return time_steps(args, ctx, ls, flush, stream, clock, steps=steps)
 
 
 def run_batched(args, ctx, precision, flush, stream, clock=None, steps=None):
@@ -342,46 +443,52 @@ class _Null:
         pass
 
 
-def e2e_method(args, ctx, ls, precision):
-    """Host-resident step through the C ABI: upload from pinned host, step, download."""
+def e2e_method(args, ctx, ls, precision, steps=None):
+    """Host-resident step through the C ABI (vlr_ls_step_host): upload of the
+    leaves from pinned host memory, one step, download of the result into
+    pinned host memory, all inside the wall-clock timed region."""
+    import ctypes as C
+
     import numpy as np
     import torch
+
+    from sharc.volrus_b200._lib import ptr
+    steps = steps or args.steps
     o, m, v = ls.arrays()
     n = len(o)
-    cap = n + 4096
-    pin_o = torch.empty((cap, 3), dtype=torch.int32).pin_memory().numpy()
-    pin_m = torch.empty((cap, 8), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
-    pin_v = torch.empty((cap, 512), dtype=torch.float32).pin_memory().numpy()
-    pin_o[:n], pin_m[:n], pin_v[:n] = o, m, v
-    out_o = torch.empty((cap, 3), dtype=torch.int32).pin_memory().numpy()
-    out_m = torch.empty((cap, 8), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
-    out_v = torch.empty((cap, 512), dtype=torch.float32).pin_memory().numpy()
-    import ctypes as C
-    from sharc.volrus_b200._lib import ptr
+    cap = n + n // 16 + 4096  # the band may gain leaves during the step
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    pin_o, pin_m, pin_v = pinned((n, 3), torch.int32), pinned((n, 8), torch.int64).view(np.uint64), \
+        pinned((n, 512), torch.float32)
+    pin_o[:], pin_m[:], pin_v[:] = o, m, v
+    del o, m, v
+    out_o, out_m, out_v = pinned((cap, 3), torch.int32), pinned((cap, 8), torch.int64).view(np.uint64), \
+        pinned((cap, 512), torch.float32)
     h2d = d2h = 0
-    cur = n
 
     def call():
-        nonlocal cur, h2d, d2h
+        nonlocal h2d, d2h
         nn = C.c_size_t()
         ctx.check(ctx.lib.vlr_ls_step_host(ctx.handle, ls.handle, ptr(pin_o, C.c_int32), ptr(pin_m, C.c_uint64),
-                                           ptr(pin_v, C.c_float), cur, 1, ptr(out_o, C.c_int32),
+                                           ptr(pin_v, C.c_float), n, 1, ptr(out_o, C.c_int32),
                                            ptr(out_m, C.c_uint64), ptr(out_v, C.c_float), cap, C.byref(nn)),
                   "vlr_ls_step_host")
-        h2d = cur * (12 + 64 + 2048)
+        h2d = n * (12 + 64 + 2048)
         d2h = nn.value * (12 + 64 + 2048)
         return nn.value
 
-    for _ in range(max(1, args.warmup)):
-        call()
+    call()
     _, a, _ = ls.info()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         call()
-    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = (time.perf_counter() - t0) / steps
     return {"value": a / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "seconds_per_step": e2e_s,
-            "path": "vlr_ls_step_host (upload, one step, download), pinned host buffers"}
+            "seconds_per_step": e2e_s, "steps": steps,
+            "path": "vlr_ls_step_host (upload, one step, sorted download), pinned host buffers, f32 values on the host"}
 
 
 def roofline_of(r, value_bytes, peak, peak_kind, workload):
@@ -569,19 +676,6 @@ def bench_adjoint(args, ctx):
             "kernels_launches_per_pass": {k: v[1] for k, v in kern.items()}}
 
 
-def large_grid(n_spheres: int, seed: int):
-    """One grid: n seeded random spheres, radii U(6, 40) voxels, centres uniform
-    in an 8192^3 extent, with a 3-octave curl-noise velocity of 1 voxel/step."""
-    import numpy as np
-    from sharc.volrus_b200.method import curl_noise
-    rng = np.random.default_rng(seed)
-    e = LARGE["extent"]
-    sph = np.column_stack([rng.uniform(0.0, e, (n_spheres, 3)), rng.uniform(*LARGE["radius"], n_spheres)])
-    vel = curl_noise(int(rng.integers(1 << 30)), e, 1.0, 3)
-    vel["domain"] = ((-256, -256, -256), (int(e) + 256, int(e) + 256, int(e) + 256))
-    return sph, vel
-
-
 def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
     """Frozen-band adjoint of a level set's own step (vlr_adj_create_level_set):
     K = steps, checkpoints every chk (~sqrt K), L = sum over the band of
@@ -629,14 +723,136 @@ def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
             "timing": "device buffers, CUDA events on the library stream (forward_device + backward_device)"}
 
 
-def bench_large_line(args, ctx, peak, peak_kind):
-    """The large single grid: FP16 line with FP32 beside it."""
-    import torch
+def large_config(args) -> dict:
+    """The large single grid's configuration (both arms print this dict)."""
+    return {"workload": "large8192", "spheres": args.large_spheres, "seed": LARGE["seed"], "extent": "8192^3",
+            "radius": "U(6, 40)", "velocity": "curl noise, 3 octaves, 1 voxel/step", "integrator": "SSP-RK3",
+            "dt": 1.0, "half_width": 3, "reinit_iters": 2,
+            "l2": "inputs larger than L2 (126 MB) and flushed between steps"}
+
+
+def curl_velocity(vel: dict, x, y, z, xp):
+    """Curl-noise velocity (voxels per unit time) at index points, the field of
+    the method's curl velocity: v = sum_o grad f_o x e_o with
+    f_o = A_o prod_a sin(k_o p_a + ph_{o,a}); `xp` is numpy or torch."""
+    u = [0.0 * x, 0.0 * x, 0.0 * x]
+    for A, k, ph, e in vel["octaves"]:
+        s = [xp.sin(k * q + f) for q, f in zip((x, y, z), ph)]
+        c = [xp.cos(k * q + f) for q, f in zip((x, y, z), ph)]
+        g = [A * k * c[0] * s[1] * s[2], A * k * s[0] * c[1] * s[2], A * k * s[0] * s[1] * c[2]]
+        u[0] = u[0] + g[1] * e[2] - g[2] * e[1]
+        u[1] = u[1] + g[2] * e[0] - g[0] * e[2]
+        u[2] = u[2] + g[0] * e[1] - g[1] * e[0]
+    return u
+
+
+def data_path(args, ctx, flush, stream, clk, sph, peak, peak_kind):
+    """The same grid with the lightest arithmetic the step allows: constant
+    velocity (0.6, -0.4, 0.3) voxels/step, Euler backtrace, no reinitialisation
+    iteration (trim and re-track only).  Shows what the staging and the
+    topology kernels reach on their own, and what FP16 storage buys there."""
     from sharc.volrus_b200.method import F16, F32, LevelSet
+    out = {"velocity": "constant (0.6, -0.4, 0.3) voxels/step", "integrator": "Euler", "reinit_iters": 0}
+    steps = min(args.steps, 10)
+    for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
+        ls = LevelSet.spheres([(sph, {"kind": "constant", "c": (0.6, -0.4, 0.3)})], 1.0, half_width=3.0,
+                              precision=prec, integrator=1, reinit_iters=0, ctx=ctx)
+        r = time_steps(args, ctx, ls, flush, stream, clk, steps=steps)
+        out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "steps": steps,
+                     "kernels_ms_per_launch": r["kernels"],
+                     "roofline": roofline_of(r, nb, peak, peak_kind, "large8192-data-path")}
+        ls.close()
+    out["fp16_over_fp32"] = out["f16"]["value"] / out["f32"]["value"]
+    return out
+
+
+def ref_step_leg(args, ctx, ls, flush, stream, clk):
+    """The crate's own step on the GPU, vlr_advect_level_set +
+    vlr_rebuild_narrow_band (src/tools/advection.rs:32-56,
+    src/tools/level_set_track.rs:80-114), over the same grid: the FP32 level
+    set's leaves as a world-unit grid (voxel size 1, background 3) and the
+    curl-noise velocity sampled at every voxel of those leaves into three grids
+    (the crate's VelocityField; the crate samples it at voxel positions, where
+    trilinear interpolation returns the voxel's own value).  Each timed step
+    advects the same input grid."""
+    import torch
+    from sharc.volrus_b200 import VelocityField
+    from sharc.volrus_b200.method import large_sphere_grid
+    from sharc.volrus_b200.tools import DeviceGrid, advect_level_set, rebuild_narrow_band
+    dev = torch.device("cuda", args.device)
+    n = ls.leaf_count()
+    o = torch.empty((n, 3), dtype=torch.int32, device=dev)
+    m = torch.empty((n, 8), dtype=torch.int64, device=dev)
+    p = torch.empty((n, 512), dtype=torch.float32, device=dev)
+    k = ls.download_device(o.data_ptr(), m.data_ptr(), p.data_ptr(), n)
+    lo = (o[:k] >> 3).long() + (1 << 20)
+    order = torch.argsort((lo[:, 0] << 42) | (lo[:, 1] << 21) | lo[:, 2])
+    o, m, p = o[:k][order].contiguous(), m[:k][order].contiguous(), p[:k][order].contiguous()
+    del lo, order
+    g0 = DeviceGrid.from_device(o.data_ptr(), m.data_ptr(), p.data_ptr(), k, 3.0, 1.0, ctx)
+    del p
+    _, vel = large_sphere_grid(args.large_spheres, LARGE["seed"])
+    off = torch.arange(512, device=dev)
+    rel = torch.stack([off >> 6, (off >> 3) & 7, off & 7], dim=1).double()
+    comps = [torch.empty((k, 512), dtype=torch.float32, device=dev) for _ in range(3)]
+    chunk = 1 << 16
+    for a in range(0, k, chunk):
+        b = min(k, a + chunk)
+        q = o[a:b].double()[:, None, :] + rel[None]
+        u = curl_velocity(vel, q[..., 0], q[..., 1], q[..., 2], torch)
+        for c in range(3):
+            comps[c][a:b] = u[c].float()
+    vgrids = [DeviceGrid.from_device(o.data_ptr(), m.data_ptr(), c.data_ptr(), k, 0.0, 1.0, ctx) for c in comps]
+    del comps, o, m
+    dvel = VelocityField(*vgrids)
+    n_active = g0.active_voxel_count()
+
+    def step():
+        out = advect_level_set(g0, dvel, 1.0, ctx=ctx)
+        rebuild_narrow_band(out, 3.0, ctx=ctx)
+        return out
+
+    for _ in range(2):
+        step().close()
+    ctx.synchronize()
+    steps = min(args.steps, 10)
+    times = []
+    ctx.profile(True)
+    with clk.mark():
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            out = step()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            ctx.synchronize()
+            times.append(e0.elapsed_time(e1))
+            out_active = out.active_voxel_count()
+            out.close()
+    kern = {kk: ctx.kernel_time(kk) for kk in ("k_advect_ref", "k_crossings", "k_rebuild_window")}
+    ctx.profile(False)
+    ms = sum(times) / len(times)
+    for gg in (g0, *vgrids):
+        gg.close()
+    return {"value": n_active / (ms * 1e-3), "unit": "voxels/s", "ms_per_step": ms, "steps": steps,
+            "leaves": k, "active_voxels": n_active, "active_after": out_active,
+            "kernels_ms_per_launch": {kk: v[0] / max(v[1], 1) for kk, v in kern.items()},
+            "step": "vlr_advect_level_set (three-grid curl-noise VelocityField, dt 1) + vlr_rebuild_narrow_band (hw 3), "
+                    "f32 world values: the crate's algorithm, bit-exact to its CPU code",
+            "timing": "CUDA events on the library stream, L2 flushed before each step, same input grid every step"}
+
+
+def bench_large_line(args, ctx, peak, peak_kind):
+    """The large single grid: FP16 line with FP32, the data-path diagnostic,
+    the crate's own step on the GPU and the end-to-end host step beside it."""
+    import torch
+    from sharc.volrus_b200.method import F16, F32, LevelSet, large_sphere_grid
     dev = torch.device("cuda", args.device)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    sph, vel = large_grid(args.large_spheres, LARGE["seed"])
+    sph, vel = large_sphere_grid(args.large_spheres, LARGE["seed"])
     out = {}
     with ClockSampler(args.device) as clk:
         for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
@@ -644,26 +860,61 @@ def bench_large_line(args, ctx, peak, peak_kind):
             ls = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=prec, integrator=3, reinit_iters=2,
                                   ctx=ctx)
             build_s = time.perf_counter() - t0
-            r = time_steps(args, ctx, ls, flush, stream, clk, steps=min(args.steps, 5))
+            r = time_steps(args, ctx, ls, flush, stream, clk)
             out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves": r["leaves"],
                          "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"],
-                         "launch_shape": r["launch"], "create_s": build_s,
+                         "launch_shape": r["launch"], "create_s": build_s, "_r": r,
                          "roofline": roofline_of(r, nb, peak, peak_kind, "large8192")}
-            if prec == F16 and not args.no_adjoint:
-                out["adjoint"] = bench_level_set_adjoint(args, ctx, ls)
+            if prec == F16:
+                out["e2e"] = e2e_method(args, ctx, ls, prec, steps=min(args.steps, 3))
+                if not args.no_adjoint:
+                    out["adjoint"] = bench_level_set_adjoint(args, ctx, ls)
+            elif not args.no_ref_step:
+                out["ref_step"] = ref_step_leg(args, ctx, ls, flush, stream, clk)
             ls.close()
+        if not args.no_data_path:
+            out["data_path"] = data_path(args, ctx, flush, stream, clk, sph, peak, peak_kind)
+        if not args.no_batched:
+            b = bench_batched(args, ctx, peak, peak_kind, flush, stream, clk, steps=min(args.steps, 10))
+            for kk in ("f16", "f32"):
+                b[kk].pop("_r", None)
+            out["batched256"] = b
+        if not args.no_deformation:
+            d = {}
+            for prec, name in ((F16, "f16"), (F32, "f32")):
+                r = run_method(args, ctx, prec, flush, stream, clk, steps=min(args.steps, 10))
+                d[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "leaves": r["leaves"],
+                           "active_voxels": r["active"], "kernels_ms_per_launch": r["kernels"]}
+                r["ls"].close()
+            d["fp16_over_fp32"] = d["f16"]["value"] / d["f32"]["value"]
+            d["config"] = {"workload": "deformation512", "domain": "unit cube at 512^3",
+                           "sphere": "r=0.15 at (0.35,0.35,0.35)", "velocity": "vortex T=3, analytic",
+                           "integrator": "RK2 midpoint", "cfl": 0.5, "half_width": 3, "reinit_iters": 2,
+                           "l2": "inputs smaller than L2; flushed between steps"}
+            out["deformation512"] = d
+    ck = clk.summary()
     f = out["f16"]
-    return {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
-            "dtype": "f16 storage, f32 arithmetic",
-            "config": {"workload": "large8192", "spheres": args.large_spheres, "extent": "8192^3",
-                       "radius": "U(6, 40)", "velocity": "curl noise, 3 octaves, 1 voxel/step",
-                       "integrator": "SSP-RK3", "half_width": 3, "reinit_iters": 2,
-                       "active_voxels": f["active_voxels"], "leaves": f["leaves"],
-                       "l2": "inputs larger than L2 and flushed between steps"},
-            "fp32": out["f32"], "fp16_over_fp32": f["value"] / out["f32"]["value"], "roofline": f["roofline"],
-            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "launch_shape": f["launch_shape"], "e2e": None,
-            "clocks": clk.summary(), "gpu_launches": len(STEP_KERNELS) * min(args.steps, 5),
-            "adjoint": out.get("adjoint")}
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = {"f16": full_period(args, ctx, F16), "f32": full_period(args, ctx, F32),
+                    "f16_subcell_fix": full_period(args, ctx, F16, reinit_mode=1)}
+    mesh = None if args.no_mesh else bench_mesh(args, ctx, peak, peak_kind)
+    line = {"metric": METRIC, "value": f["value"], "unit": "voxels/s", "ms_per_step": f["ms_per_step"],
+            "dtype": "f16 storage, f32 arithmetic", "config": large_config(args),
+            "active_voxels": f["active_voxels"], "leaves": f["leaves"], "create_s": f["create_s"],
+            "fp32": {k: v for k, v in out["f32"].items() if k != "_r"},
+            "fp16_over_fp32": f["value"] / out["f32"]["value"], "roofline": f["roofline"],
+            "issue_roofline": issue_roofline(f["_r"], "large8192", ck.get("sm_mhz")),
+            "kernels_ms_per_launch": f["kernels_ms_per_launch"], "launch_shape": f["launch_shape"],
+            "e2e": out["e2e"], "clocks": ck, "gpu_launches": len(STEP_KERNELS) * args.steps}
+    for k in ("ref_step", "data_path", "adjoint", "batched256", "deformation512"):
+        if k in out:
+            line[k] = out[k]
+    if accuracy is not None:
+        line["full_period"] = accuracy
+    if mesh is not None:
+        line["volume_to_mesh"] = mesh
+    return line
 
 
 MESH = dict(radius=96.0, center=(0.5, -0.25, 0.125), voxel_size=1.0, half_width=3.0)
@@ -1027,7 +1278,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["deformation512", "batched256", "large8192", "adjoint256",
                                            "reference-sphere128", "mesh96", "tools160"],
-                    default="deformation512")
+                    default="large8192")
     ap.add_argument("--grids", type=int, default=BATCH["grids"], help="grids of the batched workload")
     ap.add_argument("--large-spheres", type=int, default=LARGE["spheres"], help="spheres of the large single grid")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1035,6 +1286,9 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the full-period accuracy run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-mesh", action="store_true", help="skip the volume_to_mesh measurement")
+    ap.add_argument("--no-ref-step", action="store_true", help="skip the GPU run of the crate's own step (large8192)")
+    ap.add_argument("--no-data-path", action="store_true", help="skip the data-path diagnostic (large8192)")
+    ap.add_argument("--no-deformation", action="store_true", help="skip the deformation512 section (large8192)")
     ap.add_argument("--launch-shape", default="",
                     help="threads,CTAs[,staging] of advect then reinit, e.g. 128,1184,0,128,888,0 (default: "
                          "autotuned; 128 threads and staging 0 are the only kernels built)")
@@ -1082,6 +1336,25 @@ def main():
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": 1, "kind": "port",
                              "sample": "oracle restatement of volume_to_mesh on the full sphere, one call per step"},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+    if args.impl == "reference" and args.workload == "large8192":
+        if rank != 0:
+            return
+        ref = RefLargeSample(args)
+        for _ in range(args.warmup):
+            ref.step()
+        samples = [ref.step() for _ in range(args.steps)]
+        value = statistics.median(x["value"] for x in samples)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+            "config": large_config(args),
+            "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": 1, "kind": "port", "sample": ref.describe()},
+            "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "box": {k: statistics.median(x[k] for x in samples)
+                    for k in ("box_value", "advect_only_value", "t_advect_s", "t_cross_s", "t_pair_ns",
+                              "box_crossings", "grid_crossings_est")},
         }))
         return
     if args.impl == "reference":
@@ -1135,20 +1408,24 @@ def main():
     if world > 1:
         import torch.distributed as dist
         if args.workload != "batched256":
+            active = res.get("active_voxels", res["config"].get("active_voxels"))
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-            value = world * res["config"]["active_voxels"] / (ms * 1e-3)
+            value = world * active / (ms * 1e-3)
             if res.get("e2e"):
                 e = torch.tensor([res["e2e"]["seconds_per_step"]], device="cuda")
                 dist.all_reduce(e, op=dist.ReduceOp.MAX)
-                res["e2e"]["value"] = world * res["config"]["active_voxels"] / float(e.item())
+                res["e2e"]["value"] = world * active / float(e.item())
         dist.barrier()
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
             if args.workload == "deformation512":
                 v, cores, desc = cpu_method_oracle()
+                cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": desc}
+            elif args.workload == "large8192":
+                v, cores, desc = cpu_method_oracle_large(args)
                 cpu = {"value": v, "unit": "voxels/s", "cores": cores, "kind": "port", "sample": desc}
             elif args.workload == "reference-sphere128":
                 v, desc = cpu_reference_algorithm(sphere, vel_world, ref_dt)
@@ -1159,8 +1436,9 @@ def main():
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
                 "kernels_ms_per_launch": res["kernels_ms_per_launch"]}
-        for k in ("issue_roofline", "fp32", "fp16_over_fp32", "launch_shape", "batched256", "full_period", "adjoint",
-                  "volume_to_mesh", "tools_ms_per_call", "tools_voxels_per_s", "advect_particles"):
+        for k in ("active_voxels", "leaves", "create_s", "issue_roofline", "fp32", "fp16_over_fp32", "launch_shape",
+                  "ref_step", "data_path", "batched256", "deformation512", "full_period", "adjoint", "volume_to_mesh",
+                  "tools_ms_per_call", "tools_voxels_per_s", "advect_particles"):
             if k in res and res[k] is None:
                 continue
             if k in res:

@@ -88,6 +88,13 @@ int vlr_ctx_test_stall(vlr_ctx* ctx, int on);
  * Leaves must have distinct, 8-aligned origins; any order is accepted. */
 int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* origins,
                     const uint64_t* masks, const float* values, size_t n_leaves, vlr_grid** out);
+/* Device-resident form of vlr_grid_create, for leaves already in this
+ * context's device memory (origins i32[3], masks u64[8], values f32[512]):
+ * they must be sorted by (x, y, z) with distinct 8-aligned origins, the order
+ * a device grid keeps (VLR_ERR_INVALID otherwise).  Masks and values are
+ * copied on the device; only the origins visit the host. */
+int vlr_grid_create_device(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* d_origins,
+                           const uint64_t* d_masks, const float* d_values, size_t n_leaves, vlr_grid** out);
 /* Leaf count, active voxel count, background and transform of a grid. */
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf);
@@ -375,6 +382,25 @@ int vlr_ls_upload_device(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* d_origi
                          const float* d_phi, size_t n_leaves);
 int vlr_ls_download_device(vlr_ctx* ctx, const vlr_level_set* ls, int32_t* d_origins, uint64_t* d_masks,
                            float* d_phi, size_t cap_leaves, size_t* n_out);
+/* In-place edits of a single-grid level set's pool, for a grid divided over
+ * GPUs whose ranks keep their owned leaves resident.  Values travel in the
+ * pool's own type: f16[512] for an FP16 level set, f32[512] otherwise.
+ * vlr_ls_gather_device copies the leaves at list positions d_pos[0..n) (or
+ * the first n when d_pos is null) into device buffers: origins i32[3], and
+ * masks and values where those pointers are non-null; a position outside
+ * the list fails with VLR_ERR_INVALID.
+ * vlr_ls_edit_device drops the listed leaves whose d_drop byte (one per list
+ * position, n_list = the current leaf count) is non-zero, keeps the others in
+ * their order, appends n_add leaves (origins on the 8-voxel lattice, masks,
+ * values) and rebuilds the index.  No room for them fails with
+ * VLR_ERR_CAPACITY before anything changes; an added leaf off the lattice,
+ * outside the hashable range or already listed fails with a device error
+ * that leaves the state undefined until the next upload.  Both return after
+ * their work. */
+int vlr_ls_gather_device(vlr_ctx* ctx, const vlr_level_set* ls, const int32_t* d_pos, size_t n,
+                         int32_t* d_origins, uint64_t* d_masks, void* d_phi);
+int vlr_ls_edit_device(vlr_ctx* ctx, vlr_level_set* ls, const uint8_t* d_drop, size_t n_list,
+                       const int32_t* d_origins, const uint64_t* d_masks, const void* d_phi, size_t n_add);
 /* The host-resident form of n_steps steps in one call: replace the state with
  * host leaves (as vlr_ls_upload), step, and write the result (as
  * vlr_ls_download) into caller buffers of cap_leaves leaves; *n_out = leaves

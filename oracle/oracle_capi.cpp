@@ -217,7 +217,8 @@ size_t vo_volume_to_mesh(void* g, float iso, const int8_t* tri, double* verts, s
 // O(N x M) loop is extrapolated linearly from that sample).  Returns seconds
 // for advect and for the sampled rebuild; the advected grid replaces *g.
 void vo_time_ref_step(void** gp, void* vx, void* vy, void* vz, double dt, float hw,
-                      size_t rebuild_sample, double* t_advect, double* t_rebuild, size_t* n_rebuilt) {
+                      size_t rebuild_sample, double* t_advect, double* t_rebuild, size_t* n_rebuilt,
+                      double* t_cross, size_t* n_cross) {
     using clk = std::chrono::steady_clock;
     Grid* g = (Grid*)*gp;
     auto t0 = clk::now();
@@ -227,6 +228,7 @@ void vo_time_ref_step(void** gp, void* vx, void* vy, void* vz, double dt, float 
     float vs = (float)a->voxel_size;
     float band = hw * vs;
     auto cross = find_zero_crossings(*a);
+    auto t1c = clk::now();
     std::vector<std::pair<Coord, float>> active;
     a->for_each_active([&](Coord c, float v) { active.push_back({c, v}); });
     size_t n = active.size();
@@ -251,6 +253,8 @@ void vo_time_ref_step(void** gp, void* vx, void* vy, void* vz, double dt, float 
     *t_advect = std::chrono::duration<double>(t1 - t0).count();
     *t_rebuild = std::chrono::duration<double>(t2 - t1).count();
     *n_rebuilt = n;
+    if (t_cross) *t_cross = std::chrono::duration<double>(t1c - t1).count();
+    if (n_cross) *n_cross = cross.size();
     delete g;
     *gp = a;
 }

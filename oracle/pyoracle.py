@@ -51,7 +51,8 @@ SIGS = {
     "vo_flood_fill_sign": (None, [P]),
     "vo_volume_to_mesh": (C.c_size_t, [P, C.c_float, C.POINTER(C.c_int8), dbl_p, C.c_size_t,
                                        C.POINTER(C.c_uint32), C.c_size_t, size_p]),
-    "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p]),
+    "vo_time_ref_step": (None, [C.POINTER(P), P, P, P, C.c_double, C.c_float, C.c_size_t, dbl_p, dbl_p, size_p,
+                                dbl_p, size_p]),
     "vm_sphere": (P, [C.c_double, dbl_p, C.c_double, dbl_p, C.c_double]),
     "vm_free": (None, [P]),
     "vm_spheres": (P, [dbl_p, C.c_int, C.c_double]),

@@ -96,6 +96,7 @@ SIGNATURES = {
     "vlr_ctx_set_wait_limit": (C.c_int, [P, C.c_uint32]),
     "vlr_ctx_test_stall": (C.c_int, [P, C.c_int]),
     "vlr_grid_create": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, i32_p, u64_p, flt_p, C.c_size_t, PP]),
+    "vlr_grid_create_device": (C.c_int, [P, C.POINTER(vlr_transform), C.c_float, P, P, P, C.c_size_t, PP]),
     "vlr_grid_info": (C.c_int, [P, P, size_p, C.POINTER(C.c_uint64), flt_p, C.POINTER(vlr_transform)]),
     "vlr_grid_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
     "vlr_extend_velocity": (C.c_int, [P, P, P, P, P, C.c_float]),
@@ -153,6 +154,8 @@ SIGNATURES = {
     "vlr_ls_volume_partials": (C.c_int, [P, P, dbl_p, P, C.c_size_t, size_p]),
     "vlr_ls_upload_device": (C.c_int, [P, P, P, P, P, C.c_size_t]),
     "vlr_ls_download_device": (C.c_int, [P, P, P, P, P, C.c_size_t, size_p]),
+    "vlr_ls_gather_device": (C.c_int, [P, P, P, C.c_size_t, P, P, P]),
+    "vlr_ls_edit_device": (C.c_int, [P, P, P, C.c_size_t, P, P, P, C.c_size_t]),
     "vlr_ls_volume": (C.c_int, [P, P, dbl_p, dbl_p]),
     "vlr_ls_destroy": (None, [P]),
 }

@@ -232,6 +232,53 @@ int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, con
     return VLR_OK;
 }
 
+__global__ void k_origins_to_int4(const int32_t* o3, size_t n, int4* origin) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        origin[i] = make_int4(o3[3 * i], o3[3 * i + 1], o3[3 * i + 2], 0);
+}
+
+int vlr_grid_create_device(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* d_origins,
+                           const uint64_t* d_masks, const float* d_values, size_t n_leaves, vlr_grid** out) {
+    if (!ctx || !xf || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (n_leaves && (!d_origins || !d_masks || !d_values)) return set_error(ctx, VLR_ERR_INVALID, "null leaf arrays");
+    if (n_leaves > (size_t)(1 << 30)) return set_error(ctx, VLR_ERR_CAPACITY, "too many leaves");
+    *out = nullptr;
+    // the origins come to the host (12 bytes a leaf) for the order check and
+    // the hash-key base; masks and values stay on the device
+    std::vector<int32_t> o(3 * n_leaves);
+    if (n_leaves) {
+        VLR_CUDA(ctx, cudaMemcpyAsync(o.data(), d_origins, 12 * n_leaves, cudaMemcpyDeviceToHost, ctx->stream));
+        VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    for (size_t i = 0; i < 3 * n_leaves; ++i)
+        if (o[i] & 7) return set_error(ctx, VLR_ERR_INVALID, "leaf origin not a multiple of 8");
+    for (size_t i = 1; i < n_leaves; ++i)
+        if (!lex_less(&o[3 * (i - 1)], &o[3 * i]))
+            return set_error(ctx, VLR_ERR_INVALID, "device leaves not sorted by (x, y, z) or origin repeated");
+    vlr_grid* g = new_grid(ctx);
+    g->kind = VLR_KIND_F32_WORLD;
+    g->background = background;
+    g->xf = *xf;
+    int rc = choose_base(ctx, o.data(), n_leaves, g->base);
+    if (!rc) rc = grid_alloc(ctx, g, (int)std::max<size_t>(n_leaves, 1));
+    if (!rc && n_leaves) {
+        g->n = (int)n_leaves;
+        k_origins_to_int4<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>(d_origins, n_leaves, g->origin);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(g->mask, d_masks, 64 * n_leaves, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(g->values, d_values, 2048 * n_leaves, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) rc = check_cuda(ctx, e, "vlr_grid_create_device");
+    }
+    if (!rc) rc = grid_index(ctx, g);
+    if (rc) {
+        vlr_grid_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return VLR_OK;
+}
+
 int vlr_grid_info(vlr_ctx* ctx, const vlr_grid* g, size_t* n_leaves, uint64_t* n_active, float* background,
                   vlr_transform* xf) {
     if (!ctx || !g) return set_error(ctx, VLR_ERR_INVALID, "null argument");

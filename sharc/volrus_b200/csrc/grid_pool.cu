@@ -145,7 +145,11 @@ int consume_device_errors(vlr_ctx* ctx, const char* what) {
     if (e & kErrCapacity) { m += " leaf capacity exceeded;"; code = VLR_ERR_CAPACITY; }
     if (e & kErrHashFull) { m += " hash table full;"; code = VLR_ERR_CAPACITY; }
     if (e & kErrTimeout) { m += " bounded wait timed out;"; code = VLR_ERR_TIMEOUT; }
-    if (e & kErrInput) { m += " leaf origin not a multiple of 8;"; code = VLR_ERR_INVALID; }
+    if (e & kErrInput) {
+        m += " device input failed a check (a leaf origin off the 8-voxel lattice, a leaf listed twice or a list "
+             "position out of range);";
+        code = VLR_ERR_INVALID;
+    }
     return set_error(ctx, code, m);
 }
 

@@ -311,6 +311,11 @@ __global__ void k_h_insert(const int* list, const int* count_ptr, const int4* or
                 done = true;
                 break;
             }
+            if (prev == key) {  // the same leaf listed twice
+                atomicOr(err, kErrInput);
+                done = true;
+                break;
+            }
             p = (p + 1u) & m;
         }
         if (!done) atomicOr(err, kErrHashFull);

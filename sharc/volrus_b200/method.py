@@ -101,6 +101,34 @@ def random_sphere_grids(n_grids: int, seed: int, extent_log2=(6.0, 10.0), sphere
     return out
 
 
+def large_sphere_grid(n_spheres: int = 8000, seed: int = 7, extent: float = 8192.0, radius=(6.0, 40.0),
+                      amplitude: float = 1.0, octaves: int = 3):
+    """One large grid: n seeded random spheres, radii U(radius) voxels, centres
+    uniform in an extent^3 index box, with a curl-noise velocity of `amplitude`
+    voxels per unit time sampled over the extent plus a 256-voxel margin.
+    Returns (spheres (n, 4), velocity dict)."""
+    rng = np.random.default_rng(seed)
+    sph = np.column_stack([rng.uniform(0.0, extent, (n_spheres, 3)), rng.uniform(*radius, n_spheres)])
+    vel = curl_noise(int(rng.integers(1 << 30)), extent, amplitude, octaves)
+    m = 256
+    vel["domain"] = ((-m, -m, -m), (int(extent) + m, int(extent) + m, int(extent) + m))
+    return sph, vel
+
+
+def spheres_near_box(spheres: np.ndarray, lo, hi, margin: float) -> np.ndarray:
+    """Spheres whose narrow band (radius + margin) reaches the box [lo, hi)^3."""
+    c, r = spheres[:, :3], spheres[:, 3]
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    d = np.maximum(np.maximum(lo - c, c - hi), 0.0)
+    return spheres[np.sqrt((d * d).sum(axis=1)) <= r + margin]
+
+
+def leaves_in_box(origins: np.ndarray, lo, hi) -> np.ndarray:
+    """Boolean selector of the leaves whose 8^3 block lies inside [lo, hi)^3."""
+    o = np.asarray(origins)
+    return np.all((o >= np.asarray(lo)) & (o + 8 <= np.asarray(hi)), axis=1)
+
+
 class LevelSet:
     """A narrow-band level set (method grid) resident on the GPU."""
 
@@ -300,6 +328,26 @@ class LevelSet:
                                                            C.c_void_p(d_masks), C.c_void_p(d_phi), int(cap),
                                                            C.byref(k)), "vlr_ls_download_device")
         return k.value
+
+    def gather_device(self, d_pos: int | None, n: int, d_origins: int, d_masks: int | None = None,
+                      d_phi: int | None = None):
+        """Leaves at list positions ``d_pos[0..n)`` (device i32; None: the first
+        n) into device buffers: origins i32[3], and masks u64[8] and values
+        (the pool's type, f16 or f32 [512]) where given."""
+        self.ctx.check(self.ctx.lib.vlr_ls_gather_device(self.ctx.handle, self.handle, C.c_void_p(d_pos or None),
+                                                         int(n), C.c_void_p(d_origins), C.c_void_p(d_masks or None),
+                                                         C.c_void_p(d_phi or None)), "vlr_ls_gather_device")
+
+    def edit_device(self, d_drop: int | None, n_list: int, d_origins: int | None = None, d_masks: int | None = None,
+                    d_phi: int | None = None, n_add: int = 0):
+        """Drop the listed leaves whose ``d_drop`` byte is non-zero (one per list
+        position, ``n_list`` = the leaf count), keep the rest in order, append
+        ``n_add`` leaves (device origins i32[3], masks u64[8], values in the
+        pool's type) and rebuild the index."""
+        self.ctx.check(self.ctx.lib.vlr_ls_edit_device(self.ctx.handle, self.handle, C.c_void_p(d_drop or None),
+                                                       int(n_list), C.c_void_p(d_origins or None),
+                                                       C.c_void_p(d_masks or None), C.c_void_p(d_phi or None),
+                                                       int(n_add)), "vlr_ls_edit_device")
 
     def volume_partials(self, d_partials: int, cap: int, ref=(0.0, 0.0, 0.0)) -> int:
         """One FP64 volume term per allocated leaf, in list order, into a device

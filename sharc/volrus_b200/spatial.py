@@ -198,6 +198,59 @@ def _member(keys: torch.Tensor, sorted_set: torch.Tensor) -> torch.Tensor:
     return sorted_set[i] == keys
 
 
+def ghost_positions(c: torch.Tensor, part: Partition, rank: int) -> dict[int, torch.Tensor]:
+    """Per other rank q, the indices of the leaves at coordinates ``c`` (owned
+    by ``rank``) within GHOST_DEPTH leaves of a coordinate q owns."""
+    if len(c) == 0 or part.world == 1:
+        return {}
+    if part.world > 63:
+        raise NotImplementedError("more than 63 ranks")
+    d = GHOST_DEPTH
+    # the owners over a leaf's box lie between those of its corner keys (keys
+    # grow along each axis, owners along the keys): leaves whose whole box
+    # is this rank's send nothing
+    lo = part.owner(morton_keys_of_leaf_coords(c - d))
+    hi = part.owner(morton_keys_of_leaf_coords(c + d))
+    cand = torch.nonzero((lo != rank) | (hi != rank)).reshape(-1)
+    if len(cand) == 0:
+        return {}
+    offs = _offsets(d, c.device)
+    hits = {q: [] for q in range(part.world) if q != rank}
+    step = max(1, _CHUNK // len(offs))
+    for i in range(0, len(cand), step):
+        ci = cand[i:i + step]
+        box = (c[ci][:, None, :] + offs[None]).reshape(-1, 3)
+        own = part.owner(morton_keys_of_leaf_coords(box, False)).reshape(len(ci), len(offs))
+        for q in hits:
+            hits[q].append(ci[(own == q).any(dim=1)])
+    out = {}
+    for q, parts in hits.items():
+        sel = torch.cat(parts)
+        if len(sel):
+            out[q] = sel
+    return out
+
+
+def exact_outputs(k: torch.Tensor, c: torch.Tensor, owned_keys: torch.Tensor) -> torch.Tensor:
+    """Which outputs (keys ``k``, coordinates ``c``) of a local step are exact:
+    an owned input leaf itself, or a leaf with an owned input leaf
+    (``owned_keys``, sorted) among its 26 neighbours."""
+    exact = _member(k, owned_keys)
+    rest = torch.nonzero(~exact).reshape(-1)
+    if len(rest):
+        cr = c[rest]
+        morton_keys_of_leaf_coords(torch.cat([cr - 1, cr + 1]))  # range check of the whole 3^3 box
+        offs = _offsets(1, k.device)
+        step = max(1, _CHUNK // len(offs))
+        near = []
+        for i in range(0, len(cr), step):
+            box = (cr[i:i + step][:, None, :] + offs[None]).reshape(-1, 3)
+            near.append(_member(morton_keys_of_leaf_coords(box, False), owned_keys).reshape(-1, len(offs))
+                        .any(dim=1))
+        exact[rest] = torch.cat(near)
+    return exact
+
+
 class Shard:
     """The leaves one rank owns and the three local phases of a decomposed step."""
 
@@ -215,35 +268,7 @@ class Shard:
     # phase 1: ghost leaves for the other ranks
     def ghost_sends(self) -> dict[int, Leaves]:
         """Owned leaves within GHOST_DEPTH leaves of a coordinate another rank owns, per rank."""
-        if len(self.owned) == 0 or self.part.world == 1:
-            return {}
-        if self.part.world > 63:
-            raise NotImplementedError("more than 63 ranks")
-        c = self.owned.coords()
-        d = GHOST_DEPTH
-        # the owners over a leaf's box lie between those of its corner keys (keys
-        # grow along each axis, owners along the keys): leaves whose whole box
-        # is this rank's send nothing
-        lo = self.part.owner(morton_keys_of_leaf_coords(c - d))
-        hi = self.part.owner(morton_keys_of_leaf_coords(c + d))
-        cand = torch.nonzero((lo != self.rank) | (hi != self.rank)).reshape(-1)
-        out = {}
-        if len(cand) == 0:
-            return out
-        offs = _offsets(d, c.device)
-        hits = {q: [] for q in range(self.part.world) if q != self.rank}
-        step = max(1, _CHUNK // len(offs))
-        for i in range(0, len(cand), step):
-            ci = cand[i:i + step]
-            box = (c[ci][:, None, :] + offs[None]).reshape(-1, 3)
-            own = self.part.owner(morton_keys_of_leaf_coords(box, False)).reshape(len(ci), len(offs))
-            for q in hits:
-                hits[q].append(ci[(own == q).any(dim=1)])
-        for q, parts in hits.items():
-            sel = torch.cat(parts)
-            if len(sel):
-                out[q] = self.owned.take(sel)
-        return out
+        return {q: self.owned.take(sel) for q, sel in ghost_positions(self.owned.coords(), self.part, self.rank).items()}
 
     # phase 2: the single-device step on owned + ghost leaves
     def step_local(self, ghosts: Sequence[Leaves]) -> Leaves:
@@ -255,20 +280,7 @@ class Shard:
         an output that is itself an owned input leaf, or one with an owned
         input leaf among its 26 neighbours."""
         k = out.keys()
-        exact = _member(k, self.owned_keys)
-        rest = torch.nonzero(~exact).reshape(-1)
-        if len(rest):
-            cr = out.coords()[rest]
-            morton_keys_of_leaf_coords(torch.cat([cr - 1, cr + 1]))  # range check of the whole 3^3 box
-            offs = _offsets(1, k.device)
-            step = max(1, _CHUNK // len(offs))
-            near = []
-            for i in range(0, len(cr), step):
-                box = (cr[i:i + step][:, None, :] + offs[None]).reshape(-1, 3)
-                near.append(_member(morton_keys_of_leaf_coords(box, False), self.owned_keys).reshape(-1, len(offs))
-                            .any(dim=1))
-            exact[rest] = torch.cat(near)
-        sel = torch.nonzero(exact).reshape(-1)
+        sel = torch.nonzero(exact_outputs(k, out.coords(), self.owned_keys)).reshape(-1)
         own = self.part.owner(k[sel])
         return {int(q): out.take(sel[own == q]) for q in torch.unique(own).tolist()}
 
@@ -492,12 +504,261 @@ class DeviceStepper:
             self.ls = None
 
 
+class DevicePool:
+    """A rank's leaves resident in a single-grid ``LevelSet`` on its device.
+
+    Between steps the pool holds exactly the rank's owned leaves; during a
+    step it also holds the ghost ring.  Leaves come in and go out through the
+    pool edits of the C ABI (``vlr_ls_gather_device``, ``vlr_ls_edit_device``)
+    with values in the pool's own type (FP16 for an FP16 level set), so a
+    ghost is its owner's copy bit for bit and the owned leaves never leave
+    HBM.  The level set is re-created from its own leaves (step counter
+    carried over, values converted f16 -> f32 -> f16 exactly) when the leaves
+    it must hold outgrow half its capacity, or, for a curl velocity without a
+    domain, come within 64 voxels of the box its tables cover."""
+
+    def __init__(self, leaves: Leaves, velocity: dict, dt: float, half_width: float = 3.0, precision: int = 1,
+                 integrator: int = 3, reinit_iters: int = 2, t0: float = 0.0, reinit_mode: int = 0, ctx=None,
+                 margin: int = 512):
+        self.velocity, self.dt, self.hw = dict(velocity), dt, half_width
+        self.precision, self.integrator, self.reinit_iters = precision, integrator, reinit_iters
+        self.t0, self.reinit_mode, self.ctx, self.margin = t0, reinit_mode, ctx, margin
+        self.device = leaves.device
+        self.dtype = torch.float16 if precision == 1 else torch.float32
+        self.steps = 0
+        self.ls = None
+        self.box = None
+        self._create(leaves, 2 * len(leaves))
+
+    def _create(self, lv: Leaves, room: int):
+        from .method import LevelSet
+        if self.ls is not None:
+            self.ls.close()
+        o, m, p = lv.numpy()
+        vel = dict(self.velocity)
+        self.box = None
+        if vel["kind"] == "curl" and "domain" not in vel:
+            # tables of sin/cos per integer index: the same values whatever box they cover
+            lo = (o.min(axis=0) if len(o) else np.zeros(3, np.int64)) - self.margin
+            hi = (o.max(axis=0) if len(o) else np.zeros(3, np.int64)) + 7 + self.margin
+            vel["domain"] = (tuple(int(v) for v in lo), tuple(int(v) for v in hi))
+            self.box = (lo, hi)
+        self.cap = 2 * max(room, len(lv)) + 4096
+        self.ls = LevelSet.from_leaves(o, m, p.astype(np.float32), vel, self.dt, self.hw, self.precision,
+                                       self.integrator, self.reinit_iters, self.t0, self.cap, self.reinit_mode,
+                                       ctx=self.ctx)
+        self.ls.set_step(self.steps)
+
+    def _sync(self):
+        if self.device.type == "cuda":
+            torch.cuda.current_stream(self.device).synchronize()  # the library runs on its own stream
+
+    def count(self) -> int:
+        return self.ls.leaf_count()
+
+    def origins(self) -> torch.Tensor:
+        n = self.count()
+        o = torch.empty((n, 3), dtype=torch.int32, device=self.device)
+        self._sync()
+        self.ls.gather_device(None, n, o.data_ptr())
+        return o
+
+    def gather(self, pos: torch.Tensor | None = None) -> Leaves:
+        """Leaves at list positions ``pos`` (all when None), values in the pool's type."""
+        n = self.count() if pos is None else len(pos)
+        out = Leaves(torch.empty((n, 3), dtype=torch.int32, device=self.device),
+                     torch.empty((n, 8), dtype=torch.int64, device=self.device),
+                     torch.empty((n, 512), dtype=self.dtype, device=self.device))
+        if n:
+            p = None if pos is None else pos.to(device=self.device, dtype=torch.int32).contiguous()
+            self._sync()
+            self.ls.gather_device(None if p is None else p.data_ptr(), n, out.origins.data_ptr(),
+                                  out.masks.data_ptr(), out.phi.data_ptr())
+        return out
+
+    def _room(self, n_new: int):
+        """Re-create the level set if ``n_new`` leaves (and the step's growth)
+        would not fit, or would leave the velocity tables' box."""
+        if 2 * n_new + 64 <= self.cap and self.box is None:
+            return
+        o = self.origins()
+        inside = True
+        if self.box is not None and len(o):
+            lo = o.min(dim=0).values.cpu().numpy()
+            hi = o.max(dim=0).values.cpu().numpy() + 7
+            inside = bool(np.all(lo >= self.box[0] + 64) and np.all(hi <= self.box[1] - 64))
+        if 2 * n_new + 64 > self.cap or not inside:
+            self._create(self.gather(), n_new)
+
+    def edit(self, drop: torch.Tensor | None, add: Leaves):
+        """Drop the listed leaves flagged in ``drop`` (bool per list position;
+        None drops none), keep the rest in order, append ``add``."""
+        n = self.count()
+        keep_n = n if drop is None else n - int(drop.sum())
+        self._room(keep_n + len(add))
+        n = self.count()  # unchanged by a re-creation, which keeps the list order
+        d = torch.zeros(n, dtype=torch.uint8, device=self.device) if drop is None else \
+            drop.to(device=self.device, dtype=torch.uint8).contiguous()
+        a = Leaves(add.origins.to(self.device, torch.int32).contiguous(),
+                   add.masks.to(self.device, torch.int64).contiguous(),
+                   add.phi.to(self.device, self.dtype).contiguous())
+        self._sync()
+        self.ls.edit_device(d.data_ptr() if n else None, n, a.origins.data_ptr() if len(a) else None,
+                            a.masks.data_ptr() if len(a) else None, a.phi.data_ptr() if len(a) else None, len(a))
+
+    def step(self):
+        self._room(self.count())
+        self.ls.step(1)
+        self.steps += 1
+
+    def skip(self):
+        """A step of a rank with no leaves: only the counter moves."""
+        self.steps += 1
+        self.ls.set_step(self.steps)
+
+    def volume_partials(self, ref=(0.0, 0.0, 0.0)) -> torch.Tensor:
+        n = self.count()
+        buf = torch.empty(max(n, 1), dtype=torch.float64, device=self.device)
+        self._sync()
+        self.ls.volume_partials(buf.data_ptr(), len(buf), ref)
+        return buf[:n]
+
+    def close(self):
+        if self.ls is not None:
+            self.ls.close()
+            self.ls = None
+
+
+class ResidentShard:
+    """A shard whose owned leaves stay in a leaf pool (``DevicePool``) between
+    steps.  The phases are those of ``Shard`` with the same selections
+    (``ghost_positions``, ``exact_outputs``) over the pool's list: ghosts are
+    gathered from the pool and added to the receiving pool in place; after
+    the step the pool drops what the rank does not own and appends the exact
+    outputs other ranks computed for it (a key it already holds keeps its own
+    copy, which is the same bits).  Any object with the pool's methods
+    (count, origins, gather, edit, step, skip, volume_partials, device,
+    dtype) serves."""
+
+    def __init__(self, rank: int, part: Partition, pool, check_duplicates: bool = False):
+        self.rank, self.part, self.pool = rank, part, pool
+        self.check_duplicates = check_duplicates
+        self.like = Leaves.empty(pool.dtype, pool.device)
+        self.owned_keys = torch.sort(morton_keys_of_leaf_coords(pool.origins() >> 3)).values
+        self._keep = None
+        self._keys = None
+
+    @property
+    def owned(self) -> Leaves:
+        """The owned leaves (gathered from the pool; values in its type)."""
+        return self.pool.gather()
+
+    def ghost_sends(self) -> dict[int, Leaves]:
+        c = self.pool.origins() >> 3
+        return {q: self.pool.gather(sel) for q, sel in ghost_positions(c, self.part, self.rank).items()}
+
+    def step_local(self, ghosts: Sequence[Leaves]):
+        self.pool.edit(None, Leaves.concat(list(ghosts), self.like))
+        if self.pool.count():
+            self.pool.step()
+        else:
+            self.pool.skip()
+
+    def route(self, _out=None) -> dict[int, Leaves]:
+        o = self.pool.origins()
+        c = o >> 3
+        k = morton_keys_of_leaf_coords(c)
+        exact = exact_outputs(k, c, self.owned_keys)
+        own = self.part.owner(k)
+        self._keep = exact & (own == self.rank)
+        self._keys = k
+        sel = torch.nonzero(exact & (own != self.rank)).reshape(-1)
+        own_s = own[sel]
+        return {int(q): self.pool.gather(sel[own_s == q]) for q in torch.unique(own_s).tolist()}
+
+    def absorb(self, parts: Sequence[Leaves]):
+        recv = Leaves.concat(list(parts), self.like)
+        kept_keys = torch.sort(self._keys[self._keep]).values
+        if len(recv):
+            rk = recv.keys()
+            ks, order = torch.sort(rk, stable=True)
+            first = torch.ones(len(ks), dtype=torch.bool, device=ks.device)
+            first[1:] = ks[1:] != ks[:-1]
+            new = first & ~_member(ks, kept_keys)
+            if self.check_duplicates:
+                self._check_copies(recv, ks, order, first, kept_keys)
+            recv = recv.take(order[new])
+            add_keys = ks[new]
+        else:
+            add_keys = torch.zeros(0, dtype=torch.int64, device=kept_keys.device)
+        self.pool.edit(~self._keep, recv)
+        self.owned_keys = torch.sort(torch.cat([kept_keys, add_keys.to(kept_keys.device)])).values
+        self._keep = self._keys = None
+
+    def _check_copies(self, recv, ks, order, first, kept_keys):
+        """A key that arrives twice, or that this rank keeps too, must carry the same bits."""
+        dup = torch.nonzero(~first).reshape(-1)
+        a, b = order[dup - 1], order[dup]
+        same = torch.equal(recv.masks[a], recv.masks[b]) and torch.equal(
+            recv.phi[a].contiguous().view(torch.uint8), recv.phi[b].contiguous().view(torch.uint8))
+        held = torch.nonzero(first & _member(ks, kept_keys)).reshape(-1)
+        if len(held):
+            pos = torch.nonzero(self._keep).reshape(-1)
+            mine = self.pool.gather(pos)
+            mk, mo = torch.sort(mine.keys())
+            j = torch.searchsorted(mk, ks[held])
+            r, m = recv.take(order[held]), mine.take(mo[j])
+            same = same and torch.equal(r.masks, m.masks) and torch.equal(
+                r.phi.contiguous().view(torch.uint8), m.phi.contiguous().view(torch.uint8))
+        if not same:
+            raise AssertionError("a leaf arrived from two ranks with different contents")
+
+    def migrate(self, part: Partition) -> dict[int, Leaves]:
+        """All pool leaves grouped by their owner under a new partition; the
+        following absorb replaces the pool with what arrives."""
+        self.part = part
+        o = self.pool.origins()
+        k = morton_keys_of_leaf_coords(o >> 3)
+        own = part.owner(k)
+        self._keep = torch.zeros(len(k), dtype=torch.bool, device=k.device)
+        self._keys = k
+        return {int(q): self.pool.gather(torch.nonzero(own == q).reshape(-1)) for q in torch.unique(own).tolist()}
+
+    def volume(self, ghosts: Sequence[Leaves], ref=(0.0, 0.0, 0.0)) -> float:
+        """FP64 enclosed volume of the owned leaves, the ghosts supplying the
+        gradients at the range's edges (added for the call, dropped after)."""
+        n_owned = self.pool.count()
+        add = Leaves.concat(list(ghosts), self.like)
+        self.pool.edit(None, add)
+        v = float(self.pool.volume_partials(ref)[:n_owned].sum()) if n_owned else 0.0
+        drop = torch.zeros(self.pool.count(), dtype=torch.bool, device=self.pool.device)
+        drop[n_owned:] = True
+        self.pool.edit(drop, Leaves.empty(self.pool.dtype, self.pool.device))
+        return v
+
+
+def emulate_resident(leaves: Leaves, world: int, make_pool: Callable[[int, Leaves], object], steps: int,
+                     rebalance_every: int = 0, check_duplicates: bool = True):
+    """``emulate`` with resident shards: ``make_pool(rank, owned leaves)``
+    builds each rank's pool.  Returns the union of the owned leaves in
+    (x, y, z) order (values in the pools' type) and the shards."""
+    part, shares = split(leaves, world)
+    shards = [ResidentShard(r, part, make_pool(r, shares[r]), check_duplicates) for r in range(world)]
+    ex = LocalExchange()
+    for s in range(steps):
+        step_shards(shards, ex)
+        if rebalance_every and (s + 1) % rebalance_every == 0:
+            rebalance_shards(shards, ex)
+    return Leaves.concat([sh.owned for sh in shards], shards[0].like).sorted_xyz(), shards
+
+
 def volume_shards(shards: Sequence[Shard], exchange, ref=(0.0, 0.0, 0.0)) -> list[float]:
     """Each shard's FP64 volume over its owned leaves, with the ghost ring
     exchanged first so the gradients at the range edges are the undivided
     grid's.  The stepper must provide ``volume(leaves, n_owned, ref)``."""
     ghosts = exchange([s.ghost_sends() for s in shards])
-    return [s.stepper.volume(Leaves.concat([s.owned, *g], s.like), len(s.owned), ref) for s, g in zip(shards, ghosts)]
+    return [s.volume(g, ref) if isinstance(s, ResidentShard) else
+            s.stepper.volume(Leaves.concat([s.owned, *g], s.like), len(s.owned), ref) for s, g in zip(shards, ghosts)]
 
 
 def split(leaves: Leaves, world: int) -> tuple[Partition, list[Leaves]]:
@@ -534,11 +795,22 @@ class SpatialLevelSet:
     first transfer of a group is an all_gather that every rank joins, so the
     point-to-point batches that follow may leave a rank out."""
 
-    def __init__(self, leaves: Leaves, stepper: Callable[[Leaves], Leaves], group=None,
-                 check_duplicates: bool = False):
-        self.ex = DistExchange(Leaves.empty(leaves.phi.dtype, leaves.device), group)
-        part, shares = split(leaves, self.ex.world)
-        self.shard = Shard(self.ex.rank, part, shares[self.ex.rank], stepper, check_duplicates)
+    def __init__(self, leaves: Leaves, stepper: Callable[[Leaves], Leaves] | None = None, group=None,
+                 check_duplicates: bool = False, make_pool: Callable[[Leaves], object] | None = None):
+        """``stepper`` steps the local leaves copied in and out each step
+        (``DeviceStepper``); ``make_pool(owned leaves)`` instead keeps them
+        resident in a leaf pool (``DevicePool``) and moves only ghosts and
+        routed outputs."""
+        import torch.distributed as dist
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+        part, shares = split(leaves, world)
+        if make_pool is not None:
+            pool = make_pool(shares[rank])
+            self.ex = DistExchange(Leaves.empty(pool.dtype, pool.device), group)
+            self.shard = ResidentShard(rank, part, pool, check_duplicates)
+        else:
+            self.ex = DistExchange(Leaves.empty(leaves.phi.dtype, leaves.device), group)
+            self.shard = Shard(rank, part, shares[rank], stepper, check_duplicates)
 
     def step(self, n: int = 1):
         for _ in range(n):

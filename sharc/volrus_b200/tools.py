@@ -50,6 +50,20 @@ class DeviceGrid:
                   "vlr_grid_create")
         return cls(ctx, h, grid.name, grid.grid_class)
 
+    @classmethod
+    def from_device(cls, d_origins: int, d_masks: int, d_values: int, n: int, background: float,
+                    voxel_size: float = 1.0, ctx: Context | None = None) -> "DeviceGrid":
+        """A grid from n leaves in device memory (pointers: i32[3] origins, u64[8]
+        masks, f32[512] world-unit values), sorted by (x, y, z), with the
+        transform of a voxel size and zero origin."""
+        ctx = ctx or Context.default()
+        t = Grid(background, voxel_size).c_transform()
+        h = C.c_void_p()
+        ctx.check(ctx.lib.vlr_grid_create_device(ctx.handle, C.byref(t), C.c_float(background), C.c_void_p(d_origins),
+                                                 C.c_void_p(d_masks), C.c_void_p(d_values), int(n), C.byref(h)),
+                  "vlr_grid_create_device")
+        return cls(ctx, h)
+
     def info(self):
         n = C.c_size_t()
         a = C.c_uint64()

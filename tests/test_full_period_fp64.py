@@ -2,30 +2,27 @@
 
 The deformation configuration (sphere r = 0.15 at (0.35, 0.35, 0.35) in the
 unit cube at 512^3, half-width 3, the vortex with T = 3, RK2 midpoint, CFL 0.5:
-dt = vs / 4, 6,144 steps) run for one full period on the device in FP32 and
-in FP16 leaves, and by the FP64 oracle of the same method
-(oracle/method_oracle.hpp) from the same start sphere.  Reported per
-precision: the largest and RMS difference of phi on the interface (voxels
-active in both runs with |phi_FP64| <= 1 voxel), the largest difference on
-the whole common band, and the voxels active in one run only.  Measured on
-B200 against an 18-minute FP64 run (8 host threads): FP32 5.1e-5 voxel max, 1.8e-5 RMS, same
-topology; FP16 0.059 max, 0.017 RMS, 621 voxels active in one run only (at
-the band's edge, |phi| near the half-width).
+dt = vs / 4, 6,144 steps) runs for one full period on the device in FP32 and
+in FP16 leaves.  The FP64 method oracle's final state of the same run is the
+committed fixture tests/golden/full_period_fp64_512.npz, made by
+tests/golden/make_full_period_fp64.py (15-25 minutes on 6-8 host threads).
 
-Opt-in: the FP64 oracle takes 10-20 minutes on 8-16 host threads, so the test
-runs only with VLR_FULL_PERIOD=1.  VLR_FULL_PERIOD_CACHE=<file.npz> stores the
-oracle's final state there on the first run and reads it on later ones (the
-oracle's result does not depend on the device).  VLR_FULL_PERIOD_OUT=<file>
-writes the statistics as JSON.
+Reported per precision: the largest and RMS difference of phi on the
+interface (voxels active in both runs with |phi_FP64| <= 1 voxel), the
+largest difference on the whole common band, the voxels active in one run
+only, and the relative change of the enclosed volume over the period beside
+the FP64 run's.  FP32 leaves meet the 0.05-voxel interface bar with orders of
+magnitude to spare; FP16 leaves miss it (measured 0.059 voxel), recorded as
+an expected failure with its number.
 """
 import json
 import os
+from pathlib import Path
 
 import numpy as np
 import pytest
 
-pytestmark = [pytest.mark.gpu, pytest.mark.slow,
-              pytest.mark.skipif(os.environ.get("VLR_FULL_PERIOD") != "1", reason="opt-in: VLR_FULL_PERIOD=1")]
+FIXTURE = Path(__file__).resolve().parent / "golden" / "full_period_fp64_512.npz"
 
 VS = 1.0 / 512.0
 R, C, HW, T = 0.15, (0.35, 0.35, 0.35), 3.0, 3.0
@@ -34,38 +31,33 @@ STEPS = int(round(T / DT))
 VEL = {"kind": "vortex", "vs": VS, "period": T}
 
 
-def oracle_full_period(nthreads=None):
-    """Final (origins, masks, phi f64) of the FP64 oracle after one period."""
-    from oracle import pyoracle
-    cache = os.environ.get("VLR_FULL_PERIOD_CACHE")
-    if cache and os.path.exists(cache):
-        z = np.load(cache)
-        return z["o"], z["m"], z["p"]
-    nthreads = nthreads or os.cpu_count()
-    g = pyoracle.MOGrid.sphere(R, C, VS, HW)
-    for s in range(STEPS):
-        assert g.step(VEL, 2, 2, s * DT, DT, nthreads=nthreads), s
-    o, m, p = g.arrays()
-    if cache:
-        np.savez(cache, o=o, m=m, p=p)
-    return o, m, p
-
-
-def device_full_period(ctx, precision):
-    from sharc.volrus_b200.method import LevelSet
-    ls = LevelSet.sphere(R, C, VS, VEL, DT, half_width=HW, precision=precision, integrator=2, reinit_iters=2,
-                         capacity=200_000, ctx=ctx)
-    for _ in range(16):
-        ls.step(STEPS // 16)
-    ls.step(STEPS - 16 * (STEPS // 16))
-    out = ls.arrays()
-    ls.close()
-    return out
-
-
 def _bits(m):
     return np.unpackbits(np.ascontiguousarray(m).view(np.uint8).reshape(-1, 64), axis=1,
                          bitorder="little").astype(bool)
+
+
+def load_fixture():
+    """(origins, masks, phi (n, 512) f64 with zeros off the mask), volumes."""
+    z = np.load(FIXTURE)
+    o, m = z["origins"], z["masks"]
+    p = np.zeros((len(o), 512), np.float64)
+    p[_bits(m)] = z["active_phi"].astype(np.float64)
+    return (o, m, p), float(z["volume_start"]), float(z["volume_end"])
+
+
+def test_fixture_consistent():
+    z = np.load(FIXTURE)
+    o, m, a = z["origins"], z["masks"], z["active_phi"]
+    assert int(z["steps"]) == STEPS and float(z["dt"]) == DT
+    assert len(o) > 1000 and int(_bits(m).sum()) == len(a)
+    assert np.all(o % 8 == 0)
+    key = (o[:, 0].astype(np.int64) << 42) | (o[:, 1].astype(np.int64) << 21) | o[:, 2].astype(np.int64)
+    assert np.all(np.diff(key) > 0), "leaves sorted (x, y, z)"
+    assert np.abs(a).max() < HW
+    # the method loses the thin sheet of the stretched shape (trilinear
+    # semi-Lagrangian advection cannot carry it below a voxel): the FP64 run
+    # ends with 14.5 % of its start volume
+    assert abs(float(z["volume_end"]) / float(z["volume_start"]) - 0.1446) < 2e-3
 
 
 def compare(dev, ref):
@@ -93,26 +85,67 @@ def compare(dev, ref):
             "voxels_active_in_one_run_only": only, "leaves_device": len(go), "leaves_fp64": len(oo)}
 
 
-def test_full_period_against_fp64(ctx, oracle):
-    ref = oracle_full_period()
-    stats = {"steps": STEPS, "dt": DT}
-    for name, prec in (("f32", 0), ("f16", 1)):
-        stats[name] = compare(device_full_period(ctx, prec), ref)
+_RUNS = {}
+
+
+def device_full_period(ctx, precision):
+    """Final state and volumes of one full period on the device (cached per precision)."""
+    if precision in _RUNS:
+        return _RUNS[precision]
+    from sharc.volrus_b200.method import LevelSet
+    ls = LevelSet.sphere(R, C, VS, VEL, DT, half_width=HW, precision=precision, integrator=2, reinit_iters=2,
+                         capacity=200_000, ctx=ctx)
+    v0 = ls.volume()
+    for _ in range(16):
+        ls.step(STEPS // 16)
+    ls.step(STEPS - 16 * (STEPS // 16))
+    v1 = ls.volume()
+    out = ls.arrays()
+    ls.close()
+    _RUNS[precision] = (out, v0, v1)
+    return _RUNS[precision]
+
+
+def _stats(ctx, precision):
+    ref, fv0, fv1 = load_fixture()
+    dev, v0, v1 = device_full_period(ctx, precision)
+    s = compare(dev, ref)
+    s["volume_change_rel"] = (v1 - v0) / v0
+    s["volume_change_rel_fp64"] = (fv1 - fv0) / fv0
+    s["volume_end_vs_fp64_rel"] = (v1 - fv1) / fv1
     out = os.environ.get("VLR_FULL_PERIOD_OUT")
     if out:
-        with open(out, "w") as f:
-            json.dump(stats, f, indent=1)
-    print(json.dumps(stats))
-    for name in ("f32", "f16"):
-        assert stats[name]["interface_voxels"] > 1000
-    # FP32 leaves meet the 0.05-voxel bar with three orders of magnitude to
-    # spare, and the topology is the FP64 run's
-    assert stats["f32"]["max_interface_err_vox"] <= 1e-3, stats["f32"]
-    assert stats["f32"]["voxels_active_in_one_run_only"] == 0, stats["f32"]
-    # FP16 leaves miss it (measured 0.059 voxel max, 0.017 RMS): the state is
-    # rounded to FP16 once per step (half an ulp, 2^-12 voxel near the
-    # interface) and the rounding errors walk over 6,144 steps; rounding the
-    # advected field once instead of twice per step changes nothing (0.063 /
-    # 0.019 measured), so the bound here is the measured one with margin
-    assert stats["f16"]["max_interface_err_vox"] <= 0.1, stats["f16"]
-    assert stats["f16"]["rms_interface_err_vox"] <= 0.03, stats["f16"]
+        with open(f"{out}.{'f32' if precision == 0 else 'f16'}.json", "w") as f:
+            json.dump(s, f, indent=1)
+    print(json.dumps(s))
+    return s
+
+
+@pytest.mark.gpu
+def test_full_period_fp32_against_fp64(ctx):
+    s = _stats(ctx, 0)
+    assert s["interface_voxels"] > 1000
+    assert s["max_interface_err_vox"] <= 1e-3, s
+    assert s["voxels_active_in_one_run_only"] == 0, s
+    # the enclosed volume follows the FP64 run's
+    assert abs(s["volume_end_vs_fp64_rel"]) < 1e-4, s
+
+
+@pytest.mark.gpu
+def test_full_period_fp16_bounds(ctx):
+    """FP16 leaves: the state is rounded to FP16 once per step (half an ulp,
+    2^-12 voxel near the interface) and the rounding errors walk over 6,144
+    steps; the bounds are the measured ones (0.059 max, 0.017 RMS) with margin."""
+    s = _stats(ctx, 1)
+    assert s["interface_voxels"] > 1000
+    assert s["max_interface_err_vox"] <= 0.1, s
+    assert s["rms_interface_err_vox"] <= 0.03, s
+    assert abs(s["volume_end_vs_fp64_rel"]) < 5e-3, s
+
+
+@pytest.mark.gpu
+@pytest.mark.xfail(reason="FP16 leaves miss the 0.05-voxel interface bar after a full period: measured 0.059 voxel "
+                          "max (0.017 RMS) against FP64", strict=False)
+def test_full_period_fp16_meets_0_05_voxel(ctx):
+    s = _stats(ctx, 1)
+    assert s["max_interface_err_vox"] <= 0.05, s

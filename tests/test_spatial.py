@@ -7,11 +7,17 @@ stepper: 2-4 emulated ranks with rebalancing, and two gloo processes over
 torch.distributed, each bit-identical to the undivided oracle run (curl noise
 with RK3, and the time-dependent vortex).
 
+Resident shards (each rank's owned leaves kept in its pool between steps,
+only ghosts and routed outputs moved) against the same undivided runs: on
+the CPU with a pool stepped by the FP64 oracle (emulated ranks and two gloo
+processes), on the device with the library's pool edits.
+
 GPU: the same decomposition with the library's step on each emulated rank
 (one device, ranks stepped in turn, exchanges in process) is bit-identical to
 the undivided run on the device, in FP32 and FP16, with the leaves moved
 into and out of each rank's level set by the device-resident C ABI, and with
-level sets re-created mid-run with their step counter carried over.
+level sets re-created mid-run with their step counter carried over; the
+resident form likewise, with ghosts exchanged in FP16 for FP16 leaves.
 """
 import os
 import socket
@@ -194,6 +200,65 @@ def test_emulated_ranks_some_owning_nothing(oracle):
         assert world <= len(lv) or any(len(s.owned) == 0 for s in shards)
 
 
+class OraclePool:
+    """A rank's leaves held in list order on the CPU (FP64 values) with the
+    pool methods of spatial.DevicePool, stepped by the FP64 method oracle: the
+    host logic of the resident shards without a device (test checker)."""
+
+    device = torch.device("cpu")
+    dtype = torch.float64
+
+    def __init__(self, lv, vel, integrator, reinit_iters, dt, hw, t0=0.0):
+        self.lv = Leaves(lv.origins.clone(), lv.masks.clone(), lv.phi.to(torch.float64).clone())
+        self.stepper = OracleStepper(vel, integrator, reinit_iters, dt, hw, t0)
+
+    def count(self):
+        return len(self.lv)
+
+    def origins(self):
+        return self.lv.origins.clone()
+
+    def gather(self, pos=None):
+        if pos is None:
+            return Leaves(self.lv.origins.clone(), self.lv.masks.clone(), self.lv.phi.clone())
+        return self.lv.take(pos)
+
+    def edit(self, drop, add):
+        keep = self.lv if drop is None else self.lv.take(~drop)
+        self.lv = Leaves.concat([keep, add], self.lv)
+        ks = self.lv.keys()
+        assert len(torch.unique(ks)) == len(ks), "a leaf listed twice"
+
+    def step(self):
+        self.lv = self.stepper(self.lv)
+
+    def skip(self):
+        self.stepper.steps += 1
+
+
+@pytest.mark.parametrize("world,rebalance", [(2, 0), (3, 2), (4, 1)])
+def test_resident_emulated_ranks_match_undivided_oracle(oracle, world, rebalance):
+    """The resident shards (leaves kept in each rank's pool, only ghosts and
+    routed outputs moved) give the undivided run bit for bit."""
+    lv, vel, integ, dt, hw = _curl_case()
+    steps = 4
+    ref = _undivided(lv, OracleStepper(vel, integ, 2, dt, hw), steps)
+    got, shards = spatial.emulate_resident(lv, world, lambda r, own: OraclePool(own, vel, integ, 2, dt, hw), steps,
+                                           rebalance)
+    _assert_same(got, ref)
+    assert sum(s.pool.count() for s in shards) == len(ref)
+
+
+def test_resident_emulated_ranks_some_owning_nothing(oracle):
+    from oracle import pyoracle
+    g = pyoracle.MOGrid.spheres(np.array([[20.0, 20.0, 20.0, 4.0]]), 3.0)
+    lv = Leaves.from_numpy(*g.arrays())
+    vel = {"kind": "constant", "c": (0.7, 0.3, -0.2)}
+    ref = _undivided(lv, OracleStepper(vel, 1, 2, 1.0, 3.0), 3)
+    got, shards = spatial.emulate_resident(lv, 9, lambda r, own: OraclePool(own, vel, 1, 2, 1.0, 3.0), 3, 1)
+    _assert_same(got, ref)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -218,12 +283,32 @@ def _rank_main(rank, world, port, steps, q):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_match_undivided_oracle(oracle):
+def _rank_main_resident(rank, world, port, steps, q):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        lv, vel, integ, dt, hw = _curl_case()
+        sls = spatial.SpatialLevelSet(lv, check_duplicates=True,
+                                      make_pool=lambda own: OraclePool(own, vel, integ, 2, dt, hw))
+        sls.step(2)
+        sls.rebalance()
+        sls.step(steps - 2)
+        whole = sls.gather()
+        q.put((rank, whole.numpy(), len(sls.arrays()), sls.active_voxels()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("main", [_rank_main, _rank_main_resident], ids=["copied", "resident"])
+def test_two_gloo_ranks_match_undivided_oracle(oracle, main):
     world, steps = 2, 3
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, steps, q)) for r in range(world)]
+    procs = [ctx.Process(target=main, args=(r, world, port, steps, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda t: t[0])
@@ -323,4 +408,111 @@ def test_device_upload_download_round_trip_and_errors(ctx):
     ls.upload_device(lv.origins.data_ptr(), lv.masks.data_ptr(), lv.phi.data_ptr(), len(lv))
     ls.step(1)
     assert ls.leaf_count() > 0
+    ls.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,precision,world", [("curl", 0, 2), ("curl", 1, 3), ("vortex", 1, 3)],
+                         ids=["curl_f32_2", "curl_f16_3", "vortex_f16_3"])
+def test_resident_device_ranks_match_undivided_device_run(ctx, kind, precision, world):
+    """Owned leaves resident in each rank's pool, ghosts and routed outputs in
+    the pool's type (FP16 for FP16 leaves): bit-identical to the undivided
+    device run, with a rebalance mid-run; FP64 volume over the owned leaves."""
+    from sharc.volrus_b200.method import LevelSet
+    (o, m, p), vel, integ, dt = _device_case(kind)
+    steps = 6
+    ls = LevelSet.from_leaves(o, m, p, vel, dt, 3.0, precision, integ, 2, 0.0)
+    o, m, p = ls.arrays()
+    ls.step(steps)
+    ref = Leaves.from_numpy(*ls.arrays())
+    ls.close()
+    pools = []
+
+    def make(r, own):
+        pool = spatial.DevicePool(own, vel, dt, 3.0, precision, integ, 2, 0.0)
+        pools.append(pool)
+        return pool
+
+    got, shards = spatial.emulate_resident(Leaves.from_numpy(o, m, p, "cuda"), world, make, steps,
+                                           rebalance_every=3)
+    assert got.phi.dtype == (torch.float16 if precision == 1 else torch.float32)
+    got = Leaves(got.origins, got.masks, got.phi.to(torch.float32))
+    _assert_same(got, ref)
+    assert all(s.pool.count() for s in shards)
+    ls = LevelSet.from_leaves(*ref.numpy(), vel, dt, 3.0, precision, integ, 2, 0.0)
+    v_ref = ls.volume((1.0, 2.0, 3.0))
+    ls.close()
+    v = sum(spatial.volume_shards(shards, spatial.LocalExchange(), (1.0, 2.0, 3.0)))
+    assert abs(v - v_ref) <= 1e-12 * abs(v_ref), (v, v_ref)
+    for pool in pools:
+        pool.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1], ids=["f32", "f16"])
+def test_pool_edits_and_their_errors(ctx, precision):
+    """vlr_ls_gather_device / vlr_ls_edit_device: a drop-and-append edit holds
+    exactly the kept and added leaves (values in the pool's type, bit for
+    bit); no room is refused before anything changes; a leaf added twice is
+    refused and the state stays refused until an upload; a gather position
+    outside the list is refused."""
+    from sharc.volrus_b200._lib import VolrusError
+    from sharc.volrus_b200.method import LevelSet
+    (o, m, p), vel, integ, dt = _device_case("curl")
+    n = len(o)
+    half = n // 2
+    ls = LevelSet.from_leaves(o[:half], m[:half], p[:half], vel, dt, 3.0, precision, integ, 2, 0.0, capacity=n + 8)
+    pool_dtype = torch.float16 if precision == 1 else torch.float32
+    add = Leaves.from_numpy(o[half:], m[half:], p[half:], "cuda")
+    add = Leaves(add.origins, add.masks, add.phi.to(pool_dtype))
+    drop = torch.zeros(half, dtype=torch.uint8, device="cuda")
+    drop[::3] = 1
+    torch.cuda.synchronize()
+    ls.edit_device(drop.data_ptr(), half, add.origins.data_ptr(), add.masks.data_ptr(), add.phi.data_ptr(), len(add))
+    cnt = ls.leaf_count()
+    assert cnt == half - int(drop.sum()) + len(add)
+    go = torch.empty((cnt, 3), dtype=torch.int32, device="cuda")
+    gm = torch.empty((cnt, 8), dtype=torch.int64, device="cuda")
+    gp = torch.empty((cnt, 512), dtype=pool_dtype, device="cuda")
+    ls.gather_device(None, cnt, go.data_ptr(), gm.data_ptr(), gp.data_ptr())
+    keep = np.nonzero(drop.cpu().numpy() == 0)[0]
+    want_o = np.concatenate([o[keep], o[half:]])
+    want_m = np.concatenate([m[keep], m[half:]])
+    want_p = torch.from_numpy(np.concatenate([p[keep], p[half:]])).to(pool_dtype)
+    assert np.array_equal(go.cpu().numpy(), want_o)
+    assert np.array_equal(gm.cpu().numpy().view(np.uint64), want_m)
+    assert torch.equal(gp.cpu().view(torch.uint8 if precision == 0 else torch.int16),
+                       want_p.view(torch.uint8 if precision == 0 else torch.int16))
+    # positions: the same leaves picked one by one
+    pos = torch.tensor([cnt - 1, 0, 5], dtype=torch.int32, device="cuda")
+    po = torch.empty((3, 3), dtype=torch.int32, device="cuda")
+    ls.gather_device(pos.data_ptr(), 3, po.data_ptr())
+    assert np.array_equal(po.cpu().numpy(), want_o[[cnt - 1, 0, 5]])
+    bad = torch.tensor([cnt], dtype=torch.int32, device="cuda")
+    with pytest.raises(VolrusError):
+        ls.gather_device(bad.data_ptr(), 1, po.data_ptr())
+    # no room: refused, nothing changed
+    none = torch.zeros(cnt, dtype=torch.uint8, device="cuda")
+    big = Leaves.from_numpy(o, m, p, "cuda")
+    big = Leaves(big.origins + 8 * 4096, big.masks, big.phi.to(pool_dtype))
+    with pytest.raises(VolrusError) as e:
+        ls.edit_device(none.data_ptr(), cnt, big.origins.data_ptr(), big.masks.data_ptr(), big.phi.data_ptr(),
+                       len(big))
+    assert "room" in str(e.value)
+    assert ls.leaf_count() == cnt
+    ls.step(1)  # still a usable state
+    # a leaf added twice: refused, then refused until an upload
+    cnt = ls.leaf_count()
+    one = ls.leaf_count()
+    go = torch.empty((1, 3), dtype=torch.int32, device="cuda")
+    gm = torch.empty((1, 8), dtype=torch.int64, device="cuda")
+    gp = torch.empty((1, 512), dtype=pool_dtype, device="cuda")
+    ls.gather_device(None, 1, go.data_ptr(), gm.data_ptr(), gp.data_ptr())
+    none = torch.zeros(one, dtype=torch.uint8, device="cuda")
+    with pytest.raises(VolrusError):
+        ls.edit_device(none.data_ptr(), one, go.data_ptr(), gm.data_ptr(), gp.data_ptr(), 1)
+    with pytest.raises(VolrusError):
+        ls.step(1)
+    ls.upload(o, m, p)
+    ls.step(1)
     ls.close()
