@@ -357,7 +357,12 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
     if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
     issue_stage<T, H>(s_desc, s_nbr[0], src, A.mask, stage_of(0), masks_of(0), threadIdx.x, kNT);
+    // leaves ahead: the next one's list slot and neighbour row, and the slot
+    // of the one after (its neighbour row is loaded one iteration before it
+    // is needed, so no global load sits in front of a barrier)
     int slot_n = (li + Gs < count) ? A.list[li + Gs] : -1;
+    int nb_next = (warp == 0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
+    int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
 
     int cur_gid = -1;
     LeafVel L{};
@@ -367,8 +372,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
         // loads for the leaves ahead (consumed one iteration later)
         int4 o_n = make_int4(0, 0, 0, -1);
         if (slot_n >= 0) o_n = A.origin[slot_n];
-        const int nb_n = (warp == 0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
-        const int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
+        const int slot_nnn = (li + 3 * Gs < count) ? A.list[li + 3 * Gs] : -1;
+        const int nb_after = (warp == 0 && lane < kNbr && slot_nn >= 0) ? A.nbr[(size_t)slot_nn * kNbr + lane] : -1;
         if (o.w != cur_gid) {
             __syncthreads();
             load_params(params, o.w, &s_P);
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
                 tvalid = true;
             }
         }
-        if (warp == 0) s_nbr[b ^ 1][lane] = nb_n;
+        if (warp == 0) s_nbr[b ^ 1][lane] = nb_next;
         // barrier A: this leaf's stage and masks are in shared memory, and
         // every thread is done with the previous leaf
         cp_async_wait_all();
@@ -447,6 +452,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
         slot = slot_n;
         o = o_n;
         slot_n = slot_nn;
+        slot_nn = slot_nnn;
+        nb_next = nb_after;
     }
     if (bad) atomicOr(err, kErrReach);
 }

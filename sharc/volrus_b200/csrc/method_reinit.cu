@@ -15,24 +15,26 @@
 //              absent leaves are set to NaN when the copies are issued, so
 //              the stage is complete at its barrier; a 6-neighbour stencil
 //              reads NaN as copysign(hw, its centre value).
-//   phase 1    every warp owns rows of the 10^3 box (row r = lane * 4 + warp):
-//              it copies them from the stage into the phi2 tile, builds their
-//              dilated-mask bits, and runs iteration 1 on its rows' voxels of
-//              D (compacted per warp, no CTA barrier); the faces of the box
-//              are included, its edges and corners are not (iteration 2
-//              never reads them).  Meanwhile every voxel's outside-D result
-//              copysign(hw, value) is written to global memory, coalesced.
-//   phase 2    iteration 2 on the leaf's voxels of D (compacted per warp over
-//              the dilated mask's x-planes), trim, stores over the outside-D
-//              results, activity bits into a shared mask.
-//   phase 3    mask out, spill toward absent neighbours, keep flags and
+//   phase 1    warp 0 compacts the voxel lists: the box voxels of D for
+//              iteration 1 (the 10^3 box around the leaf without its edges
+//              and corners, which iteration 2 never reads) and the leaf's
+//              voxels of D.  Warps 1-3 issue the next leaf's copies, write
+//              every voxel's outside-D result copysign(hw, value) to global
+//              memory (coalesced) and copy phi1 onto the phi2 box.
+//   phase 2    iteration 1 on the box list, consecutive voxels on
+//              consecutive lanes (bank-conflict-free stage reads).
+//   phase 3    iteration 2 (or the only one) on the leaf list, trim, stores
+//              over the outside-D results, activity bits into a shared mask.
+//   phase 4    mask out, spill toward absent neighbours, keep flags and
 //              proposals (hash of the missing leaf, atomicMin of the
 //              proposer's direction).
 //
-// Three CTA barriers per leaf.  Every leaf is computed by one CTA with the
-// same arithmetic whatever the grid size; side effects on shared per-step
-// state are idempotent (flags set to 1, atomicMin), so relaunching the kernel
-// on the same inputs leaves the step's result unchanged.
+// Four CTA barriers per leaf (three without iteration 1).  Neighbour rows
+// are loaded one leaf before the iteration that stores them, so no global
+// load waits in front of a barrier.  Every leaf is computed by one CTA with
+// the same arithmetic whatever the grid size; side effects on shared
+// per-step state are idempotent (flags set to 1, atomicMin), so relaunching
+// the kernel on the same inputs leaves the step's result unchanged.
 #include "method_kernels.hpp"
 
 namespace vlr {
@@ -44,7 +46,7 @@ constexpr int kH = 2;                            // halo of the stage
 constexpr int kE = 8 + 2 * kH;                   // 12: stage rows per axis
 constexpr int kF = 10;                           // phi2 box and D rows: leaf + 1-voxel ring
 constexpr int kNP = 3 * kE * kE;                 // pieces per stage
-constexpr int kRPW = (kF * kF + kNW - 1) / kNW;  // box rows per warp
+constexpr int kBox = kF * kF * kF;               // 1000 voxels of the phi2 box
 
 __device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -82,8 +84,9 @@ __device__ __forceinline__ unsigned piece_desc(int p) {
 // absent leaves, and the 27 dilated masks (zero for absent leaves).
 template <typename T>
 __device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s_nb, const T* __restrict__ vals,
-                                            const uint64_t* __restrict__ masks, T* stage, uint64_t* s_m) {
-    for (int p = threadIdx.x; p < kNP; p += kNT) {
+                                            const uint64_t* __restrict__ masks, T* stage, uint64_t* s_m, int t,
+                                            int ns) {
+    for (int p = t; p < kNP; p += ns) {
         const unsigned dsc = s_desc[p];
         const int sl = s_nb[dsc & 31u];
         T* dst = stage + ((dsc >> 14) & 8191u);
@@ -111,8 +114,8 @@ __device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s
             if (k == 1) cp_async16(dst + 4, src + 4);
         }
     }
-    if (threadIdx.x < kNbr * 4) {
-        const int d = threadIdx.x >> 2, q = threadIdx.x & 3;
+    for (int u = t; u < kNbr * 4; u += ns) {
+        const int d = u >> 2, q = u & 3;
         const int sl = s_nb[d];
         if (sl >= 0) cp_async16(s_m + d * 8 + 2 * q, masks + (size_t)sl * 8 + 2 * q);
         else *reinterpret_cast<uint4*>(s_m + d * 8 + 2 * q) = make_uint4(0u, 0u, 0u, 0u);
@@ -195,6 +198,36 @@ __device__ __forceinline__ unsigned d_row(const uint64_t* s_m, int x, int y) {
            (((unsigned)m[(base + 2) * 64 + bi] & 1u) << 9);
 }
 
+// Bits [32 l, 32 l + 32) of the box's voxels of D in flat order t = (bx *
+// 10 + by) * 10 + bz (b = voxel + 1): the dilated mask on the 10^3 box
+// without its edges and corners, which the second iteration never reads.
+__device__ __forceinline__ unsigned box_word(const uint64_t* s_m, int l) {
+    const int t0 = 32 * l;
+    if (t0 >= kBox) return 0u;
+    unsigned w = 0u;
+    const int r1 = min(t0 + 31, kBox - 1) / kF;
+    for (int r = t0 / kF; r <= r1; ++r) {
+        const int bx = r / kF, by = r - bx * kF;
+        const int edges = (bx == 0 || bx == kF - 1) + (by == 0 || by == kF - 1);
+        const unsigned keep = edges == 0 ? 0x3FFu : (edges == 1 ? 0x1FEu : 0u);
+        const unsigned rb = d_row(s_m, bx - 1, by - 1) & keep;
+        const int sh = r * kF - t0;  // in [-9, 31]
+        w |= sh >= 0 ? (rb << sh) : (rb >> -sh);
+    }
+    return w;
+}
+
+// Inclusive warp scan of c.
+__device__ __forceinline__ int warp_incl_scan(int c, int lane) {
+    int incl = c;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    return incl;
+}
+
 // copysign(hw, value) of every voxel of the leaf, row by row into the output
 // (coalesced); the voxels of D are overwritten in phase 2.
 template <typename T>
@@ -228,8 +261,8 @@ template <typename T, int NIT, int FIX>
 struct ReinitLayout {
     static constexpr size_t stage = (size_t)kE * kE * Row<T>::RP * sizeof(T);
     static constexpr size_t masks = (size_t)kNbr * 64;
-    static constexpr size_t p2 = NIT == 2 ? (size_t)kF * kF * kF * 4 : 0;               // phi2 on the 10^3 box
-    static constexpr size_t dist = (NIT == 2 && FIX) ? (size_t)kF * kF * kF * 4 : 0;    // cut distances
+    static constexpr size_t p2 = NIT == 2 ? (size_t)kBox * 4 : 0;               // phi2 on the 10^3 box
+    static constexpr size_t dist = (NIT == 2 && FIX) ? (size_t)kBox * 4 : 0;    // cut distances
     static constexpr size_t bytes = 2 * stage + 2 * masks + p2 + dist;
     static_assert(stage % 16 == 0, "16-byte aligned buffers");
 };
@@ -250,9 +283,10 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     auto stage_of = [&](int b) { return reinterpret_cast<T*>(smem_dyn + b * Lay::stage); };
     auto masks_of = [&](int b) { return reinterpret_cast<uint64_t*>(mk0 + b * Lay::masks); };
     __shared__ unsigned s_desc[kNP];
-    __shared__ unsigned short s_list1[kNW][kRPW * kF];
-    __shared__ unsigned short s_list2[kNW][128];
+    __shared__ unsigned short s_list1[NIT == 2 ? kBox : 1];
+    __shared__ unsigned short s_list2[kLeafVoxels];
     __shared__ int s_nbr[2][32];
+    __shared__ int s_n1, s_n2;
     __shared__ __align__(16) unsigned s_M[16];
 
     const int count = *A.count;
@@ -266,17 +300,22 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     int4 o = A.origin[slot];
     if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
-    issue_stage<T>(s_desc, s_nbr[0], src, A.dmask, stage_of(0), masks_of(0));
+    issue_stage<T>(s_desc, s_nbr[0], src, A.dmask, stage_of(0), masks_of(0), threadIdx.x, kNT);
+    // leaves ahead: the next one's list slot and neighbour row, and the slot
+    // of the one after (its neighbour row is loaded one iteration before it
+    // is needed, so no global load sits in front of a barrier)
     int slot_n = (li + Gs < count) ? A.list[li + Gs] : -1;
+    int nb_next = (warp == 0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
+    int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
     float hw = params[o.w].hw;
 
     for (unsigned it = 0;; ++it) {
         const int b = it & 1;
         int4 o_n = make_int4(0, 0, 0, -1);
         if (slot_n >= 0) o_n = A.origin[slot_n];
-        const int nb_n = (warp == 0 && lane < kNbr && slot_n >= 0) ? A.nbr[(size_t)slot_n * kNbr + lane] : -1;
-        const int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
-        if (warp == 0) s_nbr[b ^ 1][lane] = nb_n;
+        const int slot_nnn = (li + 3 * Gs < count) ? A.list[li + 3 * Gs] : -1;
+        const int nb_after = (warp == 0 && lane < kNbr && slot_nn >= 0) ? A.nbr[(size_t)slot_nn * kNbr + lane] : -1;
+        if (warp == 0) s_nbr[b ^ 1][lane] = nb_next;
         cp_async_wait_all();
         __syncthreads();  // barrier A: this leaf's stage is complete; the previous leaf is done
         const T* stage = stage_of(b);
@@ -286,78 +325,68 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         // buffer before its barrier A, while warp 1 may still be proposing
         const int my_nb = lane < kNbr ? s_nbr[b][lane] : -1;
         T* out = dst + (size_t)slot * kLeafVoxels;
-        if (slot_n >= 0) issue_stage<T>(s_desc, s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1));
-        write_outside<T>(stage, out, hw, threadIdx.x);
-        if (threadIdx.x < 16) s_M[threadIdx.x] = 0u;
-        if (NIT == 2) {
-            // iteration 1 on this warp's rows of the 10^3 box: r = lane * kNW + warp
-            const int r = lane * kNW + warp;
-            const int rx = r / kF, ry = r - rx * kF;
-            unsigned row = 0;
-            if (r < kF * kF) {
-                // phi2 starts as phi1 on the row; iteration 1 overwrites the voxels of D
-                const T* c = at(stage, rx - 1, ry - 1, -1);
-                float* d2 = s_p2 + r * kF;
-#pragma unroll
-                for (int i = 0; i < kF; ++i) d2[i] = to_f(c[i]);
-                const int edges = (rx == 0 || rx == kF - 1) + (ry == 0 || ry == kF - 1);
-                const unsigned keep = edges == 0 ? 0x3FFu : (edges == 1 ? 0x1FEu : 0u);
-                row = d_row(s_m, rx - 1, ry - 1) & keep;
+        if (warp == 0) {
+            // the voxel lists: box voxels of D for iteration 1 (flat index
+            // t = (bx * 10 + by) * 10 + bz, ascending) and the leaf's voxels
+            // of D for the last iteration (offset x * 64 + y * 8 + z)
+            if (NIT == 2) {
+                unsigned bw = box_word(s_m, lane);
+                const int c = __popc(bw);
+                const int incl = warp_incl_scan(c, lane);
+                int pos = incl - c;
+                while (bw) {
+                    const int z = __ffs(bw) - 1;
+                    bw &= bw - 1u;
+                    s_list1[pos++] = (unsigned short)(32 * lane + z);
+                }
+                if (lane == 31) s_n1 = incl;
             }
-            const int c = __popc(row);
-            int incl = c;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= off) incl += y;
-            }
-            const int nW = __shfl_sync(0xffffffffu, incl, 31);
+            const int q = lane >> 2, cq = lane & 3;
+            unsigned bits = (unsigned)(s_m[13 * 8 + q] >> (16 * cq)) & 0xffffu;
+            const int c = __popc(bits);
+            const int incl = warp_incl_scan(c, lane);
             int pos = incl - c;
-            unsigned short* wl = s_list1[warp];
-            while (row) {
-                const int z = __ffs(row) - 1;
-                row &= row - 1u;
-                wl[pos++] = (unsigned short)(r * kF + z);
+            while (bits) {
+                const int z = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                s_list2[pos++] = (unsigned short)(q * 64 + 16 * cq + z);
             }
-            __syncwarp();
-            for (int i = lane; i < nW; i += 32) {
-                const int t = wl[i];
-                const int rr = t / kF, zr = t - rr * kF;
-                const int xr = rr / kF, yr = rr - xr * kF;
-                const T* c1 = at(stage, xr - 1, yr - 1, zr - 1);
+            if (lane == 31) s_n2 = incl;
+        } else {
+            const int t = threadIdx.x - 32;
+            if (slot_n >= 0)
+                issue_stage<T>(s_desc, s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
+            write_outside<T>(stage, out, hw, t);
+            if (t < 16) s_M[t] = 0u;
+            if (NIT == 2) {
+                // phi2 starts as phi1 on the whole box; iteration 1 overwrites the voxels of D
+                for (int u = t; u < kBox; u += kNT - 32) {
+                    const int bx = u / (kF * kF), r = u - bx * (kF * kF), by = r / kF, bz = r - by * kF;
+                    s_p2[u] = to_f(*at(stage, bx - 1, by - 1, bz - 1));
+                }
+            }
+        }
+        __syncthreads();  // barrier B: lists, outside-D results and the phi2 copy are in place
+        if (NIT == 2) {
+            // iteration 1 on the box voxels of D, consecutive voxels on consecutive lanes
+            const int n1 = s_n1;
+            for (int i = threadIdx.x; i < n1; i += kNT) {
+                const int t = s_list1[i];
+                const int bx = t / (kF * kF), r = t - bx * (kF * kF), by = r / kF, bz = r - by * kF;
+                const T* c1 = at(stage, bx - 1, by - 1, bz - 1);
                 const float p = to_f(c1[0]);
                 const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p, hw);
                 const float d = FIX ? cut_distance(p, n) : __int_as_float(0x7fc00000);
                 if (FIX) s_dist[t] = d;
                 s_p2[t] = (d == d) ? cut_relax(p, p, d) : godunov_update(p, n, p * rsqrtf(p * p + 1.0f));
             }
+            __syncthreads();  // barrier C: phi2 complete on the box
         }
-        __syncthreads();  // barrier C: phi2 complete on the box, outside-D results stored
         {
-            // iteration 2 (or 1) on the leaf's voxels of D: warp w takes x-planes
-            // w and w + 4; lane l the 4 bits 4 (l & 15) .. of plane w + 4 (l >> 4)
-            const uint64_t* dm = s_m + 13 * 8;
-            const int q = warp + kNW * (lane >> 4);
-            const unsigned bits = (unsigned)(dm[q] >> (4 * (lane & 15))) & 0xFu;
-            const int c = __popc(bits);
-            int incl = c;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= off) incl += y;
-            }
-            const int nW = __shfl_sync(0xffffffffu, incl, 31);
-            int pos = incl - c;
-            unsigned short* wl = s_list2[warp];
-            unsigned bb = bits;
-            while (bb) {
-                const int z = __ffs(bb) - 1;
-                bb &= bb - 1u;
-                wl[pos++] = (unsigned short)(q * 64 + 4 * (lane & 15) + z);
-            }
-            __syncwarp();
-            for (int i = lane; i < nW; i += 32) {
-                const int off = wl[i];
+            // the last iteration (or none) on the leaf's voxels of D, trim, stores
+            const int n2 = s_n2;
+            for (int i = threadIdx.x; i < n2; i += kNT) {
+                const int off = s_list2[i];
                 const int x = off >> 6, y = (off >> 3) & 7, z = off & 7;
                 const T* c1 = at(stage, x, y, z);
                 const float p1 = to_f(c1[0]);
@@ -452,6 +481,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         if (o_n.w != o.w) hw = params[o_n.w].hw;
         o = o_n;
         slot_n = slot_nn;
+        slot_nn = slot_nnn;
+        nb_next = nb_after;
     }
 }
 
