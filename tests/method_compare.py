@@ -37,8 +37,18 @@ def compare(gpu_arrays, oracle_arrays, hw, tol_threshold=1e-3):
             near = np.abs(np.abs(ov[b][diff]) - hw) < tol_threshold
             unexplained += int((~near).sum())
     e = np.concatenate(errs) if errs else np.zeros(1)
+    # active voxels of leaves on one side only that lie farther than 1e-2
+    # from the half width (a leaf that appears through a threshold flip at
+    # a neighbour's face holds none)
+    deep = 0
+    for side_idx, k_list, bits_of, vals in ((gi, only_gpu, gb, gv), (oi, only_oracle, ob, ov)):
+        for k in k_list:
+            i = side_idx[k]
+            act = bits_of[i]
+            deep += int((np.abs(np.asarray(vals[i], np.float64)[act]) < hw - 1e-2).sum())
     return {
         "leaves_gpu": len(go), "leaves_oracle": len(oo), "only_gpu": len(only_gpu), "only_oracle": len(only_oracle),
+        "unmatched_leaf_voxels_inside": deep,
         "active_gpu": int(gb.sum()), "active_oracle": int(ob.sum()), "mask_flips": flips,
         "unexplained_flips": unexplained, "max_err": float(e.max()), "rms_err": float(np.sqrt((e ** 2).mean())),
         "frac_over_1e-2": float((e > 1e-2).mean()),
