@@ -10,20 +10,21 @@
 //              other of two stage buffers, row-packed: tile row (x, y),
 //              x, y in [-H, 8+H), holds the upper half-row of the leaf below
 //              in z, the leaf's own row and the lower half-row of the leaf
-//              above, z in [-4, 12) contiguous; the 27 neighbour masks arrive
-//              the same way.  The tile is sampled where it lands (no copy
-//              into a second tile).
+//              above, z in [-4, 12) contiguous; the pieces of absent leaves
+//              are set to NaN when the copies are issued; the 27 neighbour
+//              masks arrive the same way.  The tile is sampled where it lands
+//              (no copy into a second tile).
 //   phase 1    (after the stage barrier) warp 0 builds D from the 27 masks
 //              with 64-bit plane operations (z- and y-dilation inside a
 //              plane word, x-dilation across planes) and compacts it into a
-//              voxel list; warps 1-3 issue the next leaf's copies, fill the
-//              rows of absent neighbour leaves in place with the missing-leaf
-//              rule (copysign(hw, value of the leaf at the clamped
-//              position)), and write every voxel's outside-D result
+//              voxel list; warps 1-3 issue the next leaf's copies, one tile
+//              row per thread, and write every voxel's outside-D result
 //              copysign(hw, previous value) to global memory, coalesced.
 //   phase 2    (after the second barrier) every thread backtraces voxels of
 //              the list and stores the trilinear sample over the outside-D
-//              value written in phase 1.
+//              value written in phase 1; a corner that falls in an absent
+//              leaf (NaN) takes the missing-leaf rule, copysign(hw, the
+//              leaf's own value at the clamped position).
 //
 // Two CTA barriers per leaf; the stage buffer of leaf i is refilled for leaf
 // i + 2 only after leaf i + 1's stage barrier, when every read of it is done.
@@ -64,54 +65,63 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Stage geometry for halo H.  Piece p = 3 r + k of row r: k = 0 / 1 / 2 for
-// the leaf below / at / above the row in z.
+// Stage geometry for halo H: E x E tile rows (x, y), each with three pieces
+// from the leaves below / at / above the row in z.
 template <int H>
 struct Geo {
     static constexpr int E = 8 + 2 * H;
     static constexpr int NROW = E * E;
-    static constexpr int NP = 3 * NROW;
     static_assert(H >= 1 && H <= 4, "the half-rows hold up to 4 values");
-    static_assert(NROW * 24 < (1 << 13), "stage offsets fit 13 bits");
 };
 
-// Copy descriptor of piece p (built once per CTA):
-//   bits 0-4   neighbour index d of the leaf holding the piece
-//   bits 5-13  first value of the piece within that leaf (x*64 + y*8 + z)
-//   bits 14-26 first value of the piece within the stage
-//   bits 27-28 k
-template <typename T, int H>
-__device__ __forceinline__ unsigned piece_desc(int p) {
-    constexpr int E = Geo<H>::E, RP = Row<T>::RP, Z0 = Row<T>::Z0;
-    const int r = p / 3, k = p - 3 * r;
-    const int x = r / E - H, y = r % E - H;
-    const unsigned d = (unsigned)(nb_axis(x) * 9 + nb_axis(y) * 3 + k);
-    const unsigned g = (unsigned)(((x & 7) << 6) | ((y & 7) << 3) | (k == 0 ? 4 : 0));
-    const unsigned s = (unsigned)(r * RP + (k == 0 ? Z0 - 4 : (k == 1 ? Z0 : Z0 + 8)));
-    return d | (g << 5) | (s << 14) | ((unsigned)k << 27);
+// One piece of a stage row: 8 values (full: the own z range) or 4 (a half
+// row of a z neighbour) of leaf slot sl starting at value `off`, by asynchronous
+// copy; NaN when the leaf is absent (the sampler resolves it with the
+// missing-leaf rule).
+template <typename T>
+__device__ __forceinline__ void stage_piece(int sl, const T* __restrict__ vals, int off, T* dst, bool full) {
+    if (sl < 0) {
+        if constexpr (sizeof(T) == 2) {
+            const uint64_t nan4 = 0x7e007e007e007e00ull;
+            uint64_t* o = reinterpret_cast<uint64_t*>(dst);
+            o[0] = nan4;
+            if (full) o[1] = nan4;
+        } else {
+            const unsigned nan = 0x7fc00000u;
+            uint4* o = reinterpret_cast<uint4*>(dst);
+            o[0] = make_uint4(nan, nan, nan, nan);
+            if (full) o[1] = make_uint4(nan, nan, nan, nan);
+        }
+        return;
+    }
+    const T* src = vals + (size_t)sl * kLeafVoxels + off;
+    if constexpr (sizeof(T) == 2) {
+        if (full) cp_async16(dst, src);
+        else cp_async8(dst, src);
+    } else {
+        cp_async16(dst, src);
+        if (full) cp_async16(dst + 4, src + 4);
+    }
 }
 
-// Copies of one leaf's present pieces into `stage` and of its 27 masks into
-// s_m (masks of absent neighbours are zeroed) by a group of ns threads, this
-// thread being number t of the group.
+// Copies of one leaf's stage rows into `stage` and of its 27 masks into s_m
+// (masks of absent neighbours are zeroed) by a group of ns threads, this
+// thread being number t of the group: one tile row (x, y) at a time, its
+// three pieces from the z-lower, own and z-upper leaves of that column.
 template <typename T, int H>
-__device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s_nb, const T* __restrict__ vals,
+__device__ __forceinline__ void issue_stage(const int* s_nb, const T* __restrict__ vals,
                                             const uint64_t* __restrict__ masks, T* stage, uint64_t* s_m, int t,
                                             int ns) {
-    for (int p = t; p < Geo<H>::NP; p += ns) {
-        const unsigned dsc = s_desc[p];
-        const int sl = s_nb[dsc & 31u];
-        if (sl < 0) continue;
-        const T* src = vals + (size_t)sl * kLeafVoxels + ((dsc >> 5) & 511u);
-        T* dst = stage + ((dsc >> 14) & 8191u);
-        const unsigned k = dsc >> 27;
-        if constexpr (sizeof(T) == 2) {
-            if (k == 1) cp_async16(dst, src);
-            else cp_async8(dst, src);
-        } else {
-            cp_async16(dst, src);
-            if (k == 1) cp_async16(dst + 4, src + 4);
-        }
+    constexpr int E = Geo<H>::E, RP = Row<T>::RP, Z0 = Row<T>::Z0;
+    for (int r = t; r < Geo<H>::NROW; r += ns) {
+        const int rx = r / E;
+        const int x = rx - H, y = r - rx * E - H;
+        const int d0 = nb_axis(x) * 9 + nb_axis(y) * 3;
+        const int g = ((x & 7) << 6) | ((y & 7) << 3);
+        T* row = stage + r * RP;
+        stage_piece<T>(s_nb[d0], vals, g + 4, row + Z0 - 4, false);
+        stage_piece<T>(s_nb[d0 + 1], vals, g, row + Z0, true);
+        stage_piece<T>(s_nb[d0 + 2], vals, g, row + Z0 + 8, false);
     }
     for (int u = t; u < kNbr * 4; u += ns) {
         const int d = u >> 2, q = u & 3;
@@ -126,51 +136,6 @@ __device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s
 __device__ __forceinline__ uint64_t rep4(uint64_t h) { return h | (h << 16) | (h << 32) | (h << 48); }
 constexpr uint64_t kSign4 = 0x8000800080008000ull;  // sign bits of four f16 values
 constexpr unsigned kSign = 0x80000000u;             // sign bit of an f32
-
-// Fill the pieces of absent neighbours in `stage` with the missing-leaf rule:
-// the value at tile voxel (x, y, z) of an absent leaf is copysign(hw, v) with
-// v the centre leaf's value at (clamp(x), clamp(y), clamp(z)).
-template <typename T, int H>
-__device__ __forceinline__ void fill_absent(const unsigned* s_desc, const int* s_nb, T* stage, float hw, int t,
-                                            int ns) {
-    constexpr int E = Geo<H>::E, RP = Row<T>::RP, Z0 = Row<T>::Z0;
-    for (int p = t; p < Geo<H>::NP; p += ns) {
-        const unsigned dsc = s_desc[p];
-        if (s_nb[dsc & 31u] >= 0) continue;
-        const int r = p / 3;
-        const unsigned k = dsc >> 27;
-        const int x = r / E - H, y = r % E - H;
-        const int rc = (min(max(x, 0), 7) + H) * E + (min(max(y, 0), 7) + H);
-        T* row = stage + r * RP;
-        const T* crow = stage + rc * RP + Z0;
-        if constexpr (sizeof(T) == 2) {
-            const uint64_t hw4 = rep4(__half_as_ushort(__float2half_rn(hw)) & 0x7fffu);
-            if (k == 1) {
-                const uint64_t* c = reinterpret_cast<const uint64_t*>(crow);
-                uint64_t* o = reinterpret_cast<uint64_t*>(row + Z0);
-                o[0] = hw4 | (c[0] & kSign4);
-                o[1] = hw4 | (c[1] & kSign4);
-            } else {
-                const uint64_t v = __half_as_ushort(crow[k == 0 ? 0 : 7]) & 0x8000u;
-                *reinterpret_cast<uint64_t*>(row + (k == 0 ? Z0 - 4 : Z0 + 8)) = hw4 | rep4(v);
-            }
-        } else {
-            const unsigned hb = __float_as_uint(hw) & 0x7fffffffu;
-            if (k == 1) {
-                const uint4* c = reinterpret_cast<const uint4*>(crow);
-                uint4* o = reinterpret_cast<uint4*>(row + Z0);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint4 v = c[h];
-                    o[h] = make_uint4(hb | (v.x & kSign), hb | (v.y & kSign), hb | (v.z & kSign), hb | (v.w & kSign));
-                }
-            } else {
-                const unsigned v = hb | (__float_as_uint(crow[k == 0 ? 0 : 7]) & kSign);
-                *reinterpret_cast<uint4*>(row + (k == 0 ? Z0 - 4 : Z0 + 8)) = make_uint4(v, v, v, v);
-            }
-        }
-    }
-}
 
 // Every voxel's outside-D result, copysign(hw, previous value), written to
 // the leaf's output row by row (coalesced); the voxels of D are overwritten
@@ -237,7 +202,7 @@ struct LeafVel {
 template <typename T, int H, int VK, int OC, int SER>
 __device__ __forceinline__ void advect_list(const LeafVel& L, const float2 (*s_tab)[3][8],
                                             const unsigned short* s_list, int nD, const T* stage, T* __restrict__ out,
-                                            float dt, int integrator, unsigned& bad) {
+                                            float dt, int integrator, float hwT, unsigned& bad) {
     constexpr int E = Geo<H>::E, RP = Row<T>::RP, Z0 = Row<T>::Z0;
     for (int i = threadIdx.x; i < nD; i += kNT) {
         const int off = s_list[i];
@@ -259,9 +224,26 @@ __device__ __forceinline__ void advect_list(const LeafVel& L, const float2 (*s_t
         }
         // tile (ii, jj, kk) = row (ii, jj), element kk - H + Z0
         const T* q = stage + (ii * E + jj) * RP + (Z0 - H) + kk;
-        const float c000 = to_f(q[0]), c001 = to_f(q[1]), c010 = to_f(q[RP]), c011 = to_f(q[RP + 1]);
-        const float c100 = to_f(q[E * RP]), c101 = to_f(q[E * RP + 1]), c110 = to_f(q[E * RP + RP]),
-                    c111 = to_f(q[E * RP + RP + 1]);
+        float c000 = to_f(q[0]), c001 = to_f(q[1]), c010 = to_f(q[RP]), c011 = to_f(q[RP + 1]);
+        float c100 = to_f(q[E * RP]), c101 = to_f(q[E * RP + 1]), c110 = to_f(q[E * RP + RP]),
+              c111 = to_f(q[E * RP + RP + 1]);
+        const float sum = ((c000 + c001) + (c010 + c011)) + ((c100 + c101) + (c110 + c111));
+        if (sum != sum) {
+            // a corner in an absent leaf (NaN): the missing-leaf rule,
+            // copysign(hw, the leaf's own value at the clamped position)
+            auto own = [&](int ti, int tj, int tk) {
+                const int cx = min(max(ti - H, 0), 7), cy = min(max(tj - H, 0), 7), cz = min(max(tk - H, 0), 7);
+                return copysignf(hwT, to_f(stage[((cx + H) * E + (cy + H)) * RP + Z0 + cz]));
+            };
+            if (c000 != c000) c000 = own(ii, jj, kk);
+            if (c001 != c001) c001 = own(ii, jj, kk + 1);
+            if (c010 != c010) c010 = own(ii, jj + 1, kk);
+            if (c011 != c011) c011 = own(ii, jj + 1, kk + 1);
+            if (c100 != c100) c100 = own(ii + 1, jj, kk);
+            if (c101 != c101) c101 = own(ii + 1, jj, kk + 1);
+            if (c110 != c110) c110 = own(ii + 1, jj + 1, kk);
+            if (c111 != c111) c111 = own(ii + 1, jj + 1, kk + 1);
+        }
         const float c00 = c000 * (1.f - wx) + c100 * wx, c01 = c001 * (1.f - wx) + c101 * wx;
         const float c10 = c010 * (1.f - wx) + c110 * wx, c11 = c011 * (1.f - wx) + c111 * wx;
         const float c0 = c00 * (1.f - wy) + c10 * wy, c1 = c01 * (1.f - wy) + c11 * wy;
@@ -272,17 +254,18 @@ __device__ __forceinline__ void advect_list(const LeafVel& L, const float2 (*s_t
 template <typename T, int H, int VK>
 __device__ __forceinline__ void advect_dispatch(const LeafVel& L, const float2 (*s_tab)[3][8],
                                                 const unsigned short* s_list, int nD, const T* stage,
-                                                T* __restrict__ out, float dt, int integrator, unsigned& bad) {
+                                                T* __restrict__ out, float dt, int integrator, float hwT,
+                                                unsigned& bad) {
     const bool oc3 = L.V.octaves == 3;
     if (L.series == kSeriesMicro) {
-        if (oc3) advect_list<T, H, VK, 3, kSeriesMicro>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
-        else advect_list<T, H, VK, 0, kSeriesMicro>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
+        if (oc3) advect_list<T, H, VK, 3, kSeriesMicro>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
+        else advect_list<T, H, VK, 0, kSeriesMicro>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
     } else if (L.series == kSeriesTiny) {
-        if (oc3) advect_list<T, H, VK, 3, kSeriesTiny>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
-        else advect_list<T, H, VK, 0, kSeriesTiny>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
+        if (oc3) advect_list<T, H, VK, 3, kSeriesTiny>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
+        else advect_list<T, H, VK, 0, kSeriesTiny>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
     } else {
-        if (oc3) advect_list<T, H, VK, 3, kSeriesFull>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
-        else advect_list<T, H, VK, 0, kSeriesFull>(L, s_tab, s_list, nD, stage, out, dt, integrator, bad);
+        if (oc3) advect_list<T, H, VK, 3, kSeriesFull>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
+        else advect_list<T, H, VK, 0, kSeriesFull>(L, s_tab, s_list, nD, stage, out, dt, integrator, hwT, bad);
     }
 }
 
@@ -333,7 +316,6 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
     unsigned char* const mk0 = smem_dyn + 2 * Lay::stage;
     auto stage_of = [&](int b) { return reinterpret_cast<T*>(smem_dyn + b * Lay::stage); };
     auto masks_of = [&](int b) { return reinterpret_cast<uint64_t*>(mk0 + b * Lay::masks); };
-    __shared__ unsigned s_desc[G::NP];
     __shared__ unsigned short s_list[kLeafVoxels];
     __shared__ int s_nbr[2][32];
     __shared__ int s_nD;
@@ -350,13 +332,12 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned bad = 0;
 
-    // prologue: descriptors, then the first leaf's stage
-    for (int p = threadIdx.x; p < G::NP; p += kNT) s_desc[p] = piece_desc<T, H>(p);
+    // prologue: the first leaf's stage
     int slot = A.list[li];
     int4 o = A.origin[slot];
     if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
-    issue_stage<T, H>(s_desc, s_nbr[0], src, A.mask, stage_of(0), masks_of(0), threadIdx.x, kNT);
+    issue_stage<T, H>(s_nbr[0], src, A.mask, stage_of(0), masks_of(0), threadIdx.x, kNT);
     // leaves ahead: the next one's list slot and neighbour row, and the slot
     // of the one after (its neighbour row is loaded one iteration before it
     // is needed, so no global load sits in front of a barrier)
@@ -440,13 +421,12 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
         } else {
             const int t = threadIdx.x - 32;
             if (slot_n >= 0)
-                issue_stage<T, H>(s_desc, s_nbr[b ^ 1], src, A.mask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
-            fill_absent<T, H>(s_desc, s_nbr[b], stage, hw, t, kNT - 32);
+                issue_stage<T, H>(s_nbr[b ^ 1], src, A.mask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
             write_outside<T, H>(stage, out, hw, t);
         }
         if (tvalid) (&s_tab[0][0][0])[threadIdx.x] = tv;
         __syncthreads();  // barrier B: list, tables and filled tile are ready
-        advect_dispatch<T, H, VK>(L, s_tab, s_list, s_nD, stage, out, dt, sp.integrator, bad);
+        advect_dispatch<T, H, VK>(L, s_tab, s_list, s_nD, stage, out, dt, sp.integrator, to_f(from_f<T>(hw)), bad);
         if (slot_n < 0) break;
         li += Gs;
         slot = slot_n;

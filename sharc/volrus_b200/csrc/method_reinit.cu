@@ -14,17 +14,21 @@
 //              leaf ahead into the other of two buffers.  The pieces of
 //              absent leaves are set to NaN when the copies are issued, so
 //              the stage is complete at its barrier; a 6-neighbour stencil
-//              reads NaN as copysign(hw, its centre value).
+//              reads NaN as copysign(hw, its centre value), which needs no
+//              work in the common case (see godunov_update_raw).
 //   phase 1    warp 0 compacts the voxel lists: the box voxels of D for
 //              iteration 1 (the 10^3 box around the leaf without its edges
 //              and corners, which iteration 2 never reads) and the leaf's
-//              voxels of D.  Warps 1-3 issue the next leaf's copies, write
-//              every voxel's outside-D result copysign(hw, value) to global
-//              memory (coalesced) and copy phi1 onto the phi2 box.
+//              voxels of D, and keeps the box list's bit words.  Warps 1-3
+//              issue the next leaf's copies and write every voxel's
+//              outside-D result copysign(hw, value) to global memory
+//              (coalesced).
 //   phase 2    iteration 1 on the box list, consecutive voxels on
-//              consecutive lanes (bank-conflict-free stage reads).
-//   phase 3    iteration 2 (or the only one) on the leaf list, trim, stores
-//              over the outside-D results, activity bits into a shared mask.
+//              consecutive lanes (bank-conflict-free stage reads), into phi2.
+//   phase 3    iteration 2 (or the only one) on the leaf list, its
+//              neighbours from phi2 where the box bit is set and from the
+//              stage (phi1) elsewhere; trim, stores over the outside-D
+//              results, activity bits into a shared mask.
 //   phase 4    mask out, spill toward absent neighbours, keep flags and
 //              proposals (hash of the missing leaf, atomicMin of the
 //              proposer's direction).
@@ -45,7 +49,6 @@ constexpr int kNW = kNT / 32;
 constexpr int kH = 2;                            // halo of the stage
 constexpr int kE = 8 + 2 * kH;                   // 12: stage rows per axis
 constexpr int kF = 10;                           // phi2 box and D rows: leaf + 1-voxel ring
-constexpr int kNP = 3 * kE * kE;                 // pieces per stage
 constexpr int kBox = kF * kF * kF;               // 1000 voxels of the phi2 box
 
 __device__ __forceinline__ int nb_axis(int c) { return (c < 0) ? 0 : (c > 7 ? 2 : 1); }
@@ -67,52 +70,53 @@ struct Row {
     static constexpr int Z0 = sizeof(T) == 2 ? 8 : 4;
 };
 
-// Copy descriptor of piece p = 3 r + k: neighbour d (bits 0-4), first value
-// in the leaf (5-13), first value in the stage (14-26), k (27-28).
+// One piece of a stage row: 8 values (full: the own z range) or 4 (a half
+// row of a z neighbour) of leaf slot sl from value `off`, by asynchronous
+// copy; NaN when the leaf is absent.
 template <typename T>
-__device__ __forceinline__ unsigned piece_desc(int p) {
-    constexpr int RP = Row<T>::RP, Z0 = Row<T>::Z0;
-    const int r = p / 3, k = p - 3 * r;
-    const int x = r / kE - kH, y = r % kE - kH;
-    const unsigned d = (unsigned)(nb_axis(x) * 9 + nb_axis(y) * 3 + k);
-    const unsigned g = (unsigned)(((x & 7) << 6) | ((y & 7) << 3) | (k == 0 ? 4 : 0));
-    const unsigned s = (unsigned)(r * RP + (k == 0 ? Z0 - 4 : (k == 1 ? Z0 : Z0 + 8)));
-    return d | (g << 5) | (s << 14) | ((unsigned)k << 27);
+__device__ __forceinline__ void stage_piece(int sl, const T* __restrict__ vals, int off, T* dst, bool full) {
+    if (sl < 0) {
+        if constexpr (sizeof(T) == 2) {
+            const uint64_t nan4 = 0x7e007e007e007e00ull;
+            uint64_t* o = reinterpret_cast<uint64_t*>(dst);
+            o[0] = nan4;
+            if (full) o[1] = nan4;
+        } else {
+            const unsigned nan = 0x7fc00000u;
+            uint4* o = reinterpret_cast<uint4*>(dst);
+            o[0] = make_uint4(nan, nan, nan, nan);
+            if (full) o[1] = make_uint4(nan, nan, nan, nan);
+        }
+        return;
+    }
+    const T* src = vals + (size_t)sl * kLeafVoxels + off;
+    if constexpr (sizeof(T) == 2) {
+        if (full) cp_async16(dst, src);
+        else cp_async8(dst, src);
+    } else {
+        cp_async16(dst, src);
+        if (full) cp_async16(dst + 4, src + 4);
+    }
 }
 
-// One leaf's stage: copies of the present pieces, NaN in the pieces of
-// absent leaves, and the 27 dilated masks (zero for absent leaves).
+// One leaf's stage, one tile row (x, y) at a time with its three pieces from
+// the z-lower, own and z-upper leaves of that column (NaN for absent leaves),
+// and the 27 dilated masks (zero for absent leaves), by a group of ns
+// threads, this thread being number t.
 template <typename T>
-__device__ __forceinline__ void issue_stage(const unsigned* s_desc, const int* s_nb, const T* __restrict__ vals,
+__device__ __forceinline__ void issue_stage(const int* s_nb, const T* __restrict__ vals,
                                             const uint64_t* __restrict__ masks, T* stage, uint64_t* s_m, int t,
                                             int ns) {
-    for (int p = t; p < kNP; p += ns) {
-        const unsigned dsc = s_desc[p];
-        const int sl = s_nb[dsc & 31u];
-        T* dst = stage + ((dsc >> 14) & 8191u);
-        const unsigned k = dsc >> 27;
-        if (sl < 0) {
-            if constexpr (sizeof(T) == 2) {
-                const uint64_t nan4 = 0x7e007e007e007e00ull;
-                uint64_t* o = reinterpret_cast<uint64_t*>(dst);
-                o[0] = nan4;
-                if (k == 1) o[1] = nan4;
-            } else {
-                const unsigned nan = 0x7fc00000u;
-                uint4* o = reinterpret_cast<uint4*>(dst);
-                o[0] = make_uint4(nan, nan, nan, nan);
-                if (k == 1) o[1] = make_uint4(nan, nan, nan, nan);
-            }
-            continue;
-        }
-        const T* src = vals + (size_t)sl * kLeafVoxels + ((dsc >> 5) & 511u);
-        if constexpr (sizeof(T) == 2) {
-            if (k == 1) cp_async16(dst, src);
-            else cp_async8(dst, src);
-        } else {
-            cp_async16(dst, src);
-            if (k == 1) cp_async16(dst + 4, src + 4);
-        }
+    constexpr int RP = Row<T>::RP, Z0 = Row<T>::Z0;
+    for (int r = t; r < kE * kE; r += ns) {
+        const int rx = r / kE;
+        const int x = rx - kH, y = r - rx * kE - kH;
+        const int d0 = nb_axis(x) * 9 + nb_axis(y) * 3;
+        const int g = ((x & 7) << 6) | ((y & 7) << 3);
+        T* row = stage + r * RP;
+        stage_piece<T>(s_nb[d0], vals, g + 4, row + Z0 - 4, false);
+        stage_piece<T>(s_nb[d0 + 1], vals, g, row + Z0, true);
+        stage_piece<T>(s_nb[d0 + 2], vals, g, row + Z0 + 8, false);
     }
     for (int u = t; u < kNbr * 4; u += ns) {
         const int d = u >> 2, q = u & 3;
@@ -162,9 +166,27 @@ __device__ __forceinline__ Nb6 load_nb6(const T* c, float p, float hw) {
                nbv(to_f(c[SY]), p, hw),  nbv(to_f(c[-1]), p, hw), nbv(to_f(c[1]), p, hw)};
 }
 
+// The 6 neighbours of the value at c as stored (NaN for an unallocated leaf).
+template <typename T, int SX, int SY>
+__device__ __forceinline__ Nb6 load_nb6_raw(const T* c) {
+    return Nb6{to_f(c[-SX]), to_f(c[SX]), to_f(c[-SY]), to_f(c[SY]), to_f(c[-1]), to_f(c[1])};
+}
+
 __device__ __forceinline__ float godunov_update(float p, const Nb6& n, float s) {
     const float G = godunov_g(p, n.xm, n.xp, n.ym, n.yp, n.zm, n.zp, s);
     return p - 0.5f * s * (G - 1.0f);
+}
+
+// godunov_update with raw neighbours, NaN marking an unallocated leaf.  The
+// missing-leaf value copysign(hw, p) gives an upwind term max(<= 0, 0) = 0
+// whenever |p| <= hw and p's sign bit matches the upwind sign of s, and
+// fmaxf gives the same 0 for the NaN itself, so the NaNs are resolved only
+// outside that case: bit for bit the update of the resolved neighbours.
+__device__ __forceinline__ float godunov_update_raw(float p, Nb6 n, float s, float hw) {
+    if (!(fabsf(p) <= hw && (signbit(p) != 0) == (s < 0.f)))
+        n = Nb6{nbv(n.xm, p, hw), nbv(n.xp, p, hw), nbv(n.ym, p, hw),
+                nbv(n.yp, p, hw), nbv(n.zm, p, hw), nbv(n.zp, p, hw)};
+    return godunov_update(p, n, s);
 }
 
 // Subcell fix of the reinitialisation (Russo & Smereka, J. Comput. Phys. 163,
@@ -282,11 +304,11 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     float* s_dist = reinterpret_cast<float*>(mk0 + 2 * Lay::masks + Lay::p2);
     auto stage_of = [&](int b) { return reinterpret_cast<T*>(smem_dyn + b * Lay::stage); };
     auto masks_of = [&](int b) { return reinterpret_cast<uint64_t*>(mk0 + b * Lay::masks); };
-    __shared__ unsigned s_desc[kNP];
     __shared__ unsigned short s_list1[NIT == 2 ? kBox : 1];
     __shared__ unsigned short s_list2[kLeafVoxels];
     __shared__ int s_nbr[2][32];
     __shared__ int s_n1, s_n2;
+    __shared__ unsigned s_bx[32];  // the box voxels of D, one bit per flat index
     __shared__ __align__(16) unsigned s_M[16];
 
     const int count = *A.count;
@@ -295,12 +317,11 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     if (li >= count) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-    for (int p = threadIdx.x; p < kNP; p += kNT) s_desc[p] = piece_desc<T>(p);
     int slot = A.list[li];
     int4 o = A.origin[slot];
     if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
     __syncthreads();
-    issue_stage<T>(s_desc, s_nbr[0], src, A.dmask, stage_of(0), masks_of(0), threadIdx.x, kNT);
+    issue_stage<T>(s_nbr[0], src, A.dmask, stage_of(0), masks_of(0), threadIdx.x, kNT);
     // leaves ahead: the next one's list slot and neighbour row, and the slot
     // of the one after (its neighbour row is loaded one iteration before it
     // is needed, so no global load sits in front of a barrier)
@@ -331,6 +352,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
             // of D for the last iteration (offset x * 64 + y * 8 + z)
             if (NIT == 2) {
                 unsigned bw = box_word(s_m, lane);
+                s_bx[lane] = bw;
                 const int c = __popc(bw);
                 const int incl = warp_incl_scan(c, lane);
                 int pos = incl - c;
@@ -355,18 +377,11 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         } else {
             const int t = threadIdx.x - 32;
             if (slot_n >= 0)
-                issue_stage<T>(s_desc, s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
+                issue_stage<T>(s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
             write_outside<T>(stage, out, hw, t);
             if (t < 16) s_M[t] = 0u;
-            if (NIT == 2) {
-                // phi2 starts as phi1 on the whole box; iteration 1 overwrites the voxels of D
-                for (int u = t; u < kBox; u += kNT - 32) {
-                    const int bx = u / (kF * kF), r = u - bx * (kF * kF), by = r / kF, bz = r - by * kF;
-                    s_p2[u] = to_f(*at(stage, bx - 1, by - 1, bz - 1));
-                }
-            }
         }
-        __syncthreads();  // barrier B: lists, outside-D results and the phi2 copy are in place
+        __syncthreads();  // barrier B: lists and outside-D results are in place
         if (NIT == 2) {
             // iteration 1 on the box voxels of D, consecutive voxels on consecutive lanes
             const int n1 = s_n1;
@@ -375,10 +390,14 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
                 const int bx = t / (kF * kF), r = t - bx * (kF * kF), by = r / kF, bz = r - by * kF;
                 const T* c1 = at(stage, bx - 1, by - 1, bz - 1);
                 const float p = to_f(c1[0]);
-                const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p, hw);
-                const float d = FIX ? cut_distance(p, n) : __int_as_float(0x7fc00000);
-                if (FIX) s_dist[t] = d;
-                s_p2[t] = (d == d) ? cut_relax(p, p, d) : godunov_update(p, n, p * rsqrtf(p * p + 1.0f));
+                if (FIX) {
+                    const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p, hw);
+                    const float d = cut_distance(p, n);
+                    s_dist[t] = d;
+                    s_p2[t] = (d == d) ? cut_relax(p, p, d) : godunov_update(p, n, p * rsqrtf(p * p + 1.0f));
+                } else {
+                    s_p2[t] = godunov_update_raw(p, load_nb6_raw<T, kE * RP, RP>(c1), p * rsqrtf(p * p + 1.0f), hw);
+                }
             }
             __syncthreads();  // barrier C: phi2 complete on the box
         }
@@ -394,20 +413,29 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
                 if (NIT == 0) {
                     v = p1;
                 } else if (NIT == 1) {
-                    const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p1, hw);
-                    const float d = FIX ? cut_distance(p1, n) : __int_as_float(0x7fc00000);
-                    v = (d == d) ? cut_relax(p1, p1, d) : godunov_update(p1, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                    if (FIX) {
+                        const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p1, hw);
+                        const float d = cut_distance(p1, n);
+                        v = (d == d) ? cut_relax(p1, p1, d) : godunov_update(p1, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                    } else {
+                        v = godunov_update_raw(p1, load_nb6_raw<T, kE * RP, RP>(c1), p1 * rsqrtf(p1 * p1 + 1.0f), hw);
+                    }
                 } else {
                     const int t10 = ((x + 1) * kF + (y + 1)) * kF + (z + 1);
-                    const float* c2 = s_p2 + t10;
-                    const float p2 = c2[0];
+                    const float p2 = s_p2[t10];  // the leaf's voxels of D are box voxels of D
                     const float d = FIX ? s_dist[t10] : __int_as_float(0x7fc00000);
                     if (d == d) {
                         v = cut_relax(p2, p1, d);
                     } else {
-                        const Nb6 n{nbv(c2[-kF * kF], p2, hw), nbv(c2[kF * kF], p2, hw), nbv(c2[-kF], p2, hw),
-                                    nbv(c2[kF], p2, hw),       nbv(c2[-1], p2, hw),      nbv(c2[1], p2, hw)};
-                        v = godunov_update(p2, n, p1 * rsqrtf(p1 * p1 + 1.0f));
+                        // a neighbour's phi2 is iteration 1's result on the box voxels
+                        // of D and phi1 (the stage) elsewhere
+                        auto nb = [&](int dt, int ds) {
+                            const int u = t10 + dt;
+                            return ((s_bx[u >> 5] >> (u & 31)) & 1u) ? s_p2[u] : to_f(c1[ds]);
+                        };
+                        const Nb6 n{nb(-kF * kF, -kE * RP), nb(kF * kF, kE * RP), nb(-kF, -RP),
+                                    nb(kF, RP),             nb(-1, -1),           nb(1, 1)};
+                        v = godunov_update_raw(p2, n, p1 * rsqrtf(p1 * p1 + 1.0f), hw);
                     }
                 }
                 const bool on = fabsf(v) < hw;
