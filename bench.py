@@ -307,26 +307,40 @@ class RefLargeSample:
 STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_t_nbr")
 
 
-# DRAM bytes (read + write) per leaf of one launch, from ncu captures of the
-# bench's own commands (dram__bytes_read.sum + dram__bytes_write.sum divided by
-# the leaves of that launch); keyed by (workload, kernel, value bytes).
-# profiles/stencils_deformation512_full.md (2,853 leaves) and
-# profiles/stencils_batched256_subset48_full.md (151,238 leaves).
+# DRAM bytes (read + write) per leaf of one launch of the stencil kernels,
+# dram__bytes_read.sum + dram__bytes_write.sum over the launch's leaves, from
+# ncu captures of these bench commands (one GPU, --clock-control none,
+# -k 'regex:k_m_(advect|reinit)' -c 2, the fixed launch shape
+# 128,1184,0,128,1184,0 so no tuning launch precedes the captured step);
+# keyed by (workload, kernel, value bytes):
+#   large8192: the same generator with 1,500 spheres (466k leaves; traffic per
+#     leaf does not depend on the sphere count), `bench.py --large-spheres 1500
+#     --steps 1 --warmup 3 --no-...`, FP16 at -s 6, FP32 at -s 20;
+#   batched256: its first 48 grids (151k leaves), `bench.py --workload
+#     batched256 --grids 48 --steps 1 --warmup 3`, -s 6;
+#   deformation512: `bench.py --workload deformation512 --steps 1 --warmup 3`,
+#     -s 6 (2,858 leaves, L2-resident).
 TRAFFIC_PER_LEAF: dict = {
-    ("deformation512", "k_m_advect", 2): 3531264 / 2853,
-    ("deformation512", "k_m_reinit", 2): 3518464 / 2853,
-    ("batched256", "k_m_advect", 2): (191877632 + 158914816) / 151238,
-    ("batched256", "k_m_reinit", 2): (194146816 + 136635904) / 151238,
+    ("large8192", "k_m_advect", 2): 2565.0,
+    ("large8192", "k_m_reinit", 2): 2331.0,
+    ("large8192", "k_m_advect", 4): 4913.0,
+    ("large8192", "k_m_reinit", 4): 4504.6,
+    ("batched256", "k_m_advect", 2): 2330.1,
+    ("batched256", "k_m_reinit", 2): 2069.0,
+    ("deformation512", "k_m_advect", 2): 1238.0,
+    ("deformation512", "k_m_reinit", 2): 1223.0,
 }
 
 
-# Warp instructions per leaf of one launch (smsp__inst_executed.sum / leaves)
-# from the same ncu captures, FP16, 128-thread CTAs.
+# Warp instructions per leaf of one launch (smsp__inst_executed.sum over the
+# launch's leaves) from the same captures, FP16, 128-thread CTAs.
 INST_PER_LEAF: dict = {
-    ("deformation512", "k_m_advect"): 12236456 / 2853,
-    ("deformation512", "k_m_reinit"): 16721413 / 2853,
-    ("batched256", "k_m_advect"): 1064426333 / 151238,
-    ("batched256", "k_m_reinit"): 821863623 / 151238,
+    ("large8192", "k_m_advect"): 4453.0,
+    ("large8192", "k_m_reinit"): 4335.0,
+    ("batched256", "k_m_advect"): 4768.3,
+    ("batched256", "k_m_reinit"): 4326.2,
+    ("deformation512", "k_m_advect"): 3001.4,
+    ("deformation512", "k_m_reinit"): 4541.2,
 }
 SM_COUNT = 148
 ISSUE_PER_SM_PER_CYCLE = 4  # one warp instruction per scheduler per cycle
@@ -501,6 +515,7 @@ def roofline_of(r, value_bytes, peak, peak_kind, workload):
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": None if tr is None else tr * r["leaves"],
+            "traffic_per_leaf_ncu": tr,
             "algorithmic_bytes": per[dom] * r["leaves"], "algorithmic_bytes_per_leaf": per[dom],
             "launch_ms": dom_ms}
 
@@ -753,10 +768,11 @@ def data_path(args, ctx, flush, stream, clk, sph, peak, peak_kind):
     topology kernels reach on their own, and what FP16 storage buys there."""
     from sharc.volrus_b200.method import F16, F32, LevelSet
     out = {"velocity": "constant (0.6, -0.4, 0.3) voxels/step", "integrator": "Euler", "reinit_iters": 0}
-    steps = min(args.steps, 10)
+    steps = min(args.steps, 5)
     for prec, name, nb in ((F16, "f16", 2), (F32, "f32", 4)):
+        # without reinitialisation the band widens every step: room for 3.2x the start's leaves
         ls = LevelSet.spheres([(sph, {"kind": "constant", "c": (0.6, -0.4, 0.3)})], 1.0, half_width=3.0,
-                              precision=prec, integrator=1, reinit_iters=0, ctx=ctx)
+                              precision=prec, integrator=1, reinit_iters=0, capacity=8_000_000, ctx=ctx)
         r = time_steps(args, ctx, ls, flush, stream, clk, steps=steps)
         out[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "steps": steps,
                      "kernels_ms_per_launch": r["kernels"],
