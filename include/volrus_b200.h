@@ -454,6 +454,13 @@ int vlr_adj_displacement(vlr_ctx* ctx, const vlr_adjoint* a, float* out);
  * d_out[b] = phi_0(x_b - s), device buffer of n_band floats, enqueued on the
  * context stream (the target of an L2 loss against a translated copy). */
 int vlr_adj_shifted_phi0(vlr_ctx* ctx, const vlr_adjoint* a, int sx, int sy, int sz, float* d_out);
+/* The kernel of the backward pass's lambda transpose: 0 (default) the quad
+ * gather for bands under 2^20 voxels at a reach of one voxel per step, the
+ * windowed gather otherwise; 1 always the windowed gather; 2 always the quad
+ * gather (reach 1 only, VLR_ERR_INVALID otherwise).  Both sum each voxel's
+ * terms in a fixed order but associate them differently, so a grid divided
+ * over ranks pins one kernel to reproduce the undivided sums bit for bit. */
+int vlr_adj_set_gather(vlr_ctx* ctx, vlr_adjoint* a, int mode);
 /* Band voxel coordinates (int32[n][3]); coords may be null to query n. */
 int vlr_adj_band(vlr_ctx* ctx, const vlr_adjoint* a, int32_t* coords, size_t cap, size_t* n);
 /* Replace phi_0 on the band and/or the staggered field (either may be null). */

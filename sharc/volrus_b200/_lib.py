@@ -134,6 +134,7 @@ SIGNATURES = {
     "vlr_adj_create_level_set": (C.c_int, [P, P, C.c_int, C.c_int, PP]),
     "vlr_adj_displacement": (C.c_int, [P, P, flt_p]),
     "vlr_adj_shifted_phi0": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, P]),
+    "vlr_adj_set_gather": (C.c_int, [P, P, C.c_int]),
     "vlr_adj_set_inputs": (C.c_int, [P, P, flt_p, flt_p]),
     "vlr_adj_forward": (C.c_int, [P, P, flt_p]),
     "vlr_adj_backward": (C.c_int, [P, P, flt_p, flt_p, flt_p]),

@@ -80,6 +80,12 @@ class AdvectionFunction:
         self.n_band = nb.value
         return self
 
+    def set_gather(self, mode: int):
+        """Pin the backward pass's lambda-transpose kernel (0 automatic, 1
+        windowed, 2 quad); the two kernels associate each voxel's sum
+        differently, so runs compared bit for bit use the same one."""
+        self.ctx.check(self.ctx.lib.vlr_adj_set_gather(self.ctx.handle, self.handle, int(mode)), "vlr_adj_set_gather")
+
     def shifted_phi0_device(self, shift, out_ptr: int):
         """phi_0 translated by `shift` voxels (each within +-8), read on the band,
         into a device buffer of n_band floats (enqueued, no wait)."""

@@ -59,6 +59,7 @@ struct vlr_adjoint {
     float* gvel = nullptr;               // dL/dV, 3 x n^3
     float3* G = nullptr;
     int reach = 1;                       // displacement bound per step, voxels (ceil of dt max|V|)
+    int gather = 0;                      // transpose kernel: 0 by band size and reach, 1 windowed, 2 quad
     int disp = 0;                        // 1: ub holds each band voxel's fixed backtrace displacement
                                          // (a level set's time-independent velocity), step factor 1
     unsigned* foot_pk = nullptr;         // per pool voxel: packed foot offsets of band voxels, 0 elsewhere
@@ -600,7 +601,7 @@ int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
             const int nl = a->n_leaves;
             // the narrowed window pays when the whole window is large (reach >= 2)
             // or the band is, where its two small per-leaf passes are cheap
-            if (a->reach == 1 && nb < (1u << 20)) {
+            if (a->gather == 2 || (a->gather == 0 && a->reach == 1 && nb < (1u << 20))) {
                 // small band: a quad of lanes per band voxel fills the GPU
                 VLR_TIMED(ctx, "k_adj_lambda",
                           k_adj_lambda_quad<<<blocks_for(ctx, 4ll * nb), 256, 0, st>>>(
@@ -811,6 +812,16 @@ int vlr_adj_create_level_set(vlr_ctx* ctx, vlr_level_set* ls, int steps, int che
     a->reach = std::max(1, (int)std::ceil((double)mx * (1.0 + 1e-6)));
     if (a->reach > 6) return fail(set_error(ctx, VLR_ERR_REACH, "backtrace displacement exceeds 6 voxels per step"));
     *out = a;
+    return VLR_OK;
+}
+
+int vlr_adj_set_gather(vlr_ctx* ctx, vlr_adjoint* a, int mode) {
+    if (!ctx || !a) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (mode < 0 || mode > 2) return set_error(ctx, VLR_ERR_INVALID, "gather mode must be 0, 1 or 2");
+    if (mode == 2 && a->reach != 1)
+        return set_error(ctx, VLR_ERR_INVALID, "the quad gather covers a reach of one voxel per step only");
+    if (mode != a->gather) adj_drop_graphs(a);
+    a->gather = mode;
     return VLR_OK;
 }
 

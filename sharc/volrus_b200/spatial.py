@@ -198,14 +198,14 @@ def _member(keys: torch.Tensor, sorted_set: torch.Tensor) -> torch.Tensor:
     return sorted_set[i] == keys
 
 
-def ghost_positions(c: torch.Tensor, part: Partition, rank: int) -> dict[int, torch.Tensor]:
+def ghost_positions(c: torch.Tensor, part: Partition, rank: int, depth: int = GHOST_DEPTH) -> dict[int, torch.Tensor]:
     """Per other rank q, the indices of the leaves at coordinates ``c`` (owned
-    by ``rank``) within GHOST_DEPTH leaves of a coordinate q owns."""
+    by ``rank``) within ``depth`` leaves of a coordinate q owns."""
     if len(c) == 0 or part.world == 1:
         return {}
     if part.world > 63:
         raise NotImplementedError("more than 63 ranks")
-    d = GHOST_DEPTH
+    d = depth
     # the owners over a leaf's box lie between those of its corner keys (keys
     # grow along each axis, owners along the keys): leaves whose whole box
     # is this rank's send nothing
@@ -782,6 +782,175 @@ def emulate(leaves: Leaves, world: int, make_stepper: Callable[[int], Callable[[
         if rebalance_every and (s + 1) % rebalance_every == 0:
             rebalance_shards(shards, ex)
     return Leaves.concat([sh.owned for sh in shards], shards[0].like).sorted_xyz(), shards
+
+
+# ------------------------------------------------------------------ divided adjoint
+
+def adjoint_ghost_depth(steps: int, reach: int = 2) -> int:
+    """Leaves of ghost ring that make a rank's K-step frozen-band adjoint exact
+    on its owned voxels without exchanges between steps.  One step reads phi
+    (forward) or lambda (backward) within reach + 1 voxels of a voxel, so K
+    steps reach K (reach + 1) voxels; one more leaf covers the 27-leaf
+    neighbourhood lookups at the ring's inner edge."""
+    return -(-steps * (reach + 1) // 8) + 1
+
+
+def adjoint_locals(owned: Sequence[Leaves], part: Partition, depth: int, exchange,
+                   ranks: Sequence[int] | None = None):
+    """Each rank's local leaves for the divided adjoint, its owned leaves and
+    every other rank's leaf within ``depth`` leaves of them, sorted (x, y, z)
+    (the order fixes the adjoint's band order, and a sorted subset keeps the
+    undivided band's relative order); also each rank's ghost sends (rank q ->
+    indices into its owned leaves), which the gradient exchange reuses."""
+    ranks = list(range(len(owned))) if ranks is None else list(ranks)
+    sends_idx = [ghost_positions(o.coords(), part, r, depth) for r, o in zip(ranks, owned)]
+    got = exchange([{q: o.take(sel) for q, sel in si.items()} for o, si in zip(owned, sends_idx)])
+    locals_ = [Leaves.concat([o, *g], o).sorted_xyz() for o, g in zip(owned, got)]
+    return locals_, sends_idx
+
+
+def _voxel_keys(coords: torch.Tensor) -> torch.Tensor:
+    """Packed 63-bit keys of voxel coordinates (21 bits per axis, biased)."""
+    c = coords.to(torch.int64) + (1 << 20)
+    return (c[:, 0] << 42) | (c[:, 1] << 21) | c[:, 2]
+
+
+def _band_grad_leaves(leaves: Leaves, coords: torch.Tensor, grad: torch.Tensor) -> Leaves:
+    """Leaf records carrying a band function: phi holds grad at the band voxels
+    (coords, a subset of the leaves' voxels) and 0 elsewhere."""
+    phi = torch.zeros((len(leaves), 512), dtype=leaves.phi.dtype, device=leaves.device)
+    if len(coords):
+        lk = morton_keys_of_leaf_coords(leaves.coords())
+        order = torch.argsort(lk)
+        ck = morton_keys_of_leaf_coords(torch.div(coords, 8, rounding_mode="floor"))
+        li = order[torch.searchsorted(lk[order], ck)]
+        loc = coords - torch.div(coords, 8, rounding_mode="floor") * 8
+        off = (loc[:, 0] << 6) | (loc[:, 1] << 3) | loc[:, 2]
+        phi[li, off] = grad.to(phi.dtype)
+    return Leaves(leaves.origins, leaves.masks, phi)
+
+
+def divided_adjoint(owned: Sequence[Leaves], part: Partition, make_engine: Callable[[int, Leaves], object],
+                    loss_grad: Callable[[object, torch.Tensor, torch.Tensor], torch.Tensor], exchange,
+                    steps: int, reach: int = 2, ranks: Sequence[int] | None = None, depth: int | None = None):
+    """The frozen-band adjoint of a level set divided over ranks, exact on
+    every rank's owned band voxels: forward phi_K and dL/dphi_0 equal the
+    undivided adjoint's bit for bit when the engines sum each voxel's terms
+    in the same order (a band order that is a sorted subset of the undivided
+    one, and the same transpose kernel).
+
+    Each rank builds its engine over its owned leaves plus a ghost ring of
+    ``adjoint_ghost_depth(steps, reach)`` leaves and runs the K forward steps
+    with no exchange between them.  The loss gradient dL/dphi_K is taken on
+    the owned band voxels only (``loss_grad(engine, phi_K, owned_mask)``
+    returns it for the masked band voxels), then sent the reverse way to the ranks that hold those
+    voxels as ghosts, so every local band voxel starts the backward pass with
+    the undivided lambda_K; the K backward steps again need no exchange.
+
+    ``make_engine(rank, local leaves)`` returns an object with
+    ``band_coords()`` (band voxel coordinates, (n, 3) int tensor),
+    ``forward()`` (phi_K on the band) and ``backward(lambda_K)``
+    (dL/dphi_0 on the band).  Returns per rank (coords, phi_K, dL/dphi_0) of
+    its owned band voxels, and the engines.  ``owned`` holds the shards of
+    this process, of ranks ``ranks`` (all ranks, 0..n-1, when emulated; this
+    process's one rank with a ``DistExchange``).  ``depth`` overrides the
+    ghost ring's depth in leaves."""
+    ranks = list(range(len(owned))) if ranks is None else list(ranks)
+    depth = adjoint_ghost_depth(steps, reach) if depth is None else depth
+    locals_, sends_idx = adjoint_locals(owned, part, depth, exchange, ranks)
+    engines = [make_engine(r, lv) for r, lv in zip(ranks, locals_)]
+    coords = [e.band_coords() for e in engines]
+    own = [part.owner(morton_keys_of_leaf_coords(torch.div(c, 8, rounding_mode="floor"))) == r
+           for r, c in zip(ranks, coords)]
+    phik = [e.forward() for e in engines]
+    grads = []
+    for e, c, m, p in zip(engines, coords, own, phik):
+        g = torch.zeros(len(c), dtype=p.dtype, device=p.device)
+        g[m] = loss_grad(e, p, m).to(p.dtype)
+        grads.append(g)
+    # dL/dphi_K of owned voxels to the ranks holding them as ghosts (the
+    # leaves of the ghost sends, carrying the gradient in place of values)
+    sends = []
+    for o, si, c, m, g in zip(owned, sends_idx, coords, own, grads):
+        gl = _band_grad_leaves(o, c[m], g[m])
+        sends.append({q: gl.take(sel) for q, sel in si.items()})
+    got = exchange(sends)
+    results = []
+    for e, c, m, g, p, parts in zip(engines, coords, own, grads, phik, got):
+        lam = g.clone()
+        ghost = torch.nonzero(~m).reshape(-1)
+        if len(ghost) and parts:
+            rl = Leaves.concat(list(parts), parts[0])
+            rk = morton_keys_of_leaf_coords(rl.coords())
+            order = torch.argsort(rk)
+            cg = c[ghost]
+            cl = torch.div(cg, 8, rounding_mode="floor")
+            want = morton_keys_of_leaf_coords(cl)
+            pos = torch.clamp(torch.searchsorted(rk[order], want), max=len(rk) - 1)
+            if not bool((rk[order][pos] == want).all()):
+                raise AssertionError("a ghost band voxel's gradient did not arrive with its leaf")
+            li = order[pos]
+            loc = cg - cl * 8
+            off = (loc[:, 0] << 6) | (loc[:, 1] << 3) | loc[:, 2]
+            lam[ghost] = rl.phi[li, off].to(lam.dtype)
+        g0 = e.backward(lam)
+        results.append((c[m], p[m], g0[m]))
+    return results, engines
+
+
+class DeviceAdjointEngine:
+    """A rank's frozen-band adjoint of its local leaves on its device: a
+    single-grid ``LevelSet`` over them (the level set's velocity must be
+    time-independent) and its adjoint (``vlr_adj_create_level_set``), with the
+    lambda transpose pinned to the windowed gather so every rank and the
+    undivided run sum each voxel's terms in the same order.  Tensors stay on
+    the device; calls return after their work."""
+
+    def __init__(self, leaves: Leaves, velocity: dict, dt: float, steps: int, checkpoint_every: int,
+                 half_width: float = 3.0, precision: int = 1, integrator: int = 3, ctx=None, gather: int = 1):
+        from .adjoint import AdvectionFunction
+        from .method import LevelSet
+        o, m, p = leaves.numpy()
+        self.device = leaves.device
+        self.ls = LevelSet.from_leaves(o, m, p.astype(np.float32), velocity, dt, half_width, precision, integrator,
+                                       2, 0.0, 0, 0, ctx=ctx)
+        self.ctx = self.ls.ctx
+        self.fn = AdvectionFunction.from_level_set(self.ls, steps, checkpoint_every)
+        self.fn.set_gather(gather)
+
+    def _sync(self):
+        if self.device.type == "cuda":
+            torch.cuda.current_stream(self.device).synchronize()
+
+    def band_coords(self) -> torch.Tensor:
+        return torch.from_numpy(self.fn.band().astype(np.int64)).to(self.device)
+
+    def forward(self) -> torch.Tensor:
+        out = torch.empty(self.fn.n_band, dtype=torch.float32, device=self.device)
+        self._sync()
+        self.fn.forward_device(out.data_ptr())
+        self.ctx.check_device()
+        return out
+
+    def backward(self, lam_k: torch.Tensor) -> torch.Tensor:
+        lam = lam_k.to(device=self.device, dtype=torch.float32).contiguous()
+        out = torch.empty(self.fn.n_band, dtype=torch.float32, device=self.device)
+        self._sync()
+        self.fn.backward_device(lam.data_ptr(), out.data_ptr(), 0)
+        self.ctx.check_device()
+        return out
+
+    def shifted_phi0(self, shift) -> torch.Tensor:
+        """phi_0 translated by ``shift`` voxels, on the band (a loss target)."""
+        out = torch.empty(self.fn.n_band, dtype=torch.float32, device=self.device)
+        self._sync()
+        self.fn.shifted_phi0_device(shift, out.data_ptr())
+        self.ctx.check_device()
+        return out
+
+    def close(self):
+        self.fn.close()
+        self.ls.close()
 
 
 class SpatialLevelSet:

@@ -516,3 +516,198 @@ def test_pool_edits_and_their_errors(ctx, precision):
     ls.upload(o, m, p)
     ls.step(1)
     ls.close()
+
+
+# ------------------------------------------------------------------ divided adjoint
+
+ADJ_STEPS = 6
+
+
+def _adj_disp(coords):
+    """A smooth per-voxel displacement (voxels, |d| < 1) standing in for a backtrace."""
+    x, y, z = (coords[:, a].astype(np.float64) for a in range(3))
+    return np.stack([0.8 * np.sin(0.11 * y + 0.07 * z), 0.6 * np.sin(0.09 * z + 0.05 * x),
+                     -0.7 * np.sin(0.13 * x + 0.03 * y)], axis=1)
+
+
+def _adj_target(coords):
+    x, y, z = (coords[:, a].astype(np.float64) for a in range(3))
+    return 0.3 * np.sin(0.05 * x) * np.cos(0.04 * y) + 0.1 * z / 256.0
+
+
+class OracleAdjointEngine:
+    """The FP64 oracle's frozen-band adjoint over a rank's local leaves, band in
+    leaf then offset order, driven by _adj_disp (test checker)."""
+
+    def __init__(self, lv, steps):
+        from oracle.pyadjoint import AdjointOracle
+        o, m, p = lv.numpy()
+        bits = np.unpackbits(m.view(np.uint8).reshape(-1, 64), axis=1, bitorder="little").astype(bool)
+        li, vi = np.nonzero(bits)
+        rel = np.stack([vi >> 6, (vi >> 3) & 7, vi & 7], axis=1)
+        self.coords = o[li].astype(np.int64) + rel
+        self.orc = AdjointOracle.from_displacement(o, m, p, 3.0, _adj_disp(self.coords), steps)
+
+    def band_coords(self):
+        return torch.from_numpy(self.coords)
+
+    def forward(self):
+        return torch.from_numpy(self.orc.forward())
+
+    def backward(self, lam):
+        return torch.from_numpy(self.orc.backward(lam.numpy())[0])
+
+
+def _adj_loss_grad(engine, phik, mask):
+    return 2.0 * (phik[mask] - torch.from_numpy(_adj_target(engine.coords[mask.numpy()])))
+
+
+def _adj_case():
+    from oracle import pyoracle
+    rng = np.random.default_rng(23)
+    sph = np.column_stack([rng.uniform(0, 256, (24, 3)), rng.uniform(6, 14, 24)])
+    return Leaves.from_numpy(*pyoracle.MOGrid.spheres(sph, 3.0).arrays())
+
+
+def _adj_undivided(lv):
+    e = OracleAdjointEngine(lv.sorted_xyz(), ADJ_STEPS)
+    phik = e.forward()
+    mask = torch.ones(len(phik), dtype=torch.bool)
+    g0 = e.backward(_adj_loss_grad(e, phik, mask))
+    keys = spatial._voxel_keys(e.band_coords())
+    return {int(k): (float(a), float(b)) for k, a, b in zip(keys, phik, g0)}
+
+
+def _adj_check(results, ref, exact=True):
+    n = 0
+    bad = 0
+    for coords, phik, g0 in results:
+        for k, a, b in zip(spatial._voxel_keys(coords).tolist(), phik.tolist(), g0.tolist()):
+            ra, rb = ref[k]
+            bad += (a != ra) or (b != rb)
+            n += 1
+    assert n == len(ref), (n, len(ref))
+    return bad
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_divided_adjoint_matches_undivided_oracle(oracle, world):
+    """Each rank's forward phi_K and dL/dphi_0 on its owned band voxels equal
+    the undivided FP64 adjoint's bit for bit (ghost ring of
+    adjoint_ghost_depth leaves, no exchange between steps, the loss gradient
+    sent the reverse way once); a ring of one leaf over twice the steps
+    changes them (the dependency cone is wider than the ring)."""
+    lv = _adj_case()
+    ref = _adj_undivided(lv)
+    part, shares = spatial.split(lv, world)
+    mk = lambda r, local: OracleAdjointEngine(local, ADJ_STEPS)  # noqa: E731
+    res, _ = spatial.divided_adjoint(shares, part, mk, _adj_loss_grad, spatial.LocalExchange(), ADJ_STEPS, reach=1)
+    assert _adj_check(res, ref) == 0
+    assert spatial.adjoint_ghost_depth(ADJ_STEPS, 1) == 3
+    if world == 2:
+        steps = 3 * ADJ_STEPS
+        e = OracleAdjointEngine(lv.sorted_xyz(), steps)
+        phik = e.forward()
+        g0 = e.backward(_adj_loss_grad(e, phik, torch.ones(len(phik), dtype=torch.bool)))
+        ref2 = {int(k): (float(a), float(b)) for k, a, b in zip(spatial._voxel_keys(e.band_coords()), phik, g0)}
+        mk2 = lambda r, local: OracleAdjointEngine(local, steps)  # noqa: E731
+        thin, _ = spatial.divided_adjoint(shares, part, mk2, _adj_loss_grad, spatial.LocalExchange(), steps, reach=1,
+                                          depth=1)
+        assert _adj_check(thin, ref2) > 0
+
+
+def _rank_main_adjoint(rank, world, port, q):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        lv = _adj_case()
+        part, shares = spatial.split(lv, world)
+        ex = spatial.DistExchange(Leaves.empty(torch.float64), None)
+        res, _ = spatial.divided_adjoint([shares[rank]], part, lambda r, local: OracleAdjointEngine(local, ADJ_STEPS),
+                                         _adj_loss_grad, ex, ADJ_STEPS, reach=1, ranks=[rank])
+        (coords, phik, g0), = res
+        q.put((rank, coords.numpy(), phik.numpy(), g0.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_divided_adjoint_two_gloo_ranks(oracle):
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main_adjoint, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in range(world)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ref = _adj_undivided(_adj_case())
+    res = [(torch.from_numpy(c), torch.from_numpy(a), torch.from_numpy(b)) for _, c, a, b in out]
+    assert _adj_check(res, ref) == 0
+    assert min(len(c) for _, c, _, _ in out) > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,world", [(1, 2), (0, 3)], ids=["f16_2", "f32_3"])
+def test_divided_level_set_adjoint_matches_undivided_device_run(ctx, precision, world):
+    """The level-set adjoint of a grid divided over emulated ranks (one device,
+    a DeviceAdjointEngine per rank over its owned leaves and ghost ring): phi_K
+    and dL/dphi_0 on every rank's owned band voxels equal the undivided
+    device adjoint's bit for bit (both with the windowed lambda transpose),
+    for an L2 loss against phi_0 translated by 4 voxels in x."""
+    (o, m, p), vel, integ, dt = _device_case("curl")
+    steps, chk = 6, 2
+    lv = Leaves.from_numpy(o, m, p, "cuda").sorted_xyz()
+
+    def loss_grad(engine, phik, mask):
+        return 2.0 * (phik[mask] - engine.shifted_phi0((4, 0, 0))[mask])
+
+    full = spatial.DeviceAdjointEngine(lv, vel, dt, steps, chk, precision=precision, integrator=integ)
+    phik = full.forward()
+    g0 = full.backward(loss_grad(full, phik, torch.ones(len(phik), dtype=torch.bool, device="cuda")))
+    ref = {int(k): (float(a), float(b)) for k, a, b in zip(spatial._voxel_keys(full.band_coords()).tolist(),
+                                                            phik.tolist(), g0.tolist())}
+    full.close()
+    part, shares = spatial.split(lv, world)
+    engines = []
+
+    def make(r, local):
+        e = spatial.DeviceAdjointEngine(local, vel, dt, steps, chk, precision=precision, integrator=integ)
+        engines.append(e)
+        return e
+
+    res, _ = spatial.divided_adjoint(shares, part, make, loss_grad, spatial.LocalExchange(), steps, reach=2)
+    n = 0
+    for coords, a, b in res:
+        for k, x, y in zip(spatial._voxel_keys(coords).tolist(), a.tolist(), b.tolist()):
+            assert ref[k] == (x, y), k
+            n += 1
+    assert n == len(ref)
+    assert any(float(torch.abs(b).max()) > 0 for _, _, b in res)
+    for e in engines:
+        e.close()
+
+
+@pytest.mark.gpu
+def test_adjoint_gather_modes(ctx):
+    """vlr_adj_set_gather: the windowed and quad transposes agree to rounding,
+    each is deterministic, and the quad is refused above a reach of one."""
+    from sharc.volrus_b200._lib import VolrusError
+    (o, m, p), vel, integ, dt = _device_case("curl")
+    e = spatial.DeviceAdjointEngine(Leaves.from_numpy(o, m, p, "cuda").sorted_xyz(), vel, dt, 4, 2, precision=0,
+                                    integrator=integ)
+    lam = torch.linspace(-1.0, 1.0, e.fn.n_band, device="cuda")
+    outs = {}
+    for mode in (1, 2, 1):
+        e.fn.set_gather(mode)
+        outs.setdefault(mode, []).append(e.backward(lam))
+    assert torch.equal(outs[1][0], outs[1][1])
+    assert torch.allclose(outs[1][0], outs[2][0], rtol=1e-5, atol=1e-6)
+    with pytest.raises(VolrusError):
+        e.fn.set_gather(3)
+    e.close()
