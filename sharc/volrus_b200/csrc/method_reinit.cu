@@ -135,19 +135,22 @@ __device__ __forceinline__ const T* at(const T* stage, int x, int y, int z) {
 
 // Godunov upwind |grad phi| for the sign of s.  Per axis the upwind one-sided
 // differences are u = max(sg (p - phi_-), 0) and w = max(sg (p - phi_+), 0),
-// sg = +-1 the sign of s (exact), and the axis term is max(u, w)^2, which
-// equals max(u^2, w^2) bit for bit (u, w >= 0 and rounding is monotone): the
-// same value as the sign-split form max(max(a-, 0)^2, min(a+, 0)^2) for s >=
-// 0 and its mirror for s < 0, without the sign branch.
+// sg = +-1 the sign of s, and the axis term is max(u, w)^2, the same value as
+// the sign-split form max(max(a-, 0)^2, min(a+, 0)^2) for s >= 0 and its
+// mirror for s < 0, without the sign branch.  max(u, w) is evaluated as
+// max(sg p - min(sg phi_-, sg phi_+), 0): negation is exact and rounding is
+// monotone, so this is the same value, and fminf drops a NaN neighbour just
+// as fmaxf drops its NaN difference.  |grad phi| = g2 g2^(-1/2) (rsqrtf).
 __device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym, float yp, float zm, float zp, float s) {
     const float sg = (s >= 0.f) ? 1.f : -1.f;
-    const float mx = fmaxf(fmaxf(sg * (p - xm), 0.f), fmaxf(sg * (p - xp), 0.f));
-    const float my = fmaxf(fmaxf(sg * (p - ym), 0.f), fmaxf(sg * (p - yp), 0.f));
-    const float mz = fmaxf(fmaxf(sg * (p - zm), 0.f), fmaxf(sg * (p - zp), 0.f));
-    // squares rounded before the sums, as in the sign-split form (no contraction)
+    const float q = sg * p;
+    const float mx = fmaxf(q - fminf(sg * xm, sg * xp), 0.f);
+    const float my = fmaxf(q - fminf(sg * ym, sg * yp), 0.f);
+    const float mz = fmaxf(q - fminf(sg * zm, sg * zp), 0.f);
+    // squares rounded before the sums (no contraction)
     float g2 = __fmul_rn(mx, mx) + __fmul_rn(my, my);
     g2 += __fmul_rn(mz, mz);
-    return sqrtf(g2);
+    return g2 > 0.f ? g2 * rsqrtf(g2) : 0.f;
 }
 
 // NaN marks a voxel of an unallocated leaf; a 6-neighbour stencil reads it as
@@ -309,6 +312,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     __shared__ int s_nbr[2][32];
     __shared__ int s_n1, s_n2;
     __shared__ unsigned s_bx[32];  // the box voxels of D, one bit per flat index
+    __shared__ short s_roff[kF * kF];  // stage offset of box row (bx, by) at bz = 0
     __shared__ __align__(16) unsigned s_M[16];
 
     const int count = *A.count;
@@ -317,6 +321,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     if (li >= count) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
+    for (int r = threadIdx.x; r < kF * kF; r += kNT)
+        s_roff[r] = (short)(((r / kF - 1 + kH) * kE + (r % kF - 1 + kH)) * RP + Row<T>::Z0 - 1);
     int slot = A.list[li];
     int4 o = A.origin[slot];
     if (warp == 0) s_nbr[0][lane] = (lane < kNbr) ? A.nbr[(size_t)slot * kNbr + lane] : -1;
@@ -387,8 +393,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
             const int n1 = s_n1;
             for (int i = threadIdx.x; i < n1; i += kNT) {
                 const int t = s_list1[i];
-                const int bx = t / (kF * kF), r = t - bx * (kF * kF), by = r / kF, bz = r - by * kF;
-                const T* c1 = at(stage, bx - 1, by - 1, bz - 1);
+                const int r = t / kF;
+                const T* c1 = stage + s_roff[r] + (t - r * kF);
                 const float p = to_f(c1[0]);
                 if (FIX) {
                     const Nb6 n = load_nb6<T, kE * RP, RP>(c1, p, hw);
