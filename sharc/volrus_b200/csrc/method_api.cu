@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "method_state.hpp"
+#include "sort_reduce.hpp"
 
 namespace vlr {
 
@@ -599,12 +600,107 @@ int enqueue_one_step(vlr_ctx* ctx, vlr_level_set* ls) {
 
 // Leaves of one grid (grid < 0: all) of a level set holding n listed leaves,
 // sorted by (grid, x, y, z), into host buffers.
+// Leaf keys of list positions 0..n-1 of a single grid (leaf coordinates
+// relative to the hash base, `bits` each: key order is the origins'
+// lexicographic order), their low words and the identity permutation.
+__global__ void k_leaf_keys(const int* __restrict__ list, int n, const int4* __restrict__ origin, long long b0,
+                            long long b1, long long b2, int bits, unsigned long long* __restrict__ keys,
+                            unsigned* __restrict__ lo, unsigned* __restrict__ idx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 o = origin[list[i]];
+        const unsigned long long k = ((unsigned long long)((o.x >> 3) - b0) << (2 * bits)) |
+                                     ((unsigned long long)((o.y >> 3) - b1) << bits) |
+                                     (unsigned long long)((o.z >> 3) - b2);
+        keys[i] = k;
+        lo[i] = (unsigned)k;
+        idx[i] = (unsigned)i;
+    }
+}
+
+__global__ void k_leaf_keys_hi(const unsigned long long* __restrict__ keys, const unsigned* __restrict__ perm, int n,
+                               unsigned* __restrict__ hi) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        hi[i] = (unsigned)(keys[perm[i]] >> 32);
+}
+
+// Origins (i32[3]) of the list positions perm[0..n) in that order.
+__global__ void k_sorted_origins(const int* __restrict__ list, const unsigned* __restrict__ perm, int n,
+                                 const int4* __restrict__ origin, int32_t* __restrict__ o3) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 o = origin[list[perm[i]]];
+        o3[3 * i] = o.x;
+        o3[3 * i + 1] = o.y;
+        o3[3 * i + 2] = o.z;
+    }
+}
+
+// The sorted download of all leaves of a single grid with the order made on
+// the device: 64-bit leaf keys sorted by two stable 32-bit radix passes (low
+// word, then high word), then origins, masks and f32 values gathered in that
+// order and copied once into the caller's buffers.
+int download_sorted_device(vlr_ctx* ctx, const vlr_level_set* ls, size_t n, int32_t* origins, uint64_t* masks,
+                           float* phi) {
+    cudaStream_t st = ctx->stream;
+    const int nn = (int)n;
+    const size_t sort_bytes = sort_reduce_scratch_bytes(nn);
+    const size_t vbytes = sizeof(float) * kLeafVoxels * n;
+    char* buf = nullptr;
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&buf, vbytes + n * (8 + 4 * 3 + 12 + 64) + sort_bytes + 512,
+                                          ctx->pool, st));
+    auto done = [&](int code) {
+        cudaFreeAsync(buf, st);
+        return code;
+    };
+    char* q = buf;
+    float* v = (float*)q;  q += vbytes;
+    unsigned long long* keys = (unsigned long long*)q;  q += n * 8;
+    uint64_t* mm = (uint64_t*)q;  q += n * 64;
+    unsigned* lo = (unsigned*)q;  q += n * 4;
+    unsigned* idx = (unsigned*)q;  q += n * 4;
+    unsigned* hi = (unsigned*)q;  q += n * 4;
+    int32_t* o3 = (int32_t*)q;  q += n * 12;
+    void* scratch = (void*)(((uintptr_t)q + 255) & ~(uintptr_t)255);
+    const vlr::MGridParams& P = ls->h_params[0];
+    const int B = ctx->sm_count * 8;
+    k_leaf_keys<<<B, 256, 0, st>>>(ls->list, nn, ls->origin, P.base[0], P.base[1], P.base[2], ls->key_bits, keys, lo,
+                                   idx);
+    unsigned *k1, *v1, *k2, *v2;
+    int rc = radix_sort_pairs(ctx, lo, idx, nn, 0xffffffffu, scratch, &k1, &v1);
+    if (rc) return done(rc);
+    k_leaf_keys_hi<<<B, 256, 0, st>>>(keys, v1, nn, hi);
+    if (v1 != idx) VLR_CUDA(ctx, cudaMemcpyAsync(idx, v1, n * 4, cudaMemcpyDeviceToDevice, st));
+    rc = radix_sort_pairs(ctx, hi, idx, nn, 0x7fffffffu, scratch, &k2, &v2);
+    if (rc) return done(rc);
+    (void)k1;
+    (void)k2;
+    const int* sel = (const int*)v2;
+    if (origins) k_sorted_origins<<<B, 256, 0, st>>>(ls->list, v2, nn, ls->origin, o3);
+    if (masks || phi) {
+        const int G = (int)std::min<size_t>(n, (size_t)ctx->sm_count * 8);
+        if (ls->precision == VLR_PREC_F16)
+            k_gather_sel<__half><<<G, 256, 0, st>>>(ls->list, sel, nn, ls->mask, (const __half*)ls->vals[0], mm, v);
+        else
+            k_gather_sel<float><<<G, 256, 0, st>>>(ls->list, sel, nn, ls->mask, (const float*)ls->vals[0], mm, v);
+    }
+    VLR_CUDA(ctx, cudaGetLastError());
+    if (origins && (rc = d2h_copy(ctx, origins, o3, n * 12))) return done(rc);
+    if (masks && (rc = d2h_copy(ctx, masks, mm, n * 64))) return done(rc);
+    if (phi && (rc = d2h_copy(ctx, phi, v, vbytes))) return done(rc);
+    VLR_CUDA(ctx, cudaStreamSynchronize(st));
+    return done(VLR_OK);
+}
+
 int download_n(vlr_ctx* ctx, const vlr_level_set* ls, size_t n, int grid, int32_t* grid_ids, int32_t* origins,
                uint64_t* masks, float* phi, size_t cap_leaves, size_t* n_out) {
     int rc = VLR_OK;
     *n_out = 0;
     if (grid < 0 && n > cap_leaves) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
     if (!n) return VLR_OK;
+    if (grid < 0 && !grid_ids && ls->n_grids == 1 && 3 * ls->key_bits <= 63 && n <= (size_t)INT_MAX / 16) {
+        rc = download_sorted_device(ctx, ls, n, origins, masks, phi);
+        if (rc == VLR_OK) *n_out = n;
+        return rc;
+    }
     // origins in list order -> host, output order sorted by (grid, x, y, z)
     // there; masks and values are then gathered on the device in that order
     // and copied once, straight into the caller's buffers
