@@ -140,7 +140,9 @@ __device__ __forceinline__ const T* at(const T* stage, int x, int y, int z) {
 // mirror for s < 0, without the sign branch.  max(u, w) is evaluated as
 // max(sg p - min(sg phi_-, sg phi_+), 0): negation is exact and rounding is
 // monotone, so this is the same value, and fminf drops a NaN neighbour just
-// as fmaxf drops its NaN difference.  |grad phi| = g2 g2^(-1/2) (rsqrtf).
+// as fmaxf drops its NaN difference.  The correctly rounded sqrtf keeps a
+// full deformation period's FP32 topology equal to the FP64 run's (an
+// rsqrtf-based magnitude measured two voxels flipping at the band's edge).
 __device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym, float yp, float zm, float zp, float s) {
     const float sg = (s >= 0.f) ? 1.f : -1.f;
     const float q = sg * p;
@@ -150,7 +152,7 @@ __device__ __forceinline__ float godunov_g(float p, float xm, float xp, float ym
     // squares rounded before the sums (no contraction)
     float g2 = __fmul_rn(mx, mx) + __fmul_rn(my, my);
     g2 += __fmul_rn(mz, mz);
-    return g2 > 0.f ? g2 * rsqrtf(g2) : 0.f;
+    return sqrtf(g2);
 }
 
 // NaN marks a voxel of an unallocated leaf; a 6-neighbour stencil reads it as
