@@ -16,13 +16,12 @@
 //              the stage is complete at its barrier; a 6-neighbour stencil
 //              reads NaN as copysign(hw, its centre value), which needs no
 //              work in the common case (see godunov_update_raw).
-//   phase 1    warp 0 compacts the voxel lists: the box voxels of D for
-//              iteration 1 (the 10^3 box around the leaf without its edges
-//              and corners, which iteration 2 never reads) and the leaf's
-//              voxels of D, and keeps the box list's bit words.  Warps 1-3
-//              issue the next leaf's copies and write every voxel's
-//              outside-D result copysign(hw, value) to global memory
-//              (coalesced).
+//   phase 1    warp 0 compacts the box voxels of D for iteration 1 (the
+//              10^3 box around the leaf without its edges and corners, which
+//              iteration 2 never reads) and keeps their bit words; warp 1
+//              compacts the leaf's voxels of D; warps 1-3 issue the next
+//              leaf's copies and write every voxel's outside-D result
+//              copysign(hw, value) to global memory (coalesced).
 //   phase 2    iteration 1 on the box list, consecutive voxels on
 //              consecutive lanes (bank-conflict-free stage reads), into phi2.
 //   phase 3    iteration 2 (or the only one) on the leaf list, its
@@ -354,10 +353,23 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         // buffer before its barrier A, while warp 1 may still be proposing
         const int my_nb = lane < kNbr ? s_nbr[b][lane] : -1;
         T* out = dst + (size_t)slot * kLeafVoxels;
+        // the leaf's voxels of D for the last iteration (offset x * 64 + y * 8 + z)
+        auto leaf_list = [&]() {
+            const int q = lane >> 2, cq = lane & 3;
+            unsigned bits = (unsigned)(s_m[13 * 8 + q] >> (16 * cq)) & 0xffffu;
+            const int c = __popc(bits);
+            const int incl = warp_incl_scan(c, lane);
+            int pos = incl - c;
+            while (bits) {
+                const int z = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                s_list2[pos++] = (unsigned short)(q * 64 + 16 * cq + z);
+            }
+            if (lane == 31) s_n2 = incl;
+        };
         if (warp == 0) {
-            // the voxel lists: box voxels of D for iteration 1 (flat index
-            // t = (bx * 10 + by) * 10 + bz, ascending) and the leaf's voxels
-            // of D for the last iteration (offset x * 64 + y * 8 + z)
+            // the box voxels of D for iteration 1 (flat index t = (bx * 10 +
+            // by) * 10 + bz, ascending); without iteration 1 the leaf list
             if (NIT == 2) {
                 unsigned bw = box_word(s_m, lane);
                 s_bx[lane] = bw;
@@ -370,19 +382,12 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
                     s_list1[pos++] = (unsigned short)(32 * lane + z);
                 }
                 if (lane == 31) s_n1 = incl;
+            } else {
+                leaf_list();
             }
-            const int q = lane >> 2, cq = lane & 3;
-            unsigned bits = (unsigned)(s_m[13 * 8 + q] >> (16 * cq)) & 0xffffu;
-            const int c = __popc(bits);
-            const int incl = warp_incl_scan(c, lane);
-            int pos = incl - c;
-            while (bits) {
-                const int z = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                s_list2[pos++] = (unsigned short)(q * 64 + 16 * cq + z);
-            }
-            if (lane == 31) s_n2 = incl;
         } else {
+            // warp 1 builds the leaf list first when warp 0 has the box list
+            if (NIT == 2 && warp == 1) leaf_list();
             const int t = threadIdx.x - 32;
             if (slot_n >= 0)
                 issue_stage<T>(s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
