@@ -85,7 +85,11 @@ int vlr_ctx_test_stall(vlr_ctx* ctx, int on);
 /* ---- grids (reference semantics: f32 values in world units) ------------ */
 
 /* Upload a Grid<f32>: replaces NanoGrid::from_grid + upload (src/nano/layout.rs:89-170).
- * Leaves must have distinct, 8-aligned origins; any order is accepted. */
+ * Leaves must have distinct, 8-aligned origins; any order is accepted.
+ * Grids hold leaves only: a tree with tiles (made only by RootNode::prune,
+ * src/tree/internal.rs:253-299) passes each active tile as a leaf record
+ * with all 512 bits set and the tile's value in every voxel, which reads and
+ * iterates as the tile does (src/tree/internal.rs:118-124, 319-349). */
 int vlr_grid_create(vlr_ctx* ctx, const vlr_transform* xf, float background, const int32_t* origins,
                     const uint64_t* masks, const float* values, size_t n_leaves, vlr_grid** out);
 /* Device-resident form of vlr_grid_create, for leaves already in this

@@ -233,6 +233,44 @@ class Grid:
         g._index = {tuple(int(v) for v in o[i]): i for i in range(g._n)}
         return g
 
+    def add_tiles(self, origins, values, active):
+        """Insert the tiles of a pruned tree as leaf records.
+
+        ``RootNode::prune`` (src/tree/root.rs:151-158, src/tree/internal.rs:253-299)
+        collapses a leaf whose 512 values lie within a tolerance of its first
+        value into a tile holding that value, active when the leaf had an active
+        voxel.  The tree then reads the tile's value at each of its voxels
+        (``get``, src/tree/internal.rs:118-124) and iterates an active tile as
+        512 active voxels of that value (``iter_active``,
+        src/tree/internal.rs:319-349).  A leaf record holding the tile's value in
+        all 512 voxels, with all bits set for an active tile and none for an
+        inactive one, reads and iterates the same, so a pruned tree crosses the
+        C ABI as these records beside its leaves.
+
+        Tile origins must be leaf-aligned and must not hold a leaf (a slot of the
+        internal node is either a child or a tile); ValueError otherwise.
+        """
+        o = np.ascontiguousarray(origins, np.int64).reshape(-1, 3)
+        val = np.ascontiguousarray(values, np.float32).reshape(-1)
+        act = np.ascontiguousarray(active, bool).reshape(-1)
+        if not (len(o) == len(val) == len(act)):
+            raise ValueError("tile origins, values and flags differ in length")
+        if np.any(o & 7):
+            raise ValueError("tile origins must be multiples of 8")
+        keys = [tuple(int(x) for x in r) for r in o]
+        if len(set(keys)) != len(keys) or any(k in self._index for k in keys):
+            raise ValueError("a tile overlaps a leaf or another tile")
+        full = np.uint64(0xFFFFFFFFFFFFFFFF)
+        for k, v, a in zip(keys, val, act):
+            if self._n == len(self._o):
+                self._grow()
+            row = self._n
+            self._n += 1
+            self._o[row] = k
+            self._m[row] = full if a else np.uint64(0)
+            self._v[row] = v
+            self._index[k] = row
+
     def set_transform(self, vt: VoxelTransform):
         """``Grid::set_transform`` (src/grid.rs:432-435): also resets the affine map."""
         self.transform = vt

@@ -11,7 +11,9 @@ which assembles the leaf arrays the C ABI uploads, passes the same cases.
 The internal-node count is read as the number of
 distinct 128^3-aligned origins among the leaves.  Not restated, because the
 path never creates them: tiles, and the `prune(tolerance)` that makes them
-(internal.rs:470-538, root.rs:276-285); and `clear` (root.rs:262-274).
+(internal.rs:470-538, root.rs:276-285); and `clear` (root.rs:262-274).  A
+pruned tree still crosses the C ABI: its tiles travel as leaf records
+(``Grid.add_tiles``), checked by the last test here.
 """
 import numpy as np
 import pytest
@@ -244,3 +246,28 @@ def test_root_remove_empty_leaves(new):  # root.rs:287-295
     g.deactivate((0, 0, 0))
     g.remove_empty_leaves()
     assert g.leaf_count() == 1
+
+
+# ---- tiles at the boundary: a pruned tree crosses the C ABI as leaf records
+
+def test_pruned_tiles_cross_as_leaf_records():
+    """internal.rs:497-509 prunes a leaf of constant 5.0 with an active voxel
+    into an active tile; the tree then reads 5.0 at its voxels and iterates it
+    as 512 active voxels (internal.rs:169-184, 319-349).  ``Grid.add_tiles``
+    carries that tile, and an inactive one, as leaf records that read and
+    iterate the same."""
+    from sharc.volrus_b200.grid import Grid
+    g = Grid(5.0, 1.0)
+    g.set((20, 0, 0), 1.0)
+    g.add_tiles([(0, 0, 0), (0, 8, 0)], [5.0, -2.5], [True, False])
+    assert g.leaf_count() == 3
+    assert g.active_voxel_count() == 1 + 512
+    act = dict(g.iter_active())
+    tile = {(x, y, z) for x in range(8) for y in range(8) for z in range(8)}
+    assert tile <= set(act) and all(act[c] == 5.0 for c in tile)
+    assert all(g.get((x, 8 + y, z)) == -2.5 and not g.is_active((x, 8 + y, z)) for x, y, z in tile)
+    assert g.get((100, 100, 100)) == 5.0
+    with pytest.raises(ValueError):
+        g.add_tiles([(16, 0, 0)], [0.0], [True])  # holds a leaf
+    with pytest.raises(ValueError):
+        g.add_tiles([(4, 0, 64)], [0.0], [True])  # not leaf-aligned
