@@ -321,12 +321,12 @@ STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_
 #   deformation512: `bench.py --workload deformation512 --steps 1 --warmup 3`,
 #     -s 6 (2,858 leaves, L2-resident).
 TRAFFIC_PER_LEAF: dict = {
-    ("large8192", "k_m_advect", 2): 2565.0,
-    ("large8192", "k_m_reinit", 2): 2331.0,
-    ("large8192", "k_m_advect", 4): 4913.0,
-    ("large8192", "k_m_reinit", 4): 4504.6,
-    ("batched256", "k_m_advect", 2): 2330.1,
-    ("batched256", "k_m_reinit", 2): 2069.0,
+    ("large8192", "k_m_advect", 2): 2560.7,
+    ("large8192", "k_m_reinit", 2): 2360.0,
+    ("large8192", "k_m_advect", 4): 4889.7,
+    ("large8192", "k_m_reinit", 4): 4508.9,
+    ("batched256", "k_m_advect", 2): 2323.0,
+    ("batched256", "k_m_reinit", 2): 2079.1,
     ("deformation512", "k_m_advect", 2): 1238.0,
     ("deformation512", "k_m_reinit", 2): 1223.0,
 }
@@ -335,12 +335,12 @@ TRAFFIC_PER_LEAF: dict = {
 # Warp instructions per leaf of one launch (smsp__inst_executed.sum over the
 # launch's leaves) from the same captures, FP16, 128-thread CTAs.
 INST_PER_LEAF: dict = {
-    ("large8192", "k_m_advect"): 4453.0,
-    ("large8192", "k_m_reinit"): 4335.0,
+    ("large8192", "k_m_advect"): 4452.5,
+    ("large8192", "k_m_reinit"): 4196.9,
     ("batched256", "k_m_advect"): 4768.3,
-    ("batched256", "k_m_reinit"): 4326.2,
+    ("batched256", "k_m_reinit"): 4188.0,
     ("deformation512", "k_m_advect"): 3001.4,
-    ("deformation512", "k_m_reinit"): 4541.2,
+    ("deformation512", "k_m_reinit"): 4445.2,
 }
 SM_COUNT = 148
 ISSUE_PER_SM_PER_CYCLE = 4  # one warp instruction per scheduler per cycle
