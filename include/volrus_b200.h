@@ -411,8 +411,22 @@ int vlr_ls_edit_device(vlr_ctx* ctx, vlr_level_set* ls, const uint8_t* d_drop, s
  * written.  The copies of the first min(n_leaves, cap_leaves) records start
  * before the leaf count is known, so records past *n_out (up to that bound)
  * may be overwritten; the call then waits once for the count, the device
- * errors and those copies, and copies any records beyond them.  No
- * counterpart in the reference (its step is serial Rust). */
+ * errors and those copies, and copies any records beyond them.
+ * One step of a large single-grid state (at least 2^18 leaves by default)
+ * whose host leaves are sorted by x and whose six host buffers are pinned
+ * runs as a pipeline over slabs of consecutive x instead: each slab steps its
+ * leaves with the input leaves within 16 voxels beside it and keeps the
+ * outputs in its own x range, which are bit for bit the one-pass step's; its
+ * input goes up and its outputs, sorted (x, y, z), go down on copy streams
+ * while other slabs step, so the two copy directions overlap.  The result and
+ * the level set's state afterwards are those of the one-pass call, and no
+ * record past *n_out is written; an error (the output buffers or the pool
+ * too small, a device error) leaves the state undefined until the next
+ * upload.  vlr_ls_set_host_slabs sets the slab count: 0 automatic (one slab
+ * per 2^17 leaves, at most 16), 1 always one pass, k >= 2 at most k slabs
+ * (fewer when the leaves have fewer distinct x).  No counterpart in the
+ * reference (its step is serial Rust). */
+int vlr_ls_set_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, int slabs);
 int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, const uint64_t* masks, const float* phi,
                      size_t n_leaves, int n_steps, int32_t* out_origins, uint64_t* out_masks, float* out_phi,
                      size_t cap_leaves, size_t* n_out);

@@ -152,6 +152,7 @@ SIGNATURES = {
     "vlr_ls_download": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
     "vlr_ls_upload": (C.c_int, [P, P, i32_p, u64_p, flt_p, C.c_size_t]),
     "vlr_ls_set_step": (C.c_int, [P, P, C.c_int]),
+    "vlr_ls_set_host_slabs": (C.c_int, [P, P, C.c_int]),
     "vlr_ls_volume_partials": (C.c_int, [P, P, dbl_p, P, C.c_size_t, size_p]),
     "vlr_ls_upload_device": (C.c_int, [P, P, P, P, P, C.c_size_t]),
     "vlr_ls_download_device": (C.c_int, [P, P, P, P, P, C.c_size_t, size_p]),

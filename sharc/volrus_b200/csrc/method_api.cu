@@ -2,6 +2,7 @@
 // uploaded leaves), per-grid velocity tables, graph-captured steps,
 // download and the FP64 volume.  C entry points vlr_ls_* (include/volrus_b200.h).
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -21,6 +22,14 @@ static int next_pow2i(long long v) {
 }
 
 void ls_free(vlr_level_set* ls) {
+    for (cudaEvent_t& e : ls->slab_ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    for (cudaStream_t& s : ls->slab_stream) {
+        if (s) cudaStreamDestroy(s);
+        s = nullptr;
+    }
     if (ls->graph_exec) cudaGraphExecDestroy(ls->graph_exec);
     if (ls->graph) cudaGraphDestroy(ls->graph);
     ls->graph_exec = nullptr;
@@ -760,6 +769,333 @@ int download_n(vlr_ctx* ctx, const vlr_level_set* ls, size_t n, int grid, int32_
     return VLR_OK;
 }
 
+// ------------------------------------------------- host step over x-slabs
+//
+// A host step of a large single-grid state whose host leaves are sorted by x
+// (the order every download writes) runs as a pipeline over slabs of
+// consecutive x.  Slab s owns the leaves with x in [X_s, X_{s+1}); it steps
+// them together with the input leaves within kSlabRing voxels in x on either
+// side, and keeps the outputs whose x lies in its own range.  A step reads
+// within 5 voxels of a voxel (a backtrace of at most 3 voxels, two one-voxel
+// reinitialisation sweeps), so the new values and mask of a leaf, whether
+// the re-track keeps or allocates it, and the neighbour that fills a new leaf
+// depend only on the input leaves within one leaf of it; those lie inside
+// the slab's input for every output the slab keeps, so each kept output is
+// bit for bit the one-pass step's (the kernels compute a leaf the same way
+// whatever else is listed).  The kept outputs of a slab, sorted by (x, y, z),
+// are one contiguous run of the sorted result.
+//
+// Copies: every slab's input goes up on one stream in slab order; slab s
+// steps as soon as its input (its leaves and its ring) is on the device; its
+// kept outputs go down on another stream while the next slab steps and later
+// input goes up, so the copies in both directions overlap each other and the
+// steps.  At the end the sorted result is loaded back into the pool, so the
+// level set holds the stepped state as after a one-pass host step.
+constexpr int kSlabRing = 16;                   // voxels: two leaves of input beside a slab
+constexpr size_t kSlabLeavesAuto = 1u << 17;    // automatic count: one slab per this many leaves
+constexpr unsigned long long kSlabOther = 0x7fffffffffffffffull;  // key of a leaf the slab does not keep
+
+// Keys of the listed leaves (as k_leaf_keys) for those with x in [xlo, xhi),
+// kSlabOther for the others (sorted after every kept leaf), and the number
+// of kept leaves added to *kept.
+__global__ void k_slab_keys(const int* __restrict__ list, const int* __restrict__ count,
+                            const int4* __restrict__ origin, long long b0, long long b1, long long b2, int bits,
+                            long long xlo, long long xhi, unsigned long long* __restrict__ keys,
+                            unsigned* __restrict__ lo, unsigned* __restrict__ idx, int* __restrict__ kept) {
+    const int n = *count;
+    int c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 o = origin[list[i]];
+        unsigned long long k = kSlabOther;
+        if (o.x >= xlo && o.x < xhi) {
+            k = ((unsigned long long)((o.x >> 3) - b0) << (2 * bits)) |
+                ((unsigned long long)((o.y >> 3) - b1) << bits) | (unsigned long long)((o.z >> 3) - b2);
+            ++c;
+        }
+        keys[i] = k;
+        lo[i] = (unsigned)k;
+        idx[i] = (unsigned)i;
+    }
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(kept, c);
+}
+
+// Origins, masks and f32 values of the first min(*kept, room) sorted list
+// positions sel[i], one CTA per leaf.
+template <typename T>
+__global__ void k_gather_slab(const int* __restrict__ list, const unsigned* __restrict__ sel,
+                              const int* __restrict__ kept, int room, const int4* __restrict__ origin,
+                              const uint64_t* __restrict__ mask, const T* __restrict__ vals, int32_t* __restrict__ o3,
+                              uint64_t* __restrict__ m_out, float* __restrict__ v_out) {
+    const int k = min(*kept, room);
+    for (int i = blockIdx.x; i < k; i += gridDim.x) {
+        const int s = list[sel[i]];
+        if (threadIdx.x < 3) {
+            const int4 o = origin[s];
+            o3[3 * i + threadIdx.x] = threadIdx.x == 0 ? o.x : (threadIdx.x == 1 ? o.y : o.z);
+        }
+        if (threadIdx.x < 8) m_out[(size_t)i * 8 + threadIdx.x] = mask[(size_t)s * 8 + threadIdx.x];
+        for (int t = threadIdx.x; t < kLeafVoxels; t += blockDim.x)
+            v_out[(size_t)i * kLeafVoxels + t] = to_f(vals[(size_t)s * kLeafVoxels + t]);
+    }
+}
+
+__global__ void k_set_step(int* scalars, const int* step) { scalars[1] = *step; }
+
+bool host_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    const bool ok = cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return ok;
+}
+
+// Leaves [n_first, n_first + n) of a device copy of host records (o3, masks,
+// f32 values) as the pool's state, index enqueued; no wait.
+int load_pool(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* o3, const uint64_t* masks, const float* phi, size_t n) {
+    cudaStream_t st = ctx->stream;
+    if (n) {
+        k_unpack_upload<<<ls->grid_blocks, 256, 0, st>>>(o3, (int)n, ls->origin);
+        VLR_CUDA(ctx, cudaMemcpyAsync(ls->mask, masks, 64 * n, cudaMemcpyDeviceToDevice, st));
+        if (ls->precision == VLR_PREC_F16)
+            k_from_f32<__half><<<ls->grid_blocks, 256, 0, st>>>(phi, (__half*)ls->vals[0], kLeafVoxels * n);
+        else
+            VLR_CUDA(ctx, cudaMemcpyAsync(ls->vals[0], phi, sizeof(float) * kLeafVoxels * n, cudaMemcpyDeviceToDevice,
+                                          st));
+    }
+    k_init_lists<<<ls->grid_blocks, 256, 0, st>>>(ls->list, ls->free_stack, ls->scalars, (int)n, ls->cap, 0);
+    VLR_CUDA(ctx, cudaGetLastError());
+    return ls_enqueue_index(ctx, ls);
+}
+
+// The slabs of a host step, or false when the one-pass path serves it (a
+// small or unsorted state, pageable buffers, one slab asked for).
+struct SlabPlan {
+    std::vector<size_t> first;    // owned leaves of slab s: [first[s], first[s + 1])
+    std::vector<long long> x;     // owned x range of slab s: [x[s], x[s + 1])
+    std::vector<size_t> lo, hi;   // stepped input of slab s: [lo[s], hi[s])
+};
+
+bool plan_slabs(const vlr_level_set* ls, const int32_t* origins, size_t n, SlabPlan* p) {
+    int S = ls->host_slabs;
+    if (S == 1 || n < 2 || n > (size_t)ls->cap) return false;
+    if (S == 0) S = (int)std::min<size_t>(kHostSlabsMax, n / kSlabLeavesAuto);
+    S = std::min(S, kHostSlabsMax);
+    if (S < 2) return false;
+    for (size_t i = 0; i < n; ++i) {
+        if ((origins[3 * i] | origins[3 * i + 1] | origins[3 * i + 2]) & 7) return false;  // the one pass reports it
+        if (i && origins[3 * i] < origins[3 * i - 3]) return false;
+    }
+    auto xat = [&](size_t i) { return (long long)origins[3 * i]; };
+    auto lower = [&](long long x) {  // first leaf with x at or above
+        size_t a = 0, b = n;
+        while (a < b) {
+            const size_t m = a + (b - a) / 2;
+            if (xat(m) < x) a = m + 1;
+            else b = m;
+        }
+        return a;
+    };
+    p->first.assign(1, 0);
+    for (int s = 1; s < S; ++s) {
+        const size_t j = lower(xat((size_t)s * n / S));
+        if (j > p->first.back() && j < n) p->first.push_back(j);
+    }
+    p->first.push_back(n);
+    const int ns = (int)p->first.size() - 1;
+    if (ns < 2) return false;
+    p->x.assign(ns + 1, 0);
+    p->x[0] = LLONG_MIN;
+    p->x[ns] = LLONG_MAX;
+    for (int s = 1; s < ns; ++s) p->x[s] = xat(p->first[s]);
+    p->lo.resize(ns);
+    p->hi.resize(ns);
+    for (int s = 0; s < ns; ++s) {
+        p->lo[s] = s == 0 ? 0 : lower(p->x[s] - kSlabRing);
+        p->hi[s] = s == ns - 1 ? n : lower(p->x[s + 1] + kSlabRing);
+    }
+    return true;
+}
+
+// VLR_OK for cudaSuccess, else the error recorded on the context.
+int cuda_rc(vlr_ctx* ctx, cudaError_t e, const char* what) {
+    return e == cudaSuccess ? VLR_OK : check_cuda(ctx, e, what);
+}
+
+int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const int32_t* origins,
+                    const uint64_t* masks, const float* phi, size_t n, int32_t* out_o, uint64_t* out_m,
+                    float* out_v, size_t cap_leaves, size_t* n_out) {
+    cudaStream_t st = ctx->stream;
+    const int ns = (int)P.first.size() - 1;
+    for (cudaStream_t& s : ls->slab_stream)
+        if (!s) VLR_CUDA(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ls->slab_ev)
+        if (!e) VLR_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t up = ls->slab_stream[0], down = ls->slab_stream[1];
+    cudaEvent_t* ev_up = ls->slab_ev;                      // [ns]: slab s's input is on the device
+    cudaEvent_t* ev_out = ls->slab_ev + kHostSlabsMax;     // [ns]: slab s's kept outputs are gathered
+    cudaEvent_t ev_ready = ls->slab_ev[2 * kHostSlabsMax];  // buffers allocated
+    cudaEvent_t ev_down = ls->slab_ev[2 * kHostSlabsMax + 1];
+    const size_t cap_out = std::min(cap_leaves, (size_t)ls->cap);
+    const size_t cmax = (size_t)ls->cap;
+    const size_t rec = sizeof(float) * kLeafVoxels + 64 + 12;
+    const size_t sort_bytes = sort_reduce_scratch_bytes((int)cmax);
+    const size_t bytes = n * rec + cap_out * rec + cmax * (8 + 12) + sort_bytes + 64 * sizeof(int) +
+                         16 * 256;  // each of the 12 pieces below starts on a 256-byte boundary
+    char* buf = nullptr;
+    VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&buf, bytes, ctx->pool, st));
+    char* q = buf;
+    auto take = [&](size_t b) {
+        char* r = q;
+        q += (b + 255) & ~(size_t)255;
+        return r;
+    };
+    float* in_v = (float*)take(n * 4 * kLeafVoxels);
+    uint64_t* in_m = (uint64_t*)take(n * 64);
+    int32_t* in_o = (int32_t*)take(n * 12);
+    float* out_sv = (float*)take(cap_out * 4 * kLeafVoxels);
+    uint64_t* out_sm = (uint64_t*)take(cap_out * 64);
+    int32_t* out_so = (int32_t*)take(cap_out * 12);
+    unsigned long long* keys = (unsigned long long*)take(cmax * 8);
+    unsigned* klo = (unsigned*)take(cmax * 4);
+    unsigned* kidx = (unsigned*)take(cmax * 4);
+    unsigned* khi = (unsigned*)take(cmax * 4);
+    int* d_small = (int*)take(64 * sizeof(int));  // [0, ns) kept per slab, [32] step at entry
+    void* scratch = take(sort_bytes);
+    int* h_count = static_cast<int*>(ctx->pinned) + 64;  // pool count after slab s's step
+    int* h_kept = static_cast<int*>(ctx->pinned) + 96;   // outputs slab s keeps
+    unsigned* h_err = static_cast<unsigned*>(ctx->pinned) + 128;
+
+    int rc = VLR_OK;
+    auto finish = [&](int code) {
+        // nothing may still read or write the buffers when they go back to the pool
+        cudaEventRecord(ev_down, down);
+        cudaStreamWaitEvent(st, ev_down, 0);
+        cudaEventRecord(ev_down, up);
+        cudaStreamWaitEvent(st, ev_down, 0);
+        cudaFreeAsync(buf, st);
+        if (code) {
+            cudaStreamSynchronize(st);
+            ls->state_lost = true;
+        }
+        return code;
+    };
+    VLR_CUDA(ctx, cudaMemsetAsync(d_small, 0, 64 * sizeof(int), st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(d_small + 32, ls->scalars + 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    VLR_CUDA(ctx, cudaEventRecord(ev_ready, st));
+    VLR_CUDA(ctx, cudaStreamWaitEvent(up, ev_ready, 0));
+    VLR_CUDA(ctx, cudaStreamWaitEvent(down, ev_ready, 0));
+    // every slab's input, in slab order
+    size_t done = 0;
+    for (int s = 0; s < ns; ++s) {
+        const size_t a = done, b = P.hi[s];
+        if (b > a) {
+            const size_t k = b - a;
+            if ((rc = cuda_rc(ctx, cudaMemcpyAsync(in_o + 3 * a, origins + 3 * a, 12 * k, cudaMemcpyHostToDevice,
+                                                      up), "slab input copy")) ||
+                (rc = cuda_rc(ctx, cudaMemcpyAsync(in_m + 8 * a, masks + 8 * a, 64 * k, cudaMemcpyHostToDevice,
+                                                      up), "slab input copy")) ||
+                (rc = cuda_rc(ctx, cudaMemcpyAsync(in_v + kLeafVoxels * a, phi + kLeafVoxels * a,
+                                                      sizeof(float) * kLeafVoxels * k, cudaMemcpyHostToDevice, up),
+                                 "slab input copy")))
+                return finish(rc);
+            done = b;
+        }
+        if ((rc = cuda_rc(ctx, cudaEventRecord(ev_up[s], up), "cudaEventRecord"))) return finish(rc);
+    }
+    const vlr::MGridParams& G = ls->h_params[0];
+    const int B = ctx->sm_count * 8;
+    size_t off = 0;  // kept outputs of the slabs before
+    std::vector<size_t> offs(ns, 0);
+    auto copy_down = [&](int s) -> int {
+        const size_t k = (size_t)h_kept[s], o = offs[s];
+        if (o + k > cap_out) return set_error(ctx, VLR_ERR_CAPACITY, "output buffers too small");
+        if (!k) return VLR_OK;
+        VLR_CUDA(ctx, cudaStreamWaitEvent(down, ev_out[s], 0));
+        VLR_CUDA(ctx, cudaMemcpyAsync(out_o + 3 * o, out_so + 3 * o, 12 * k, cudaMemcpyDeviceToHost, down));
+        VLR_CUDA(ctx, cudaMemcpyAsync(out_m + 8 * o, out_sm + 8 * o, 64 * k, cudaMemcpyDeviceToHost, down));
+        VLR_CUDA(ctx, cudaMemcpyAsync(out_v + kLeafVoxels * o, out_sv + kLeafVoxels * o,
+                                      sizeof(float) * kLeafVoxels * k, cudaMemcpyDeviceToHost, down));
+        return VLR_OK;
+    };
+    for (int s = 0; s < ns; ++s) {
+        // slab s: its input as the pool's state, the step counter and the scan
+        // status words as at entry, one step, its pool count to the host
+        const size_t a = P.lo[s], m = P.hi[s] - P.lo[s];
+        if ((rc = cuda_rc(ctx, cudaStreamWaitEvent(st, ev_up[s], 0), "cudaStreamWaitEvent")) ||
+            (rc = load_pool(ctx, ls, in_o + 3 * a, in_m + 8 * a, in_v + kLeafVoxels * a, m)))
+            return finish(rc);
+        k_set_step<<<1, 1, 0, st>>>(ls->scalars, d_small + 32);
+        if ((rc = cuda_rc(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (ls->cap + 1 + scan_scratch_ints(ls->cap)),
+                                                  st), "cudaMemsetAsync")) ||
+            (rc = enqueue_one_step(ctx, ls)) ||
+            (rc = cuda_rc(ctx, cudaMemcpyAsync(h_count + s, ls->scalars, sizeof(int), cudaMemcpyDeviceToHost, st),
+                             "count read-back")) ||
+            (rc = cuda_rc(ctx, cudaMemcpyAsync(h_err, ctx->d_errword, sizeof(unsigned), cudaMemcpyDeviceToHost, st),
+                             "error read-back")))
+            return finish(rc);
+        // the previous slab's kept outputs go down while this slab steps
+        if (s > 0) {
+            if ((rc = cuda_rc(ctx, cudaEventSynchronize(ev_out[s - 1]), "cudaEventSynchronize"))) return finish(rc);
+            off += (size_t)h_kept[s - 1];
+            if ((rc = copy_down(s - 1))) return finish(rc);
+        }
+        if ((rc = cuda_rc(ctx, cudaStreamSynchronize(st), "cudaStreamSynchronize"))) return finish(rc);
+        const int c = h_count[s];
+        if (*h_err || c < 0 || c > ls->cap) {
+            rc = consume_device_errors(ctx, "vlr_ls_step_host");
+            return finish(rc ? rc : set_error(ctx, VLR_ERR_CUDA, "slab step left an inconsistent leaf count"));
+        }
+        // its kept outputs, sorted by (x, y, z), gathered after those of the slabs before
+        offs[s] = off;
+        if (c) {
+            k_slab_keys<<<B, 256, 0, st>>>(ls->list, ls->scalars, ls->origin, G.base[0], G.base[1], G.base[2],
+                                           ls->key_bits, P.x[s], P.x[s + 1], keys, klo, kidx, d_small + s);
+            unsigned *k1, *v1, *k2, *v2;
+            if ((rc = radix_sort_pairs(ctx, klo, kidx, c, 0xffffffffu, scratch, &k1, &v1))) return finish(rc);
+            k_leaf_keys_hi<<<B, 256, 0, st>>>(keys, v1, c, khi);
+            if (v1 != kidx &&
+                (rc = cuda_rc(ctx, cudaMemcpyAsync(kidx, v1, (size_t)c * 4, cudaMemcpyDeviceToDevice, st),
+                                 "cudaMemcpyAsync")))
+                return finish(rc);
+            if ((rc = radix_sort_pairs(ctx, khi, kidx, c, 0x7fffffffu, scratch, &k2, &v2))) return finish(rc);
+            (void)k1;
+            (void)k2;
+            const size_t o = std::min(off, cap_out);
+            const int room = (int)(cap_out - o);
+            if (ls->precision == VLR_PREC_F16)
+                k_gather_slab<__half><<<B, 256, 0, st>>>(ls->list, v2, d_small + s, room, ls->origin, ls->mask,
+                                                         (const __half*)ls->vals[0], out_so + 3 * o, out_sm + 8 * o,
+                                                         out_sv + kLeafVoxels * o);
+            else
+                k_gather_slab<float><<<B, 256, 0, st>>>(ls->list, v2, d_small + s, room, ls->origin, ls->mask,
+                                                        (const float*)ls->vals[0], out_so + 3 * o, out_sm + 8 * o,
+                                                        out_sv + kLeafVoxels * o);
+            if ((rc = cuda_rc(ctx, cudaGetLastError(), "slab gather"))) return finish(rc);
+        }
+        if ((rc = cuda_rc(ctx, cudaMemcpyAsync(h_kept + s, d_small + s, sizeof(int), cudaMemcpyDeviceToHost, st),
+                             "kept read-back")) ||
+            (rc = cuda_rc(ctx, cudaEventRecord(ev_out[s], st), "cudaEventRecord")))
+            return finish(rc);
+    }
+    if ((rc = cuda_rc(ctx, cudaEventSynchronize(ev_out[ns - 1]), "cudaEventSynchronize")) ||
+        (rc = copy_down(ns - 1)))
+        return finish(rc);
+    const size_t total = offs[ns - 1] + (size_t)h_kept[ns - 1];
+    // the stepped state back into the pool (its step counter is already one
+    // past the entry value), while the last outputs go down
+    if ((rc = load_pool(ctx, ls, out_so, out_sm, out_sv, total))) return finish(rc);
+    rc = finish(VLR_OK);
+    if (rc) return rc;
+    rc = consume_device_errors(ctx, "vlr_ls_step_host");
+    if (rc) {
+        ls->state_lost = true;
+        return rc;
+    }
+    *n_out = total;
+    return VLR_OK;
+}
+
+
 }  // namespace
 
 extern "C" {
@@ -911,6 +1247,13 @@ int vlr_ls_step_host(vlr_ctx* ctx, vlr_level_set* ls, const int32_t* origins, co
     if (!ctx || !ls || !origins || !masks || !phi || !n_out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
     if (ls->n_grids != 1) return set_error(ctx, VLR_ERR_UNSUPPORTED, "host steps replace single-grid states only");
     *n_out = 0;
+    // large x-sorted states in pinned buffers: one step as a pipeline over x-slabs
+    SlabPlan plan;
+    if (n_steps == 1 && 3 * ls->key_bits <= 63 && out_origins && out_masks && out_phi && host_pinned(origins) &&
+        host_pinned(masks) && host_pinned(phi) && host_pinned(out_origins) && host_pinned(out_masks) &&
+        host_pinned(out_phi) && plan_slabs(ls, origins, n_leaves, &plan))
+        return step_host_slabs(ctx, ls, plan, origins, masks, phi, n_leaves, out_origins, out_masks, out_phi,
+                               cap_leaves, n_out);
     // staging for the device-sorted download (sized first, so the upload
     // never regrows it while its copies are in flight)
     const size_t kv = (size_t)kDevSortLeaves;
@@ -1076,6 +1419,13 @@ int vlr_ls_set_step(vlr_ctx* ctx, vlr_level_set* ls, int step) {
     VLR_CUDA(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (ls->cap + 1 + scan_scratch_ints(ls->cap)), ctx->stream));
     VLR_CUDA(ctx, cudaMemcpyAsync(ls->scalars + 1, &step, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     VLR_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLR_OK;
+}
+
+int vlr_ls_set_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, int slabs) {
+    if (!ctx || !ls) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    if (slabs < 0) return set_error(ctx, VLR_ERR_INVALID, "slabs must be >= 0");
+    ls->host_slabs = std::min(slabs, kHostSlabsMax);
     return VLR_OK;
 }
 

@@ -15,6 +15,9 @@ struct StencilShape {
     int stage = 0;    // staging of the halo tile: 0, row pieces by cp.async (the only mode)
 };
 
+// Most slabs a host step is cut into (vlr_ls_set_host_slabs).
+constexpr int kHostSlabsMax = 16;
+
 // One timed candidate of the launch autotuner.
 struct TuneEntry {
     StencilShape shape;
@@ -73,6 +76,11 @@ struct vlr_level_set {
     bool tuned = false;      // shapes chosen (by the autotuner or the caller)
     bool state_lost = false; // a step failed with VLR_ERR_TIMEOUT or VLR_ERR_CAPACITY: the state is undefined
     bool autotune = true;    // choose the shapes on the first step
+    // host steps over x-slabs (vlr_ls_step_host): 0 automatic, 1 one pass,
+    // k >= 2 at most k slabs; the copy streams and events, made on first use
+    int host_slabs = 0;
+    cudaStream_t slab_stream[2] = {nullptr, nullptr};  // host -> device, device -> host
+    cudaEvent_t slab_ev[2 * kHostSlabsMax + 2] = {};
     std::vector<TuneEntry> tune_log[2];  // candidates timed by the autotuner (advect, reinit)
     int scan_levels = 0;
 

@@ -359,6 +359,14 @@ class LevelSet:
                        "vlr_ls_volume_partials")
         return k.value
 
+    def set_host_slabs(self, slabs: int):
+        """Slab count of the next host steps (``step_host``): 0 automatic, 1
+        always one pass, k >= 2 at most k slabs of consecutive x, whose copies
+        to and from the host overlap the other slabs' steps (one step of an
+        x-sorted state in pinned buffers only; the result is the one pass's)."""
+        self.ctx.check(self.ctx.lib.vlr_ls_set_host_slabs(self.ctx.handle, self.handle, int(slabs)),
+                       "vlr_ls_set_host_slabs")
+
     def set_step(self, step: int):
         """Set the step counter (time = t0 + step * dt): resume a run in a new level set."""
         self.ctx.check(self.ctx.lib.vlr_ls_set_step(self.ctx.handle, self.handle, int(step)), "vlr_ls_set_step")
