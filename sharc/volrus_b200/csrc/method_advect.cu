@@ -305,6 +305,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_advect(MLeafArrays A, const T* __r
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         topo.scalars[4] = 0;  // new count (set by the last scan chunk)
+        topo.scalars[5] = 0;  // dropped count (read by the last step's k_t_nbr)
         topo.scalars[7] = 0;  // scan chunk ticket
     }
     using G = Geo<H>;

@@ -14,7 +14,9 @@
 //                  of dropped leaves go to a recycle list
 //   k_t_finalize   new list, fill of new leaves (clamped-sign rule from the
 //                  owner), hash insertion, recycled slots back on the stack
-//   k_t_nbr        27-neighbour table of every listed leaf; publishes counts
+//   k_t_nbr        27-neighbour rows updated where a neighbour was dropped or
+//                  is new (the rows of an upload are built whole by k_nbr);
+//                  publishes counts
 //
 // The reference's counterparts are dilate (src/tools/morphology.rs:20-35),
 // trim_narrow_band's deactivation (src/tools/level_set_track.rs:53-68) and
@@ -200,8 +202,10 @@ __global__ void __launch_bounds__(kChunk) k_t_scanalloc(MLeafArrays A, int4* ori
     }
 }
 
-// One warp per new-list position (grid-stride): copy the list, insert the
-// hash key, fill new leaves from their owner; thread 0 recycles dropped slots.
+// One thread per new-list position, a block's 256 positions at a time: copy
+// the list and insert the leaf's hash key; the block's new leaves, queued in
+// shared memory, are then filled from their owners one warp each (coalesced
+// stores).  The dropped slots go back on the free stack.
 template <typename T>
 __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const int* newinfo, int* list, const int4* origin,
                                                    T* vals, uint64_t* hkey, int* hval, int hcap,
@@ -210,23 +214,27 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
     dep_wait();
     dep_launch();
     if (step_aborted(err)) return;
+    __shared__ int s_q[256];
+    __shared__ int s_nq;
     const int n = min(scalars[4], cap);
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int p = warp; p < n; p += nwarps) {
-        const int s = list_new[p];
-        const int info = newinfo[p];
-        if (lane == 0) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_nq = 0;
+    __syncthreads();
+    for (int base = blockIdx.x * 256; base < n; base += gridDim.x * 256) {
+        const int p = base + threadIdx.x;
+        if (p < n) {
+            const int s = list_new[p];
+            const int info = newinfo[p];
             list[p] = s;
             if (info != -2) {
-                uint64_t key = leaf_key(origin[s], 0, 0, 0, params, bits);
+                const uint64_t key = leaf_key(origin[s], 0, 0, 0, params, bits);
                 bool done = false;
                 if (key != kEmptyKey) {
                     uint32_t m = (uint32_t)hcap - 1u, q = (uint32_t)mix64(key) & m;
                     for (int probe = 0; probe < hcap; ++probe) {
-                        unsigned long long prev = atomicCAS((unsigned long long*)&hkey[q],
-                                                            (unsigned long long)kEmptyKey, (unsigned long long)key);
+                        const unsigned long long prev = atomicCAS((unsigned long long*)&hkey[q],
+                                                                  (unsigned long long)kEmptyKey,
+                                                                  (unsigned long long)key);
                         if (prev == kEmptyKey) {
                             hval[q] = s;
                             done = true;
@@ -237,19 +245,27 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
                 }
                 if (!done) atomicOr(err, key == kEmptyKey ? kErrExtent : kErrHashFull);
             }
+            if (info >= 0) s_q[atomicAdd(&s_nq, 1)] = p;
         }
-        if (info >= 0) {
+        __syncthreads();
+        const int nq = s_nq;
+        for (int j = warp; j < nq; j += 256 / 32) {
+            const int q = s_q[j];
+            const int s = list_new[q], info = newinfo[q];
             const int owner = info >> 5, d = info & 31;
             int dx, dy, dz;
             dir_of(d, dx, dy, dz);
             const float hw = params[origin[owner].w].hw;
             for (int off = lane; off < kLeafVoxels; off += 32) {
-                int x = 8 * dx + (off >> 6), y = 8 * dy + ((off >> 3) & 7), z = 8 * dz + (off & 7);
-                int cx = min(max(x, 0), 7), cy = min(max(y, 0), 7), cz = min(max(z, 0), 7);
-                float v = to_f(vals[(size_t)owner * kLeafVoxels + ((cx << 6) | (cy << 3) | cz)]);
+                const int x = 8 * dx + (off >> 6), y = 8 * dy + ((off >> 3) & 7), z = 8 * dz + (off & 7);
+                const int cx = min(max(x, 0), 7), cy = min(max(y, 0), 7), cz = min(max(z, 0), 7);
+                const float v = to_f(vals[(size_t)owner * kLeafVoxels + ((cx << 6) | (cy << 3) | cz)]);
                 vals[(size_t)s * kLeafVoxels + off] = from_f<T>(copysignf(hw, v));
             }
         }
+        __syncthreads();
+        if (threadIdx.x == 0) s_nq = 0;
+        __syncthreads();
     }
     // dropped slots go back on the free stack above the remaining free slots
     const int top = max(scalars[2], 0);
@@ -259,26 +275,57 @@ __global__ void __launch_bounds__(256) k_t_finalize(const int* list_new, const i
     if (blockIdx.x == 0 && threadIdx.x == 0) scalars[6] = min(top + nrec, cap);
 }
 
-__global__ void k_t_nbr(const int* list, int* scalars, const int4* origin, const uint64_t* hkey, const int* hval,
-                        int hcap, const MGridParams* __restrict__ params, int bits, int* nbr, int cap,
-                        const unsigned* err) {
+// Neighbour rows carried from step to step.  A survivor keeps its slot and
+// its position, so its row changes only at a neighbour that was dropped or is
+// new (a dropped leaf's slot returns to the free stack after this step's new
+// leaves took theirs, so no slot is both).  One warp per dropped leaf: its
+// old row names its listed neighbours, and those that survive clear the
+// entry that points back at it.  One warp per new leaf (found by a ballot
+// over 32 list positions): lane d looks neighbour d up in the hash rebuilt
+// by k_t_finalize, writes the new leaf's row and, for a present neighbour,
+// the entry that points back at the new leaf (two adjacent new leaves write
+// each other's entries with the same values).  Publishes the counts; the
+// dropped count is cleared by the next step's advect.
+__global__ void k_t_nbr(const int* list, const int* newinfo, const int* recycled, const int* keep, int* scalars,
+                        const int4* origin, const uint64_t* hkey, const int* hval, int hcap,
+                        const MGridParams* __restrict__ params, int bits, int* nbr, int cap, const unsigned* err) {
     dep_wait();
     dep_launch();
     if (step_aborted(err)) return;
     const int count = min(scalars[4], cap);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)count * kNbr;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / kNbr), d = (int)(t % kNbr);
-        const int s = list[i];
-        int dx, dy, dz;
-        dir_of(d, dx, dy, dz);
-        nbr[(size_t)s * kNbr + d] = (d == 13) ? s : hfind(hkey, hval, hcap, leaf_key(origin[s], dx, dy, dz, params, bits));
+    const int nrec = min(scalars[5], cap);
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = gw; i < nrec; i += nw) {
+        const int D = recycled[i];
+        if (lane < kNbr && lane != 13) {
+            const int M = nbr[(size_t)D * kNbr + lane];
+            if (M >= 0 && keep[M]) nbr[(size_t)M * kNbr + (kNbr - 1 - lane)] = -1;
+        }
+    }
+    for (int base = gw * 32; base < count; base += nw * 32) {
+        const int p = base + lane;
+        unsigned b = __ballot_sync(0xffffffffu, p < count && newinfo[p] >= 0);
+        while (b) {
+            const int j = __ffs(b) - 1;
+            b &= b - 1u;
+            const int N = list[base + j];
+            if (lane < kNbr) {
+                int M = N;
+                if (lane != 13) {
+                    int dx, dy, dz;
+                    dir_of(lane, dx, dy, dz);
+                    M = hfind(hkey, hval, hcap, leaf_key(origin[N], dx, dy, dz, params, bits));
+                }
+                nbr[(size_t)N * kNbr + lane] = M;
+                if (M >= 0 && M != N) nbr[(size_t)M * kNbr + (kNbr - 1 - lane)] = N;
+            }
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         scalars[0] = count;
         scalars[1] += 1;
         scalars[2] = scalars[6];
-        scalars[5] = 0;
     }
 }
 
@@ -410,7 +457,8 @@ int ls_enqueue_retrack(vlr_ctx* ctx, vlr_level_set* ls) {
                                            (const MGridParams*)ls->d_params, ls->key_bits, ls->free_stack,
                                            (const int*)ls->owned, ls->scalars, ls->cap, ctx->d_errword)));
     VLR_TIMED(ctx, "k_t_nbr",
-              VLR_CUDA(ctx, pdl_launch(k_t_nbr, B, 256, 0, st, (const int*)ls->list, ls->scalars,
+              VLR_CUDA(ctx, pdl_launch(k_t_nbr, B, 256, 0, st, (const int*)ls->list, (const int*)ls->newinfo,
+                                       (const int*)ls->owned, (const int*)ls->keep, ls->scalars,
                                        (const int4*)ls->origin, (const uint64_t*)ls->hkey, (const int*)ls->hval,
                                        ls->hcap, (const MGridParams*)ls->d_params, ls->key_bits, ls->nbr, ls->cap,
                                        (const unsigned*)ctx->d_errword)));
