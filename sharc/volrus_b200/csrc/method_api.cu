@@ -939,7 +939,7 @@ int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const in
     const size_t cmax = (size_t)ls->cap;
     const size_t rec = sizeof(float) * kLeafVoxels + 64 + 12;
     const size_t sort_bytes = sort_reduce_scratch_bytes((int)cmax);
-    const size_t bytes = n * rec + cap_out * rec + cmax * (8 + 12) + sort_bytes + 64 * sizeof(int) +
+    const size_t bytes = n * rec + cap_out * rec + cmax * (8 + 12) + sort_bytes + 2 * kHostSlabsMax * sizeof(int) +
                          16 * 256;  // each of the 12 pieces below starts on a 256-byte boundary
     char* buf = nullptr;
     VLR_CUDA(ctx, cudaMallocFromPoolAsync((void**)&buf, bytes, ctx->pool, st));
@@ -959,11 +959,12 @@ int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const in
     unsigned* klo = (unsigned*)take(cmax * 4);
     unsigned* kidx = (unsigned*)take(cmax * 4);
     unsigned* khi = (unsigned*)take(cmax * 4);
-    int* d_small = (int*)take(64 * sizeof(int));  // [0, ns) kept per slab, [32] step at entry
+    // [0, ns) kept per slab, [kHostSlabsMax] step at entry
+    int* d_small = (int*)take(2 * kHostSlabsMax * sizeof(int));
     void* scratch = take(sort_bytes);
-    int* h_count = static_cast<int*>(ctx->pinned) + 64;  // pool count after slab s's step
-    int* h_kept = static_cast<int*>(ctx->pinned) + 96;   // outputs slab s keeps
-    unsigned* h_err = static_cast<unsigned*>(ctx->pinned) + 128;
+    int* h_count = static_cast<int*>(ctx->pinned) + 64;                  // pool count after slab s's step
+    int* h_kept = static_cast<int*>(ctx->pinned) + 64 + kHostSlabsMax;   // outputs slab s keeps
+    unsigned* h_err = static_cast<unsigned*>(ctx->pinned) + 64 + 2 * kHostSlabsMax;
 
     int rc = VLR_OK;
     auto finish = [&](int code) {
@@ -979,8 +980,8 @@ int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const in
         }
         return code;
     };
-    VLR_CUDA(ctx, cudaMemsetAsync(d_small, 0, 64 * sizeof(int), st));
-    VLR_CUDA(ctx, cudaMemcpyAsync(d_small + 32, ls->scalars + 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    VLR_CUDA(ctx, cudaMemsetAsync(d_small, 0, 2 * kHostSlabsMax * sizeof(int), st));
+    VLR_CUDA(ctx, cudaMemcpyAsync(d_small + kHostSlabsMax, ls->scalars + 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
     VLR_CUDA(ctx, cudaEventRecord(ev_ready, st));
     VLR_CUDA(ctx, cudaStreamWaitEvent(up, ev_ready, 0));
     VLR_CUDA(ctx, cudaStreamWaitEvent(down, ev_ready, 0));
@@ -1024,7 +1025,7 @@ int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const in
         if ((rc = cuda_rc(ctx, cudaStreamWaitEvent(st, ev_up[s], 0), "cudaStreamWaitEvent")) ||
             (rc = load_pool(ctx, ls, in_o + 3 * a, in_m + 8 * a, in_v + kLeafVoxels * a, m)))
             return finish(rc);
-        k_set_step<<<1, 1, 0, st>>>(ls->scalars, d_small + 32);
+        k_set_step<<<1, 1, 0, st>>>(ls->scalars, d_small + kHostSlabsMax);
         if ((rc = cuda_rc(ctx, cudaMemsetAsync(ls->pos, 0, sizeof(int) * (ls->cap + 1 + scan_scratch_ints(ls->cap)),
                                                   st), "cudaMemsetAsync")) ||
             (rc = enqueue_one_step(ctx, ls)) ||
