@@ -980,11 +980,13 @@ int step_host_slabs(vlr_ctx* ctx, vlr_level_set* ls, const SlabPlan& P, const in
         }
         return code;
     };
-    VLR_CUDA(ctx, cudaMemsetAsync(d_small, 0, 2 * kHostSlabsMax * sizeof(int), st));
-    VLR_CUDA(ctx, cudaMemcpyAsync(d_small + kHostSlabsMax, ls->scalars + 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
-    VLR_CUDA(ctx, cudaEventRecord(ev_ready, st));
-    VLR_CUDA(ctx, cudaStreamWaitEvent(up, ev_ready, 0));
-    VLR_CUDA(ctx, cudaStreamWaitEvent(down, ev_ready, 0));
+    if ((rc = cuda_rc(ctx, cudaMemsetAsync(d_small, 0, 2 * kHostSlabsMax * sizeof(int), st), "cudaMemsetAsync")) ||
+        (rc = cuda_rc(ctx, cudaMemcpyAsync(d_small + kHostSlabsMax, ls->scalars + 1, sizeof(int),
+                                           cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync")) ||
+        (rc = cuda_rc(ctx, cudaEventRecord(ev_ready, st), "cudaEventRecord")) ||
+        (rc = cuda_rc(ctx, cudaStreamWaitEvent(up, ev_ready, 0), "cudaStreamWaitEvent")) ||
+        (rc = cuda_rc(ctx, cudaStreamWaitEvent(down, ev_ready, 0), "cudaStreamWaitEvent")))
+        return finish(rc);
     // every slab's input, in slab order
     size_t done = 0;
     for (int s = 0; s < ns; ++s) {
