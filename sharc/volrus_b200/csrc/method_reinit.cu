@@ -30,9 +30,11 @@
 //              results, activity bits into a shared mask.
 //   phase 4    mask out, spill toward absent neighbours, keep flags and
 //              proposals (hash of the missing leaf, atomicMin of the
-//              proposer's direction).
+//              proposer's direction), by warp 3 during the next leaf's
+//              phase 1 (its mask words, neighbour row, slot and origin kept
+//              in shared memory), after the loop for the CTA's last leaf.
 //
-// Four CTA barriers per leaf (three without iteration 1).  Neighbour rows
+// Three CTA barriers per leaf (two without iteration 1).  Neighbour rows
 // are loaded one leaf before the iteration that stores them, so no global
 // load waits in front of a barrier.  Every leaf is computed by one CTA with
 // the same arithmetic whatever the grid size; side effects on shared
@@ -281,6 +283,69 @@ __device__ __forceinline__ void write_outside(const T* stage, T* __restrict__ ou
     }
 }
 
+// Phase 4 of a leaf, by one warp: its mask words to global memory, the
+// spill toward absent neighbours, keep flags and re-tracking proposals.
+// sM: the leaf's 16 mask words in shared memory; nb: the leaf's neighbour
+// slot for the lane's direction (-1 absent).
+__device__ __forceinline__ void spill_and_propose(const unsigned* sM, int slot, int4 o, int nb, int lane,
+                                                  const MLeafArrays& A, const MTopo& topo,
+                                                  const MGridParams* __restrict__ params, unsigned* err) {
+    if (lane < 16) reinterpret_cast<unsigned*>(A.mask + (size_t)slot * 8)[lane] = sM[lane];
+    // spill mask from 64-bit (x*8+y) plane masks of z = 0, z = 7 and any z
+    const unsigned char* B = (const unsigned char*)sM;
+    const unsigned b0 = B[lane], b1 = B[lane + 32];
+    const uint64_t z0 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 1u) |
+                        ((uint64_t)__ballot_sync(0xffffffffu, b1 & 1u) << 32);
+    const uint64_t z7 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 0x80u) |
+                        ((uint64_t)__ballot_sync(0xffffffffu, b1 & 0x80u) << 32);
+    const uint64_t za = (uint64_t)__ballot_sync(0xffffffffu, b0 != 0u) |
+                        ((uint64_t)__ballot_sync(0xffffffffu, b1 != 0u) << 32);
+    bool spl = false;
+    if (lane < kNbr && lane != 13) {
+        const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+        const uint64_t plane = dz < 0 ? z0 : (dz > 0 ? z7 : za);
+        const uint64_t xs = dx < 0 ? 0xFFull : (dx > 0 ? (0xFFull << 56) : ~0ull);
+        const uint64_t ys = dy < 0 ? 0x0101010101010101ull : (dy > 0 ? 0x8080808080808080ull : ~0ull);
+        spl = (plane & xs & ys) != 0ull;
+    }
+    // spill toward absent neighbours only: those are the proposals the
+    // allocation scan resolves (present ones are kept right here)
+    const unsigned sbits = __ballot_sync(0xffffffffu, spl && nb < 0);
+    if (lane == 0) {
+        A.spill[slot] = sbits;
+        A.nonempty[slot] = (za != 0ull) ? 1 : 0;
+        if (za != 0ull) topo.keep[slot] = 1;
+    }
+    // re-tracking proposals: an existing neighbour touched by the spill
+    // survives; a missing one is proposed, keeping the proposer whose
+    // direction seen from the new leaf comes first (atomicMin).
+    if (spl) {
+        if (nb >= 0) {
+            topo.keep[nb] = 1;
+        } else {
+            const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+            const MGridParams& P = params[o.w];
+            const uint64_t key = mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy,
+                                      (long long)(o.z >> 3) + dz, o.w, P.base, topo.key_bits);
+            bool done = false;
+            if (key != kEmptyKey) {
+                uint32_t m = (uint32_t)topo.hcap - 1u, pp = (uint32_t)mix64(key) & m;
+                for (int probe = 0; probe < topo.hcap; ++probe) {
+                    const unsigned long long prev = atomicCAS((unsigned long long*)&topo.pkey[pp],
+                                                              (unsigned long long)kEmptyKey, (unsigned long long)key);
+                    if (prev == kEmptyKey || prev == key) {
+                        atomicMin(&topo.pval[pp], kNbr - 1 - lane);
+                        done = true;
+                        break;
+                    }
+                    pp = (pp + 1u) & m;
+                }
+            }
+            if (!done) atomicOr(err, key == kEmptyKey ? kErrExtent : kErrHashFull);
+        }
+    }
+}
+
 }  // namespace
 
 template <typename T, int NIT, int FIX>
@@ -310,11 +375,13 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     auto masks_of = [&](int b) { return reinterpret_cast<uint64_t*>(mk0 + b * Lay::masks); };
     __shared__ unsigned short s_list1[NIT == 2 ? kBox : 1];
     __shared__ unsigned short s_list2[kLeafVoxels];
-    __shared__ int s_nbr[2][32];
+    __shared__ int s_nbr[3][32];   // neighbour rows of the previous, current and next leaf
     __shared__ int s_n1, s_n2;
     __shared__ unsigned s_bx[32];  // the box voxels of D, one bit per flat index
     __shared__ short s_roff[kF * kF];  // stage offset of box row (bx, by) at bz = 0
-    __shared__ __align__(16) unsigned s_M[16];
+    __shared__ __align__(16) unsigned s_M2[2][16];  // new mask words (this leaf, the previous one)
+    __shared__ int s_pslot[2];
+    __shared__ int4 s_po[2];
 
     const int count = *A.count;
     const int Gs = gridDim.x;
@@ -337,21 +404,19 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
     int slot_nn = (li + 2 * Gs < count) ? A.list[li + 2 * Gs] : -1;
     float hw = params[o.w].hw;
 
-    for (unsigned it = 0;; ++it) {
+    unsigned it = 0;
+    for (;; ++it) {
         const int b = it & 1;
+        const int nx = (int)((it + 1u) % 3u), pv = (int)((it + 2u) % 3u);  // next and previous rows
         int4 o_n = make_int4(0, 0, 0, -1);
         if (slot_n >= 0) o_n = A.origin[slot_n];
         const int slot_nnn = (li + 3 * Gs < count) ? A.list[li + 3 * Gs] : -1;
         const int nb_after = (warp == 0 && lane < kNbr && slot_nn >= 0) ? A.nbr[(size_t)slot_nn * kNbr + lane] : -1;
-        if (warp == 0) s_nbr[b ^ 1][lane] = nb_next;
+        if (warp == 0) s_nbr[nx][lane] = nb_next;
         cp_async_wait_all();
         __syncthreads();  // barrier A: this leaf's stage is complete; the previous leaf is done
         const T* stage = stage_of(b);
         const uint64_t* s_m = masks_of(b);
-        // this leaf's neighbour slot for the lane's direction, read into a
-        // register here: the next iteration's neighbour row lands in this
-        // buffer before its barrier A, while warp 1 may still be proposing
-        const int my_nb = lane < kNbr ? s_nbr[b][lane] : -1;
         T* out = dst + (size_t)slot * kLeafVoxels;
         // the leaf's voxels of D for the last iteration (offset x * 64 + y * 8 + z)
         auto leaf_list = [&]() {
@@ -390,9 +455,20 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
             if (NIT == 2 && warp == 1) leaf_list();
             const int t = threadIdx.x - 32;
             if (slot_n >= 0)
-                issue_stage<T>(s_nbr[b ^ 1], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
+                issue_stage<T>(s_nbr[nx], src, A.dmask, stage_of(b ^ 1), masks_of(b ^ 1), t, kNT - 32);
             write_outside<T>(stage, out, hw, t);
-            if (t < 16) s_M[t] = 0u;
+            if (t < 16) s_M2[b][t] = 0u;
+            if (warp == kNW - 1) {
+                // phase 4 of the previous leaf, whose mask words are complete
+                // since barrier A; this warp has the least phase-1 work
+                if (lane == 0) {
+                    s_pslot[b] = slot;
+                    s_po[b] = o;
+                }
+                if (it > 0)
+                    spill_and_propose(s_M2[b ^ 1], s_pslot[b ^ 1], s_po[b ^ 1], s_nbr[pv][lane], lane, A, topo, params,
+                                      err);
+            }
         }
         __syncthreads();  // barrier B: lists and outside-D results are in place
         if (NIT == 2) {
@@ -454,66 +530,7 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
                 const bool on = fabsf(v) < hw;
                 if (!on) v = copysignf(hw, v);
                 out[off] = from_f<T>(v);
-                if (on) atomicOr(&s_M[off >> 5], 1u << (off & 31));
-            }
-        }
-        __syncthreads();  // barrier D: the new mask words are in shared memory
-        if (threadIdx.x < 16) reinterpret_cast<unsigned*>(A.mask + (size_t)slot * 8)[threadIdx.x] = s_M[threadIdx.x];
-        if (warp == 1) {
-            // spill mask from 64-bit (x*8+y) plane masks of z = 0, z = 7 and any z
-            const unsigned char* B = (const unsigned char*)s_M;
-            const unsigned b0 = B[lane], b1 = B[lane + 32];
-            const uint64_t z0 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 1u) |
-                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 1u) << 32);
-            const uint64_t z7 = (uint64_t)__ballot_sync(0xffffffffu, b0 & 0x80u) |
-                                ((uint64_t)__ballot_sync(0xffffffffu, b1 & 0x80u) << 32);
-            const uint64_t za = (uint64_t)__ballot_sync(0xffffffffu, b0 != 0u) |
-                                ((uint64_t)__ballot_sync(0xffffffffu, b1 != 0u) << 32);
-            bool spl = false;
-            if (lane < kNbr && lane != 13) {
-                const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-                const uint64_t plane = dz < 0 ? z0 : (dz > 0 ? z7 : za);
-                const uint64_t xs = dx < 0 ? 0xFFull : (dx > 0 ? (0xFFull << 56) : ~0ull);
-                const uint64_t ys = dy < 0 ? 0x0101010101010101ull : (dy > 0 ? 0x8080808080808080ull : ~0ull);
-                spl = (plane & xs & ys) != 0ull;
-            }
-            // spill toward absent neighbours only: those are the proposals the
-            // allocation scan resolves (present ones are kept right here)
-            const unsigned sbits = __ballot_sync(0xffffffffu, spl && my_nb < 0);
-            if (lane == 0) {
-                A.spill[slot] = sbits;
-                A.nonempty[slot] = (za != 0ull) ? 1 : 0;
-                if (za != 0ull) topo.keep[slot] = 1;
-            }
-            // re-tracking proposals: an existing neighbour touched by the spill
-            // survives; a missing one is proposed, keeping the proposer whose
-            // direction seen from the new leaf comes first (atomicMin).
-            if (spl) {
-                const int n = my_nb;
-                if (n >= 0) {
-                    topo.keep[n] = 1;
-                } else {
-                    const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-                    const MGridParams& P = params[o.w];
-                    const uint64_t key = mkey((long long)(o.x >> 3) + dx, (long long)(o.y >> 3) + dy,
-                                              (long long)(o.z >> 3) + dz, o.w, P.base, topo.key_bits);
-                    bool done = false;
-                    if (key != kEmptyKey) {
-                        uint32_t m = (uint32_t)topo.hcap - 1u, pp = (uint32_t)mix64(key) & m;
-                        for (int probe = 0; probe < topo.hcap; ++probe) {
-                            const unsigned long long prev = atomicCAS((unsigned long long*)&topo.pkey[pp],
-                                                                      (unsigned long long)kEmptyKey,
-                                                                      (unsigned long long)key);
-                            if (prev == kEmptyKey || prev == key) {
-                                atomicMin(&topo.pval[pp], kNbr - 1 - lane);
-                                done = true;
-                                break;
-                            }
-                            pp = (pp + 1u) & m;
-                        }
-                    }
-                    if (!done) atomicOr(err, key == kEmptyKey ? kErrExtent : kErrHashFull);
-                }
+                if (on) atomicOr(&s_M2[b][off >> 5], 1u << (off & 31));
             }
         }
         if (slot_n < 0) break;
@@ -525,6 +542,8 @@ __global__ void __launch_bounds__(kNT, 8) k_m_reinit(MLeafArrays A, const T* __r
         slot_nn = slot_nnn;
         nb_next = nb_after;
     }
+    __syncthreads();  // the last leaf's mask words are complete
+    if (warp == kNW - 1) spill_and_propose(s_M2[it & 1u], slot, o, s_nbr[it % 3u][lane], lane, A, topo, params, err);
 }
 
 #define VLR_REINIT_ARGS(T) MLeafArrays, const T*, T*, const MGridParams*, MTopo, unsigned*
