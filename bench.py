@@ -315,20 +315,21 @@ STEP_KERNELS = ("k_m_advect", "k_m_reinit", "k_t_scanalloc", "k_t_finalize", "k_
 # keyed by (workload, kernel, value bytes):
 #   large8192: the same generator with 1,500 spheres (466k leaves; traffic per
 #     leaf does not depend on the sphere count), `bench.py --large-spheres 1500
-#     --steps 1 --warmup 3 --no-...`, FP16 at -s 6, FP32 at -s 20;
+#     --steps 1 --warmup 3 --no-...`, FP16 at -s 6, FP32 at -s 6 of the
+#     float kernels (--kernel-name-base mangled -k 'regex:k_m_(advect|reinit)If');
 #   batched256: its first 48 grids (151k leaves), `bench.py --workload
 #     batched256 --grids 48 --steps 1 --warmup 3`, -s 6;
 #   deformation512: `bench.py --workload deformation512 --steps 1 --warmup 3`,
 #     -s 6 (2,858 leaves, L2-resident).
 TRAFFIC_PER_LEAF: dict = {
-    ("large8192", "k_m_advect", 2): 2560.7,
-    ("large8192", "k_m_reinit", 2): 2360.0,
-    ("large8192", "k_m_advect", 4): 4889.7,
-    ("large8192", "k_m_reinit", 4): 4508.9,
-    ("batched256", "k_m_advect", 2): 2323.0,
-    ("batched256", "k_m_reinit", 2): 2079.1,
+    ("large8192", "k_m_advect", 2): 2548.8,
+    ("large8192", "k_m_reinit", 2): 2342.5,
+    ("large8192", "k_m_advect", 4): 4864.1,
+    ("large8192", "k_m_reinit", 4): 4509.9,
+    ("batched256", "k_m_advect", 2): 2327.1,
+    ("batched256", "k_m_reinit", 2): 2081.1,
     ("deformation512", "k_m_advect", 2): 1238.0,
-    ("deformation512", "k_m_reinit", 2): 1223.0,
+    ("deformation512", "k_m_reinit", 2): 1224.9,
 }
 
 
@@ -336,11 +337,11 @@ TRAFFIC_PER_LEAF: dict = {
 # launch's leaves) from the same captures, FP16, 128-thread CTAs.
 INST_PER_LEAF: dict = {
     ("large8192", "k_m_advect"): 4452.5,
-    ("large8192", "k_m_reinit"): 4196.9,
+    ("large8192", "k_m_reinit"): 4198.8,
     ("batched256", "k_m_advect"): 4768.3,
-    ("batched256", "k_m_reinit"): 4188.0,
-    ("deformation512", "k_m_advect"): 3001.4,
-    ("deformation512", "k_m_reinit"): 4445.2,
+    ("batched256", "k_m_reinit"): 4194.8,
+    ("deformation512", "k_m_advect"): 3003.1,
+    ("deformation512", "k_m_reinit"): 4440.2,
 }
 SM_COUNT = 148
 ISSUE_PER_SM_PER_CYCLE = 4  # one warp instruction per scheduler per cycle
