@@ -620,6 +620,30 @@ def full_period(args, ctx, precision, reinit_mode=0):
             "against": "exact signed distance of the start sphere (the flow returns to it after one period)"}
 
 
+# Algorithmic bytes per band voxel of one launch of the adjoint's kernels,
+# each array counted once per launch (the trilinear corners and the
+# candidates' feet are read through the cache by up to 27 neighbours):
+#   k_adj_forward: band index 4 + displacement 12 + phi_k 4 + phi_k+1 4
+#   k_adj_pack:    band index 4 + displacement 12 + lambda 4 + foot word 4 + weights and lambda 16
+#   k_adj_lambda:  band index 4 + own foot 20 + phi_k 4 + G read and written 24 + lambda out 4
+ADJ_BYTES_PER_BAND_VOXEL = {"k_adj_forward": 24, "k_adj_pack": 40, "k_adj_lambda": 56}
+
+
+def adjoint_roofline(kern, nb, peak, peak_kind):
+    """HBM roofline of the adjoint's dominant kernel from a profiled pass:
+    kern = {name: (total ms, launches)}."""
+    timed = {k: v for k, v in kern.items() if k in ADJ_BYTES_PER_BAND_VOXEL and v[1] > 0}
+    if not timed:
+        return None
+    dom = max(timed, key=lambda k: timed[k][0])
+    ms = timed[dom][0] / timed[dom][1]
+    per = ADJ_BYTES_PER_BAND_VOXEL[dom]
+    achieved = per * nb / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_band_voxel": per,
+            "algorithmic_bytes": per * nb, "launch_ms": ms}
+
+
 def bench_adjoint(args, ctx):
     """The adjoint configuration: sphere r = 32 centred in 256^3, FP32, K = 64
     steps of the deformation field (T = 2), checkpoints every 8 steps, a 128^3
@@ -696,7 +720,8 @@ def bench_adjoint(args, ctx):
                     "h2d_bytes_per_step": nb * 4, "d2h_bytes_per_step": nb * 8 + 3 * n ** 3 * 4},
             "forward_voxels_per_s": nb * steps / (f * 1e-3),
             "kernels_ms_total_per_pass": {k: v[0] for k, v in kern.items()},
-            "kernels_launches_per_pass": {k: v[1] for k, v in kern.items()}}
+            "kernels_launches_per_pass": {k: v[1] for k, v in kern.items()},
+            "roofline": adjoint_roofline(kern, nb, *measured_peaks())}
 
 
 def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
@@ -735,6 +760,15 @@ def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
             bw.append(e[1].elapsed_time(e[2]))
     loss = float(((d_phik - d_target) ** 2).sum().item())
     gnorm = float(d_g0.norm().item())
+    ctx.profile(True)  # kernel times from a separate pass (the events would perturb the timed passes)
+    with torch.cuda.stream(stream):
+        fn.forward_device(d_phik.data_ptr())
+        torch.sub(d_phik, d_target, out=d_lam)
+        d_lam.mul_(2.0)
+        fn.backward_device(d_lam.data_ptr(), d_g0.data_ptr(), 0)
+    ctx.check_device()
+    kern = {k: ctx.kernel_time(k) for k in ("k_adj_forward", "k_adj_pack", "k_adj_lambda")}
+    ctx.profile(False)
     fn.close()
     f, b = statistics.median(fw), statistics.median(bw)
     return {"workload": f"level-set adjoint, K={steps}, checkpoint every {chk}, L2 loss against phi_0 shifted by "
@@ -743,6 +777,8 @@ def bench_level_set_adjoint(args, ctx, ls, steps=32, chk=6, shift=(4, 0, 0)):
             "device_gib_held": held, "loss": loss, "grad_norm": gnorm,
             "value": nb * steps / ((f + b) * 1e-3), "unit": "band voxel-steps/s (forward + backward)",
             "forward_voxels_per_s": nb * steps / (f * 1e-3),
+            "kernels_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in kern.items()},
+            "roofline": adjoint_roofline(kern, nb, *measured_peaks()),
             "timing": "device buffers, CUDA events on the library stream (forward_device + backward_device)"}
 
 
@@ -1031,8 +1067,9 @@ def bench_adjoint_line(args, ctx):
             "unit": "voxels/s", "ms_per_step": (a["forward_ms"] + a["backward_ms"]) / 64.0, "dtype": "f32",
             "config": {"workload": "adjoint256", "active_voxels": a["band_voxels"], "steps": 64,
                        "checkpoint_every": 8, "velocity": "128^3 staggered, trilinear upsample"},
-            "roofline": None, "e2e": None, "clocks": clk.summary(), "gpu_launches": None,
-            "kernels_ms_per_launch": {}, "adjoint": a}
+            "roofline": a["roofline"], "e2e": None, "clocks": clk.summary(), "gpu_launches": None,
+            "kernels_ms_per_launch": {k: a["kernels_ms_total_per_pass"][k] / max(a["kernels_launches_per_pass"][k], 1)
+                                      for k in a["kernels_ms_total_per_pass"]}, "adjoint": a}
 
 
 def bench_mesh_line(args, ctx, peak, peak_kind):
