@@ -204,6 +204,17 @@ __global__ void k_adj_pack(const int* __restrict__ bvox, int nb, const float3* _
     }
 }
 
+// k_adj_pack for a displacement fixed over the steps (a level set's
+// time-independent velocity): the feet and weights of the first step stand,
+// so later steps write only lambda, the fourth word of each band voxel's
+// foot record.
+__global__ void k_adj_pack_lambda(const int* __restrict__ bvox, int nb, const float* __restrict__ lam,
+                                  float4* __restrict__ foot_w) {
+    float* w = reinterpret_cast<float*>(foot_w);
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        w[4 * (size_t)bvox[b] + 3] = lam[b];
+}
+
 // Per leaf, the smallest and largest foot offset per axis over its band
 // voxels at this step (empty leaves: min > max).  One warp per leaf.
 __global__ void k_adj_leafrange(const unsigned* __restrict__ foot_pk, int n_leaves, int* __restrict__ lrange) {
@@ -594,9 +605,16 @@ int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
                                                                     a->segment + (size_t)(k - k0) * nb, a->phi[0]);
             float* lam_out = (lam == a->lam[1]) ? a->lam[0] : a->lam[1];
             const float sk = step_factor(a, k);
-            VLR_TIMED(ctx, "k_adj_pack",
-                      k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk, a->foot_pk,
-                                                                      a->foot_w));
+            // a fixed displacement keeps the feet, their weights and the
+            // leaves' windows of the backward pass's first step
+            const bool feet_stand = a->disp && k != a->steps - 1;
+            if (feet_stand)
+                VLR_TIMED(ctx, "k_adj_pack",
+                          k_adj_pack_lambda<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, lam, a->foot_w));
+            else
+                VLR_TIMED(ctx, "k_adj_pack",
+                          k_adj_pack<<<blocks_for(ctx, nb), 256, 0, st>>>(a->bvox, (int)nb, a->ub, lam, sk,
+                                                                          a->foot_pk, a->foot_w));
             const int gb = blocks_for(ctx, nb);
             const int nl = a->n_leaves;
             // the narrowed window pays when the whole window is large (reach >= 2)
@@ -607,11 +625,13 @@ int adj_backward_enqueue(vlr_ctx* ctx, vlr_adjoint* a) {
                           k_adj_lambda_quad<<<blocks_for(ctx, 4ll * nb), 256, 0, st>>>(
                               a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk, a->foot_w, sk, a->hw, lam_out, a->G));
             } else {
-                VLR_TIMED(ctx, "k_adj_leafrange",
-                          k_adj_leafrange<<<blocks_for(ctx, 32ll * nl), 256, 0, st>>>(a->foot_pk, nl, a->lrange));
-                VLR_TIMED(ctx, "k_adj_window",
-                          k_adj_window<<<blocks_for(ctx, nl), 256, 0, st>>>(a->nbr, a->lrange, nl, a->reach,
-                                                                            a->wrange));
+                if (!feet_stand) {
+                    VLR_TIMED(ctx, "k_adj_leafrange",
+                              k_adj_leafrange<<<blocks_for(ctx, 32ll * nl), 256, 0, st>>>(a->foot_pk, nl, a->lrange));
+                    VLR_TIMED(ctx, "k_adj_window",
+                              k_adj_window<<<blocks_for(ctx, nl), 256, 0, st>>>(a->nbr, a->lrange, nl, a->reach,
+                                                                                a->wrange));
+                }
                 VLR_TIMED(ctx, "k_adj_lambda",
                           k_adj_lambda<0><<<gb, 256, 0, st>>>(a->bvox, (int)nb, a->nbr, a->phi[0], a->foot_pk,
                                                               a->foot_w, sk, a->hw, a->wrange, lam_out, a->G));
