@@ -89,3 +89,18 @@ def test_slabs_output_too_small(grid):
         ls.step(1)  # the state waits for an upload
     ref = _host_step(ls, inp, 1)
     assert _same(_host_step(ls, inp, 4), ref)
+
+
+def test_slabs_on_a_fresh_level_set(grid):
+    """A level set whose first step is a slab pipeline (the launch autotuner
+    runs inside the first slab) gives the one pass's result."""
+    from sharc.volrus_b200.method import LevelSet, large_sphere_grid
+    ls, inp = grid
+    ref = _host_step(ls, inp, 1)
+    sph, vel = large_sphere_grid(1100, seed=11, extent=4096.0)
+    fresh = LevelSet.spheres([(sph, vel)], 1.0, half_width=3.0, precision=ls.precision, integrator=3,
+                             reinit_iters=2)
+    try:
+        assert _same(_host_step(fresh, inp, 4), ref)
+    finally:
+        fresh.close()
