@@ -62,6 +62,13 @@ int vlr_ctx_synchronize(vlr_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work or events with the library's.  No counterpart in the reference. */
 int vlr_ctx_stream(vlr_ctx* ctx, void** stream);
+/* Page-locked host memory (freed with vlr_host_free): the buffers that let
+ * host-resident calls copy at the link's full rate and overlap their copies
+ * (vlr_ls_step_host's slab pipeline takes effect only on such buffers), for
+ * callers without a CUDA runtime of their own.  No counterpart in the
+ * reference. */
+int vlr_host_alloc(vlr_ctx* ctx, size_t bytes, void** out);
+int vlr_host_free(vlr_ctx* ctx, void* p);
 /* Per-kernel timing with CUDA events on the context stream: enable/disable,
  * and read the accumulated milliseconds and launch count of one kernel
  * (reading resets nothing; vlr_ctx_profile(ctx, 1) clears the totals).

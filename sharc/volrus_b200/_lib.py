@@ -90,6 +90,8 @@ SIGNATURES = {
     "vlr_ctx_destroy": (None, [P]),
     "vlr_last_error": (C.c_char_p, [P]),
     "vlr_ctx_synchronize": (C.c_int, [P]),
+    "vlr_host_alloc": (C.c_int, [P, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "vlr_host_free": (C.c_int, [P, C.c_void_p]),
     "vlr_ctx_stream": (C.c_int, [P, PP]),
     "vlr_ctx_profile": (C.c_int, [P, C.c_int]),
     "vlr_ctx_profile_read": (C.c_int, [P, C.c_char_p, dbl_p, C.POINTER(C.c_longlong)]),
@@ -188,6 +190,18 @@ def ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+class _PinnedBlock:
+    """A page-locked host allocation of a context, freed with the object."""
+
+    def __init__(self, ctx, ptr: int, nbytes: int):
+        self.ctx, self.ptr, self.nbytes = ctx, ptr, nbytes
+
+    def __del__(self):
+        if self.ptr and getattr(self.ctx, "handle", None):
+            self.ctx.lib.vlr_host_free(self.ctx.handle, C.c_void_p(self.ptr))
+            self.ptr = 0
+
+
 class Context:
     """One CUDA device + stream; owns device grids created through it."""
 
@@ -219,6 +233,20 @@ class Context:
     def check_device(self):
         """Wait for the context stream and raise on device-side errors."""
         self.check(self.lib.vlr_ctx_check(self.handle), "vlr_ctx_check")
+
+    def pinned(self, shape, dtype):
+        """A numpy array in page-locked host memory (vlr_host_alloc), freed when
+        the array and its views are gone: host buffers that host-resident
+        calls copy at full rate (the slab pipeline of vlr_ls_step_host)."""
+        import numpy as np
+        dt = np.dtype(dtype)
+        n = int(np.prod(shape)) * dt.itemsize
+        p = C.c_void_p()
+        self.check(self.lib.vlr_host_alloc(self.handle, max(n, 1), C.byref(p)), "vlr_host_alloc")
+        holder = _PinnedBlock(self, p.value, max(n, 1))
+        buf = (C.c_byte * max(n, 1)).from_address(p.value)
+        buf._vlr_holder = holder  # the block lives as long as the buffer object
+        return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
 
     def stream_ptr(self) -> int:
         """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

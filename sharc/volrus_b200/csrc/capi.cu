@@ -191,6 +191,28 @@ int vlr_ctx_stream(vlr_ctx* ctx, void** stream) {
     return VLR_OK;
 }
 
+int vlr_host_alloc(vlr_ctx* ctx, size_t bytes, void** out) {
+    if (!ctx || !out) return set_error(ctx, VLR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (!bytes) return VLR_OK;
+    vlr::DeviceGuard guard(ctx->device);
+    const cudaError_t e = cudaMallocHost(out, bytes);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        cudaGetLastError();
+        return set_error(ctx, VLR_ERR_NOMEM, "page-locked host allocation failed");
+    }
+    return VLR_OK;
+}
+
+int vlr_host_free(vlr_ctx* ctx, void* p) {
+    if (!ctx) return VLR_ERR_INVALID;
+    if (!p) return VLR_OK;
+    vlr::DeviceGuard guard(ctx->device);
+    const cudaError_t e = cudaFreeHost(p);
+    return e == cudaSuccess ? VLR_OK : vlr::check_cuda(ctx, e, "cudaFreeHost");
+}
+
 int vlr_ctx_profile(vlr_ctx* ctx, int enable) {
     if (!ctx) return VLR_ERR_INVALID;
     int rc = timer_collect(ctx);

@@ -104,3 +104,19 @@ def test_slabs_on_a_fresh_level_set(grid):
         assert _same(_host_step(fresh, inp, 4), ref)
     finally:
         fresh.close()
+
+
+def test_slabs_on_library_pinned_buffers(grid):
+    """Buffers from vlr_host_alloc (what a caller without a CUDA runtime of
+    its own uses) take the slab pipeline and give the one pass's result."""
+    ls, inp = grid
+    ref = _host_step(ls, inp, 1)
+    ctx = ls.ctx
+    lib_in = []
+    for a in inp:
+        b = ctx.pinned(a.shape, a.dtype)
+        b[:] = a
+        lib_in.append(b)
+    cap = 2 * len(inp[0]) + 64
+    out = tuple(ctx.pinned((cap,) + a.shape[1:], a.dtype) for a in inp)
+    assert _same(_host_step(ls, tuple(lib_in), 4, out=out), ref)
